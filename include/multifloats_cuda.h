@@ -1,0 +1,184 @@
+/* libmultifloats_cuda -- B200 (sm_100a) implementation of the multifloats
+ * double-double array hot path behind a plain C ABI.
+ *
+ * Two families of entry points:
+ *
+ *  1. Drop-in symbols with the reference's own names and signatures
+ *     (matmuldd_mm, matmuldd_mv, matmuldd_vm and their matmulf64x2_* aliases),
+ *     plus array forms of the Fortran-only reductions and elemental functions
+ *     (expdd_array, dotdd_array, ...).  They take HOST pointers, copy to the
+ *     GPU, run the kernel and copy back before returning (synchronous).  Like
+ *     the reference they return no status: NaN-in-NaN-out for the data; a CUDA
+ *     or argument failure is latched per thread and read with
+ *     mfcuda_last_error().
+ *
+ *  2. mfcuda_* entry points taking DEVICE pointers and a cudaStream_t (passed
+ *     as void*), returning 0 on success or an MFCUDA_ERR_* code.  They are
+ *     asynchronous on the stream.
+ *
+ * Layout: float64x2 is two back-to-back binary64 limbs {hi, lo} (16 bytes),
+ * complex64x2 is {re, im} (32 bytes), matrices are column-major with the
+ * leading dimension equal to the first extent, exactly as in the reference
+ * (include/multifloats/float64x2.h:125-186, :348-378, :654-696).
+ *
+ * Reference citations are paths inside multifloats 0.10.3.
+ */
+#ifndef MULTIFLOATS_CUDA_H
+#define MULTIFLOATS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__) || defined(__clang__)
+#define MULTIFLOATS_CUDA_API __attribute__((visibility("default")))
+#else
+#define MULTIFLOATS_CUDA_API
+#endif
+
+/* Interchange types.  When the reference header multifloats/float64x2.h has
+ * already been included (it defines MULTIFLOATS_ABI_VERSION) its identical
+ * structs are used instead. */
+#ifndef MULTIFLOATS_ABI_VERSION
+struct float64x2 {
+  double limbs[2];
+};
+struct complex64x2 {
+  struct float64x2 re;
+  struct float64x2 im;
+};
+#ifndef __cplusplus
+typedef struct float64x2 float64x2;
+typedef struct complex64x2 complex64x2;
+#endif
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ------------------------------------------------------------- */
+enum {
+  MFCUDA_OK = 0,
+  MFCUDA_ERR_INVALID_ARG = 1,   /* negative size, NULL pointer with size > 0, overflow */
+  MFCUDA_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  MFCUDA_ERR_ALLOC = 3,         /* device or host allocation failed */
+  MFCUDA_ERR_NO_DEVICE = 4,     /* no sm_100 device visible */
+  MFCUDA_ERR_TIMEOUT = 5,       /* a bounded device-side wait expired */
+  MFCUDA_ERR_WORKSPACE = 6,     /* caller workspace too small */
+  MFCUDA_ERR_UNSUPPORTED = 7    /* shape/parameter outside what the kernel supports */
+};
+/* Status of the calling thread's last drop-in call (0 = success). */
+MULTIFLOATS_CUDA_API int mfcuda_last_error(void);
+MULTIFLOATS_CUDA_API const char *mfcuda_error_string(int code);
+/* Library version, e.g. "0.1.0". */
+MULTIFLOATS_CUDA_API const char *mfcuda_version(void);
+
+/* ==========================================================================
+ * 1. Drop-in symbols (host pointers, synchronous)
+ * ========================================================================== */
+
+/* Compensated DD matmul, column-major, C overwritten.  Replaces
+ * matmuldd_mm / matmuldd_mv / matmuldd_vm (include/multifloats/float64x2.h:682-696,
+ * src/float64x2/abi.inc:133-149, kernels src/float64x2/matmul.inc:6-239).
+ * Bit-identical to the reference: every output runs the reference MAC over
+ * p = 0..k-1 in order with the same renormalisation cadence. */
+MULTIFLOATS_CUDA_API void matmuldd_mm(const float64x2 *a, const float64x2 *b, float64x2 *c,
+                                      int64_t m, int64_t k, int64_t n,
+                                      int64_t renorm_interval);
+MULTIFLOATS_CUDA_API void matmuldd_mv(const float64x2 *a, const float64x2 *x, float64x2 *y,
+                                      int64_t m, int64_t k, int64_t renorm_interval);
+MULTIFLOATS_CUDA_API void matmuldd_vm(const float64x2 *x, const float64x2 *b, float64x2 *y,
+                                      int64_t k, int64_t n, int64_t renorm_interval);
+/* f64x2-tagged spellings (src/float64x2/f64x2_aliases.inc:114-116). */
+MULTIFLOATS_CUDA_API void matmulf64x2_mm(const float64x2 *a, const float64x2 *b, float64x2 *c,
+                                         int64_t m, int64_t k, int64_t n,
+                                         int64_t renorm_interval);
+MULTIFLOATS_CUDA_API void matmulf64x2_mv(const float64x2 *a, const float64x2 *x, float64x2 *y,
+                                         int64_t m, int64_t k, int64_t renorm_interval);
+MULTIFLOATS_CUDA_API void matmulf64x2_vm(const float64x2 *x, const float64x2 *b, float64x2 *y,
+                                         int64_t k, int64_t n, int64_t renorm_interval);
+
+/* Complex matmul as 4 real compensated products combined with DD -/+, the
+ * Fortran cdd_matmul_mm (fsrc/multifloats.fypp:2609-2621), fused in one pass.
+ * Bit-identical to that composition. */
+MULTIFLOATS_CUDA_API void cmatmuldd_mm(const complex64x2 *a, const complex64x2 *b,
+                                       complex64x2 *c, int64_t m, int64_t k, int64_t n,
+                                       int64_t renorm_interval);
+
+/* Elementwise y[i] = f(x[i]): the Fortran elemental exp/log/sin/cos/sqrt over an
+ * array (fsrc/multifloats.fypp:792-798, :1407-1412), one expdd / logdd / sindd /
+ * cosdd / sqrtdd per element (src/float64x2/abi.inc:30, :53, :59, :67, :68).
+ * Bit-identical per element.  x and y may alias. */
+MULTIFLOATS_CUDA_API void expdd_array(const float64x2 *x, float64x2 *y, int64_t n);
+MULTIFLOATS_CUDA_API void logdd_array(const float64x2 *x, float64x2 *y, int64_t n);
+MULTIFLOATS_CUDA_API void sindd_array(const float64x2 *x, float64x2 *y, int64_t n);
+MULTIFLOATS_CUDA_API void cosdd_array(const float64x2 *x, float64x2 *y, int64_t n);
+MULTIFLOATS_CUDA_API void sqrtdd_array(const float64x2 *x, float64x2 *y, int64_t n);
+
+/* Reductions: the Fortran-only sum / dot_product / norm2 generics
+ * (fsrc/multifloats.fypp:1980-2019, :2094-2158, :2254-2331, :2338-2352) as
+ * C entry points.  Each thread of the device runs the reference's per-element
+ * compensated update over a fixed strided subsequence; partials are combined
+ * with DD addition in a fixed tree that depends only on n, so results are
+ * run-to-run reproducible and bit-identical to the CPU restatement of that order. */
+MULTIFLOATS_CUDA_API float64x2 sumdd_array(const float64x2 *x, int64_t n);
+MULTIFLOATS_CUDA_API float64x2 dotdd_array(const float64x2 *a, const float64x2 *b, int64_t n,
+                                           int64_t renorm_interval);
+MULTIFLOATS_CUDA_API float64x2 norm2dd_array(const float64x2 *x, int64_t n);
+MULTIFLOATS_CUDA_API complex64x2 csumdd_array(const complex64x2 *x, int64_t n);
+/* conj(a) . b, as the Fortran cdd_dot_product (fypp:2321-2331). */
+MULTIFLOATS_CUDA_API complex64x2 cdotdd_array(const complex64x2 *a, const complex64x2 *b,
+                                              int64_t n, int64_t renorm_interval);
+/* sqrt(sum re^2 + im^2): norm2 of the array viewed as 2n reals (re0, im0, re1, ...). */
+MULTIFLOATS_CUDA_API float64x2 cnorm2dd_array(const complex64x2 *x, int64_t n);
+
+/* ==========================================================================
+ * 2. Device-pointer API (asynchronous on `stream`, a cudaStream_t; NULL = legacy
+ *    default stream).  Return MFCUDA_OK or an error code.
+ * ========================================================================== */
+MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm(const float64x2 *a, const float64x2 *b, float64x2 *c,
+                                            int64_t m, int64_t k, int64_t n,
+                                            int64_t renorm_interval, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mv(const float64x2 *a, const float64x2 *x, float64x2 *y,
+                                            int64_t m, int64_t k, int64_t renorm_interval,
+                                            void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_matmuldd_vm(const float64x2 *x, const float64x2 *b, float64x2 *y,
+                                            int64_t k, int64_t n, int64_t renorm_interval,
+                                            void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_cmatmuldd_mm(const complex64x2 *a, const complex64x2 *b,
+                                             complex64x2 *c, int64_t m, int64_t k, int64_t n,
+                                             int64_t renorm_interval, void *stream);
+
+/* op: 0 exp, 1 log, 2 sin, 3 cos, 4 sqrt */
+enum { MFCUDA_EXP = 0, MFCUDA_LOG = 1, MFCUDA_SIN = 2, MFCUDA_COS = 3, MFCUDA_SQRT = 4 };
+MULTIFLOATS_CUDA_API int mfcuda_unary_dd(int op, const float64x2 *x, float64x2 *y, int64_t n,
+                                         void *stream);
+
+/* Reductions write their result to DEVICE memory `out`.  `workspace` may be
+ * NULL (stream-ordered allocation inside) or point to at least
+ * mfcuda_reduce_workspace_size(n) bytes of device memory. */
+MULTIFLOATS_CUDA_API size_t mfcuda_reduce_workspace_size(int64_t n);
+MULTIFLOATS_CUDA_API int mfcuda_sumdd(const float64x2 *x, int64_t n, float64x2 *out,
+                                      void *workspace, size_t workspace_bytes, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_dotdd(const float64x2 *a, const float64x2 *b, int64_t n,
+                                      int64_t renorm_interval, float64x2 *out, void *workspace,
+                                      size_t workspace_bytes, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_norm2dd(const float64x2 *x, int64_t n, float64x2 *out,
+                                        void *workspace, size_t workspace_bytes, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_csumdd(const complex64x2 *x, int64_t n, complex64x2 *out,
+                                       void *workspace, size_t workspace_bytes, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_cdotdd(const complex64x2 *a, const complex64x2 *b, int64_t n,
+                                       int64_t renorm_interval, complex64x2 *out,
+                                       void *workspace, size_t workspace_bytes, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_cnorm2dd(const complex64x2 *x, int64_t n, float64x2 *out,
+                                         void *workspace, size_t workspace_bytes, void *stream);
+
+/* Fixed launch geometry of the reductions for a given n (it depends on n only,
+ * never on the device), exposed so a CPU restatement can follow the same order:
+ * *blocks = number of thread blocks, *threads = threads per block. */
+MULTIFLOATS_CUDA_API void mfcuda_reduce_geometry(int64_t n, int64_t *blocks, int64_t *threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MULTIFLOATS_CUDA_H */

@@ -1,0 +1,107 @@
+"""ctypes binding of libmultifloats_cuda.so (the C ABI in include/multifloats_cuda.h).
+
+The shared library is built in-tree (``python -m multifloats_b200.build``).  There
+is no fallback: if the library is missing or fails to load, :func:`lib` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmultifloats_cuda.so")
+
+
+class float64x2(C.Structure):
+    """The reference's interchange struct: limbs[0] = hi, limbs[1] = lo."""
+
+    _fields_ = [("hi", C.c_double), ("lo", C.c_double)]
+
+
+class complex64x2(C.Structure):
+    _fields_ = [("re", float64x2), ("im", float64x2)]
+
+
+class MFCudaError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        msg = _lib.mfcuda_error_string(code).decode() if _lib is not None else str(code)
+        super().__init__(f"{where}: {msg} (code {code})")
+
+
+P = C.c_void_p
+I64 = C.c_int64
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "mfcuda_last_error": (C.c_int, []),
+    "mfcuda_error_string": (C.c_char_p, [C.c_int]),
+    "mfcuda_version": (C.c_char_p, []),
+    # drop-in
+    "matmuldd_mm": (None, [P, P, P, I64, I64, I64, I64]),
+    "matmuldd_mv": (None, [P, P, P, I64, I64, I64]),
+    "matmuldd_vm": (None, [P, P, P, I64, I64, I64]),
+    "matmulf64x2_mm": (None, [P, P, P, I64, I64, I64, I64]),
+    "matmulf64x2_mv": (None, [P, P, P, I64, I64, I64]),
+    "matmulf64x2_vm": (None, [P, P, P, I64, I64, I64]),
+    "cmatmuldd_mm": (None, [P, P, P, I64, I64, I64, I64]),
+    "expdd_array": (None, [P, P, I64]),
+    "logdd_array": (None, [P, P, I64]),
+    "sindd_array": (None, [P, P, I64]),
+    "cosdd_array": (None, [P, P, I64]),
+    "sqrtdd_array": (None, [P, P, I64]),
+    "sumdd_array": (float64x2, [P, I64]),
+    "dotdd_array": (float64x2, [P, P, I64, I64]),
+    "norm2dd_array": (float64x2, [P, I64]),
+    "csumdd_array": (complex64x2, [P, I64]),
+    "cdotdd_array": (complex64x2, [P, P, I64, I64]),
+    "cnorm2dd_array": (float64x2, [P, I64]),
+    # device-pointer API
+    "mfcuda_matmuldd_mm": (C.c_int, [P, P, P, I64, I64, I64, I64, P]),
+    "mfcuda_matmuldd_mv": (C.c_int, [P, P, P, I64, I64, I64, P]),
+    "mfcuda_matmuldd_vm": (C.c_int, [P, P, P, I64, I64, I64, P]),
+    "mfcuda_cmatmuldd_mm": (C.c_int, [P, P, P, I64, I64, I64, I64, P]),
+    "mfcuda_unary_dd": (C.c_int, [C.c_int, P, P, I64, P]),
+    "mfcuda_reduce_workspace_size": (C.c_size_t, [I64]),
+    "mfcuda_reduce_geometry": (None, [I64, C.POINTER(I64), C.POINTER(I64)]),
+    "mfcuda_sumdd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
+    "mfcuda_dotdd": (C.c_int, [P, P, I64, I64, P, P, C.c_size_t, P]),
+    "mfcuda_norm2dd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
+    "mfcuda_csumdd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
+    "mfcuda_cdotdd": (C.c_int, [P, P, I64, I64, P, P, C.c_size_t, P]),
+    "mfcuda_cnorm2dd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """Load (once) and return the CUDA library; raises if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m multifloats_b200.build`")
+            handle = C.CDLL(LIB_PATH, mode=C.RTLD_LOCAL)
+            for name, (res, args) in SIGNATURES.items():
+                if not hasattr(handle, name):
+                    continue  # optional symbol; tests check the exported list
+                fn = getattr(handle, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = handle
+    return _lib
+
+
+def check(code: int, where: str) -> None:
+    if code != 0:
+        raise MFCudaError(code, where)
+
+
+def check_last(where: str) -> None:
+    check(lib().mfcuda_last_error(), where)

@@ -1,0 +1,251 @@
+"""Python mirror of the libmultifloats_cuda C ABI.
+
+Arrays are float64 buffers whose trailing axis holds the limbs: a float64x2
+array of n elements is any float64 array with 2n entries (hi, lo interleaved),
+a complex64x2 array has 4n entries (re.hi, re.lo, im.hi, im.lo).  Matrices are
+column-major with leading dimension = number of rows, exactly as in the C ABI
+(and in the reference's matmuldd_* functions).
+
+Every function accepts either host numpy arrays -- routed through the drop-in
+symbols (host pointers, synchronous) -- or CUDA torch tensors, routed through
+the mfcuda_* device API on torch's current stream.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import check, check_last, complex64x2, float64x2, lib
+
+OP = {"exp": 0, "log": 1, "sin": 2, "cos": 3, "sqrt": 4}
+
+
+def _is_dev(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(x.is_cuda)
+
+
+def _ptr(x) -> int:
+    if x is None:
+        return 0
+    if _is_dev(x):
+        return x.data_ptr()
+    return x.ctypes.data
+
+
+def _stream():
+    import torch
+
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _host(x, n_doubles: int, name: str) -> np.ndarray:
+    a = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    if a.size != n_doubles:
+        raise ValueError(f"{name}: expected {n_doubles} doubles, got {a.size}")
+    return a
+
+
+def _dev_check(x, n_doubles: int, name: str):
+    import torch
+
+    if x.dtype != torch.float64 or not x.is_contiguous() or x.numel() != n_doubles:
+        raise ValueError(f"{name}: expected a contiguous float64 CUDA tensor of {n_doubles} doubles")
+    return x
+
+
+def _empty_like_kind(ref, n_doubles: int):
+    if _is_dev(ref):
+        import torch
+
+        return torch.empty(n_doubles, dtype=torch.float64, device=ref.device)
+    return np.empty(n_doubles, dtype=np.float64)
+
+
+# ---- matmul ------------------------------------------------------------------
+def matmuldd_mm(a, b, m: int, k: int, n: int, renorm_interval: int = 8, out=None):
+    """C(m,n) = A(m,k) B(k,n), column-major DD (reference matmuldd_mm)."""
+    L = lib()
+    if _is_dev(a):
+        a, b = _dev_check(a, 2 * m * k, "a"), _dev_check(b, 2 * k * n, "b")
+        c = out if out is not None else _empty_like_kind(a, 2 * m * n)
+        check(L.mfcuda_matmuldd_mm(_ptr(a), _ptr(b), _ptr(c), m, k, n, renorm_interval, _stream()),
+              "mfcuda_matmuldd_mm")
+        return c
+    a, b = _host(a, 2 * m * k, "a"), _host(b, 2 * k * n, "b")
+    c = out if out is not None else np.empty(2 * m * n)
+    L.matmuldd_mm(_ptr(a), _ptr(b), _ptr(c), m, k, n, renorm_interval)
+    check_last("matmuldd_mm")
+    return c
+
+
+def matmuldd_mv(a, x, m: int, k: int, renorm_interval: int = 8):
+    L = lib()
+    if _is_dev(a):
+        y = _empty_like_kind(a, 2 * m)
+        check(L.mfcuda_matmuldd_mv(_ptr(_dev_check(a, 2 * m * k, "a")), _ptr(_dev_check(x, 2 * k, "x")),
+                                   _ptr(y), m, k, renorm_interval, _stream()), "mfcuda_matmuldd_mv")
+        return y
+    a, x = _host(a, 2 * m * k, "a"), _host(x, 2 * k, "x")
+    y = np.empty(2 * m)
+    L.matmuldd_mv(_ptr(a), _ptr(x), _ptr(y), m, k, renorm_interval)
+    check_last("matmuldd_mv")
+    return y
+
+
+def matmuldd_vm(x, b, k: int, n: int, renorm_interval: int = 8):
+    L = lib()
+    if _is_dev(b):
+        y = _empty_like_kind(b, 2 * n)
+        check(L.mfcuda_matmuldd_vm(_ptr(_dev_check(x, 2 * k, "x")), _ptr(_dev_check(b, 2 * k * n, "b")),
+                                   _ptr(y), k, n, renorm_interval, _stream()), "mfcuda_matmuldd_vm")
+        return y
+    x, b = _host(x, 2 * k, "x"), _host(b, 2 * k * n, "b")
+    y = np.empty(2 * n)
+    L.matmuldd_vm(_ptr(x), _ptr(b), _ptr(y), k, n, renorm_interval)
+    check_last("matmuldd_vm")
+    return y
+
+
+def cmatmuldd_mm(a, b, m: int, k: int, n: int, renorm_interval: int = 8, out=None):
+    """Complex C = A B as the Fortran cdd_matmul_mm composition (4 real products)."""
+    L = lib()
+    if _is_dev(a):
+        a, b = _dev_check(a, 4 * m * k, "a"), _dev_check(b, 4 * k * n, "b")
+        c = out if out is not None else _empty_like_kind(a, 4 * m * n)
+        check(L.mfcuda_cmatmuldd_mm(_ptr(a), _ptr(b), _ptr(c), m, k, n, renorm_interval, _stream()),
+              "mfcuda_cmatmuldd_mm")
+        return c
+    a, b = _host(a, 4 * m * k, "a"), _host(b, 4 * k * n, "b")
+    c = out if out is not None else np.empty(4 * m * n)
+    L.cmatmuldd_mm(_ptr(a), _ptr(b), _ptr(c), m, k, n, renorm_interval)
+    check_last("cmatmuldd_mm")
+    return c
+
+
+# ---- elementwise ---------------------------------------------------------------
+def unary(op: str, x, out=None):
+    """y[i] = op(x[i]) for op in exp, log, sin, cos, sqrt."""
+    L = lib()
+    code = OP[op]
+    n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 2
+    if _is_dev(x):
+        x = _dev_check(x, 2 * n, "x")
+        y = out if out is not None else _empty_like_kind(x, 2 * n)
+        check(L.mfcuda_unary_dd(code, _ptr(x), _ptr(y), n, _stream()), "mfcuda_unary_dd")
+        return y
+    x = _host(x, 2 * n, "x")
+    y = out if out is not None else np.empty(2 * n)
+    getattr(L, f"{op}dd_array")(_ptr(x), _ptr(y), n)
+    check_last(f"{op}dd_array")
+    return y
+
+
+def exp(x, out=None):
+    return unary("exp", x, out)
+
+
+def log(x, out=None):
+    return unary("log", x, out)
+
+
+def sin(x, out=None):
+    return unary("sin", x, out)
+
+
+def cos(x, out=None):
+    return unary("cos", x, out)
+
+
+def sqrt(x, out=None):
+    return unary("sqrt", x, out)
+
+
+# ---- reductions ----------------------------------------------------------------
+def _dd_tuple(r) -> tuple:
+    return (r.hi, r.lo)
+
+
+def _reduce_dev(fn: str, args: list, out_doubles: int, ref):
+    import torch
+
+    L = lib()
+    out = torch.empty(out_doubles, dtype=torch.float64, device=ref.device)
+    check(getattr(L, fn)(*args, _ptr(out), None, 0, _stream()), fn)
+    return out
+
+
+def sum_dd(x):
+    """Fortran sum(x) over a real64x2 array; returns (hi, lo) or a device tensor."""
+    n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 2
+    if _is_dev(x):
+        return _reduce_dev("mfcuda_sumdd", [_ptr(x), n], 2, x)
+    x = _host(x, 2 * n, "x")
+    r = lib().sumdd_array(_ptr(x), n)
+    check_last("sumdd_array")
+    return _dd_tuple(r)
+
+
+def dot_product(a, b, renorm_interval: int = 8):
+    n = (a.numel() if _is_dev(a) else np.asarray(a).size) // 2
+    if _is_dev(a):
+        return _reduce_dev("mfcuda_dotdd", [_ptr(a), _ptr(b), n, renorm_interval], 2, a)
+    a, b = _host(a, 2 * n, "a"), _host(b, 2 * n, "b")
+    r = lib().dotdd_array(_ptr(a), _ptr(b), n, renorm_interval)
+    check_last("dotdd_array")
+    return _dd_tuple(r)
+
+
+def norm2(x):
+    n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 2
+    if _is_dev(x):
+        return _reduce_dev("mfcuda_norm2dd", [_ptr(x), n], 2, x)
+    x = _host(x, 2 * n, "x")
+    r = lib().norm2dd_array(_ptr(x), n)
+    check_last("norm2dd_array")
+    return _dd_tuple(r)
+
+
+def csum_dd(x):
+    n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 4
+    if _is_dev(x):
+        return _reduce_dev("mfcuda_csumdd", [_ptr(x), n], 4, x)
+    x = _host(x, 4 * n, "x")
+    r = lib().csumdd_array(_ptr(x), n)
+    check_last("csumdd_array")
+    return (r.re.hi, r.re.lo, r.im.hi, r.im.lo)
+
+
+def cdot_product(a, b, renorm_interval: int = 8):
+    """conj(a) . b (Fortran dot_product on cmplx64x2)."""
+    n = (a.numel() if _is_dev(a) else np.asarray(a).size) // 4
+    if _is_dev(a):
+        return _reduce_dev("mfcuda_cdotdd", [_ptr(a), _ptr(b), n, renorm_interval], 4, a)
+    a, b = _host(a, 4 * n, "a"), _host(b, 4 * n, "b")
+    r = lib().cdotdd_array(_ptr(a), _ptr(b), n, renorm_interval)
+    check_last("cdotdd_array")
+    return (r.re.hi, r.re.lo, r.im.hi, r.im.lo)
+
+
+def cnorm2(x):
+    n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 4
+    if _is_dev(x):
+        return _reduce_dev("mfcuda_cnorm2dd", [_ptr(x), n], 2, x)
+    x = _host(x, 4 * n, "x")
+    r = lib().cnorm2dd_array(_ptr(x), n)
+    check_last("cnorm2dd_array")
+    return _dd_tuple(r)
+
+
+def reduce_geometry(n: int) -> tuple[int, int]:
+    b, t = C.c_int64(), C.c_int64()
+    lib().mfcuda_reduce_geometry(n, C.byref(b), C.byref(t))
+    return b.value, t.value
+
+
+__all__ = [
+    "matmuldd_mm", "matmuldd_mv", "matmuldd_vm", "cmatmuldd_mm",
+    "unary", "exp", "log", "sin", "cos", "sqrt",
+    "sum_dd", "dot_product", "norm2", "csum_dd", "cdot_product", "cnorm2",
+    "reduce_geometry", "float64x2", "complex64x2",
+]

@@ -1,0 +1,352 @@
+// Device double-double (DD) core for sm_100a.
+//
+// A DD value is two IEEE binary64 limbs (hi, lo) with |lo| <= ulp(hi)/2,
+// stored back to back (16 bytes) exactly like the reference's `float64x2`
+// (include/multifloats/float64x2.h:125-186).  Every operation below restates
+// the reference's arithmetic step for step with explicitly rounded device
+// intrinsics (__dadd_rn, __dmul_rn, __fma_rn, __ddiv_rn, __dsqrt_rn), so that
+// nvcc can neither contract a multiply-add into an FMA nor reassociate; the
+// library is additionally compiled with --fmad=false.  Results are therefore
+// bit-identical to the reference CPU build compiled with -ffp-contract=off.
+#pragma once
+#include <cstdint>
+#include <math_constants.h>
+
+#define MF_TABLE static __constant__
+#define MF_GTABLE static __device__ const
+#include "dd_tables.h"
+
+namespace mfdev {
+
+struct dd {
+  double hi, lo;
+};
+
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double div_(double a, double b) { return __ddiv_rn(a, b); }
+
+__device__ __forceinline__ double gload(const double* p) { return __ldg(p); }
+
+// ---- error-free transformations (float64x2.h:84-107) ----------------------
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  double ss = add(a, b);
+  double ap = sub(ss, b);
+  double bp = sub(ss, ap);
+  e = add(sub(a, ap), sub(b, bp));
+  s = ss;
+}
+__device__ __forceinline__ void fast_two_sum(double a, double b, double& s, double& e) {
+  double ss = add(a, b);
+  double bp = sub(ss, a);
+  e = sub(b, bp);
+  s = ss;
+}
+__device__ __forceinline__ void two_prod(double a, double b, double& p, double& e) {
+  double pp = mul(a, b);
+  e = fma_(a, b, -pp);
+  p = pp;
+}
+
+__device__ __forceinline__ dd make(double h, double l) { dd r; r.hi = h; r.lo = l; return r; }
+__device__ __forceinline__ dd neg(dd a) { return make(-a.hi, -a.lo); }
+
+// ---- DD operators (float64x2.h:203-311) -----------------------------------
+__device__ __forceinline__ dd dd_add(dd x, dd y) {
+  double s = add(x.hi, y.hi);
+  if (!isfinite(s)) return make(s, 0.0);
+  if (x.hi == 0.0 && y.hi == 0.0) return make(s, add(x.lo, y.lo));
+  double a, b, c, d;
+  two_sum(x.hi, y.hi, a, b);
+  two_sum(x.lo, y.lo, c, d);
+  fast_two_sum(a, c, a, c);
+  b = add(b, d);
+  b = add(b, c);
+  dd r;
+  fast_two_sum(a, b, r.hi, r.lo);
+  return r;
+}
+__device__ __forceinline__ dd dd_sub(dd x, dd y) {
+  double s = sub(x.hi, y.hi);
+  if (!isfinite(s)) return make(s, 0.0);
+  if (x.hi == 0.0 && y.hi == 0.0) return make(s, sub(x.lo, y.lo));
+  double a, b, c, d;
+  two_sum(x.hi, -y.hi, a, b);
+  two_sum(x.lo, -y.lo, c, d);
+  fast_two_sum(a, c, a, c);
+  b = add(b, d);
+  b = add(b, c);
+  dd r;
+  fast_two_sum(a, b, r.hi, r.lo);
+  return r;
+}
+__device__ __forceinline__ dd dd_mul(dd x, dd y) {
+  double p00, e00;
+  two_prod(x.hi, y.hi, p00, e00);
+  if (!isfinite(p00)) return make(p00, 0.0);
+  double p01 = mul(x.hi, y.lo);
+  double p10 = mul(x.lo, y.hi);
+  p01 = add(p01, p10);
+  e00 = add(e00, p01);
+  dd r;
+  fast_two_sum(p00, e00, r.hi, r.lo);
+  return r;
+}
+__device__ __forceinline__ dd dd_div(dd x, dd y) {
+  double q1 = div_(x.hi, y.hi);
+  if (!isfinite(q1)) return make(q1, q1);
+  if (!isfinite(y.hi)) return make(q1, 0.0);
+  double p00, e00;
+  two_prod(q1, y.hi, p00, e00);
+  double p01 = mul(q1, y.lo);
+  double qhi = p00;
+  double qlo = add(e00, p01);
+  double r0, r0e;
+  two_sum(x.hi, -qhi, r0, r0e);
+  double r1 = add(sub(x.lo, qlo), r0e);
+  double rh, rl;
+  fast_two_sum(r0, r1, rh, rl);
+  double q2 = div_(rh, y.hi);
+  dd r;
+  fast_two_sum(q1, q2, r.hi, r.lo);
+  return r;
+}
+
+// ---- sqrt (float64x2.h:2190-2212), Karp/Markstein --------------------------
+__device__ __forceinline__ dd dd_sqrt(dd x) {
+  double c = __dsqrt_rn(x.hi);
+  if (!(x.hi > 0.0) || !isfinite(c)) return make(c, 0.0);
+  double u, uu;
+  two_prod(c, c, u, uu);
+  double cc = div_(add(sub(sub(x.hi, u), uu), x.lo), mul(2.0, c));
+  dd r;
+  r.hi = add(c, cc);
+  r.lo = add(sub(c, r.hi), cc);
+  return r;
+}
+
+// ---- polynomial evaluators (src/float64x2/poly.inc) ------------------------
+// horner: n = coefficient count (poly.inc:9-16).
+__device__ __forceinline__ dd horner(dd y, const double* hi, const double* lo, int n) {
+  dd p = make(hi[n - 1], lo[n - 1]);
+  for (int i = n - 2; i >= 0; --i) p = dd_add(dd_mul(p, y), make(hi[i], lo[i]));
+  return p;
+}
+// neval (Estrin), degree 10 and 12 cases (poly.inc:33-102).  C++ `a + b * c`
+// is a + (b*c); chains of `+` associate left.
+__device__ __forceinline__ dd neval10(dd x, const double* hi, const double* lo) {
+#define MF_C(i) make(hi[i], lo[i])
+  dd x2 = dd_mul(x, x);
+  dd x4 = dd_mul(x2, x2);
+  dd x8 = dd_mul(x4, x4);
+  dd p01 = dd_add(MF_C(0), dd_mul(MF_C(1), x));
+  dd p23 = dd_add(MF_C(2), dd_mul(MF_C(3), x));
+  dd p45 = dd_add(MF_C(4), dd_mul(MF_C(5), x));
+  dd p67 = dd_add(MF_C(6), dd_mul(MF_C(7), x));
+  dd p89 = dd_add(MF_C(8), dd_mul(MF_C(9), x));
+  dd p03 = dd_add(p01, dd_mul(p23, x2));
+  dd p47 = dd_add(p45, dd_mul(p67, x2));
+  dd p810 = dd_add(p89, dd_mul(MF_C(10), x2));
+  return dd_add(dd_add(p03, dd_mul(p47, x4)), dd_mul(p810, x8));
+}
+__device__ __forceinline__ dd neval12(dd x, const double* hi, const double* lo) {
+  dd x2 = dd_mul(x, x);
+  dd x4 = dd_mul(x2, x2);
+  dd x8 = dd_mul(x4, x4);
+  dd p01 = dd_add(MF_C(0), dd_mul(MF_C(1), x));
+  dd p23 = dd_add(MF_C(2), dd_mul(MF_C(3), x));
+  dd p45 = dd_add(MF_C(4), dd_mul(MF_C(5), x));
+  dd p67 = dd_add(MF_C(6), dd_mul(MF_C(7), x));
+  dd p89 = dd_add(MF_C(8), dd_mul(MF_C(9), x));
+  dd p1011 = dd_add(MF_C(10), dd_mul(MF_C(11), x));
+  dd p03 = dd_add(p01, dd_mul(p23, x2));
+  dd p47 = dd_add(p45, dd_mul(p67, x2));
+  dd p811 = dd_add(p89, dd_mul(p1011, x2));
+  return dd_add(dd_add(p03, dd_mul(p47, x4)), dd_mul(dd_add(p811, dd_mul(MF_C(12), x4)), x8));
+#undef MF_C
+}
+
+// ---- exp (src/float64x2/exp_log.inc:26-72, :237-277) -----------------------
+__device__ __forceinline__ dd exp2_from_reduced(double n_d, double rh, double rl) {
+  if (n_d > 1100.0) return make(CUDART_INF, 0.0);
+  if (n_d < -1100.0) return make(0.0, 0.0);
+  double k_d = rint(mul(rh, 256.0));
+  int k = (int)k_d;
+  if (k > 128) k = 128;
+  if (k < -128) k = -128;
+  double sh = sub(rh, div_((double)k, 256.0));
+  double sl = rl;
+  fast_two_sum(sh, sl, sh, sl);
+  dd s = make(sh, sl);
+  dd q = make(mf_exp2_coefs_hi[9], mf_exp2_coefs_lo[9]);
+#pragma unroll
+  for (int j = 8; j >= 1; --j) {
+    q = dd_mul(q, s);
+    q = dd_add(q, make(mf_exp2_coefs_hi[j], mf_exp2_coefs_lo[j]));
+  }
+  dd pow2s = dd_add(make(1.0, 0.0), dd_mul(s, q));
+  dd T = make(gload(&mf_exp2_table_hi[k + 128]), gload(&mf_exp2_table_lo[k + 128]));
+  dd m = dd_mul(T, pow2s);
+  int n = (int)n_d;
+  return make(ldexp(m.hi, n), ldexp(m.lo, n));
+}
+
+__device__ __forceinline__ dd dd_exp(dd x) {
+  double h = x.hi;
+  if (!isfinite(h)) {
+    if (h > 0.0) return make(h, 0.0);
+    if (h < 0.0) return make(0.0, 0.0);
+    return make(h, 0.0);
+  }
+  if (h > mf_exp_max[0]) return make(CUDART_INF, 0.0);
+  if (h < mf_exp_min[0]) return make(0.0, 0.0);
+  double n_d = rint(mul(h, mf_log2_e_hi[0]));
+  double rh, rl, t;
+  two_sum(h, -mul(n_d, mf_ln2_cw[0]), rh, t);
+  rl = add(t, x.lo);
+  fast_two_sum(rh, rl, rh, rl);
+  double p_hi = mul(n_d, mf_ln2_cw[1]);
+  double p_lo = fma_(n_d, mf_ln2_cw[1], -p_hi);
+  two_sum(rh, -p_hi, rh, t);
+  rl = add(rl, sub(t, p_lo));
+  fast_two_sum(rh, rl, rh, rl);
+  two_sum(rh, -mul(n_d, mf_ln2_cw[2]), rh, t);
+  rl = add(rl, t);
+  dd rr;
+  fast_two_sum(rh, rl, rr.hi, rr.lo);
+  dd y = dd_mul(rr, make(mf_log2_e_hi[0], mf_log2_e_lo[0]));
+  return exp2_from_reduced(n_d, y.hi, y.lo);
+}
+
+// ---- log (exp_log.inc:280-341) ---------------------------------------------
+__device__ __forceinline__ dd log2_kernel(dd x) {
+  double hi = x.hi;
+  if (hi > 15.0 / 16.0 && hi < 17.0 / 16.0) {
+    dd num = dd_sub(x, make(1.0, 0.0));
+    dd den = dd_add(x, make(1.0, 0.0));
+    dd t = dd_div(num, den);
+    dd t2 = dd_mul(t, t);
+    dd p = neval10(t2, mf_log2_wide_hi, mf_log2_wide_lo);
+    return dd_mul(t, p);
+  }
+  int e = ilogb(hi);
+  dd m = make(ldexp(x.hi, -e), ldexp(x.lo, -e));
+  int idx = (int)mul(sub(m.hi, 1.0), 32.0);
+  if (idx < 0) idx = 0;
+  if (idx > 31) idx = 31;
+  dd c = make(gload(&mf_log2_centers[idx]), 0.0);
+  dd v = make(gload(&mf_log2_values_hi[idx]), gload(&mf_log2_values_lo[idx]));
+  dd num = dd_sub(m, c);
+  dd den = dd_add(m, c);
+  dd t = dd_div(num, den);
+  dd t2 = dd_mul(t, t);
+  dd p = horner(t2, mf_log2_narrow_hi, mf_log2_narrow_lo, 7);
+  return dd_add(dd_add(make((double)e, 0.0), v), dd_mul(t, p));
+}
+__device__ __forceinline__ dd dd_log2(dd x) {
+  if (isnan(x.hi) || x.hi < 0.0) return make(CUDART_NAN, 0.0);
+  if (x.hi == 0.0) return make(-CUDART_INF, 0.0);
+  if (!isfinite(x.hi)) return make(CUDART_INF, 0.0);
+  return log2_kernel(x);
+}
+__device__ __forceinline__ dd dd_log(dd x) {
+  if (!isfinite(x.hi)) return make(log(x.hi), 0.0);
+  dd l2 = dd_log2(x);
+  if (!isfinite(l2.hi)) return l2;
+  return dd_mul(l2, make(mf_ln_2_hi[0], mf_ln_2_lo[0]));
+}
+
+// ---- sin / cos (src/float64x2/trig.inc:114-266) ----------------------------
+__device__ __forceinline__ void dd_sub_step(double& rh, double& rl, double ph, double pl) {
+  double sh, sl, tl, tll;
+  two_sum(rh, -ph, sh, sl);
+  two_sum(rl, -pl, tl, tll);
+  sl = add(sl, tl);
+  fast_two_sum(sh, sl, rh, rl);
+  rl = add(rl, tll);
+  fast_two_sum(rh, rl, rh, rl);
+}
+__device__ __forceinline__ dd reduce_pi_half(dd x, int& n_mod4) {
+  double n_float = rint(mul(x.hi, 0.6366197723675814));
+  double rh = x.hi, rl = x.lo, ph, pl;
+  ph = mul(n_float, mf_pi_half_cw[0]);
+  pl = fma_(n_float, mf_pi_half_cw[0], -ph);
+  dd_sub_step(rh, rl, ph, pl);
+  ph = mul(n_float, mf_pi_half_cw[1]);
+  pl = fma_(n_float, mf_pi_half_cw[1], -ph);
+  dd_sub_step(rh, rl, ph, pl);
+  ph = mul(n_float, mf_pi_half_cw[2]);
+  dd_sub_step(rh, rl, ph, 0.0);
+  long long nn = (long long)fabs(n_float) & 3LL;
+  if (n_float < 0.0) nn = (4 - nn) & 3;
+  n_mod4 = (int)nn;
+  return make(rh, rl);
+}
+__device__ __forceinline__ dd sin_kernel(dd x) {
+  dd x2 = dd_mul(x, x);
+  return dd_mul(neval12(x2, mf_sin_taylor_hi, mf_sin_taylor_lo), x);
+}
+__device__ __forceinline__ dd cos_kernel(dd x) {
+  dd x2 = dd_mul(x, x);
+  return neval12(x2, mf_cos_taylor_hi, mf_cos_taylor_lo);
+}
+// want_sin selects sin_eval (true) or cos_eval (false) of trig.inc:165-187.
+__device__ __forceinline__ dd sincos_eval_one(dd r, bool want_sin) {
+  const double pi8 = 0.392699081698724;
+  if (fabs(r.hi) <= pi8) return want_sin ? sin_kernel(r) : cos_kernel(r);
+  dd pi4 = make(mf_pi_quarter_hi[0], mf_pi_quarter_lo[0]);
+  dd is2 = make(mf_inv_sqrt2_hi[0], mf_inv_sqrt2_lo[0]);
+  bool pos = r.hi > 0.0;
+  dd rp = pos ? dd_sub(r, pi4) : dd_add(r, pi4);
+  dd sk = sin_kernel(rp);
+  dd ck = cos_kernel(rp);
+  if (want_sin) return pos ? dd_mul(dd_add(sk, ck), is2) : dd_mul(dd_sub(sk, ck), is2);
+  return pos ? dd_mul(dd_sub(ck, sk), is2) : dd_mul(dd_add(ck, sk), is2);
+}
+__device__ __forceinline__ bool trig_arg_too_large(double a) { return !(fabs(a) < 0x1p55); }
+
+__device__ __forceinline__ dd dd_sin(dd x) {
+  if (x.hi == 0.0 && x.lo == 0.0) return x;
+  if (!isfinite(x.hi) || trig_arg_too_large(x.hi)) return make(CUDART_NAN, 0.0);
+  int q;
+  dd r = reduce_pi_half(x, q);
+  // q=0: sin, q=1: cos, q=2: -sin, q=3: -cos
+  dd v = sincos_eval_one(r, (q & 1) == 0);
+  return (q & 2) ? neg(v) : v;
+}
+__device__ __forceinline__ dd dd_cos(dd x) {
+  if (!isfinite(x.hi) || trig_arg_too_large(x.hi)) return make(CUDART_NAN, 0.0);
+  int q;
+  dd r = reduce_pi_half(x, q);
+  // q=0: cos, q=1: -sin, q=2: -cos, q=3: sin
+  dd v = sincos_eval_one(r, (q & 1) == 1);
+  return (q == 1 || q == 2) ? neg(v) : v;
+}
+
+// ---- compensated matmul MAC (src/float64x2/matmul.inc:6-39) ----------------
+__device__ __forceinline__ void mac(double ah, double al, double bh, double bl, double& s_hi,
+                                    double& s_lo) {
+  double p = mul(ah, bh);
+  double e = fma_(ah, bh, -p);
+  double cross = fma_(ah, bl, mul(al, bh));
+  double t = add(s_hi, p);
+  double bp = sub(t, s_hi);
+  double ap = sub(t, bp);
+  double aerr = sub(s_hi, ap);
+  double berr = sub(p, bp);
+  s_lo = add(s_lo, add(add(e, cross), add(aerr, berr)));
+  s_hi = t;
+}
+__device__ __forceinline__ void renorm(double& s_hi, double& s_lo) {
+  double t = add(s_hi, s_lo);
+  double bp = sub(t, s_hi);
+  double ap = sub(t, bp);
+  double aerr = sub(s_hi, ap);
+  double berr = sub(s_lo, bp);
+  s_lo = add(aerr, berr);
+  s_hi = t;
+}
+
+}  // namespace mfdev

@@ -1,0 +1,87 @@
+"""Seeded synthetic inputs with the shapes and value distributions of the
+benchmark configurations (no public dataset is involved).
+
+All generators return float64 numpy arrays with interleaved limbs (hi, lo) and
+normalised double-doubles: lo = hi * 2^-53 * U[-1, 1), then (hi, lo) passed
+through two_sum so |lo| <= ulp(hi)/2.  Matrices are column-major flat buffers.
+
+  dd_uniform          hi ~ U[-1, 1)                               (GEMM 256^3 / 4096^3, reductions)
+  dd_exp_inputs       hi ~ U[-700, 700]                           (exp)
+  dd_pow2_inputs      hi = 2^U[-1000, 1000]                       (log, sqrt)
+  dd_trig_inputs      hi ~ U[-1e6, 1e6], 10% within 1e-12 of k*pi/2 (sin, cos)
+  dd_rowcol_scaled    hi = +-u 2^e, u ~ U[1,2), e ~ U{-R..R} per row of A /
+                      column of B                                 (split-INT8 GEMM)
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _renorm(hi: np.ndarray, lo: np.ndarray) -> np.ndarray:
+    s = hi + lo
+    bb = s - hi
+    err = (hi - (s - bb)) + (lo - bb)
+    out = np.empty(hi.size * 2, dtype=np.float64)
+    out[0::2] = s.reshape(-1)
+    out[1::2] = err.reshape(-1)
+    return out
+
+
+def with_lo(hi: np.ndarray, rng: np.random.Generator) -> np.ndarray:
+    hi = np.asarray(hi, dtype=np.float64).reshape(-1)
+    lo = hi * 2.0 ** -53 * rng.uniform(-1.0, 1.0, hi.size)
+    return _renorm(hi, lo)
+
+
+def dd_uniform(n: int, seed: int = 0) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return with_lo(rng.uniform(-1.0, 1.0, n), rng)
+
+
+def dd_exp_inputs(n: int, seed: int = 1) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return with_lo(rng.uniform(-700.0, 700.0, n), rng)
+
+
+def dd_pow2_inputs(n: int, seed: int = 2) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return with_lo(np.exp2(rng.uniform(-1000.0, 1000.0, n)), rng)
+
+
+def dd_trig_inputs(n: int, seed: int = 3) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    hi = rng.uniform(-1e6, 1e6, n)
+    near = rng.random(n) < 0.10
+    kmax = int(1e6 / (np.pi / 2))
+    k = rng.integers(-kmax, kmax + 1, n)
+    hi = np.where(near, k * (np.pi / 2) + rng.uniform(-1e-12, 1e-12, n), hi)
+    return with_lo(hi, rng)
+
+
+def dd_rowcol_scaled(rows: int, cols: int, R: int, per: str, seed: int) -> np.ndarray:
+    """Column-major rows x cols matrix; exponent constant per row ('row') or per column ('col')."""
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(1.0, 2.0, (cols, rows)) * rng.choice([-1.0, 1.0], (cols, rows))
+    if per == "row":
+        e = rng.integers(-R, R + 1, rows)[None, :]
+    else:
+        e = rng.integers(-R, R + 1, cols)[:, None]
+    hi = np.ldexp(u, np.broadcast_to(e, u.shape))
+    return with_lo(hi, rng)
+
+
+def complex_from_parts(re: np.ndarray, im: np.ndarray) -> np.ndarray:
+    """Interleave two DD arrays into complex64x2 layout (re.hi, re.lo, im.hi, im.lo)."""
+    out = np.empty(re.size * 2, dtype=np.float64)
+    out.reshape(-1, 4)[:, 0:2] = re.reshape(-1, 2)
+    out.reshape(-1, 4)[:, 2:4] = im.reshape(-1, 2)
+    return out
+
+
+ELEMENTWISE_INPUTS = {
+    "exp": dd_exp_inputs,
+    "log": dd_pow2_inputs,
+    "sin": dd_trig_inputs,
+    "cos": dd_trig_inputs,
+    "sqrt": dd_pow2_inputs,
+}

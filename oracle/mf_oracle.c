@@ -1,0 +1,801 @@
+/* ORACLE -- test infrastructure only.  Nothing in the product links, loads or
+ * calls this file; only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg use it, as the checker.
+ *
+ * A plain-C (C99 + __int128) restatement of the multifloats 0.10.3 algorithms
+ * on the array hot path, compiled with -ffp-contract=off so that every
+ * operation rounds exactly as written (the reference pins the same flag,
+ * src/CMakeLists.txt:105-118).  Each function cites the reference file:line it
+ * follows.  Pinning: tests/test_oracle_pin.py compares these functions with
+ * the reference library itself (built from the reference sources into
+ * oracle/_ref/ by oracle/Makefile when the sources are present) and with the
+ * golden vectors under tests/golden/ that the reference produced.
+ *
+ * Also here: the fixed blocked order of the device reductions, restated so the
+ * GPU results can be checked bit for bit, and an exact superaccumulator used to
+ * measure GEMM / dot errors in DD ulps (1 DD ulp = 2^-104).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define MF_TABLE static const
+#define MF_GTABLE static const
+#include "../multifloats_b200/csrc/dd_tables.h"
+
+typedef struct {
+  double hi, lo;
+} dd;
+
+static dd mk(double h, double l) {
+  dd r;
+  r.hi = h;
+  r.lo = l;
+  return r;
+}
+
+/* ---- EFTs: include/multifloats/float64x2.h:84-107 ---------------------- */
+static void two_sum(double a, double b, double *s, double *e) {
+  double ss = a + b;
+  double ap = ss - b;
+  double bp = ss - ap;
+  *e = (a - ap) + (b - bp);
+  *s = ss;
+}
+static void fast_two_sum(double a, double b, double *s, double *e) {
+  double ss = a + b;
+  double bp = ss - a;
+  *e = b - bp;
+  *s = ss;
+}
+static void two_prod(double a, double b, double *p, double *e) {
+  double pp = a * b;
+  *e = fma(a, b, -pp);
+  *p = pp;
+}
+
+/* ---- DD operators: float64x2.h:203-311 ---------------------------------- */
+static dd dd_add(dd x, dd y) {
+  double s = x.hi + y.hi;
+  if (!isfinite(s)) return mk(s, 0.0);
+  if (x.hi == 0.0 && y.hi == 0.0) return mk(s, x.lo + y.lo);
+  double a, b, c, d;
+  two_sum(x.hi, y.hi, &a, &b);
+  two_sum(x.lo, y.lo, &c, &d);
+  fast_two_sum(a, c, &a, &c);
+  b += d;
+  b += c;
+  dd r;
+  fast_two_sum(a, b, &r.hi, &r.lo);
+  return r;
+}
+static dd dd_sub(dd x, dd y) {
+  double s = x.hi - y.hi;
+  if (!isfinite(s)) return mk(s, 0.0);
+  if (x.hi == 0.0 && y.hi == 0.0) return mk(s, x.lo - y.lo);
+  double a, b, c, d;
+  two_sum(x.hi, -y.hi, &a, &b);
+  two_sum(x.lo, -y.lo, &c, &d);
+  fast_two_sum(a, c, &a, &c);
+  b += d;
+  b += c;
+  dd r;
+  fast_two_sum(a, b, &r.hi, &r.lo);
+  return r;
+}
+static dd dd_mul(dd x, dd y) {
+  double p00, e00;
+  two_prod(x.hi, y.hi, &p00, &e00);
+  if (!isfinite(p00)) return mk(p00, 0.0);
+  double p01 = x.hi * y.lo;
+  double p10 = x.lo * y.hi;
+  p01 += p10;
+  e00 += p01;
+  dd r;
+  fast_two_sum(p00, e00, &r.hi, &r.lo);
+  return r;
+}
+static dd dd_div(dd x, dd y) {
+  double q1 = x.hi / y.hi;
+  if (!isfinite(q1)) return mk(q1, q1);
+  if (!isfinite(y.hi)) return mk(q1, 0.0);
+  double p00, e00;
+  two_prod(q1, y.hi, &p00, &e00);
+  double p01 = q1 * y.lo;
+  double qhi = p00, qlo = e00 + p01;
+  double r0, r0e;
+  two_sum(x.hi, -qhi, &r0, &r0e);
+  double r1 = (x.lo - qlo) + r0e;
+  double rh, rl;
+  fast_two_sum(r0, r1, &rh, &rl);
+  double q2 = rh / y.hi;
+  dd r;
+  fast_two_sum(q1, q2, &r.hi, &r.lo);
+  return r;
+}
+static dd dd_neg(dd a) { return mk(-a.hi, -a.lo); }
+
+/* ---- sqrt: float64x2.h:2190-2212 ---------------------------------------- */
+static dd dd_sqrt(dd x) {
+  double c = sqrt(x.hi);
+  if (!(x.hi > 0.0) || !isfinite(c)) return mk(c, 0.0);
+  double u, uu;
+  two_prod(c, c, &u, &uu);
+  double cc = ((x.hi - u) - uu + x.lo) / (2.0 * c);
+  dd r;
+  r.hi = c + cc;
+  r.lo = (c - r.hi) + cc;
+  return r;
+}
+
+/* ---- polynomial evaluators: src/float64x2/poly.inc:9-102 ------------------ */
+static dd horner(dd y, const double *hi, const double *lo, int n) {
+  dd p = mk(hi[n - 1], lo[n - 1]);
+  for (int i = n - 2; i >= 0; --i) p = dd_add(dd_mul(p, y), mk(hi[i], lo[i]));
+  return p;
+}
+#define C_(i) mk(hi[i], lo[i])
+static dd neval10(dd x, const double *hi, const double *lo) {
+  dd x2 = dd_mul(x, x), x4 = dd_mul(x2, x2), x8 = dd_mul(x4, x4);
+  dd p01 = dd_add(C_(0), dd_mul(C_(1), x));
+  dd p23 = dd_add(C_(2), dd_mul(C_(3), x));
+  dd p45 = dd_add(C_(4), dd_mul(C_(5), x));
+  dd p67 = dd_add(C_(6), dd_mul(C_(7), x));
+  dd p89 = dd_add(C_(8), dd_mul(C_(9), x));
+  dd p03 = dd_add(p01, dd_mul(p23, x2));
+  dd p47 = dd_add(p45, dd_mul(p67, x2));
+  dd p810 = dd_add(p89, dd_mul(C_(10), x2));
+  return dd_add(dd_add(p03, dd_mul(p47, x4)), dd_mul(p810, x8));
+}
+static dd neval12(dd x, const double *hi, const double *lo) {
+  dd x2 = dd_mul(x, x), x4 = dd_mul(x2, x2), x8 = dd_mul(x4, x4);
+  dd p01 = dd_add(C_(0), dd_mul(C_(1), x));
+  dd p23 = dd_add(C_(2), dd_mul(C_(3), x));
+  dd p45 = dd_add(C_(4), dd_mul(C_(5), x));
+  dd p67 = dd_add(C_(6), dd_mul(C_(7), x));
+  dd p89 = dd_add(C_(8), dd_mul(C_(9), x));
+  dd p1011 = dd_add(C_(10), dd_mul(C_(11), x));
+  dd p03 = dd_add(p01, dd_mul(p23, x2));
+  dd p47 = dd_add(p45, dd_mul(p67, x2));
+  dd p811 = dd_add(p89, dd_mul(p1011, x2));
+  return dd_add(dd_add(p03, dd_mul(p47, x4)), dd_mul(dd_add(p811, dd_mul(C_(12), x4)), x8));
+}
+#undef C_
+
+/* ---- exp: src/float64x2/exp_log.inc:26-72, :237-277 ---------------------- */
+static dd exp2_from_reduced(double n_d, double rh, double rl) {
+  if (n_d > 1100.0) return mk(INFINITY, 0.0);
+  if (n_d < -1100.0) return mk(0.0, 0.0);
+  double k_d = nearbyint(rh * 256.0);
+  int k = (int)k_d;
+  if (k > 128) k = 128;
+  if (k < -128) k = -128;
+  double sh = rh - (double)k / 256.0;
+  double sl = rl;
+  fast_two_sum(sh, sl, &sh, &sl);
+  dd s = mk(sh, sl);
+  dd q = mk(mf_exp2_coefs_hi[9], mf_exp2_coefs_lo[9]);
+  for (int j = 8; j >= 1; --j) {
+    q = dd_mul(q, s);
+    q = dd_add(q, mk(mf_exp2_coefs_hi[j], mf_exp2_coefs_lo[j]));
+  }
+  dd pow2s = dd_add(mk(1.0, 0.0), dd_mul(s, q));
+  dd T = mk(mf_exp2_table_hi[k + 128], mf_exp2_table_lo[k + 128]);
+  dd m = dd_mul(T, pow2s);
+  int n = (int)n_d;
+  return mk(ldexp(m.hi, n), ldexp(m.lo, n));
+}
+static dd orc_exp1(dd x) {
+  double h = x.hi;
+  if (!isfinite(h)) {
+    if (h > 0.0) return mk(h, 0.0);
+    if (h < 0.0) return mk(0.0, 0.0);
+    return mk(h, 0.0);
+  }
+  if (h > mf_exp_max[0]) return mk(INFINITY, 0.0);
+  if (h < mf_exp_min[0]) return mk(0.0, 0.0);
+  double n_d = nearbyint(h * mf_log2_e_hi[0]);
+  double rh, rl, t;
+  two_sum(h, -(n_d * mf_ln2_cw[0]), &rh, &t);
+  rl = t + x.lo;
+  fast_two_sum(rh, rl, &rh, &rl);
+  double p_hi = n_d * mf_ln2_cw[1];
+  double p_lo = fma(n_d, mf_ln2_cw[1], -p_hi);
+  two_sum(rh, -p_hi, &rh, &t);
+  rl += t - p_lo;
+  fast_two_sum(rh, rl, &rh, &rl);
+  two_sum(rh, -(n_d * mf_ln2_cw[2]), &rh, &t);
+  rl += t;
+  dd rr;
+  fast_two_sum(rh, rl, &rr.hi, &rr.lo);
+  dd y = dd_mul(rr, mk(mf_log2_e_hi[0], mf_log2_e_lo[0]));
+  return exp2_from_reduced(n_d, y.hi, y.lo);
+}
+
+/* ---- log: exp_log.inc:280-341 -------------------------------------------- */
+static dd log2_kernel(dd x) {
+  double hi = x.hi;
+  if (hi > 15.0 / 16.0 && hi < 17.0 / 16.0) {
+    dd num = dd_sub(x, mk(1.0, 0.0));
+    dd den = dd_add(x, mk(1.0, 0.0));
+    dd t = dd_div(num, den);
+    dd t2 = dd_mul(t, t);
+    return dd_mul(t, neval10(t2, mf_log2_wide_hi, mf_log2_wide_lo));
+  }
+  int e = ilogb(hi);
+  dd m = mk(ldexp(x.hi, -e), ldexp(x.lo, -e));
+  int idx = (int)((m.hi - 1.0) * 32.0);
+  if (idx < 0) idx = 0;
+  if (idx > 31) idx = 31;
+  dd c = mk(mf_log2_centers[idx], 0.0);
+  dd v = mk(mf_log2_values_hi[idx], mf_log2_values_lo[idx]);
+  dd t = dd_div(dd_sub(m, c), dd_add(m, c));
+  dd t2 = dd_mul(t, t);
+  dd p = horner(t2, mf_log2_narrow_hi, mf_log2_narrow_lo, 7);
+  return dd_add(dd_add(mk((double)e, 0.0), v), dd_mul(t, p));
+}
+static dd orc_log2(dd x) {
+  if (isnan(x.hi) || x.hi < 0.0) return mk(NAN, 0.0);
+  if (x.hi == 0.0) return mk(-INFINITY, 0.0);
+  if (!isfinite(x.hi)) return mk(INFINITY, 0.0);
+  return log2_kernel(x);
+}
+static dd orc_log1(dd x) {
+  if (!isfinite(x.hi)) return mk(log(x.hi), 0.0);
+  dd l2 = orc_log2(x);
+  if (!isfinite(l2.hi)) return l2;
+  return dd_mul(l2, mk(mf_ln_2_hi[0], mf_ln_2_lo[0]));
+}
+
+/* ---- sin / cos: src/float64x2/trig.inc:114-266 ---------------------------- */
+static void dd_sub_step(double *rh, double *rl, double ph, double pl) {
+  double sh, sl, tl, tll;
+  two_sum(*rh, -ph, &sh, &sl);
+  two_sum(*rl, -pl, &tl, &tll);
+  sl += tl;
+  fast_two_sum(sh, sl, rh, rl);
+  *rl += tll;
+  fast_two_sum(*rh, *rl, rh, rl);
+}
+static dd reduce_pi_half(dd x, int *n_mod4) {
+  double n_float = nearbyint(x.hi * 0.6366197723675814);
+  double rh = x.hi, rl = x.lo, ph, pl;
+  ph = n_float * mf_pi_half_cw[0];
+  pl = fma(n_float, mf_pi_half_cw[0], -ph);
+  dd_sub_step(&rh, &rl, ph, pl);
+  ph = n_float * mf_pi_half_cw[1];
+  pl = fma(n_float, mf_pi_half_cw[1], -ph);
+  dd_sub_step(&rh, &rl, ph, pl);
+  ph = n_float * mf_pi_half_cw[2];
+  dd_sub_step(&rh, &rl, ph, 0.0);
+  long long nn = (long long)fabs(n_float) & 3LL;
+  if (n_float < 0.0) nn = (4 - nn) & 3;
+  *n_mod4 = (int)nn;
+  return mk(rh, rl);
+}
+static dd sin_kernel(dd x) {
+  dd x2 = dd_mul(x, x);
+  return dd_mul(neval12(x2, mf_sin_taylor_hi, mf_sin_taylor_lo), x);
+}
+static dd cos_kernel(dd x) {
+  dd x2 = dd_mul(x, x);
+  return neval12(x2, mf_cos_taylor_hi, mf_cos_taylor_lo);
+}
+static dd sin_eval(dd r) {
+  const double pi8 = 0.392699081698724;
+  if (fabs(r.hi) <= pi8) return sin_kernel(r);
+  dd pi4 = mk(mf_pi_quarter_hi[0], mf_pi_quarter_lo[0]);
+  dd is2 = mk(mf_inv_sqrt2_hi[0], mf_inv_sqrt2_lo[0]);
+  int pos = r.hi > 0.0;
+  dd rp = pos ? dd_sub(r, pi4) : dd_add(r, pi4);
+  dd sk = sin_kernel(rp), ck = cos_kernel(rp);
+  return pos ? dd_mul(dd_add(sk, ck), is2) : dd_mul(dd_sub(sk, ck), is2);
+}
+static dd cos_eval(dd r) {
+  const double pi8 = 0.392699081698724;
+  if (fabs(r.hi) <= pi8) return cos_kernel(r);
+  dd pi4 = mk(mf_pi_quarter_hi[0], mf_pi_quarter_lo[0]);
+  dd is2 = mk(mf_inv_sqrt2_hi[0], mf_inv_sqrt2_lo[0]);
+  int pos = r.hi > 0.0;
+  dd rp = pos ? dd_sub(r, pi4) : dd_add(r, pi4);
+  dd sk = sin_kernel(rp), ck = cos_kernel(rp);
+  return pos ? dd_mul(dd_sub(ck, sk), is2) : dd_mul(dd_add(ck, sk), is2);
+}
+static int trig_too_large(double a) { return !(fabs(a) < 0x1p55); }
+static dd orc_sin1(dd x) {
+  if (x.hi == 0.0 && x.lo == 0.0) return x;
+  if (!isfinite(x.hi) || trig_too_large(x.hi)) return mk(NAN, 0.0);
+  int q;
+  dd r = reduce_pi_half(x, &q);
+  switch (q) {
+    case 0: return sin_eval(r);
+    case 1: return cos_eval(r);
+    case 2: return dd_neg(sin_eval(r));
+    default: return dd_neg(cos_eval(r));
+  }
+}
+static dd orc_cos1(dd x) {
+  if (!isfinite(x.hi) || trig_too_large(x.hi)) return mk(NAN, 0.0);
+  int q;
+  dd r = reduce_pi_half(x, &q);
+  switch (q) {
+    case 0: return cos_eval(r);
+    case 1: return dd_neg(sin_eval(r));
+    case 2: return dd_neg(cos_eval(r));
+    default: return sin_eval(r);
+  }
+}
+
+/* ---- elementwise array maps (Fortran elemental, fypp:792-798) ---------- */
+void orc_unary(int op, const double *x, double *y, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) {
+    dd v = mk(x[2 * i], x[2 * i + 1]), r;
+    switch (op) {
+      case 0: r = orc_exp1(v); break;
+      case 1: r = orc_log1(v); break;
+      case 2: r = orc_sin1(v); break;
+      case 3: r = orc_cos1(v); break;
+      default: r = dd_sqrt(v); break;
+    }
+    y[2 * i] = r.hi;
+    y[2 * i + 1] = r.lo;
+  }
+}
+
+/* DD binary operators on arrays, for pinning the operators themselves. */
+void orc_binary(int op, const double *a, const double *b, double *y, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) {
+    dd x = mk(a[2 * i], a[2 * i + 1]), z = mk(b[2 * i], b[2 * i + 1]), r;
+    switch (op) {
+      case 0: r = dd_add(x, z); break;
+      case 1: r = dd_sub(x, z); break;
+      case 2: r = dd_mul(x, z); break;
+      default: r = dd_div(x, z); break;
+    }
+    y[2 * i] = r.hi;
+    y[2 * i + 1] = r.lo;
+  }
+}
+
+/* ---- matmul: src/float64x2/matmul.inc:6-39, :182-239 --------------------- */
+static void mac(double ah, double al, double bh, double bl, double *s_hi, double *s_lo) {
+  double p = ah * bh;
+  double e = fma(ah, bh, -p);
+  double cross = fma(ah, bl, al * bh);
+  double t = *s_hi + p;
+  double bp = t - *s_hi;
+  double ap = t - bp;
+  double aerr = *s_hi - ap;
+  double berr = p - bp;
+  *s_lo += (e + cross) + (aerr + berr);
+  *s_hi = t;
+}
+static void renorm(double *s_hi, double *s_lo) {
+  double t = *s_hi + *s_lo;
+  double bp = t - *s_hi;
+  double ap = t - bp;
+  double aerr = *s_hi - ap;
+  double berr = *s_lo - bp;
+  *s_lo = aerr + berr;
+  *s_hi = t;
+}
+/* One output: sum_p mac(x[p*sx], y[p*sy]) with the chunked renorm cadence. */
+static dd mac_chain(const double *x, int64_t sx, const double *y, int64_t sy, int64_t k,
+                    int64_t ri) {
+  double sh = 0.0, sl = 0.0;
+  int64_t cnt = 0;
+  for (int64_t p = 0; p < k; ++p) {
+    mac(x[2 * p * sx], x[2 * p * sx + 1], y[2 * p * sy], y[2 * p * sy + 1], &sh, &sl);
+    if (ri > 0 && ++cnt == ri) {
+      cnt = 0;
+      if (p + 1 < k) renorm(&sh, &sl);
+    }
+  }
+  renorm(&sh, &sl);
+  return mk(sh, sl);
+}
+/* C(m,n) = A(m,k) B(k,n), column-major; rows [i0,i1) x cols [j0,j1) only. */
+void orc_matmul_mm_block(const double *a, const double *b, double *c, int64_t m, int64_t k,
+                         int64_t n, int64_t ri, int64_t i0, int64_t i1, int64_t j0, int64_t j1) {
+  (void)n;
+  for (int64_t j = j0; j < j1; ++j)
+    for (int64_t i = i0; i < i1; ++i) {
+      dd r = mac_chain(a + 2 * i, m, b + 2 * j * k, 1, k, ri);
+      c[2 * (j * m + i)] = r.hi;
+      c[2 * (j * m + i) + 1] = r.lo;
+    }
+}
+void orc_matmul_mm(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
+                   int64_t ri) {
+  orc_matmul_mm_block(a, b, c, m, k, n, ri, 0, m, 0, n);
+}
+void orc_matmul_mv(const double *a, const double *x, double *y, int64_t m, int64_t k, int64_t ri) {
+  for (int64_t i = 0; i < m; ++i) {
+    dd r = mac_chain(a + 2 * i, m, x, 1, k, ri);
+    y[2 * i] = r.hi;
+    y[2 * i + 1] = r.lo;
+  }
+}
+void orc_matmul_vm(const double *x, const double *b, double *y, int64_t k, int64_t n, int64_t ri) {
+  for (int64_t j = 0; j < n; ++j) {
+    dd r = mac_chain(x, 1, b + 2 * j * k, 1, k, ri);
+    y[2 * j] = r.hi;
+    y[2 * j + 1] = r.lo;
+  }
+}
+/* Fortran cdd_matmul_mm (fypp:2609-2621): 4 real products on the split
+ * parts, re = mm(ar,br) - mm(ai,bi), im = mm(ar,bi) + mm(ai,br). */
+void orc_cmatmul_mm(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
+                    int64_t ri) {
+  for (int64_t j = 0; j < n; ++j)
+    for (int64_t i = 0; i < m; ++i) {
+      const double *ar = a + 4 * i, *ai = a + 4 * i + 2;
+      const double *br = b + 4 * j * k, *bi = b + 4 * j * k + 2;
+      dd rr = mac_chain(ar, 2 * m, br, 2, k, ri);
+      dd ii = mac_chain(ai, 2 * m, bi, 2, k, ri);
+      dd rim = mac_chain(ar, 2 * m, bi, 2, k, ri);
+      dd irm = mac_chain(ai, 2 * m, br, 2, k, ri);
+      dd re = dd_sub(rr, ii), im = dd_add(rim, irm);
+      double *o = c + 4 * (j * m + i);
+      o[0] = re.hi;
+      o[1] = re.lo;
+      o[2] = im.hi;
+      o[3] = im.lo;
+    }
+}
+
+/* ---- Fortran reductions, serial (fsrc/multifloats.fypp) ----------------- */
+typedef struct {
+  double hi, lo;
+} acc2;
+/* dd_sum_1d per-element update (fypp:1994-1999) */
+static void sum_step(acc2 *s, double xh, double xl) {
+  double t = s->hi + xh;
+  double bp = t - s->hi;
+  double ap = t - bp;
+  double aerr = s->hi - ap;
+  double berr = xh - bp;
+  s->lo = s->lo + ((xl + aerr) + berr);
+  s->hi = t;
+}
+static dd sum_finish_fast(acc2 s) { /* fypp:2004-2006 */
+  double t = s.hi + s.lo;
+  double bp = t - s.hi;
+  return mk(t, s.lo - bp);
+}
+static dd sum_finish_full(acc2 s) { /* fypp:2143-2152 */
+  double t = s.hi + s.lo;
+  double bp = t - s.hi;
+  double ap = t - bp;
+  double aerr = s.hi - ap;
+  double berr = s.lo - bp;
+  return mk(t, aerr + berr);
+}
+/* dd_dot_product per-element update (fypp:2288-2298) */
+static void dot_step(acc2 *s, double ah, double al, double bh, double bl) {
+  double p = ah * bh;
+  double e = fma(ah, bh, -p);
+  double cross = ah * bl + al * bh;
+  double t = s->hi + p;
+  double bp = t - s->hi;
+  double ap = t - bp;
+  double aerr = s->hi - ap;
+  double berr = p - bp;
+  s->lo = s->lo + (((e + cross) + aerr) + berr);
+  s->hi = t;
+}
+static void dot_block_renorm(acc2 *s) { /* fypp:2301-2302 */
+  double t = s->hi + s->lo;
+  double bp = t - s->hi;
+  s->hi = t;
+  s->lo = s->lo - bp;
+}
+static dd dot_finish(acc2 s) { /* fypp:2304-2307 */
+  double t = s.hi + s.lo;
+  double bp = t - s.hi;
+  return mk(t, s.lo - bp);
+}
+
+/* Serial dot over elements x[i*sx], y[i*sy] (stride in DD units). */
+static dd dot_serial_strided(const double *x, int64_t sx, const double *y, int64_t sy, int64_t n,
+                             int64_t ri) {
+  acc2 s = {0.0, 0.0};
+  if (ri <= 0) {
+    for (int64_t i = 0; i < n; ++i)
+      dot_step(&s, x[2 * i * sx], x[2 * i * sx + 1], y[2 * i * sy], y[2 * i * sy + 1]);
+  } else {
+    for (int64_t kk = 0; kk < n; kk += ri) {
+      int64_t ke = kk + ri < n ? kk + ri : n;
+      for (int64_t i = kk; i < ke; ++i)
+        dot_step(&s, x[2 * i * sx], x[2 * i * sx + 1], y[2 * i * sy], y[2 * i * sy + 1]);
+      dot_block_renorm(&s);
+    }
+  }
+  return dot_finish(s);
+}
+
+void orc_sum_serial(const double *x, int64_t n, double *out) {
+  acc2 s = {0.0, 0.0};
+  for (int64_t i = 0; i < n; ++i) sum_step(&s, x[2 * i], x[2 * i + 1]);
+  dd r = sum_finish_fast(s);
+  out[0] = r.hi;
+  out[1] = r.lo;
+}
+void orc_csum_serial(const double *x, int64_t n, double *out) {
+  acc2 re = {0.0, 0.0}, im = {0.0, 0.0};
+  for (int64_t i = 0; i < n; ++i) {
+    sum_step(&re, x[4 * i], x[4 * i + 1]);
+    sum_step(&im, x[4 * i + 2], x[4 * i + 3]);
+  }
+  dd r = sum_finish_full(re), q = sum_finish_full(im);
+  out[0] = r.hi;
+  out[1] = r.lo;
+  out[2] = q.hi;
+  out[3] = q.lo;
+}
+void orc_dot_serial(const double *a, const double *b, int64_t n, int64_t ri, double *out) {
+  dd r = dot_serial_strided(a, 1, b, 1, n, ri);
+  out[0] = r.hi;
+  out[1] = r.lo;
+}
+/* cdd_dot_product (fypp:2321-2331): conj(a).b */
+void orc_cdot_serial(const double *a, const double *b, int64_t n, int64_t ri, double *out) {
+  dd rr = dot_serial_strided(a, 2, b, 2, n, ri);
+  dd ii = dot_serial_strided(a + 2, 2, b + 2, 2, n, ri);
+  dd rim = dot_serial_strided(a, 2, b + 2, 2, n, ri);
+  dd irm = dot_serial_strided(a + 2, 2, b, 2, n, ri);
+  dd re = dd_add(rr, ii), im = dd_sub(rim, irm);
+  out[0] = re.hi;
+  out[1] = re.lo;
+  out[2] = im.hi;
+  out[3] = im.lo;
+}
+/* dd_norm2_1d (fypp:2338-2352) */
+void orc_norm2_serial(const double *x, int64_t n, double *out) {
+  dd s = mk(0.0, 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    dd a = mk(x[2 * i], x[2 * i + 1]);
+    s = dd_add(s, dd_mul(a, a));
+  }
+  dd r = dd_sqrt(s);
+  out[0] = r.hi;
+  out[1] = r.lo;
+}
+/* complex norm2 = norm2 of the 2n real parts in storage order */
+void orc_cnorm2_serial(const double *x, int64_t n, double *out) { orc_norm2_serial(x, 2 * n, out); }
+
+/* ---- the device's fixed blocked order, restated -------------------------- */
+#define R_THREADS 256
+#define R_MAX_BLOCKS 2048
+#define R_PER_THREAD_MIN 16
+void orc_reduce_geometry(int64_t n, int64_t *blocks, int64_t *threads) {
+  int64_t per_block = (int64_t)R_THREADS * R_PER_THREAD_MIN;
+  int64_t b = (n + per_block - 1) / per_block;
+  if (b < 1) b = 1;
+  if (b > R_MAX_BLOCKS) b = R_MAX_BLOCKS;
+  *blocks = b;
+  *threads = R_THREADS;
+}
+/* warp shuffle-down tree over v[0..31] per warp, then warps 0..7 -> v[0] */
+static void block_tree(dd *v, int nv) {
+  dd wp[R_THREADS / 32][4];
+  for (int w = 0; w < R_THREADS / 32; ++w) {
+    dd *lane = v + (int64_t)w * 32 * nv;
+    for (int off = 16; off >= 1; off >>= 1)
+      for (int l = 0; l < off; ++l)
+        for (int q = 0; q < nv; ++q) lane[l * nv + q] = dd_add(lane[l * nv + q], lane[(l + off) * nv + q]);
+    for (int q = 0; q < nv; ++q) wp[w][q] = lane[q];
+  }
+  for (int off = (R_THREADS / 32) / 2; off >= 1; off >>= 1)
+    for (int l = 0; l < off; ++l)
+      for (int q = 0; q < nv; ++q) wp[l][q] = dd_add(wp[l][q], wp[l + off][q]);
+  for (int q = 0; q < nv; ++q) v[q] = wp[0][q];
+}
+/* kind: 0 sum, 1 dot, 2 norm2, 3 csum, 4 cdot, 5 cnorm2 (same as the device) */
+void orc_reduce_blocked(int kind, const double *x, const double *y, int64_t n, int64_t ri,
+                        double *out) {
+  static const int NV[6] = {1, 1, 1, 2, 4, 1};
+  static const int E[6] = {2, 2, 2, 4, 4, 4};
+  int nv = NV[kind], e = E[kind];
+  int64_t B, TPB;
+  orc_reduce_geometry(n, &B, &TPB);
+  int64_t T = B * TPB;
+  dd *part = (dd *)malloc(sizeof(dd) * (size_t)B * nv);
+  dd *v = (dd *)malloc(sizeof(dd) * R_THREADS * nv);
+  for (int64_t b = 0; b < B; ++b) {
+    for (int t = 0; t < R_THREADS; ++t) {
+      int64_t g = b * R_THREADS + t;
+      dd *o = v + (int64_t)t * nv;
+      if (kind == 0 || kind == 3) {
+        acc2 s[2] = {{0.0, 0.0}, {0.0, 0.0}};
+        for (int64_t i = g; i < n; i += T)
+          for (int q = 0; q < nv; ++q) sum_step(&s[q], x[e * i + 2 * q], x[e * i + 2 * q + 1]);
+        for (int q = 0; q < nv; ++q) o[q] = kind == 0 ? sum_finish_fast(s[q]) : sum_finish_full(s[q]);
+      } else if (kind == 1 || kind == 4) {
+        acc2 d[4] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+        int64_t cnt = 0;
+        for (int64_t i = g; i < n; i += T) {
+          if (kind == 1) {
+            dot_step(&d[0], x[2 * i], x[2 * i + 1], y[2 * i], y[2 * i + 1]);
+          } else {
+            const double *a = x + 4 * i, *bb = y + 4 * i;
+            dot_step(&d[0], a[0], a[1], bb[0], bb[1]);
+            dot_step(&d[1], a[2], a[3], bb[2], bb[3]);
+            dot_step(&d[2], a[0], a[1], bb[2], bb[3]);
+            dot_step(&d[3], a[2], a[3], bb[0], bb[1]);
+          }
+          if (ri > 0 && ++cnt == ri) {
+            cnt = 0;
+            for (int q = 0; q < nv; ++q) dot_block_renorm(&d[q]);
+          }
+        }
+        if (ri > 0 && cnt > 0)
+          for (int q = 0; q < nv; ++q) dot_block_renorm(&d[q]);
+        for (int q = 0; q < nv; ++q) o[q] = dot_finish(d[q]);
+      } else {
+        dd s = mk(0.0, 0.0);
+        for (int64_t i = g; i < n; i += T) {
+          dd a = mk(x[e * i], x[e * i + 1]);
+          s = dd_add(s, dd_mul(a, a));
+          if (kind == 5) {
+            dd bq = mk(x[e * i + 2], x[e * i + 3]);
+            s = dd_add(s, dd_mul(bq, bq));
+          }
+        }
+        o[0] = s;
+      }
+    }
+    block_tree(v, nv);
+    for (int q = 0; q < nv; ++q) part[b * nv + q] = v[q];
+  }
+  for (int t = 0; t < R_THREADS; ++t)
+    for (int q = 0; q < nv; ++q) v[(int64_t)t * nv + q] = mk(0.0, 0.0);
+  for (int t = 0; t < R_THREADS; ++t)
+    for (int64_t b = t; b < B; b += R_THREADS)
+      for (int q = 0; q < nv; ++q) {
+        dd p = part[b * nv + q];
+        v[(int64_t)t * nv + q] = (b == t) ? p : dd_add(v[(int64_t)t * nv + q], p);
+      }
+  block_tree(v, nv);
+  dd r0 = v[0], r1 = mk(0.0, 0.0);
+  if (kind == 2 || kind == 5) r0 = dd_sqrt(v[0]);
+  if (kind == 3) r1 = v[1];
+  if (kind == 4) {
+    r0 = dd_add(v[0], v[1]);
+    r1 = dd_sub(v[2], v[3]);
+  }
+  out[0] = r0.hi;
+  out[1] = r0.lo;
+  if (kind == 3 || kind == 4) {
+    out[2] = r1.hi;
+    out[3] = r1.lo;
+  }
+  free(part);
+  free(v);
+}
+
+/* ---- exact superaccumulator ------------------------------------------------
+ * Fixed-point accumulator over bit positions 2^SA_EMIN .. 2^(SA_EMIN+32*SA_LIMBS);
+ * limbs are 32-bit digits held in int64 so that up to 2^30 additions need no
+ * carry propagation.  A product of two doubles is added exactly as the 106-bit
+ * integer product of their significands. */
+#define SA_EMIN (-2400)
+#define SA_LIMBS 144
+typedef struct {
+  int64_t d[SA_LIMBS];
+} superacc;
+
+static void sa_add_int128(superacc *s, __int128 v, int e) {
+  /* adds v * 2^e */
+  if (v == 0) return;
+  int neg = v < 0;
+  unsigned __int128 u = neg ? (unsigned __int128)(-v) : (unsigned __int128)v;
+  int pos = e - SA_EMIN;
+  if (pos < 0) return; /* below 2^-2400: far under any DD error of interest */
+  int limb = pos >> 5, sh = pos & 31;
+  /* u << sh spans up to 128+31 bits: emit 32-bit pieces */
+  unsigned __int128 lo = u << sh;
+  unsigned __int128 hi = sh ? (u >> (128 - sh)) : 0;
+  for (int i = 0; i < 5; ++i) {
+    int64_t piece;
+    if (i < 4)
+      piece = (int64_t)((lo >> (32 * i)) & 0xffffffffu);
+    else
+      piece = (int64_t)(hi & 0xffffffffu);
+    if (piece && limb + i < SA_LIMBS) s->d[limb + i] += neg ? -piece : piece;
+  }
+}
+static void sa_add_double(superacc *s, double x) {
+  if (x == 0.0 || !isfinite(x)) return;
+  int ex;
+  double f = frexp(x, &ex); /* x = f * 2^ex, 0.5 <= |f| < 1 */
+  int64_t mant = (int64_t)ldexp(f, 53);
+  sa_add_int128(s, (__int128)mant, ex - 53);
+}
+static void sa_add_prod(superacc *s, double a, double b) {
+  if (a == 0.0 || b == 0.0 || !isfinite(a) || !isfinite(b)) return;
+  int ea, eb;
+  double fa = frexp(a, &ea), fb = frexp(b, &eb);
+  int64_t ma = (int64_t)ldexp(fa, 53), mb = (int64_t)ldexp(fb, 53);
+  sa_add_int128(s, (__int128)ma * (__int128)mb, ea + eb - 106);
+}
+static void sa_carry(superacc *s) {
+  for (int i = 0; i < SA_LIMBS - 1; ++i) {
+    int64_t c = s->d[i] >> 32; /* arithmetic shift: floor division */
+    s->d[i] -= c * ((int64_t)1 << 32);
+    s->d[i + 1] += c;
+  }
+}
+static double sa_value(superacc *s) {
+  /* canonical digits in [0, 2^32) below a signed top limb */
+  sa_carry(s);
+  int top = SA_LIMBS - 1;
+  while (top > 0 && s->d[top] == 0) --top;
+  double sign = 1.0;
+  if (s->d[top] < 0) { /* negate to sign-magnitude */
+    for (int i = 0; i < SA_LIMBS; ++i) s->d[i] = -s->d[i];
+    sa_carry(s);
+    sign = -1.0;
+    top = SA_LIMBS - 1;
+    while (top > 0 && s->d[top] == 0) --top;
+  }
+  double v = 0.0;
+  for (int i = top; i >= 0 && i >= top - 3; --i) v += ldexp((double)s->d[i], 32 * i + SA_EMIN);
+  return sign * v;
+}
+
+/* For selected outputs (i, j) of C = A B (column-major, DD), the exact error
+ * err = C_ij - (A B)_ij rounded to double, and absab = (|A||B|)_ij in double.
+ * complex_parts: 0 for real matrices. */
+void orc_gemm_errors(const double *a, const double *b, const double *c, int64_t m, int64_t k,
+                     int64_t n, const int64_t *ii, const int64_t *jj, int64_t count, double *err,
+                     double *absab) {
+  (void)n;
+  for (int64_t q = 0; q < count; ++q) {
+    int64_t i = ii[q], j = jj[q];
+    superacc s;
+    memset(&s, 0, sizeof(s));
+    double ab = 0.0;
+    for (int64_t p = 0; p < k; ++p) {
+      double ah = a[2 * (p * m + i)], al = a[2 * (p * m + i) + 1];
+      double bh = b[2 * (j * k + p)], bl = b[2 * (j * k + p) + 1];
+      sa_add_prod(&s, ah, bh);
+      sa_add_prod(&s, ah, bl);
+      sa_add_prod(&s, al, bh);
+      sa_add_prod(&s, al, bl);
+      ab += fabs(ah + al) * fabs(bh + bl);
+    }
+    sa_add_double(&s, -c[2 * (j * m + i)]);
+    sa_add_double(&s, -c[2 * (j * m + i) + 1]);
+    err[q] = -sa_value(&s);
+    absab[q] = ab;
+  }
+}
+
+/* Exact error of a DD reduction result: kind 0 sum, 1 dot (real only).
+ * err = result - exact, abs = sum |x| or sum |a||b|. */
+void orc_reduce_error(int kind, const double *x, const double *y, int64_t n, const double *res,
+                      double *err, double *absv) {
+  superacc s;
+  memset(&s, 0, sizeof(s));
+  double ab = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (kind == 0) {
+      sa_add_double(&s, x[2 * i]);
+      sa_add_double(&s, x[2 * i + 1]);
+      ab += fabs(x[2 * i] + x[2 * i + 1]);
+    } else {
+      double ah = x[2 * i], al = x[2 * i + 1], bh = y[2 * i], bl = y[2 * i + 1];
+      sa_add_prod(&s, ah, bh);
+      sa_add_prod(&s, ah, bl);
+      sa_add_prod(&s, al, bh);
+      sa_add_prod(&s, al, bl);
+      ab += fabs(ah + al) * fabs(bh + bl);
+    }
+  }
+  sa_add_double(&s, -res[0]);
+  sa_add_double(&s, -res[1]);
+  *err = -sa_value(&s);
+  *absv = ab;
+}

@@ -1,0 +1,274 @@
+"""ORACLE -- test infrastructure only (the checker; never part of the product path).
+
+ctypes wrappers around
+  * oracle/liboracle.so     the C restatement of the reference algorithms (mf_oracle.c)
+  * oracle/_ref/libmfref.so the reference library itself, compiled from its own
+                            sources by oracle/Makefile where they are present
+All arrays are float64 numpy buffers with interleaved limbs, as in the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmfref.so")
+
+P = C.c_void_p
+I64 = C.c_int64
+OPS = {"exp": 0, "log": 1, "sin": 2, "cos": 3, "sqrt": 4}
+KINDS = {"sum": 0, "dot": 1, "norm2": 2, "csum": 3, "cdot": 4, "cnorm2": 5}
+
+_orc = None
+_ref = None
+
+
+class _DD(C.Structure):
+    _fields_ = [("hi", C.c_double), ("lo", C.c_double)]
+
+
+def build(ref: bool = False) -> None:
+    args = ["make", "-s", "-C", HERE, "oracle"]
+    subprocess.run(args, check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def orc():
+    global _orc
+    if _orc is None:
+        src = os.path.join(HERE, "mf_oracle.c")
+        if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        L.orc_unary.argtypes = [C.c_int, P, P, I64]
+        L.orc_binary.argtypes = [C.c_int, P, P, P, I64]
+        L.orc_matmul_mm.argtypes = [P, P, P, I64, I64, I64, I64]
+        L.orc_matmul_mm_block.argtypes = [P, P, P, I64, I64, I64, I64, I64, I64, I64, I64]
+        L.orc_matmul_mv.argtypes = [P, P, P, I64, I64, I64]
+        L.orc_matmul_vm.argtypes = [P, P, P, I64, I64, I64]
+        L.orc_cmatmul_mm.argtypes = [P, P, P, I64, I64, I64, I64]
+        for f in ("orc_sum_serial", "orc_csum_serial", "orc_norm2_serial", "orc_cnorm2_serial"):
+            getattr(L, f).argtypes = [P, I64, P]
+        for f in ("orc_dot_serial", "orc_cdot_serial"):
+            getattr(L, f).argtypes = [P, P, I64, I64, P]
+        L.orc_reduce_geometry.argtypes = [I64, C.POINTER(I64), C.POINTER(I64)]
+        L.orc_reduce_blocked.argtypes = [C.c_int, P, P, I64, I64, P]
+        L.orc_gemm_errors.argtypes = [P, P, P, I64, I64, I64, P, P, I64, P, P]
+        L.orc_reduce_error.argtypes = [C.c_int, P, P, I64, P, P, P]
+        _orc = L
+    return _orc
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    """The reference library (None when it was not built here)."""
+    global _ref
+    if _ref is None and ref_available():
+        L = C.CDLL(REF_SO)
+        L.ref_unary_array.argtypes = [C.c_int, P, P, I64]
+        L.ref_unary_array_mt.argtypes = [C.c_int, P, P, I64, C.c_int]
+        L.ref_binary_array.argtypes = [C.c_int, P, P, P, I64]
+        L.matmuldd_mm.argtypes = [P, P, P, I64, I64, I64, I64]
+        L.matmuldd_mv.argtypes = [P, P, P, I64, I64, I64]
+        L.matmuldd_vm.argtypes = [P, P, P, I64, I64, I64]
+        L.ref_matmul_mm_mt.argtypes = [P, P, P, I64, I64, I64, I64, C.c_int]
+        L.ref_cmatmul_mm.argtypes = [P, P, P, I64, I64, I64, I64]
+        L.ref_norm2_serial.argtypes = [P, I64]
+        L.ref_norm2_serial.restype = _DD
+        _ref = L
+    return _ref
+
+
+def _p(a: np.ndarray) -> int:
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data
+
+
+def _c(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+
+
+# ---- C restatement ------------------------------------------------------------
+def unary(op: str, x) -> np.ndarray:
+    x = _c(x)
+    y = np.empty_like(x)
+    orc().orc_unary(OPS[op], _p(x), _p(y), x.size // 2)
+    return y
+
+
+def binary(op: int, a, b) -> np.ndarray:
+    a, b = _c(a), _c(b)
+    y = np.empty_like(a)
+    orc().orc_binary(op, _p(a), _p(b), _p(y), a.size // 2)
+    return y
+
+
+def matmul_mm(a, b, m, k, n, ri=8) -> np.ndarray:
+    a, b = _c(a), _c(b)
+    c = np.empty(2 * m * n)
+    orc().orc_matmul_mm(_p(a), _p(b), _p(c), m, k, n, ri)
+    return c
+
+
+def matmul_mm_cols(a, b, m, k, n, ri, j0, j1) -> np.ndarray:
+    """Columns [j0, j1) of C only (the others are left uninitialised)."""
+    a, b = _c(a), _c(b)
+    c = np.zeros(2 * m * n)
+    orc().orc_matmul_mm_block(_p(a), _p(b), _p(c), m, k, n, ri, 0, m, j0, j1)
+    return c
+
+
+def matmul_mv(a, x, m, k, ri=8) -> np.ndarray:
+    a, x = _c(a), _c(x)
+    y = np.empty(2 * m)
+    orc().orc_matmul_mv(_p(a), _p(x), _p(y), m, k, ri)
+    return y
+
+
+def matmul_vm(x, b, k, n, ri=8) -> np.ndarray:
+    x, b = _c(x), _c(b)
+    y = np.empty(2 * n)
+    orc().orc_matmul_vm(_p(x), _p(b), _p(y), k, n, ri)
+    return y
+
+
+def cmatmul_mm(a, b, m, k, n, ri=8) -> np.ndarray:
+    a, b = _c(a), _c(b)
+    c = np.empty(4 * m * n)
+    orc().orc_cmatmul_mm(_p(a), _p(b), _p(c), m, k, n, ri)
+    return c
+
+
+def reduce_serial(kind: str, x, y=None, ri=8) -> np.ndarray:
+    """The reference's serial Fortran semantics."""
+    x = _c(x)
+    L = orc()
+    cplx = kind.startswith("c")
+    n = x.size // (4 if cplx else 2)
+    out = np.zeros(4)
+    if kind == "sum":
+        L.orc_sum_serial(_p(x), n, _p(out))
+    elif kind == "csum":
+        L.orc_csum_serial(_p(x), n, _p(out))
+    elif kind == "norm2":
+        L.orc_norm2_serial(_p(x), n, _p(out))
+    elif kind == "cnorm2":
+        L.orc_cnorm2_serial(_p(x), n, _p(out))
+    elif kind == "dot":
+        y = _c(y)
+        L.orc_dot_serial(_p(x), _p(y), n, ri, _p(out))
+    elif kind == "cdot":
+        y = _c(y)
+        L.orc_cdot_serial(_p(x), _p(y), n, ri, _p(out))
+    return out[:4] if kind in ("csum", "cdot") else out[:2]
+
+
+def reduce_blocked(kind: str, x, y=None, ri=8) -> np.ndarray:
+    """The device's fixed blocked order, restated."""
+    x = _c(x)
+    cplx = kind.startswith("c")
+    n = x.size // (4 if cplx else 2)
+    yy = _c(y) if y is not None else x
+    out = np.zeros(4)
+    orc().orc_reduce_blocked(KINDS[kind], _p(x), _p(yy), n, ri, _p(out))
+    return out[:4] if kind in ("csum", "cdot") else out[:2]
+
+
+def reduce_geometry(n: int) -> tuple[int, int]:
+    b, t = I64(), I64()
+    orc().orc_reduce_geometry(n, C.byref(b), C.byref(t))
+    return b.value, t.value
+
+
+def gemm_errors(a, b, c, m, k, n, ii, jj):
+    """Exact err = C_ij - (AB)_ij and (|A||B|)_ij for the listed outputs."""
+    a, b, c = _c(a), _c(b), _c(c)
+    ii = np.ascontiguousarray(ii, dtype=np.int64)
+    jj = np.ascontiguousarray(jj, dtype=np.int64)
+    err = np.empty(ii.size)
+    ab = np.empty(ii.size)
+    orc().orc_gemm_errors(_p(a), _p(b), _p(c), m, k, n, ii.ctypes.data, jj.ctypes.data, ii.size,
+                          _p(err), _p(ab))
+    return err, ab
+
+
+def reduce_error(kind: str, x, y, res):
+    """Exact err = res - exact value and the sum of magnitudes, kind 'sum' or 'dot'."""
+    x = _c(x)
+    yy = _c(y) if y is not None else x
+    res = _c(res)
+    err, ab = C.c_double(), C.c_double()
+    orc().orc_reduce_error(0 if kind == "sum" else 1, _p(x), _p(yy), x.size // 2, _p(res),
+                           C.byref(err), C.byref(ab))
+    return err.value, ab.value
+
+
+# ---- the reference itself -------------------------------------------------------
+def ref_unary(op: str, x, threads: int = 1) -> np.ndarray:
+    x = _c(x)
+    y = np.empty_like(x)
+    if threads > 1:
+        ref().ref_unary_array_mt(OPS[op], _p(x), _p(y), x.size // 2, threads)
+    else:
+        ref().ref_unary_array(OPS[op], _p(x), _p(y), x.size // 2)
+    return y
+
+
+def ref_binary(op: int, a, b) -> np.ndarray:
+    a, b = _c(a), _c(b)
+    y = np.empty_like(a)
+    ref().ref_binary_array(op, _p(a), _p(b), _p(y), a.size // 2)
+    return y
+
+
+def ref_matmul_mm(a, b, m, k, n, ri=8, threads: int = 1) -> np.ndarray:
+    a, b = _c(a), _c(b)
+    c = np.empty(2 * m * n)
+    ref().ref_matmul_mm_mt(_p(a), _p(b), _p(c), m, k, n, ri, threads)
+    return c
+
+
+def ref_cmatmul_mm(a, b, m, k, n, ri=8) -> np.ndarray:
+    a, b = _c(a), _c(b)
+    c = np.empty(4 * m * n)
+    ref().ref_cmatmul_mm(_p(a), _p(b), _p(c), m, k, n, ri)
+    return c
+
+
+def ref_norm2(x) -> np.ndarray:
+    x = _c(x)
+    r = ref().ref_norm2_serial(_p(x), x.size // 2)
+    return np.array([r.hi, r.lo])
+
+
+def ref_matmul_mv(a, x, m, k, ri=8) -> np.ndarray:
+    a, x = _c(a), _c(x)
+    y = np.empty(2 * m)
+    ref().matmuldd_mv(_p(a), _p(x), _p(y), m, k, ri)
+    return y
+
+
+def ref_matmul_vm(x, b, k, n, ri=8) -> np.ndarray:
+    x, b = _c(x), _c(b)
+    y = np.empty(2 * n)
+    ref().matmuldd_vm(_p(x), _p(b), _p(y), k, n, ri)
+    return y
+
+
+# ---- comparison helpers -----------------------------------------------------------
+def same_bits(a, b) -> np.ndarray:
+    """Elementwise bit equality with every NaN treated as one class (per DD value:
+    both limbs must match; a NaN hi limb matches any NaN hi limb)."""
+    a = _c(a).reshape(-1, 2)
+    b = _c(b).reshape(-1, 2)
+    eq = (a.view(np.int64) == b.view(np.int64)).all(axis=1)
+    nan = np.isnan(a[:, 0]) & np.isnan(b[:, 0])
+    return eq | nan

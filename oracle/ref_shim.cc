@@ -1,0 +1,110 @@
+// ORACLE -- test infrastructure only.  Array loops and a multi-threaded
+// driver around the reference library's own C ABI, compiled together with the
+// reference sources into oracle/_ref/libmfref.so by oracle/Makefile.  Used to
+// pin the C restatement, to generate golden vectors, and as the timed CPU
+// baseline (bench.py --impl reference).  Every value comes from the
+// reference's exported functions (expdd, logdd, ..., matmuldd_mm); this file
+// only loops over them.
+#include <multifloats/float64x2.h>
+
+#include <cstdint>
+#include <thread>
+#include <vector>
+
+using multifloats::float64x2;
+using namespace multifloats;
+
+extern "C" {
+
+void ref_unary_array(int op, const float64x2 *x, float64x2 *y, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) {
+    switch (op) {
+      case 0: y[i] = expdd(x[i]); break;
+      case 1: y[i] = logdd(x[i]); break;
+      case 2: y[i] = sindd(x[i]); break;
+      case 3: y[i] = cosdd(x[i]); break;
+      default: y[i] = sqrtdd(x[i]); break;
+    }
+  }
+}
+
+void ref_binary_array(int op, const float64x2 *a, const float64x2 *b, float64x2 *y, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) {
+    switch (op) {
+      case 0: y[i] = adddd(a[i], b[i]); break;
+      case 1: y[i] = subdd(a[i], b[i]); break;
+      case 2: y[i] = muldd(a[i], b[i]); break;
+      default: y[i] = divdd(a[i], b[i]); break;
+    }
+  }
+}
+
+// Unary map over n elements with `threads` threads (contiguous ranges).
+void ref_unary_array_mt(int op, const float64x2 *x, float64x2 *y, int64_t n, int threads) {
+  if (threads <= 1 || n < 1024) {
+    ref_unary_array(op, x, y, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  int64_t chunk = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    int64_t lo = t * chunk, hi = lo + chunk < n ? lo + chunk : n;
+    if (lo >= hi) break;
+    pool.emplace_back([=] { ref_unary_array(op, x + lo, y + lo, hi - lo); });
+  }
+  for (auto &th : pool) th.join();
+}
+
+// matmuldd_mm with the columns of B and C sharded over `threads` threads.
+// Each output column is computed by exactly the code path a single call
+// takes, so the result is bit-identical to matmuldd_mm(a, b, c, m, k, n, ri).
+void ref_matmul_mm_mt(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k,
+                      int64_t n, int64_t ri, int threads) {
+  if (threads <= 1 || n < 4) {
+    matmuldd_mm(a, b, c, m, k, n, ri);
+    return;
+  }
+  // even column counts keep the reference's NR=2 panel pairing identical
+  int64_t chunk = (n + threads - 1) / threads;
+  chunk += chunk & 1;
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t) {
+    int64_t j0 = t * chunk, j1 = j0 + chunk < n ? j0 + chunk : n;
+    if (j0 >= j1) break;
+    pool.emplace_back([=] { matmuldd_mm(a, b + j0 * k, c + j0 * m, m, k, j1 - j0, ri); });
+  }
+  for (auto &th : pool) th.join();
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Fortran cdd_matmul_mm (fsrc/multifloats.fypp:2609-2621) composed from the
+// reference's own matmuldd_mm and DD operators: split into re/im temporaries,
+// four real products, then p_re = rr - ii, p_im = ri + ir.
+void ref_cmatmul_mm(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k,
+                    int64_t n, int64_t ri) {
+  std::vector<float64x2> ar(m * k), ai(m * k), br(k * n), bi(k * n);
+  for (int64_t i = 0; i < m * k; ++i) { ar[i] = a[2 * i]; ai[i] = a[2 * i + 1]; }
+  for (int64_t i = 0; i < k * n; ++i) { br[i] = b[2 * i]; bi[i] = b[2 * i + 1]; }
+  std::vector<float64x2> rr(m * n), ii(m * n), rim(m * n), irm(m * n);
+  matmuldd_mm(ar.data(), br.data(), rr.data(), m, k, n, ri);
+  matmuldd_mm(ai.data(), bi.data(), ii.data(), m, k, n, ri);
+  matmuldd_mm(ar.data(), bi.data(), rim.data(), m, k, n, ri);
+  matmuldd_mm(ai.data(), br.data(), irm.data(), m, k, n, ri);
+  for (int64_t i = 0; i < m * n; ++i) {
+    c[2 * i] = rr[i] - ii[i];
+    c[2 * i + 1] = rim[i] + irm[i];
+  }
+}
+
+// Fortran dd_norm2_1d (fypp:2338-2352) with the reference's DD operators
+// (bit-identical to the Fortran ones, test/integration/crosscheck.cc) and sqrtdd.
+float64x2 ref_norm2_serial(const float64x2 *x, int64_t n) {
+  float64x2 s(0.0);
+  for (int64_t i = 0; i < n; ++i) s = s + x[i] * x[i];
+  return sqrtdd(s);
+}
+
+}  // extern "C"
