@@ -173,6 +173,27 @@ MULTIFLOATS_CUDA_API int mfcuda_cdotdd(const complex64x2 *a, const complex64x2 *
 MULTIFLOATS_CUDA_API int mfcuda_cnorm2dd(const complex64x2 *x, int64_t n, float64x2 *out,
                                          void *workspace, size_t workspace_bytes, void *stream);
 
+/* Real dot product a . b that allocates nothing.  No counterpart in
+ * the reference: it exists for callers that cannot let a library allocate
+ * device memory -- a host application that gives the whole GPU memory to its
+ * own pool and forbids allocations behind its back, or code on a
+ * latency-critical path where cudaMalloc / cudaFree would synchronise the
+ * device.  Same arguments, order of operations and result (bit for bit) as
+ * mfcuda_dotdd with a NULL workspace, but the block partials live in a fixed
+ * 16 KiB device array inside the library, so:
+ *   - n is limited to 4,194,304 elements; larger n returns
+ *     MFCUDA_ERR_UNSUPPORTED without launching anything;
+ *   - the first call on each device looks up that array's device address
+ *     (once per device, with that device current); make that first call
+ *     before any stream capture;
+ *   - all calls share the one array, so calls that overlap on the GPU (for
+ *     example on two streams at once) race and corrupt each other's result;
+ *     serialise them.  No state carries from one call to the next.
+ * The array is held on every GPU that loads the library until process exit. */
+MULTIFLOATS_CUDA_API int mfcuda_dotdd_noalloc(const float64x2 *a, const float64x2 *b, int64_t n,
+                                              int64_t renorm_interval, float64x2 *out,
+                                              void *stream);
+
 /* Fixed launch geometry of the reductions for a given n (it depends on n only,
  * never on the device), exposed so a CPU restatement can follow the same order:
  * *blocks = number of thread blocks, *threads = threads per block. */

@@ -67,6 +67,7 @@ SIGNATURES = {
     "mfcuda_reduce_geometry": (None, [I64, C.POINTER(I64), C.POINTER(I64)]),
     "mfcuda_sumdd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
     "mfcuda_dotdd": (C.c_int, [P, P, I64, I64, P, P, C.c_size_t, P]),
+    "mfcuda_dotdd_noalloc": (C.c_int, [P, P, I64, I64, P, P]),
     "mfcuda_norm2dd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
     "mfcuda_csumdd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
     "mfcuda_cdotdd": (C.c_int, [P, P, I64, I64, P, P, C.c_size_t, P]),

@@ -322,6 +322,68 @@ static float64x2 nan_dd() {
   return r;
 }
 
+// ---- dot product that allocates nothing --------------------------------------
+// Some callers cannot let a library call cudaMalloc: a host application that
+// hands the whole GPU memory to its own pool and forbids allocations behind
+// its back, or code on a latency-critical path where cudaMalloc / cudaFree
+// would synchronise the device.  mfcuda_dotdd_noalloc serves them with the
+// block partials of the reduction kept in this fixed device array (16 KiB,
+// held by every GPU that loads the library until the process exits).  The
+// array holds kNoAllocMaxPartials partials, which limits n to
+// kNoAllocMaxPartials * 4096 elements (the launch geometry gives one partial
+// per 4096 elements).
+constexpr int64_t kNoAllocMaxPartials = 1024;
+static __device__ __align__(256) dd g_noalloc_partials[kNoAllocMaxPartials];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_addr[kNoAllocMaxDevices];
+
+// Device address of g_noalloc_partials on the current device.  In host code
+// the array's name only stands in for the symbol, so the address is looked up
+// once per device (with that device current) and cached.
+static int noalloc_scratch(void **p) {
+  int dev = 0;
+  MF_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return MFCUDA_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_partials);
+    if (e != cudaSuccess || !addr) {
+      (void)cudaGetLastError();
+      return MFCUDA_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = addr;
+  }
+  *p = g_noalloc_addr[dev];
+  return MFCUDA_OK;
+}
+
+static int dot_noalloc(const double *x, const double *y, int64_t n, int64_t ri, float64x2 *out,
+                       cudaStream_t s) {
+  if (!size_ok(n, 2 * sizeof(double))) return MFCUDA_ERR_INVALID_ARG;
+  if (!out || (n > 0 && (!x || !y))) return MFCUDA_ERR_INVALID_ARG;
+  int64_t blocks, threads;
+  reduce_geometry(n, &blocks, &threads);
+  if (blocks > kNoAllocMaxPartials) return MFCUDA_ERR_UNSUPPORTED;
+  MF_TRY(require_device());
+  void *scratch = nullptr;
+  MF_TRY(noalloc_scratch(&scratch));
+  // Every partial slot [0, blocks) is written by stage 1 before stage 2 reads
+  // it, so the contents left by an earlier call never leak into this one.
+  dd *part = static_cast<dd *>(scratch);
+  bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
+  if (aligned)
+    reduce_stage1<1, true><<<(unsigned)blocks, (unsigned)threads, 0, s>>>(x, y, n, ri, part);
+  else
+    reduce_stage1<1, false><<<(unsigned)blocks, (unsigned)threads, 0, s>>>(x, y, n, ri, part);
+  MF_TRY_CUDA(cudaGetLastError());
+  reduce_stage2<1><<<1, kRThreads, 0, s>>>(part, blocks, reinterpret_cast<dd *>(out));
+  MF_TRY_CUDA(cudaGetLastError());
+  return MFCUDA_OK;
+}
+
 }  // namespace mfcuda
 
 extern "C" {
@@ -341,6 +403,10 @@ MULTIFLOATS_CUDA_API int mfcuda_sumdd(const float64x2 *x, int64_t n, float64x2 *
 MULTIFLOATS_CUDA_API int mfcuda_dotdd(const float64x2 *a, const float64x2 *b, int64_t n, int64_t ri,
                                       float64x2 *out, void *ws, size_t wsb, void *stream) {
   return mfcuda::reduce_dev<1>(MF_D(a), MF_D(b), n, ri, out, ws, wsb, mfcuda::as_stream(stream));
+}
+MULTIFLOATS_CUDA_API int mfcuda_dotdd_noalloc(const float64x2 *a, const float64x2 *b, int64_t n,
+                                              int64_t ri, float64x2 *out, void *stream) {
+  return mfcuda::dot_noalloc(MF_D(a), MF_D(b), n, ri, out, mfcuda::as_stream(stream));
 }
 MULTIFLOATS_CUDA_API int mfcuda_norm2dd(const float64x2 *x, int64_t n, float64x2 *out, void *ws,
                                         size_t wsb, void *stream) {
