@@ -132,6 +132,21 @@ MULTIFLOATS_CUDA_API complex64x2 cdotdd_array(const complex64x2 *a, const comple
 /* sqrt(sum re^2 + im^2): norm2 of the array viewed as 2n reals (re0, im0, re1, ...). */
 MULTIFLOATS_CUDA_API float64x2 cnorm2dd_array(const complex64x2 *x, int64_t n);
 
+/* Split-INT8 DD matmul (no reference counterpart): the product matmuldd_mm
+ * computes, to a stated bound instead of bit for bit.  Each row of A and
+ * column of B is scaled by a power of two, every entry is rounded to a
+ * (8S-2)-bit integer and cut into S signed 8-bit slices, all slice pairs on
+ * anti-diagonals s + t <= S-1 are multiplied on the tcgen05 INT8 tensor cores
+ * with exact INT32 accumulation, and the diagonals are summed back into DD.
+ * slices = 0 picks S (<= 14) from the operands' exponent ranges so that the
+ * a-priori bound meets err_ij <= 8 k 2^-104 (|A||B|)_ij; *max_err_bound_out
+ * (may be NULL) receives that a-priori bound in units of k 2^-104 (|A||B|)_ij.
+ * A row of A or column of B holding Inf/NaN yields NaN in the affected
+ * outputs.  Host pointers, synchronous. */
+MULTIFLOATS_CUDA_API void matmuldd_mm_split(const float64x2 *a, const float64x2 *b, float64x2 *c,
+                                            int64_t m, int64_t k, int64_t n, int slices,
+                                            double *max_err_bound_out);
+
 /* ==========================================================================
  * 2. Device-pointer API (asynchronous on `stream`, a cudaStream_t; NULL = legacy
  *    default stream).  Return MFCUDA_OK or an error code.
@@ -148,6 +163,20 @@ MULTIFLOATS_CUDA_API int mfcuda_matmuldd_vm(const float64x2 *x, const float64x2 
 MULTIFLOATS_CUDA_API int mfcuda_cmatmuldd_mm(const complex64x2 *a, const complex64x2 *b,
                                              complex64x2 *c, int64_t m, int64_t k, int64_t n,
                                              int64_t renorm_interval, void *stream);
+
+/* Split-INT8 form on device pointers (16-byte aligned).  slices: 0 = choose
+ * from the exponent ranges for `target` (bound in units of k 2^-104 (|A||B|)_ij,
+ * 8 in the drop-in), 2..14 = fixed.  `workspace` may be NULL (stream-ordered
+ * allocation) or hold mfcuda_split_workspace_size(m, k, n) bytes.  info_out may
+ * be NULL or point to int[3] receiving {S, rho_A, rho_B} (slices used and the
+ * operands' exponent spreads); a non-NULL info_out makes the call wait for the
+ * result and report MFCUDA_ERR_TIMEOUT if a bounded device wait expired. */
+MULTIFLOATS_CUDA_API size_t mfcuda_split_workspace_size(int64_t m, int64_t k, int64_t n);
+MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_split(const float64x2 *a, const float64x2 *b,
+                                                  float64x2 *c, int64_t m, int64_t k, int64_t n,
+                                                  int slices, double target, void *workspace,
+                                                  size_t workspace_bytes, int *info_out,
+                                                  void *stream);
 
 /* op: 0 exp, 1 log, 2 sin, 3 cos, 4 sqrt */
 enum { MFCUDA_EXP = 0, MFCUDA_LOG = 1, MFCUDA_SIN = 2, MFCUDA_COS = 3, MFCUDA_SQRT = 4 };

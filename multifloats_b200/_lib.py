@@ -57,6 +57,10 @@ SIGNATURES = {
     "csumdd_array": (complex64x2, [P, I64]),
     "cdotdd_array": (complex64x2, [P, P, I64, I64]),
     "cnorm2dd_array": (float64x2, [P, I64]),
+    "matmuldd_mm_split": (None, [P, P, P, I64, I64, I64, C.c_int, C.POINTER(C.c_double)]),
+    "mfcuda_split_workspace_size": (C.c_size_t, [I64, I64, I64]),
+    "mfcuda_matmuldd_mm_split": (C.c_int, [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, C.c_size_t,
+                                           P, P]),
     # device-pointer API
     "mfcuda_matmuldd_mm": (C.c_int, [P, P, P, I64, I64, I64, I64, P]),
     "mfcuda_matmuldd_mv": (C.c_int, [P, P, P, I64, I64, I64, P]),

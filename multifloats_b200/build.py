@@ -28,6 +28,7 @@ SOURCES = [
     "elementwise.cu",
     "gemm_dd.cu",
     "reduce_dd.cu",
+    "split_gemm.cu",
 ]
 HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh"]
 

@@ -1,0 +1,766 @@
+// Split-INT8 double-double GEMM on tcgen05 tensor cores (no reference
+// counterpart; it computes the same product as matmuldd_mm,
+// src/float64x2/matmul.inc, to a stated error bound instead of bit for bit).
+//
+//   1. scan   : per row i of A and column j of B, the binade bound sigma_i /
+//               tau_j (every |x| < 2^sigma) and the smallest binade mu of a
+//               nonzero entry; non-finite entries are flagged.
+//   2. plan   : slice count S (given, or the smallest S meeting the requested
+//               bound for the measured exponent spreads), W = 8S-2 bits.
+//   3. slice  : every DD entry is rounded exactly (128-bit integer arithmetic)
+//               to X = round(a 2^(W - sigma_i)), |X| < 2^W, and cut into S
+//               balanced signed 8-bit digits, most significant first:
+//               X = sum_s d_s 256^(S-1-s), d_s in [-128, 127].  Slices are
+//               stored K-major ([S][rows][K_pad] int8), zero-padded.
+//   4. mma    : persistent tcgen05 kernel.  Work item = one anti-diagonal
+//               g = s + t (0 <= g <= S-1) of one 128 x 256 output tile and one
+//               K chunk: D_g = sum_{s+t=g} A_s B_t^T accumulated in INT32 in
+//               tensor memory over K' = (g+1) K.  |d| <= 128 gives products
+//               <= 2^14 and the K chunk keeps (g+1) K_chunk 2^14 < 2^31, so
+//               the integer stage is exact.  Warp 0 issues TMA loads, one thread
+//               of warp 1 issues the MMAs, warps 2-5 drain the accumulator to an
+//               INT32 scratch ([g][kc][N_pad][M_pad]).  4-stage shared-memory
+//               ring (48 KB per stage), two 256-column TMEM accumulators so the
+//               drain of one item overlaps the MMAs of the next.  No multicast.
+//   5. combine: C_ij = 2^(sigma_i + tau_j - 12) sum_g D_g 2^(-8g), summed in
+//               DD from the smallest diagonal up, then scaled exactly.
+//
+// Error (a priori, per output):
+//   |C - AB|_ij <= 2^-(W+1) (2^sigma_i sum_p |b_pj| + 2^tau_j sum_p |a_ip|)   (rounding of the operands)
+//                + k S 2^(sigma_i + tau_j + 2 - 8S)                          (diagonals g >= S dropped)
+//                + 2^-105 |C_ij|                                           (final DD rounding)
+// With |a_ip| >= 2^(sigma_i - rho_A) and |b_pj| >= 2^(tau_j - rho_B) this is at
+// most (S+1) 2^(106 - 8S + rho_A + rho_B) times k 2^-104 (|A||B|)_ij, which is
+// how the plan picks S for a target (S = 14 gives 15/16 for rho_A = rho_B = 1).
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "common.cuh"
+#include "dd_device.cuh"
+#include "tcgen05.cuh"
+
+namespace mfcuda {
+namespace split {
+
+constexpr int SMAX = 14;           // most slices per operand
+constexpr int BM = 128, BN = 256;  // output tile (UMMA M x N)
+constexpr int BK = 128;            // int8 K bytes per pipeline stage (4 UMMAs of K=32)
+constexpr int UMMA_K = 32;
+constexpr int NSTAGE = 4;
+constexpr int A_STAGE = BM * BK;  // 16 KiB
+constexpr int B_STAGE = BN * BK;  // 32 KiB
+constexpr int STAGE = A_STAGE + B_STAGE;
+constexpr int TMEM_COLS = 2 * BN;  // two accumulators
+constexpr int MMA_THREADS = 192;   // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int MMA_SMEM = NSTAGE * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+// K chunk: (SMAX pairs) * K_chunk * 2^14 < 2^31  ->  73 blocks of 128
+constexpr int KC_BLOCKS = (int)(2147483647LL / ((long long)SMAX * 16384LL * BK));
+constexpr uint64_t WAIT_NS = 2000000000ull;  // bounded waits: 2 s
+
+struct Plan {
+  int S, G, W;
+  int rho_a, rho_b;
+  int pad[3];
+};
+
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait that also gives up as soon as another role of the CTA aborted.
+__device__ __forceinline__ bool wait_bar(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
+  if (mftc::mbar_try_wait(bar, parity)) return true;
+  uint64_t t0 = globaltimer();
+  while (true) {
+    if (mftc::mbar_try_wait(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (globaltimer() - t0 > WAIT_NS) return false;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 1. scan
+// ---------------------------------------------------------------------------
+constexpr int SENT_LO = -100000, SENT_HI = 100000;
+
+__global__ void init_stats_kernel(int *sig, int *mu, int *flag, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    sig[i] = SENT_LO;
+    mu[i] = SENT_HI;
+    flag[i] = 0;
+  }
+}
+
+// binade of |hi| + |lo|: v < 2^e (frexp convention); 0 for v == 0 (unused)
+__device__ __forceinline__ int binade_above(double v) { return ilogb(v) + 1; }
+__device__ __forceinline__ int binade_below(double v) { return ilogb(v); }
+
+// A column-major m x k: thread per row, a chunk of columns per blockIdx.y.
+__global__ void __launch_bounds__(256) scan_a_kernel(const double *__restrict__ A, int64_t M,
+                                                     int64_t K, int kchunk, int *sig, int *mu,
+                                                     int *flag) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  int64_t p0 = (int64_t)blockIdx.y * kchunk, p1 = p0 + kchunk < K ? p0 + kchunk : K;
+  int hi_e = SENT_LO, lo_e = SENT_HI, bad = 0;
+  for (int64_t p = p0; p < p1; ++p) {
+    double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i));
+    if (!isfinite(v.x) || !isfinite(v.y)) {
+      bad = 1;
+      continue;
+    }
+    double a = fabs(v.x) + fabs(v.y);
+    if (a != 0.0) {
+      hi_e = max(hi_e, binade_above(a));
+      lo_e = min(lo_e, binade_below(a));
+    }
+  }
+  if (hi_e != SENT_LO) atomicMax(&sig[i], hi_e);
+  if (lo_e != SENT_HI) atomicMin(&mu[i], lo_e);
+  if (bad) atomicOr(&flag[i], 1);
+}
+
+// B column-major k x n: a block per (column j, chunk of 2048 rows).
+__global__ void __launch_bounds__(256) scan_b_kernel(const double *__restrict__ B, int64_t K,
+                                                     int64_t N, int *sig, int *mu, int *flag) {
+  int64_t j = blockIdx.y;
+  int64_t p0 = (int64_t)blockIdx.x * 2048;
+  int hi_e = SENT_LO, lo_e = SENT_HI, bad = 0;
+  for (int r = 0; r < 8; ++r) {
+    int64_t p = p0 + threadIdx.x + 256 * r;
+    if (p >= K) break;
+    double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p));
+    if (!isfinite(v.x) || !isfinite(v.y)) {
+      bad = 1;
+      continue;
+    }
+    double a = fabs(v.x) + fabs(v.y);
+    if (a != 0.0) {
+      hi_e = max(hi_e, binade_above(a));
+      lo_e = min(lo_e, binade_below(a));
+    }
+  }
+  for (int off = 16; off >= 1; off >>= 1) {
+    hi_e = max(hi_e, __shfl_xor_sync(0xffffffffu, hi_e, off));
+    lo_e = min(lo_e, __shfl_xor_sync(0xffffffffu, lo_e, off));
+    bad |= __shfl_xor_sync(0xffffffffu, bad, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (hi_e != SENT_LO) atomicMax(&sig[j], hi_e);
+    if (lo_e != SENT_HI) atomicMin(&mu[j], lo_e);
+    if (bad) atomicOr(&flag[j], 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. plan (one block)
+// ---------------------------------------------------------------------------
+__global__ void plan_kernel(int *sigA, const int *muA, int64_t M, int *sigB, const int *muB,
+                            int64_t N, int slices, double target, Plan *plan) {
+  __shared__ int red[2][32];
+  int ra = 0, rb = 0;
+  for (int64_t i = threadIdx.x; i < M; i += blockDim.x) {
+    if (sigA[i] != SENT_LO) ra = max(ra, sigA[i] - muA[i]);
+  }
+  for (int64_t j = threadIdx.x; j < N; j += blockDim.x) {
+    if (sigB[j] != SENT_LO) rb = max(rb, sigB[j] - muB[j]);
+  }
+  for (int off = 16; off >= 1; off >>= 1) {
+    ra = max(ra, __shfl_xor_sync(0xffffffffu, ra, off));
+    rb = max(rb, __shfl_xor_sync(0xffffffffu, rb, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = ra;
+    red[1][threadIdx.x >> 5] = rb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      ra = max(ra, red[0][w]);
+      rb = max(rb, red[1][w]);
+    }
+    int S = slices;
+    if (S <= 0) {
+      // smallest S with (S+1) 2^(106 - 8S + rho_a + rho_b) <= target
+      S = SMAX;
+      for (int s = 2; s <= SMAX; ++s) {
+        double ratio = (s + 1) * ldexp(1.0, 106 - 8 * s + ra + rb);
+        if (ratio <= target) {
+          S = s;
+          break;
+        }
+      }
+    }
+    plan->S = S;
+    plan->G = S - 1;
+    plan->W = 8 * S - 2;
+    plan->rho_a = ra;
+    plan->rho_b = rb;
+  }
+  // zero rows / columns: any sigma works, the digits are all zero
+  __syncthreads();
+  for (int64_t i = threadIdx.x; i < M; i += blockDim.x)
+    if (sigA[i] == SENT_LO) sigA[i] = 0;
+  for (int64_t j = threadIdx.x; j < N; j += blockDim.x)
+    if (sigB[j] == SENT_LO) sigB[j] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// 3. slice
+// ---------------------------------------------------------------------------
+// x * 2^t for the double x = m 2^e as a fixed-point integer with F fractional
+// bits (floor for the bits below).
+constexpr int FRAC = 16;
+__device__ __forceinline__ __int128 scaled_fixed(double x, int t) {
+  if (x == 0.0) return 0;
+  int e = ilogb(x);
+  long long m = (long long)ldexp(x, 52 - e);  // exact: |m| < 2^53
+  int sh = e - 52 + t + FRAC;
+  if (sh >= 0) return (__int128)m << sh;
+  if (sh <= -64) return m < 0 ? (__int128)-1 : (__int128)0;
+  return (__int128)(m >> (-sh));
+}
+
+// Balanced digits of round((hi + lo) 2^(W - sigma)), most significant first.
+__device__ __forceinline__ void dd_digits(double hi, double lo, int sigma, int S, int W, int8_t *d) {
+  int t = W - sigma;
+  __int128 xf = scaled_fixed(hi, t) + scaled_fixed(lo, t);
+  __int128 X = (xf + ((__int128)1 << (FRAC - 1))) >> FRAC;
+  const __int128 lim = ((__int128)1 << W) - 1;
+  if (X > lim) X = lim;
+  if (X < -lim) X = -lim;
+  for (int s = S - 1; s >= 1; --s) {
+    int v = (int)(X & 0xFF);
+    v = (v ^ 0x80) - 0x80;
+    d[s] = (int8_t)v;
+    X = (X - v) >> 8;
+  }
+  d[0] = (int8_t)X;  // |X| < 2^(8S-2) keeps the top digit in [-64, 64]
+}
+
+// A (m x k column-major) -> As[s][i][p]: tile of 32 rows x 64 columns per
+// block, transposed through shared memory.  Covers the padded extent.
+__global__ void __launch_bounds__(256) slice_a_kernel(const double *__restrict__ A, int64_t M,
+                                                      int64_t K, int64_t M_pad, int64_t K_pad,
+                                                      const int *sig, const int *flag,
+                                                      const Plan *plan, int8_t *__restrict__ As) {
+  __shared__ __align__(16) int8_t tile[SMAX][32][64];
+  const int S = plan->S, W = plan->W;
+  const int64_t i0 = (int64_t)blockIdx.x * 32, p0 = (int64_t)blockIdx.y * 64;
+  const int t = threadIdx.x;
+  const int ii = t % 32;
+  const int64_t i = i0 + ii;
+  const bool row_ok = i < M && !flag[i < M ? i : 0];
+  const int sigma = i < M ? sig[i] : 0;
+  for (int r = 0; r < 8; ++r) {
+    int pp = t / 32 + 8 * r;
+    int64_t p = p0 + pp;
+    int8_t d[SMAX];
+#pragma unroll
+    for (int s = 0; s < SMAX; ++s) d[s] = 0;
+    if (row_ok && p < K) {
+      double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i));
+      dd_digits(v.x, v.y, sigma, S, W, d);
+    }
+#pragma unroll
+    for (int s = 0; s < SMAX; ++s) tile[s][ii][pp] = d[s];
+  }
+  __syncthreads();
+  const int row = t / 8, seg = (t % 8) * 8;
+  for (int s = 0; s < S; ++s) {
+    uint2 v = *reinterpret_cast<const uint2 *>(&tile[s][row][seg]);
+    *reinterpret_cast<uint2 *>(As + ((s * M_pad + i0 + row) * K_pad + p0 + seg)) = v;
+  }
+}
+
+// B (k x n column-major) -> Bs[s][j][p]: each thread 4 consecutive p of one column.
+__global__ void __launch_bounds__(256) slice_b_kernel(const double *__restrict__ B, int64_t K,
+                                                      int64_t N, int64_t N_pad, int64_t K_pad,
+                                                      const int *sig, const int *flag,
+                                                      const Plan *plan, int8_t *__restrict__ Bs) {
+  const int S = plan->S, W = plan->W;
+  const int64_t j = blockIdx.y;
+  const int64_t p4 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (p4 >= K_pad) return;
+  const bool col_ok = j < N && !flag[j < N ? j : 0];
+  const int tau = j < N ? sig[j] : 0;
+  int8_t d[4][SMAX];
+  for (int q = 0; q < 4; ++q) {
+#pragma unroll
+    for (int s = 0; s < SMAX; ++s) d[q][s] = 0;
+    int64_t p = p4 + q;
+    if (col_ok && p < K) {
+      double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p));
+      dd_digits(v.x, v.y, tau, S, W, d[q]);
+    }
+  }
+  for (int s = 0; s < S; ++s) {
+    uint32_t w = (uint32_t)(uint8_t)d[0][s] | ((uint32_t)(uint8_t)d[1][s] << 8) |
+                 ((uint32_t)(uint8_t)d[2][s] << 16) | ((uint32_t)(uint8_t)d[3][s] << 24);
+    *reinterpret_cast<uint32_t *>(Bs + ((s * N_pad + j) * K_pad + p4)) = w;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 4. tcgen05 INT8 MMA, persistent
+// ---------------------------------------------------------------------------
+struct Item {
+  int g, kc, tm, tn;
+};
+__device__ __forceinline__ Item decode(int w, int G, int nkc, int ntm, int ntiles) {
+  Item it;
+  int per_g = nkc * ntiles;
+  it.g = G - w / per_g;  // heaviest diagonal first
+  int r = w % per_g;
+  it.kc = r / ntiles;
+  int tile = r % ntiles;
+  it.tm = tile % ntm;
+  it.tn = tile / ntm;
+  return it;
+}
+
+__global__ void __launch_bounds__(MMA_THREADS, 1)
+    split_mma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     const Plan *plan, int32_t *__restrict__ D, int M_pad, int N_pad, int nkc,
+                     int kblocks, int *status) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t *sA = smem;
+  uint8_t *sB = smem + NSTAGE * A_STAGE;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * STAGE);
+  uint64_t *empty = full + NSTAGE;
+  uint64_t *tfull = empty + NSTAGE;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = plan->S, G = S - 1;
+  const int ntm = M_pad / BM, ntn = N_pad / BN, ntiles = ntm * ntn;
+  const int items = (G + 1) * nkc * ntiles;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      mftc::mbar_init(&full[s], 1);
+      mftc::mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mftc::mbar_init(&tfull[a], 1);
+      mftc::mbar_init(&tempty[a], 4);
+    }
+    mftc::mbar_init(drain, 1);
+    *abort_flag = 0;
+    mftc::fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    mftc::prefetch_tmap(&tmA);
+    mftc::prefetch_tmap(&tmB);
+  }
+  if (warp == 1) {
+    mftc::tmem_alloc(tmem_slot, TMEM_COLS);
+    mftc::tmem_relinquish();
+  }
+  mftc::tc_fence_before();
+  __syncthreads();
+  mftc::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  auto fail = [&](int code) {
+    *abort_flag = 1;
+    atomicOr(status, code);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer ----
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t armed_parity[NSTAGE];
+      bool armed[NSTAGE];
+      for (int s = 0; s < NSTAGE; ++s) armed[s] = false;
+      bool ok = true;
+      for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
+        Item it = decode(w, G, nkc, ntm, ntiles);
+        int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
+        for (int s = 0; s <= it.g && ok; ++s) {
+          int t = it.g - s;
+          for (int kb = kb0; kb < kb1; ++kb) {
+            if (!wait_bar(&empty[stage], phase ^ 1, abort_flag)) {
+              fail(1);
+              ok = false;
+              break;
+            }
+            mftc::mbar_arrive_expect_tx(&full[stage], STAGE);
+            mftc::tma_load_3d(sA + stage * A_STAGE, &tmA, &full[stage], kb * BK, it.tm * BM, s);
+            mftc::tma_load_3d(sB + stage * B_STAGE, &tmB, &full[stage], kb * BK, it.tn * BN, t);
+            armed[stage] = true;
+            armed_parity[stage] = phase;
+            if (++stage == NSTAGE) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+        }
+      }
+      if (!ok) {
+        // let copies already in flight land before the CTA leaves
+        for (int s = 0; s < NSTAGE; ++s)
+          if (armed[s]) {
+            uint64_t t0 = globaltimer();
+            while (!mftc::mbar_try_wait(&full[s], armed_parity[s]) && globaltimer() - t0 < WAIT_NS) {
+            }
+          }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer ----
+      const uint32_t idesc = mftc::idesc_i8(BM, BN);
+      int stage = 0;
+      uint32_t phase = 0;
+      int acc = 0;
+      uint32_t acc_phase = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
+        Item it = decode(w, G, nkc, ntm, ntiles);
+        int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
+        if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag)) {
+          fail(2);
+          break;
+        }
+        mftc::tc_fence_after();
+        const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+        uint32_t accumulate = 0;
+        for (int s = 0; s <= it.g && ok; ++s) {
+          for (int kb = kb0; kb < kb1; ++kb) {
+            if (!wait_bar(&full[stage], phase, abort_flag)) {
+              fail(4);
+              ok = false;
+              break;
+            }
+            mftc::tc_fence_after();
+            const uint32_t a0 = mftc::smem_u32(sA + stage * A_STAGE);
+            const uint32_t b0 = mftc::smem_u32(sB + stage * B_STAGE);
+#pragma unroll
+            for (int kk = 0; kk < BK / UMMA_K; ++kk) {
+              mftc::umma_i8(d_tmem, mftc::smem_desc_k_sw128(a0 + kk * UMMA_K),
+                            mftc::smem_desc_k_sw128(b0 + kk * UMMA_K), idesc, accumulate);
+              accumulate = 1;
+            }
+            mftc::umma_commit(&empty[stage]);
+            if (++stage == NSTAGE) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+        }
+        if (!ok) break;
+        mftc::umma_commit(&tfull[acc]);
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1;
+        }
+      }
+      // every MMA issued by this thread has finished once `drain` flips
+      mftc::umma_commit(drain);
+      uint64_t t0 = globaltimer();
+      while (!mftc::mbar_try_wait(drain, 0) && globaltimer() - t0 < WAIT_NS) {
+      }
+    }
+  } else {
+    // ---- epilogue: warps 2..5, TMEM lane quadrant = warp % 4 ----
+    const int quad = warp & 3;
+    const int row = quad * 32 + lane;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    for (int w = blockIdx.x; w < items; w += gridDim.x) {
+      Item it = decode(w, G, nkc, ntm, ntiles);
+      bool got = wait_bar(&tfull[acc], acc_phase, abort_flag);
+      if (!__all_sync(0xffffffffu, got)) {
+        if (lane == 0) fail(8);
+        break;
+      }
+      mftc::tc_fence_after();
+      int32_t *dst_base = D + (((int64_t)(it.g * nkc + it.kc) * N_pad + (int64_t)it.tn * BN) * M_pad +
+                               (int64_t)it.tm * BM + row);
+#pragma unroll 1
+      for (int chunk = 0; chunk < BN / 32; ++chunk) {
+        uint32_t r[32];
+        mftc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * BN + chunk * 32), r);
+        mftc::tmem_wait_ld();
+        int32_t *dst = dst_base + (int64_t)chunk * 32 * M_pad;
+#pragma unroll
+        for (int q = 0; q < 32; ++q) dst[(int64_t)q * M_pad] = (int32_t)r[q];
+      }
+      mftc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mftc::mbar_arrive(&tempty[acc]);
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+  }
+
+  mftc::tc_fence_before();
+  __syncthreads();
+  mftc::tc_fence_after();
+  if (warp == 1) mftc::tmem_dealloc(tmem_base, TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
+// 5. combine
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) combine_kernel(const int32_t *__restrict__ D, const Plan *plan,
+                                                      const int *sigA, const int *flagA,
+                                                      const int *sigB, const int *flagB, int64_t M,
+                                                      int64_t N, int64_t M_pad, int64_t N_pad,
+                                                      int nkc, double *__restrict__ C) {
+  const int G = plan->G;
+  const int64_t total = M * N;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
+    const int64_t i = e % M, j = e / M;
+    double hi = 0.0, lo = 0.0;
+    for (int g = G; g >= 0; --g) {
+      const double scale = ldexp(1.0, -8 * g);
+      for (int kc = 0; kc < nkc; ++kc) {
+        int32_t v = __ldcs(D + ((int64_t)(g * nkc + kc) * N_pad + j) * M_pad + i);
+        double tv = mfdev::mul((double)v, scale);  // exact
+        double s, err;
+        mfdev::two_sum(hi, tv, s, err);
+        hi = s;
+        lo = mfdev::add(lo, err);
+      }
+    }
+    mfdev::two_sum(hi, lo, hi, lo);
+    double2 out;
+    if (flagA[i] | flagB[j]) {
+      out = make_double2(CUDART_NAN, 0.0);
+    } else {
+      int ex = sigA[i] + sigB[j] - 12;
+      out = make_double2(ldexp(hi, ex), ldexp(lo, ex));
+    }
+    __stcs(reinterpret_cast<double2 *>(C) + (j * M + i), out);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct Layout {
+  int64_t M_pad, N_pad, K_pad, kblocks, nkc;
+  size_t off_plan, off_sigA, off_muA, off_flagA, off_sigB, off_muB, off_flagB, off_As, off_Bs, off_D,
+      total;
+};
+
+static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+static Layout layout(int64_t m, int64_t k, int64_t n) {
+  Layout L;
+  L.M_pad = round_up(m < 1 ? 1 : m, BM);
+  L.N_pad = round_up(n < 1 ? 1 : n, BN);
+  L.K_pad = round_up(k < 1 ? 1 : k, BK);
+  L.kblocks = L.K_pad / BK;
+  L.nkc = (L.kblocks + KC_BLOCKS - 1) / KC_BLOCKS;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off = (size_t)round_up((int64_t)(off + bytes), 1024);
+    return o;
+  };
+  L.off_plan = take(sizeof(Plan));
+  L.off_sigA = take(sizeof(int) * L.M_pad);
+  L.off_muA = take(sizeof(int) * L.M_pad);
+  L.off_flagA = take(sizeof(int) * L.M_pad);
+  L.off_sigB = take(sizeof(int) * L.N_pad);
+  L.off_muB = take(sizeof(int) * L.N_pad);
+  L.off_flagB = take(sizeof(int) * L.N_pad);
+  L.off_As = take((size_t)SMAX * L.M_pad * L.K_pad);
+  L.off_Bs = take((size_t)SMAX * L.N_pad * L.K_pad);
+  L.off_D = take((size_t)SMAX * L.nkc * L.N_pad * L.M_pad * sizeof(int32_t));
+  L.total = off + 256 /* status word */;
+  return L;
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, uint32_t box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)K_pad, (cuuint64_t)rows, (cuuint64_t)SMAX};
+  cuuint64_t strides[2] = {(cuuint64_t)K_pad, (cuuint64_t)(rows * K_pad)};
+  cuuint32_t box[3] = {(cuuint32_t)BK, box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+size_t workspace_size(int64_t m, int64_t k, int64_t n) { return layout(m, k, n).total; }
+
+static std::once_flag g_attr_once;
+
+int run(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k, int64_t n,
+        int slices, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *S_used) {
+  if (m < 0 || k < 0 || n < 0 || !mul_ok(m, k) || !mul_ok(k, n) || !mul_ok(m, n))
+    return MFCUDA_ERR_INVALID_ARG;
+  if (slices < 0 || slices > SMAX || slices == 1) return MFCUDA_ERR_INVALID_ARG;
+  if (!(target > 0.0)) return MFCUDA_ERR_INVALID_ARG;
+  if (m == 0 || n == 0) return MFCUDA_OK;
+  if (!c || (k > 0 && (!a || !b))) return MFCUDA_ERR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) | reinterpret_cast<uintptr_t>(c)) & 15)
+    return MFCUDA_ERR_UNSUPPORTED;  // the split form wants 16-byte aligned operands
+  MF_TRY(require_device());
+  Layout L = layout(m, k, n);
+  if (L.M_pad > INT32_MAX / 2 || L.N_pad > INT32_MAX / 2 || L.kblocks > INT32_MAX / 2)
+    return MFCUDA_ERR_UNSUPPORTED;
+  if (k == 0) {
+    MF_TRY_CUDA(cudaMemsetAsync(c, 0, (size_t)(m * n) * sizeof(float64x2), s));
+    if (S_used) *S_used = 0;
+    return MFCUDA_OK;
+  }
+  void *own = nullptr;
+  if (!ws) {
+    MF_TRY(ws_alloc(&own, L.total, s));
+    ws = own;
+  } else if (ws_bytes < L.total) {
+    return MFCUDA_ERR_WORKSPACE;
+  }
+  uint8_t *base = static_cast<uint8_t *>(ws);
+  Plan *plan = reinterpret_cast<Plan *>(base + L.off_plan);
+  int *sigA = reinterpret_cast<int *>(base + L.off_sigA);
+  int *muA = reinterpret_cast<int *>(base + L.off_muA);
+  int *flagA = reinterpret_cast<int *>(base + L.off_flagA);
+  int *sigB = reinterpret_cast<int *>(base + L.off_sigB);
+  int *muB = reinterpret_cast<int *>(base + L.off_muB);
+  int *flagB = reinterpret_cast<int *>(base + L.off_flagB);
+  int8_t *As = reinterpret_cast<int8_t *>(base + L.off_As);
+  int8_t *Bs = reinterpret_cast<int8_t *>(base + L.off_Bs);
+  int32_t *D = reinterpret_cast<int32_t *>(base + L.off_D);
+  int *status = reinterpret_cast<int *>(base + L.total - 256);
+  const double *Ad = reinterpret_cast<const double *>(a);
+  const double *Bd = reinterpret_cast<const double *>(b);
+  int rc = MFCUDA_OK;
+  do {
+    CUtensorMap tmA, tmB;
+    if (!make_map(&tmA, As, L.M_pad, L.K_pad, BM) || !make_map(&tmB, Bs, L.N_pad, L.K_pad, BN)) {
+      rc = MFCUDA_ERR_CUDA;
+      break;
+    }
+    std::call_once(g_attr_once, [] {
+      cudaFuncSetAttribute(split_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
+    });
+    cudaMemsetAsync(status, 0, sizeof(int), s);
+    init_stats_kernel<<<(unsigned)((L.M_pad + 255) / 256), 256, 0, s>>>(sigA, muA, flagA, L.M_pad);
+    init_stats_kernel<<<(unsigned)((L.N_pad + 255) / 256), 256, 0, s>>>(sigB, muB, flagB, L.N_pad);
+    const int kch = 64;
+    scan_a_kernel<<<dim3((unsigned)((m + 255) / 256), (unsigned)((k + kch - 1) / kch)), 256, 0, s>>>(
+        Ad, m, k, kch, sigA, muA, flagA);
+    scan_b_kernel<<<dim3((unsigned)((k + 2047) / 2048), (unsigned)n), 256, 0, s>>>(Bd, k, n, sigB, muB,
+                                                                                   flagB);
+    plan_kernel<<<1, 1024, 0, s>>>(sigA, muA, m, sigB, muB, n, slices, target, plan);
+    slice_a_kernel<<<dim3((unsigned)(L.M_pad / 32), (unsigned)(L.K_pad / 64)), 256, 0, s>>>(
+        Ad, m, k, L.M_pad, L.K_pad, sigA, flagA, plan, As);
+    slice_b_kernel<<<dim3((unsigned)((L.K_pad / 4 + 255) / 256), (unsigned)L.N_pad), 256, 0, s>>>(
+        Bd, k, n, L.N_pad, L.K_pad, sigB, flagB, plan, Bs);
+    int items_max = SMAX * (int)L.nkc * (int)((L.M_pad / BM) * (L.N_pad / BN));
+    int grid = sm_count();
+    if (grid > items_max) grid = items_max;
+    split_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad, (int)L.N_pad,
+                                                         (int)L.nkc, (int)L.kblocks, status);
+    int64_t cblocks = (m * n + 255) / 256;
+    if (cblocks > (int64_t)sm_count() * 32) cblocks = (int64_t)sm_count() * 32;
+    combine_kernel<<<(unsigned)cblocks, 256, 0, s>>>(D, plan, sigA, flagA, sigB, flagB, m, n, L.M_pad,
+                                                     L.N_pad, (int)L.nkc, reinterpret_cast<double *>(c));
+    if (cudaGetLastError() != cudaSuccess) rc = MFCUDA_ERR_CUDA;
+    if (S_used && rc == MFCUDA_OK) {
+      Plan hp;
+      if (cudaMemcpyAsync(&hp, plan, sizeof(Plan), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess) {
+        rc = MFCUDA_ERR_CUDA;
+      } else {
+        int st = 0;
+        cudaMemcpy(&st, status, sizeof(int), cudaMemcpyDeviceToHost);
+        if (st) rc = MFCUDA_ERR_TIMEOUT;
+        *S_used = hp.S;
+        S_used[1] = hp.rho_a;
+        S_used[2] = hp.rho_b;
+      }
+    }
+  } while (0);
+  if (own) ws_free(own, s);
+  return rc;
+}
+
+}  // namespace split
+
+static int split_host(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k,
+                      int64_t n, int slices, double *bound_out) {
+  if (m < 0 || k < 0 || n < 0 || !mul_ok(m, k) || !mul_ok(k, n) || !mul_ok(m, n))
+    return MFCUDA_ERR_INVALID_ARG;
+  if (m == 0 || n == 0) return MFCUDA_OK;
+  if (!c || (k > 0 && (!a || !b))) return MFCUDA_ERR_INVALID_ARG;
+  MF_TRY(require_device());
+  size_t ba = (size_t)(m * k) * sizeof(float64x2), bb = (size_t)(k * n) * sizeof(float64x2),
+         bc = (size_t)(m * n) * sizeof(float64x2);
+  size_t wsb = split::workspace_size(m, k, n);
+  size_t sz[4] = {ba, bb, bc, wsb};
+  Staging st;
+  MF_TRY(staging_acquire(st, sz));
+  if (ba) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[0], a, ba, cudaMemcpyHostToDevice, st.stream));
+  if (bb) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[1], b, bb, cudaMemcpyHostToDevice, st.stream));
+  int info[3] = {0, 0, 0};
+  MF_TRY(split::run(static_cast<float64x2 *>(st.buf[0]), static_cast<float64x2 *>(st.buf[1]),
+                    static_cast<float64x2 *>(st.buf[2]), m, k, n, slices, 8.0, st.buf[3], wsb,
+                    st.stream, info));
+  MF_TRY_CUDA(cudaMemcpyAsync(c, st.buf[2], bc, cudaMemcpyDeviceToHost, st.stream));
+  MF_TRY_CUDA(cudaStreamSynchronize(st.stream));
+  if (bound_out) {
+    int S = info[0];
+    *bound_out = S > 0 ? (S + 1) * ldexp(1.0, 106 - 8 * S + info[1] + info[2]) : 0.0;
+  }
+  return MFCUDA_OK;
+}
+
+}  // namespace mfcuda
+
+extern "C" {
+
+MULTIFLOATS_CUDA_API size_t mfcuda_split_workspace_size(int64_t m, int64_t k, int64_t n) {
+  if (m < 0 || k < 0 || n < 0) return 0;
+  return mfcuda::split::workspace_size(m, k, n);
+}
+
+MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_split(const float64x2 *a, const float64x2 *b,
+                                                  float64x2 *c, int64_t m, int64_t k, int64_t n,
+                                                  int slices, double target, void *workspace,
+                                                  size_t workspace_bytes, int *info_out,
+                                                  void *stream) {
+  return mfcuda::split::run(a, b, c, m, k, n, slices, target, workspace, workspace_bytes,
+                            mfcuda::as_stream(stream), info_out);
+}
+
+MULTIFLOATS_CUDA_API void matmuldd_mm_split(const float64x2 *a, const float64x2 *b, float64x2 *c,
+                                            int64_t m, int64_t k, int64_t n, int slices,
+                                            double *max_err_bound_out) {
+  mfcuda::set_last_error(mfcuda::split_host(a, b, c, m, k, n, slices, max_err_bound_out));
+}
+
+}  // extern "C"

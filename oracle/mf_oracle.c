@@ -799,3 +799,139 @@ void orc_reduce_error(int kind, const double *x, const double *y, int64_t n, con
   *err = -sa_value(&s);
   *absv = ab;
 }
+
+/* ---- split-INT8 GEMM, restated on the CPU ------------------------------------
+ * The same algorithm as the device kernels in split_gemm.cu (scan, plan,
+ * exact rounding to (8S-2)-bit integers, balanced signed 8-bit digits, exact
+ * integer anti-diagonal sums D_g per K chunk, DD combine from the smallest
+ * diagonal up, exact scaling).  The integer stage is exact and the combine
+ * order is fixed, so the device result must match this bit for bit. */
+#define SPLIT_SMAX 14
+#define SPLIT_KC (73 * 128) /* K elements per chunk, as KC_BLOCKS * BK on the device */
+#define SPLIT_FRAC 16
+
+static __int128 split_scaled_fixed(double x, int t) {
+  if (x == 0.0) return 0;
+  int e = ilogb(x);
+  long long m = (long long)ldexp(x, 52 - e);
+  int sh = e - 52 + t + SPLIT_FRAC;
+  if (sh >= 0) return (__int128)m << sh;
+  if (sh <= -64) return m < 0 ? (__int128)-1 : (__int128)0;
+  return (__int128)(m >> (-sh));
+}
+static void split_digits(double hi, double lo, int sigma, int S, int W, int8_t *d) {
+  int t = W - sigma;
+  __int128 xf = split_scaled_fixed(hi, t) + split_scaled_fixed(lo, t);
+  __int128 X = (xf + ((__int128)1 << (SPLIT_FRAC - 1))) >> SPLIT_FRAC;
+  __int128 lim = ((__int128)1 << W) - 1;
+  if (X > lim) X = lim;
+  if (X < -lim) X = -lim;
+  for (int s = S - 1; s >= 1; --s) {
+    int v = (int)(X & 0xFF);
+    v = (v ^ 0x80) - 0x80;
+    d[s] = (int8_t)v;
+    X = (X - v) >> 8;
+  }
+  d[0] = (int8_t)X;
+}
+/* exponent statistics of one row/column: elements x[idx*stride] */
+static void split_stats(const double *x, int64_t count, int64_t stride, int *sig, int *mu, int *bad) {
+  int hi_e = -100000, lo_e = 100000, b = 0;
+  for (int64_t p = 0; p < count; ++p) {
+    double h = x[2 * p * stride], l = x[2 * p * stride + 1];
+    if (!isfinite(h) || !isfinite(l)) {
+      b = 1;
+      continue;
+    }
+    double a = fabs(h) + fabs(l);
+    if (a != 0.0) {
+      int e = ilogb(a);
+      if (e + 1 > hi_e) hi_e = e + 1;
+      if (e < lo_e) lo_e = e;
+    }
+  }
+  *sig = hi_e;
+  *mu = lo_e;
+  *bad = b;
+}
+int orc_split_plan(int S_req, double target, int rho_a, int rho_b) {
+  if (S_req > 0) return S_req;
+  for (int s = 2; s <= SPLIT_SMAX; ++s)
+    if ((s + 1) * ldexp(1.0, 106 - 8 * s + rho_a + rho_b) <= target) return s;
+  return SPLIT_SMAX;
+}
+/* info[0..2] = S, rho_a, rho_b */
+void orc_split_gemm(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
+                    int S_req, double target, int *info) {
+  int *sa = malloc(sizeof(int) * m), *ma = malloc(sizeof(int) * m), *fa = malloc(sizeof(int) * m);
+  int *sb = malloc(sizeof(int) * n), *mb = malloc(sizeof(int) * n), *fb = malloc(sizeof(int) * n);
+  int ra = 0, rb = 0;
+  for (int64_t i = 0; i < m; ++i) {
+    split_stats(a + 2 * i, k, m, &sa[i], &ma[i], &fa[i]);
+    if (sa[i] != -100000 && sa[i] - ma[i] > ra) ra = sa[i] - ma[i];
+  }
+  for (int64_t j = 0; j < n; ++j) {
+    split_stats(b + 2 * j * k, k, 1, &sb[j], &mb[j], &fb[j]);
+    if (sb[j] != -100000 && sb[j] - mb[j] > rb) rb = sb[j] - mb[j];
+  }
+  for (int64_t i = 0; i < m; ++i)
+    if (sa[i] == -100000) sa[i] = 0;
+  for (int64_t j = 0; j < n; ++j)
+    if (sb[j] == -100000) sb[j] = 0;
+  int S = orc_split_plan(S_req, target, ra, rb), G = S - 1, W = 8 * S - 2;
+  if (info) {
+    info[0] = S;
+    info[1] = ra;
+    info[2] = rb;
+  }
+  int8_t *da = calloc((size_t)S * m * k, 1), *db = calloc((size_t)S * n * k, 1);
+  for (int64_t i = 0; i < m; ++i)
+    for (int64_t p = 0; p < k; ++p) {
+      int8_t d[SPLIT_SMAX];
+      if (fa[i]) continue;
+      split_digits(a[2 * (p * m + i)], a[2 * (p * m + i) + 1], sa[i], S, W, d);
+      for (int s = 0; s < S; ++s) da[((size_t)s * m + i) * k + p] = d[s];
+    }
+  for (int64_t j = 0; j < n; ++j)
+    for (int64_t p = 0; p < k; ++p) {
+      int8_t d[SPLIT_SMAX];
+      if (fb[j]) continue;
+      split_digits(b[2 * (j * k + p)], b[2 * (j * k + p) + 1], sb[j], S, W, d);
+      for (int s = 0; s < S; ++s) db[((size_t)s * n + j) * k + p] = d[s];
+    }
+  int64_t nkc = (k + SPLIT_KC - 1) / SPLIT_KC;
+  if (nkc < 1) nkc = 1;
+  for (int64_t j = 0; j < n; ++j)
+    for (int64_t i = 0; i < m; ++i) {
+      double hi = 0.0, lo = 0.0;
+      for (int g = G; g >= 0; --g) {
+        double scale = ldexp(1.0, -8 * g);
+        for (int64_t kc = 0; kc < nkc; ++kc) {
+          int64_t p0 = kc * SPLIT_KC, p1 = p0 + SPLIT_KC < k ? p0 + SPLIT_KC : k;
+          int64_t D = 0;
+          for (int s = 0; s <= g; ++s) {
+            const int8_t *ra_ = da + ((size_t)s * m + i) * k;
+            const int8_t *rb_ = db + ((size_t)(g - s) * n + j) * k;
+            for (int64_t p = p0; p < p1; ++p) D += (int64_t)ra_[p] * rb_[p];
+          }
+          double tv = (double)(int32_t)D * scale;
+          double s_, e_;
+          two_sum(hi, tv, &s_, &e_);
+          hi = s_;
+          lo = lo + e_;
+        }
+      }
+      double h2, l2;
+      two_sum(hi, lo, &h2, &l2);
+      double *o = c + 2 * (j * m + i);
+      if (fa[i] | fb[j]) {
+        o[0] = NAN;
+        o[1] = 0.0;
+      } else {
+        int ex = sa[i] + sb[j] - 12;
+        o[0] = ldexp(h2, ex);
+        o[1] = ldexp(l2, ex);
+      }
+    }
+  free(sa); free(ma); free(fa); free(sb); free(mb); free(fb); free(da); free(db);
+}

@@ -60,6 +60,8 @@ def orc():
         L.orc_reduce_blocked.argtypes = [C.c_int, P, P, I64, I64, P]
         L.orc_gemm_errors.argtypes = [P, P, P, I64, I64, I64, P, P, I64, P, P]
         L.orc_reduce_error.argtypes = [C.c_int, P, P, I64, P, P, P]
+        L.orc_split_gemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
+        L.orc_split_plan.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int]
         _orc = L
     return _orc
 
@@ -180,6 +182,15 @@ def reduce_blocked(kind: str, x, y=None, ri=8) -> np.ndarray:
     out = np.zeros(4)
     orc().orc_reduce_blocked(KINDS[kind], _p(x), _p(yy), n, ri, _p(out))
     return out[:4] if kind in ("csum", "cdot") else out[:2]
+
+
+def split_gemm(a, b, m, k, n, slices=0, target=8.0):
+    """The split-INT8 algorithm restated on the CPU; returns (C, (S, rho_a, rho_b))."""
+    a, b = _c(a), _c(b)
+    c = np.empty(2 * m * n)
+    info = np.zeros(3, dtype=np.int32)
+    orc().orc_split_gemm(_p(a), _p(b), _p(c), m, k, n, slices, target, info.ctypes.data)
+    return c, tuple(int(v) for v in info)
 
 
 def reduce_geometry(n: int) -> tuple[int, int]:
