@@ -2,11 +2,13 @@
 """Benchmark of the DD GEMM hot path on B200: DD-GFLOP/s at M=N=K=4096.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload gemm4096|gemm256|elementwise|reduce]
 
-One step = one C = A*B of 4096^3 real64x2 operands resident in HBM (each
-operand is 256 MiB, larger than the 126 MB L2, so no flush is needed between
-steps).  DD-GFLOP/s = 2*M*N*K / seconds / 1e9.  With N GPUs (one process per
+One step = one C = A*B of 4096^3 real64x2 operands resident in HBM in the
+split-INT8 form (tcgen05 tensor cores; each operand is 256 MiB, larger than
+the 126 MB L2, so no flush is needed between steps).  DD-GFLOP/s =
+2*M*N*K / seconds / 1e9.  The plain FP64 compensated kernel is timed on the
+same operands and reported beside it, with the split result's error against
+the exact product on sampled outputs.  With N GPUs (one process per
 GPU under torchrun) every rank multiplies its own independent pair of
 matrices (weak scaling, no collective on the data path); the timed region is
 bracketed by a barrier and a device synchronise, and the time is the max over
@@ -24,7 +26,6 @@ import ctypes as C
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -78,65 +79,6 @@ def max_over_ranks(ws, value: float) -> float:
 
 
 # ------------------------------------------------------------------------ clocks
-class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
-
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-
-    def __init__(self, gpu_id: str | None):
-        self.gpu_id = gpu_id
-        self.proc = None
-        self.lines: list[str] = []
-
-    def __enter__(self):
-        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
-        if self.gpu_id:
-            cmd += ["-i", self.gpu_id]
-        try:
-            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.reader = threading.Thread(target=self._read, daemon=True)
-            self.reader.start()
-        except OSError:
-            self.proc = None
-        return self
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            self.reader.join(timeout=2)
-
-    def summary(self) -> dict:
-        sm, mx, reasons, power = [], 0.0, set(), []
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
-                power.append(float(parts[3]))
-            except ValueError:
-                continue
-            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-            for nm, val in zip(names, parts[5:9]):
-                if val.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm), "power_w_max": max(power) if power else None}
-
-
 def gpu_uuid() -> str | None:
     try:
         import torch
@@ -145,13 +87,6 @@ def gpu_uuid() -> str | None:
         return "GPU-" + str(u)
     except Exception:
         return None
-
-
-def measured_peaks() -> dict:
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
-        return json.load(open(p))
-    return {}
 
 
 # ------------------------------------------------------------------ CPU baseline
@@ -192,10 +127,77 @@ def cpu_gemm_sample(target_s: float, threads: int):
 
 
 # --------------------------------------------------------------------- GPU arm
+class NvmlClocks:
+    """Polls SM clock, power and clock-event reasons through NVML every 10 ms
+    while active (read-only queries)."""
+
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, uuid: str | None):
+        self.samples = []
+        self.handle = None
+        self.maxclk = None
+        try:
+            import pynvml as N
+
+            N.nvmlInit()
+            self.N = N
+            self.handle = N.nvmlDeviceGetHandleByUUID(uuid) if uuid else N.nvmlDeviceGetHandleByIndex(0)
+            self.maxclk = N.nvmlDeviceGetMaxClockInfo(self.handle, N.NVML_CLOCK_SM)
+        except Exception:
+            self.handle = None
+
+    def __enter__(self):
+        self.stop = threading.Event()
+        if self.handle is not None:
+            self.th = threading.Thread(target=self._run, daemon=True)
+            self.th.start()
+        return self
+
+    def _run(self):
+        N = self.N
+        get_reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            N.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop.is_set():
+            try:
+                clk = N.nvmlDeviceGetClockInfo(self.handle, N.NVML_CLOCK_SM)
+                rs = get_reasons(self.handle)
+                pw = N.nvmlDeviceGetPowerUsage(self.handle) / 1000.0
+                self.samples.append((clk, rs, pw))
+            except Exception:
+                pass
+            time.sleep(0.01)
+
+    def __exit__(self, *exc):
+        self.stop.set()
+        if self.handle is not None:
+            self.th.join(timeout=2)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.maxclk, "reasons": [], "samples": 0}
+        reasons = set()
+        for _, rs, _ in self.samples:
+            for bit, nm in self.REASONS.items():
+                if rs & bit:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(c for c, _, _ in self.samples), "sm_max_mhz": self.maxclk,
+                "reasons": sorted(reasons), "samples": len(self.samples),
+                "power_w_max": max(p for _, _, p in self.samples), "source": "NVML, 10 ms polling"}
+
+
+def load_peaks_lib():
+    p = C.CDLL(os.path.join(ROOT, "multifloats_b200", "libmfcuda_peaks.so"))
+    p.mfpeak_fp64.argtypes = [C.c_int64, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    p.mfpeak_int8.argtypes = [C.c_int, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    return p
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
-    from multifloats_b200 import _lib, api
+    from multifloats_b200 import _lib
     from multifloats_b200 import workloads as W
 
     torch.cuda.set_device(local)
@@ -216,78 +218,136 @@ def run_ours(args, ws, rank, local):
                          f"workload), ri={RI}, {threads} threads, {dt:.1f} s"}
         log("cpu baseline:", cpu)
 
-    # operands: per-row / per-column exponent ranges R=16 (split config) -- both forms see the same data
-    A = W.dd_rowcol_scaled(M, K, 16, "row", seed=10 + rank)
-    B = W.dd_rowcol_scaled(K, N, 16, "col", seed=20 + rank)
+    # split config: hi = +-u 2^e, u ~ U[1,2), e ~ U{-R..R} per row of A / column of B, R = 16
+    R = 16
+    A = W.dd_rowcol_scaled(M, K, R, "row", seed=10 + rank)
+    B = W.dd_rowcol_scaled(K, N, R, "col", seed=20 + rank)
     dA = torch.from_numpy(A).to(dev)
     dB = torch.from_numpy(B).to(dev)
     dC = torch.empty(2 * M * N, dtype=torch.float64, device=dev)
+    wsb = L.mfcuda_split_workspace_size(M, K, N)
+    dWS = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    info = (C.c_int * 3)()
+    _lib.check(L.mfcuda_matmuldd_mm_split(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, 0, 8.0,
+                                          dWS.data_ptr(), wsb, info, sp), "split (info)")
+    S, rho_a, rho_b = tuple(info)
+
+    def split_step():
+        _lib.check(L.mfcuda_matmuldd_mm_split(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, 0, 8.0,
+                                              dWS.data_ptr(), wsb, None, sp), "split")
 
     def plain_step():
         _lib.check(L.mfcuda_matmuldd_mm(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, RI, sp),
                    "mfcuda_matmuldd_mm")
 
-    # FP64 pipe peak (own probe, same process, just before timing)
-    peak_lib = C.CDLL(os.path.join(ROOT, "multifloats_b200", "libmfcuda_peaks.so"))
-    peak_lib.mfpeak_fp64.argtypes = [C.c_int64, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    # roofline denominators, measured in-process just before timing
+    pk = load_peaks_lib()
     ms_p, ins_p = C.c_double(), C.c_double()
-    peak_lib.mfpeak_fp64(200000, sp, C.byref(ms_p), C.byref(ins_p))
-    fp64_peak_instr = ins_p.value / (ms_p.value * 1e-3)
+    pk.mfpeak_fp64(200000, sp, C.byref(ms_p), C.byref(ins_p))
+    fp64_peak = ins_p.value / (ms_p.value * 1e-3)
+    ms_i, ops_i = C.c_double(), C.c_double()
+    rc_i = pk.mfpeak_int8(20000, sp, C.byref(ms_i), C.byref(ops_i))
+    int8_peak = ops_i.value / (ms_i.value * 1e-3) if rc_i == 0 else None
 
+    # ---- timed region: K split steps, every launch's phases recorded ----
     for _ in range(args.warmup):
-        plain_step()
+        split_step()
     torch.cuda.synchronize()
     barrier(ws)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(gpu_uuid()) as clk:
+    with NvmlClocks(gpu_uuid()) as clk:
         torch.cuda.synchronize()
         barrier(ws)
+        L.mfcuda_phase_profile_begin()
         e0.record(stream)
         for _ in range(args.steps):
-            plain_step()
+            split_step()
         e1.record(stream)
         e1.synchronize()
+    sums = (C.c_double * 4)()
+    ncalls = C.c_int64()
+    _lib.check(L.mfcuda_phase_profile_end(sums, C.byref(ncalls)), "phase profile")
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    ms = max_over_ranks(ws, ms)
+    ms = max_over_ranks(ws, e0.elapsed_time(e1))
     per_step = ms / args.steps
+    phase = {nm: sums[q] / max(1, ncalls.value) for q, nm in enumerate(["scan", "slice", "mma", "combine"])}
     flops = 2.0 * M * N * K
     value = ws * flops / (per_step * 1e-3) / 1e9
-    launches = args.steps * 1
+    launches = 9 * args.steps
 
-    # e2e through the drop-in (host-pointer) symbol with pinned host buffers
+    # accuracy of the result just computed, against the exact product (sampled outputs)
+    acc = None
+    if rank == 0:
+        from oracle import oracle as O
+
+        Ch = dC.cpu().numpy()
+        rng = np.random.default_rng(123)
+        ii, jj = rng.integers(0, M, 256), rng.integers(0, N, 256)
+        err, ab = O.gemm_errors(A, B, Ch, M, K, N, ii, jj)
+        acc = {"max_err_over_k_ulp_absab": float(np.max(np.abs(err) / (K * 2.0 ** -104 * ab))),
+               "max_err_over_ulp_absab": float(np.max(np.abs(err) / (2.0 ** -104 * ab))),
+               "apriori_bound_k_ulp": (S + 1) * 2.0 ** (106 - 8 * S + rho_a + rho_b),
+               "samples": 256, "oracle": "exact superaccumulator (oracle/mf_oracle.c)",
+               "ulp": "1 DD ulp = 2^-104"}
+
+    # ---- plain FP64 form on the same operands ----
+    plain_steps = max(1, min(args.steps, 3))
+    plain_step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(plain_steps):
+        plain_step()
+    p1.record(stream)
+    p1.synchronize()
+    plain_ms = max_over_ranks(ws, p0.elapsed_time(p1)) / plain_steps
+    plain_val = ws * flops / (plain_ms * 1e-3) / 1e9
+    plain_fp64 = FP64_INSTR_PER_MAC * M * N * K / (plain_ms * 1e-3)
+
+    # ---- e2e: the drop-in host-pointer symbol with pinned host buffers ----
     hA = torch.from_numpy(A).pin_memory()
     hB = torch.from_numpy(B).pin_memory()
     hC = torch.empty(2 * M * N, dtype=torch.float64).pin_memory()
-    e2e_steps = max(1, min(args.steps, 3))
-    L.matmuldd_mm(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, RI)
-    _lib.check_last("matmuldd_mm")
+    bound = C.c_double()
+    L.matmuldd_mm_split(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, 0, C.byref(bound))
+    _lib.check_last("matmuldd_mm_split")
+    e2e_steps = max(1, min(args.steps, 5))
     barrier(ws)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        L.matmuldd_mm(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, RI)
-    t_e2e = (time.perf_counter() - t0) / e2e_steps
-    t_e2e = max_over_ranks(ws, t_e2e)
-    _lib.check_last("matmuldd_mm")
+        L.matmuldd_mm_split(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, 0, C.byref(bound))
+    t_e2e = max_over_ranks(ws, (time.perf_counter() - t0) / e2e_steps)
+    _lib.check_last("matmuldd_mm_split")
 
-    # roofline of the (plain) GEMM kernel on the FP64 pipe
-    achieved = FP64_INSTR_PER_MAC * M * N * K / (per_step * 1e-3)
-    roof = {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak_instr / 1e12,
-            "unit": "T FP64-instr/s", "frac": achieved / fp64_peak_instr, "traffic": None,
-            "peak_source": "own FP64 FMA probe (multifloats_b200/csrc/peaks.cu), same process"}
+    # roofline of the dominant kernel: split_mma_kernel on the INT8 tensor pipe
+    int8_ops = (S * (S + 1) // 2) * 2.0 * M * N * K  # algorithmic INT8 ops per launch
+    achieved = int8_ops / (phase["mma"] * 1e-3)
+    roof = {"bound": "tensor", "achieved": achieved / 1e12,
+            "peak": int8_peak / 1e12 if int8_peak else None, "unit": "TFLOP/s",
+            "frac": achieved / int8_peak if int8_peak else None, "traffic": None,
+            "kernel": "split_mma_kernel", "op_kind": "INT8 tensor ops (multiply + add), S(S+1)/2 slice products",
+            "peak_source": "own tcgen05 kind::i8 M=128 N=256 probe (multifloats_b200/csrc/peaks.cu), same process"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "DD-GFLOP/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8+f64",
             "data": "synthetic (seeded; hi = +-u 2^e, u~U[1,2), e~U{-16..16} per row of A / column of B)",
-            "config": {"workload": "dd_gemm_4096_plain", "M": M, "N": N, "K": K,
-                       "renorm_interval": RI, "form": "plain FP64 compensated (split-INT8 pending)",
+            "config": {"workload": "dd_gemm_4096_split_int8", "M": M, "N": N, "K": K, "R": R,
+                       "slices": S, "rho_a": rho_a, "rho_b": rho_b, "target": "err <= 8 k 2^-104 (|A||B|)_ij",
                        "l2": "operands 256 MiB each > 126 MB L2, no flush needed",
-                       "parallelism": f"replicas x{ws}"},
+                       "parallelism": f"independent problem per GPU x{ws}"},
+            "plain": {"value": plain_val, "unit": "DD-GFLOP/s", "ms_per_step": plain_ms, "steps": plain_steps,
+                      "renorm_interval": RI, "fp64_instr_per_s": plain_fp64, "fp64_peak": fp64_peak,
+                      "frac": plain_fp64 / fp64_peak},
+            "speedup_split_vs_plain": value / plain_val,
+            "accuracy": acc,
+            "phases_ms": phase,
             "e2e": {"value": ws * flops / t_e2e / 1e9, "unit": "DD-GFLOP/s",
-                    "h2d_bytes_per_step": int(A.nbytes + B.nbytes), "d2h_bytes_per_step": int(hC.numel() * 8)},
+                    "h2d_bytes_per_step": int(A.nbytes + B.nbytes), "d2h_bytes_per_step": int(hC.numel() * 8),
+                    "call": "matmuldd_mm_split (host pointers, pinned)"},
             "gpu_launches": launches,
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -325,7 +385,7 @@ def run_reference(args, ws, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -178,6 +178,15 @@ MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_split(const float64x2 *a, const floa
                                                   size_t workspace_bytes, int *info_out,
                                                   void *stream);
 
+/* Phase profiling of the split form for the calling host thread.  Between
+ * begin and end, every mfcuda_matmuldd_mm_split / matmuldd_mm_split call
+ * records events (owned by the library) on its stream around its phases;
+ * end waits for them and writes the summed milliseconds of
+ * {exponent scan, slicing, tensor-core kernel, recombination} to
+ * phase_ms_sum[0..3] and the number of calls to *calls. */
+MULTIFLOATS_CUDA_API void mfcuda_phase_profile_begin(void);
+MULTIFLOATS_CUDA_API int mfcuda_phase_profile_end(double *phase_ms_sum, int64_t *calls);
+
 /* op: 0 exp, 1 log, 2 sin, 3 cos, 4 sqrt */
 enum { MFCUDA_EXP = 0, MFCUDA_LOG = 1, MFCUDA_SIN = 2, MFCUDA_COS = 3, MFCUDA_SQRT = 4 };
 MULTIFLOATS_CUDA_API int mfcuda_unary_dd(int op, const float64x2 *x, float64x2 *y, int64_t n,

@@ -96,7 +96,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 def _build_peaks(force: bool) -> None:
     src = os.path.join(CSRC, "peaks.cu")
-    if not force and os.path.exists(PEAKS_LIB) and os.path.getmtime(PEAKS_LIB) >= os.path.getmtime(src):
+    newest = max(os.path.getmtime(src), os.path.getmtime(os.path.join(CSRC, "tcgen05.cuh")))
+    if not force and os.path.exists(PEAKS_LIB) and os.path.getmtime(PEAKS_LIB) >= newest:
         return
     cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
            "-shared", "-cudart", "static", "-o", PEAKS_LIB, src]

@@ -292,18 +292,54 @@ __device__ __forceinline__ dd cos_kernel(dd x) {
   dd x2 = dd_mul(x, x);
   return neval12(x2, mf_cos_taylor_hi, mf_cos_taylor_lo);
 }
-// want_sin selects sin_eval (true) or cos_eval (false) of trig.inc:165-187.
+// Estrin degree-12 evaluation (poly.inc:91-102) given the powers y2 = y*y,
+// y4 = y2*y2, y8 = y4*y4 of its argument y, so the sin and cos polynomials of
+// the same argument can share them.
+__device__ __forceinline__ dd neval12_pow(dd y, dd y2, dd y4, dd y8, const double* hi,
+                                          const double* lo) {
+#define MF_C(i) make(hi[i], lo[i])
+  dd p01 = dd_add(MF_C(0), dd_mul(MF_C(1), y));
+  dd p23 = dd_add(MF_C(2), dd_mul(MF_C(3), y));
+  dd p45 = dd_add(MF_C(4), dd_mul(MF_C(5), y));
+  dd p67 = dd_add(MF_C(6), dd_mul(MF_C(7), y));
+  dd p89 = dd_add(MF_C(8), dd_mul(MF_C(9), y));
+  dd p1011 = dd_add(MF_C(10), dd_mul(MF_C(11), y));
+  dd p03 = dd_add(p01, dd_mul(p23, y2));
+  dd p47 = dd_add(p45, dd_mul(p67, y2));
+  dd p811 = dd_add(p89, dd_mul(p1011, y2));
+  return dd_add(dd_add(p03, dd_mul(p47, y4)), dd_mul(dd_add(p811, dd_mul(MF_C(12), y4)), y8));
+#undef MF_C
+}
+
+// sin_eval / cos_eval of trig.inc:165-187 without warp divergence.  The
+// reference evaluates sin_kernel(r) or cos_kernel(r) when |r| <= pi/8, and
+// both kernels at r -/+ pi/4 otherwise.  Here every thread evaluates both
+// kernels at its own argument (r, or r -/+ pi/4) with the powers of x*x
+// shared, then selects; each value is produced by exactly the reference's
+// sequence of operations, so results are bit-identical.
 __device__ __forceinline__ dd sincos_eval_one(dd r, bool want_sin) {
   const double pi8 = 0.392699081698724;
-  if (fabs(r.hi) <= pi8) return want_sin ? sin_kernel(r) : cos_kernel(r);
+  const bool small = fabs(r.hi) <= pi8;
+  const bool pos = r.hi > 0.0;
   dd pi4 = make(mf_pi_quarter_hi[0], mf_pi_quarter_lo[0]);
+  dd arg = small ? r : (pos ? dd_sub(r, pi4) : dd_add(r, pi4));
+  dd x2 = dd_mul(arg, arg);
+  dd y2 = dd_mul(x2, x2);
+  dd y4 = dd_mul(y2, y2);
+  dd y8 = dd_mul(y4, y4);
+  dd sk = dd_mul(neval12_pow(x2, y2, y4, y8, mf_sin_taylor_hi, mf_sin_taylor_lo), arg);
+  dd ck = neval12_pow(x2, y2, y4, y8, mf_cos_taylor_hi, mf_cos_taylor_lo);
+  if (small) return want_sin ? sk : ck;
   dd is2 = make(mf_inv_sqrt2_hi[0], mf_inv_sqrt2_lo[0]);
-  bool pos = r.hi > 0.0;
-  dd rp = pos ? dd_sub(r, pi4) : dd_add(r, pi4);
-  dd sk = sin_kernel(rp);
-  dd ck = cos_kernel(rp);
-  if (want_sin) return pos ? dd_mul(dd_add(sk, ck), is2) : dd_mul(dd_sub(sk, ck), is2);
-  return pos ? dd_mul(dd_sub(ck, sk), is2) : dd_mul(dd_add(ck, sk), is2);
+  dd u, v;
+  if (want_sin) {
+    u = sk;
+    v = ck;  // pos: (sk + ck), neg: (sk - ck)
+  } else {
+    u = ck;
+    v = neg(sk);  // pos: (ck - sk), neg: (ck + sk)
+  }
+  return pos ? dd_mul(dd_add(u, v), is2) : dd_mul(dd_sub(u, v), is2);
 }
 __device__ __forceinline__ bool trig_arg_too_large(double a) { return !(fabs(a) < 0x1p55); }
 

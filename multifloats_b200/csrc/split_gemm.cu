@@ -22,8 +22,9 @@
 //               INT32 scratch ([g][kc][N_pad][M_pad]).  4-stage shared-memory
 //               ring (48 KB per stage), two 256-column TMEM accumulators so the
 //               drain of one item overlaps the MMAs of the next.  No multicast.
-//   5. combine: C_ij = 2^(sigma_i + tau_j - 12) sum_g D_g 2^(-8g), summed in
-//               DD from the smallest diagonal up, then scaled exactly.
+//   5. combine: C_ij = 2^(sigma_i + tau_j - 12) sum_kc sum_g D_g,kc 2^(-8g),
+//               summed in DD chunk by chunk, each from the smallest diagonal
+//               up, then scaled exactly.
 //
 // Error (a priori, per output):
 //   |C - AB|_ij <= 2^-(W+1) (2^sigma_i sum_p |b_pj| + 2^tau_j sum_p |a_ip|)   (rounding of the operands)
@@ -35,6 +36,7 @@
 #include <cudaTypedefs.h>
 
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "dd_device.cuh"
@@ -225,84 +227,115 @@ __device__ __forceinline__ __int128 scaled_fixed(double x, int t) {
   return (__int128)(m >> (-sh));
 }
 
-// Balanced digits of round((hi + lo) 2^(W - sigma)), most significant first.
-__device__ __forceinline__ void dd_digits(double hi, double lo, int sigma, int S, int W, int8_t *d) {
+// Balanced digits of round((hi + lo) 2^(W - sigma)) in SMAX positions, most
+// significant first (fully unrolled, so the digits stay in registers).  Since
+// |X| < 2^(8S-2), the top SMAX-S digits are zero and slice s of the S-slice
+// representation is d[SMAX - S + s]; the digit left in position SMAX-S lies in
+// [-64, 64].
+__device__ __forceinline__ void dd_digits(double hi, double lo, int sigma, int W, int8_t (&d)[SMAX]) {
   int t = W - sigma;
   __int128 xf = scaled_fixed(hi, t) + scaled_fixed(lo, t);
   __int128 X = (xf + ((__int128)1 << (FRAC - 1))) >> FRAC;
   const __int128 lim = ((__int128)1 << W) - 1;
   if (X > lim) X = lim;
   if (X < -lim) X = -lim;
-  for (int s = S - 1; s >= 1; --s) {
-    int v = (int)(X & 0xFF);
+  // X = xh 2^56 + xl with 0 <= xl < 2^56: the low seven digits come from xl,
+  // the carry (0 or 1) moves into xh, the high seven digits come from xh.
+  long long xl = (long long)((unsigned long long)X & ((1ull << 56) - 1));
+  long long xh = (long long)(X >> 56);
+#pragma unroll
+  for (int q = SMAX - 1; q >= SMAX - 7; --q) {
+    int v = (int)(xl & 0xFF);
     v = (v ^ 0x80) - 0x80;
-    d[s] = (int8_t)v;
-    X = (X - v) >> 8;
+    d[q] = (int8_t)v;
+    xl = (xl - v) >> 8;
   }
-  d[0] = (int8_t)X;  // |X| < 2^(8S-2) keeps the top digit in [-64, 64]
+  xh += xl;
+#pragma unroll
+  for (int q = SMAX - 8; q >= 0; --q) {
+    int v = (int)(xh & 0xFF);
+    v = (v ^ 0x80) - 0x80;
+    d[q] = (int8_t)v;
+    xh = (xh - v) >> 8;
+  }
 }
 
-// A (m x k column-major) -> As[s][i][p]: tile of 32 rows x 64 columns per
-// block, transposed through shared memory.  Covers the padded extent.
+// A (m x k column-major) -> As[s][i][p]: a block covers 32 rows x 64
+// columns; thread (i = t % 32, group = t / 32) rounds and slices the 8
+// consecutive entries A[i, p0 + 8 group .. + 7] (coalesced across i), packs
+// the 8 digits of each slice into one 64-bit word, and the tile is transposed
+// through shared memory (row stride padded to 72 bytes: conflict-free) so
+// that every slice row is written as contiguous 8-byte words.
+constexpr int SA_ROWS = 32, SA_COLS = 64, SA_STRIDE = 72;
 __global__ void __launch_bounds__(256) slice_a_kernel(const double *__restrict__ A, int64_t M,
                                                       int64_t K, int64_t M_pad, int64_t K_pad,
                                                       const int *sig, const int *flag,
                                                       const Plan *plan, int8_t *__restrict__ As) {
-  __shared__ __align__(16) int8_t tile[SMAX][32][64];
+  __shared__ __align__(16) uint8_t tile[SMAX][SA_ROWS * SA_STRIDE];
   const int S = plan->S, W = plan->W;
-  const int64_t i0 = (int64_t)blockIdx.x * 32, p0 = (int64_t)blockIdx.y * 64;
+  const int64_t i0 = (int64_t)blockIdx.x * SA_ROWS, p0 = (int64_t)blockIdx.y * SA_COLS;
   const int t = threadIdx.x;
-  const int ii = t % 32;
+  const int ii = t % SA_ROWS, grp = t / SA_ROWS;
   const int64_t i = i0 + ii;
   const bool row_ok = i < M && !flag[i < M ? i : 0];
   const int sigma = i < M ? sig[i] : 0;
-  for (int r = 0; r < 8; ++r) {
-    int pp = t / 32 + 8 * r;
-    int64_t p = p0 + pp;
-    int8_t d[SMAX];
+  uint64_t words[SMAX];
 #pragma unroll
-    for (int s = 0; s < SMAX; ++s) d[s] = 0;
+  for (int q = 0; q < SMAX; ++q) words[q] = 0;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int64_t p = p0 + grp * 8 + e;
     if (row_ok && p < K) {
       double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i));
-      dd_digits(v.x, v.y, sigma, S, W, d);
-    }
+      int8_t d[SMAX];
+      dd_digits(v.x, v.y, sigma, W, d);
 #pragma unroll
-    for (int s = 0; s < SMAX; ++s) tile[s][ii][pp] = d[s];
+      for (int q = 0; q < SMAX; ++q) words[q] |= (uint64_t)(uint8_t)d[q] << (8 * e);
+    }
   }
+#pragma unroll
+  for (int q = 0; q < SMAX; ++q)
+    if (q >= SMAX - S)
+      *reinterpret_cast<uint64_t *>(&tile[q - (SMAX - S)][ii * SA_STRIDE + grp * 8]) = words[q];
   __syncthreads();
   const int row = t / 8, seg = (t % 8) * 8;
   for (int s = 0; s < S; ++s) {
-    uint2 v = *reinterpret_cast<const uint2 *>(&tile[s][row][seg]);
-    *reinterpret_cast<uint2 *>(As + ((s * M_pad + i0 + row) * K_pad + p0 + seg)) = v;
+    uint64_t v = *reinterpret_cast<const uint64_t *>(&tile[s][row * SA_STRIDE + seg]);
+    *reinterpret_cast<uint64_t *>(As + ((s * M_pad + i0 + row) * K_pad + p0 + seg)) = v;
   }
 }
 
-// B (k x n column-major) -> Bs[s][j][p]: each thread 4 consecutive p of one column.
+// B (k x n column-major) -> Bs[s][j][p]: each thread rounds and slices 8
+// consecutive entries of one column (128 contiguous bytes in, one 8-byte word
+// per slice out).
 __global__ void __launch_bounds__(256) slice_b_kernel(const double *__restrict__ B, int64_t K,
                                                       int64_t N, int64_t N_pad, int64_t K_pad,
                                                       const int *sig, const int *flag,
                                                       const Plan *plan, int8_t *__restrict__ Bs) {
   const int S = plan->S, W = plan->W;
   const int64_t j = blockIdx.y;
-  const int64_t p4 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
-  if (p4 >= K_pad) return;
+  const int64_t p8 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 8;
+  if (p8 >= K_pad) return;
   const bool col_ok = j < N && !flag[j < N ? j : 0];
   const int tau = j < N ? sig[j] : 0;
-  int8_t d[4][SMAX];
-  for (int q = 0; q < 4; ++q) {
+  uint64_t words[SMAX];
 #pragma unroll
-    for (int s = 0; s < SMAX; ++s) d[q][s] = 0;
-    int64_t p = p4 + q;
+  for (int q = 0; q < SMAX; ++q) words[q] = 0;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int64_t p = p8 + e;
     if (col_ok && p < K) {
       double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p));
-      dd_digits(v.x, v.y, tau, S, W, d[q]);
+      int8_t d[SMAX];
+      dd_digits(v.x, v.y, tau, W, d);
+#pragma unroll
+      for (int q = 0; q < SMAX; ++q) words[q] |= (uint64_t)(uint8_t)d[q] << (8 * e);
     }
   }
-  for (int s = 0; s < S; ++s) {
-    uint32_t w = (uint32_t)(uint8_t)d[0][s] | ((uint32_t)(uint8_t)d[1][s] << 8) |
-                 ((uint32_t)(uint8_t)d[2][s] << 16) | ((uint32_t)(uint8_t)d[3][s] << 24);
-    *reinterpret_cast<uint32_t *>(Bs + ((s * N_pad + j) * K_pad + p4)) = w;
-  }
+#pragma unroll
+  for (int q = 0; q < SMAX; ++q)
+    if (q >= SMAX - S)
+      *reinterpret_cast<uint64_t *>(Bs + (((int64_t)(q - (SMAX - S)) * N_pad + j) * K_pad + p8)) = words[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -516,37 +549,58 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
 // ---------------------------------------------------------------------------
 // 5. combine
 // ---------------------------------------------------------------------------
+// Thread per row i (consecutive threads -> consecutive rows: every load and
+// store is coalesced); the grid's y dimension strides over the columns.
 __global__ void __launch_bounds__(256) combine_kernel(const int32_t *__restrict__ D, const Plan *plan,
                                                       const int *sigA, const int *flagA,
                                                       const int *sigB, const int *flagB, int64_t M,
                                                       int64_t N, int64_t M_pad, int64_t N_pad,
                                                       int nkc, double *__restrict__ C) {
   const int G = plan->G;
-  const int64_t total = M * N;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-    const int64_t i = e % M, j = e / M;
-    double hi = 0.0, lo = 0.0;
-    for (int g = G; g >= 0; --g) {
-      const double scale = ldexp(1.0, -8 * g);
-      for (int kc = 0; kc < nkc; ++kc) {
-        int32_t v = __ldcs(D + ((int64_t)(g * nkc + kc) * N_pad + j) * M_pad + i);
-        double tv = mfdev::mul((double)v, scale);  // exact
-        double s, err;
-        mfdev::two_sum(hi, tv, s, err);
-        hi = s;
-        lo = mfdev::add(lo, err);
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  const int64_t gstride = (int64_t)nkc * N_pad * M_pad;  // distance between diagonals
+  const int sa = sigA[i], fa = flagA[i];
+  // two columns per pass: 2 x (G+1) independent loads in flight per thread
+  for (int64_t j0 = blockIdx.y; j0 < N; j0 += 2 * (int64_t)gridDim.y) {
+    const int64_t jj[2] = {j0, j0 + gridDim.y};
+    double hi[2] = {0.0, 0.0}, lo[2] = {0.0, 0.0};
+    for (int kc = 0; kc < nkc; ++kc) {
+      int32_t v[2][SMAX];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int32_t *src = D + ((int64_t)kc * N_pad + (jj[c] < N ? jj[c] : j0)) * M_pad + i;
+#pragma unroll
+        for (int g = 0; g < SMAX; ++g) v[c][g] = g <= G ? __ldcs(src + g * gstride) : 0;
       }
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int g = SMAX - 1; g >= 0; --g) {
+          if (g <= G) {
+            double tv = mfdev::mul((double)v[c][g], ldexp(1.0, -8 * g));  // exact
+            double s_, err;
+            mfdev::two_sum(hi[c], tv, s_, err);
+            hi[c] = s_;
+            lo[c] = mfdev::add(lo[c], err);
+          }
+        }
     }
-    mfdev::two_sum(hi, lo, hi, lo);
-    double2 out;
-    if (flagA[i] | flagB[j]) {
-      out = make_double2(CUDART_NAN, 0.0);
-    } else {
-      int ex = sigA[i] + sigB[j] - 12;
-      out = make_double2(ldexp(hi, ex), ldexp(lo, ex));
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int64_t j = jj[c];
+      if (j >= N) break;
+      double h, l;
+      mfdev::two_sum(hi[c], lo[c], h, l);
+      double2 out;
+      if (fa | flagB[j]) {
+        out = make_double2(CUDART_NAN, 0.0);
+      } else {
+        int ex = sa + sigB[j] - 12;
+        out = make_double2(ldexp(h, ex), ldexp(l, ex));
+      }
+      __stcs(reinterpret_cast<double2 *>(C) + (j * M + i), out);
     }
-    __stcs(reinterpret_cast<double2 *>(C) + (j * M + i), out);
   }
 }
 
@@ -613,6 +667,53 @@ static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, 
   return r == CUDA_SUCCESS;
 }
 
+// Phase profiling (per host thread): while enabled, every call records five
+// library-owned events on its stream -- before the scan, before the slicing,
+// before and after the tensor-core kernel, after the recombination -- and
+// mfcuda_phase_profile_end sums the four intervals over the recorded calls.
+struct PhaseRec {
+  cudaEvent_t ev[5];
+};
+static thread_local std::vector<PhaseRec> t_recs;
+static thread_local size_t t_used = 0;
+static thread_local bool t_prof = false;
+static thread_local PhaseRec *t_cur = nullptr;
+static void mark(int i, cudaStream_t s) {
+  if (t_cur) cudaEventRecord(t_cur->ev[i], s);
+}
+static void prof_call_begin() {
+  t_cur = nullptr;
+  if (!t_prof) return;
+  if (t_used == t_recs.size()) {
+    PhaseRec r;
+    for (int i = 0; i < 5; ++i)
+      if (cudaEventCreate(&r.ev[i]) != cudaSuccess) return;
+    t_recs.push_back(r);
+  }
+  t_cur = &t_recs[t_used++];
+}
+void profile_begin() {
+  t_prof = true;
+  t_used = 0;
+}
+int profile_end(double *sums, int64_t *calls) {
+  t_prof = false;
+  t_cur = nullptr;
+  for (int i = 0; i < 4; ++i) sums[i] = 0.0;
+  *calls = (int64_t)t_used;
+  for (size_t c = 0; c < t_used; ++c) {
+    if (cudaEventSynchronize(t_recs[c].ev[4]) != cudaSuccess) return MFCUDA_ERR_CUDA;
+    for (int i = 0; i < 4; ++i) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, t_recs[c].ev[i], t_recs[c].ev[i + 1]) != cudaSuccess)
+        return MFCUDA_ERR_CUDA;
+      sums[i] += ms;
+    }
+  }
+  t_used = 0;
+  return MFCUDA_OK;
+}
+
 size_t workspace_size(int64_t m, int64_t k, int64_t n) { return layout(m, k, n).total; }
 
 static std::once_flag g_attr_once;
@@ -667,6 +768,8 @@ int run(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t
     std::call_once(g_attr_once, [] {
       cudaFuncSetAttribute(split_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
     });
+    prof_call_begin();
+    mark(0, s);
     cudaMemsetAsync(status, 0, sizeof(int), s);
     init_stats_kernel<<<(unsigned)((L.M_pad + 255) / 256), 256, 0, s>>>(sigA, muA, flagA, L.M_pad);
     init_stats_kernel<<<(unsigned)((L.N_pad + 255) / 256), 256, 0, s>>>(sigB, muB, flagB, L.N_pad);
@@ -676,19 +779,27 @@ int run(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t
     scan_b_kernel<<<dim3((unsigned)((k + 2047) / 2048), (unsigned)n), 256, 0, s>>>(Bd, k, n, sigB, muB,
                                                                                    flagB);
     plan_kernel<<<1, 1024, 0, s>>>(sigA, muA, m, sigB, muB, n, slices, target, plan);
+    mark(1, s);
     slice_a_kernel<<<dim3((unsigned)(L.M_pad / 32), (unsigned)(L.K_pad / 64)), 256, 0, s>>>(
         Ad, m, k, L.M_pad, L.K_pad, sigA, flagA, plan, As);
-    slice_b_kernel<<<dim3((unsigned)((L.K_pad / 4 + 255) / 256), (unsigned)L.N_pad), 256, 0, s>>>(
+    slice_b_kernel<<<dim3((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad), 256, 0, s>>>(
         Bd, k, n, L.N_pad, L.K_pad, sigB, flagB, plan, Bs);
     int items_max = SMAX * (int)L.nkc * (int)((L.M_pad / BM) * (L.N_pad / BN));
     int grid = sm_count();
     if (grid > items_max) grid = items_max;
+    mark(2, s);
     split_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad, (int)L.N_pad,
                                                          (int)L.nkc, (int)L.kblocks, status);
-    int64_t cblocks = (m * n + 255) / 256;
-    if (cblocks > (int64_t)sm_count() * 32) cblocks = (int64_t)sm_count() * 32;
-    combine_kernel<<<(unsigned)cblocks, 256, 0, s>>>(D, plan, sigA, flagA, sigB, flagB, m, n, L.M_pad,
-                                                     L.N_pad, (int)L.nkc, reinterpret_cast<double *>(c));
+    mark(3, s);
+    {
+      unsigned gx = (unsigned)((m + 255) / 256);
+      int64_t want = ((int64_t)sm_count() * 32 + gx - 1) / gx;  // ~32 CTAs per SM in total
+      unsigned gy = (unsigned)(n < want ? n : want);
+      if (gy > 65535u) gy = 65535u;
+      combine_kernel<<<dim3(gx, gy), 256, 0, s>>>(D, plan, sigA, flagA, sigB, flagB, m, n, L.M_pad,
+                                                  L.N_pad, (int)L.nkc, reinterpret_cast<double *>(c));
+    }
+    mark(4, s);
     if (cudaGetLastError() != cudaSuccess) rc = MFCUDA_ERR_CUDA;
     if (S_used && rc == MFCUDA_OK) {
       Plan hp;
@@ -742,6 +853,12 @@ static int split_host(const float64x2 *a, const float64x2 *b, float64x2 *c, int6
 }  // namespace mfcuda
 
 extern "C" {
+
+MULTIFLOATS_CUDA_API void mfcuda_phase_profile_begin(void) { mfcuda::split::profile_begin(); }
+MULTIFLOATS_CUDA_API int mfcuda_phase_profile_end(double *phase_ms_sum, int64_t *calls) {
+  if (!phase_ms_sum || !calls) return MFCUDA_ERR_INVALID_ARG;
+  return mfcuda::split::profile_end(phase_ms_sum, calls);
+}
 
 MULTIFLOATS_CUDA_API size_t mfcuda_split_workspace_size(int64_t m, int64_t k, int64_t n) {
   if (m < 0 || k < 0 || n < 0) return 0;

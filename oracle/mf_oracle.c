@@ -803,8 +803,8 @@ void orc_reduce_error(int kind, const double *x, const double *y, int64_t n, con
 /* ---- split-INT8 GEMM, restated on the CPU ------------------------------------
  * The same algorithm as the device kernels in split_gemm.cu (scan, plan,
  * exact rounding to (8S-2)-bit integers, balanced signed 8-bit digits, exact
- * integer anti-diagonal sums D_g per K chunk, DD combine from the smallest
- * diagonal up, exact scaling).  The integer stage is exact and the combine
+ * integer anti-diagonal sums D_g per K chunk, DD combine chunk by chunk, each
+ * from the smallest diagonal up, exact scaling).  The integer stage is exact and the combine
  * order is fixed, so the device result must match this bit for bit. */
 #define SPLIT_SMAX 14
 #define SPLIT_KC (73 * 128) /* K elements per chunk, as KC_BLOCKS * BK on the device */
@@ -904,9 +904,9 @@ void orc_split_gemm(const double *a, const double *b, double *c, int64_t m, int6
   for (int64_t j = 0; j < n; ++j)
     for (int64_t i = 0; i < m; ++i) {
       double hi = 0.0, lo = 0.0;
-      for (int g = G; g >= 0; --g) {
-        double scale = ldexp(1.0, -8 * g);
-        for (int64_t kc = 0; kc < nkc; ++kc) {
+      for (int64_t kc = 0; kc < nkc; ++kc) {
+        for (int g = G; g >= 0; --g) {
+          double scale = ldexp(1.0, -8 * g);
           int64_t p0 = kc * SPLIT_KC, p1 = p0 + SPLIT_KC < k ? p0 + SPLIT_KC : k;
           int64_t D = 0;
           for (int s = 0; s <= g; ++s) {
