@@ -146,6 +146,14 @@ MULTIFLOATS_CUDA_API float64x2 cnorm2dd_array(const complex64x2 *x, int64_t n);
 MULTIFLOATS_CUDA_API void matmuldd_mm_split(const float64x2 *a, const float64x2 *b, float64x2 *c,
                                             int64_t m, int64_t k, int64_t n, int slices,
                                             double *max_err_bound_out);
+/* Complex split form: the four real products of the Fortran cdd_matmul_mm
+ * composition (fsrc/multifloats.fypp:2609-2621) -- re = Ar Br - Ai Bi,
+ * im = Ar Bi + Ai Br, combined with the DD operators -- each in split form
+ * with one slice count for all four (the four parts are sliced once).  The
+ * bound applies to each real product. */
+MULTIFLOATS_CUDA_API void cmatmuldd_mm_split(const complex64x2 *a, const complex64x2 *b,
+                                             complex64x2 *c, int64_t m, int64_t k, int64_t n,
+                                             int slices, double *max_err_bound_out);
 
 /* ==========================================================================
  * 2. Device-pointer API (asynchronous on `stream`, a cudaStream_t; NULL = legacy
@@ -177,6 +185,12 @@ MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_split(const float64x2 *a, const floa
                                                   int slices, double target, void *workspace,
                                                   size_t workspace_bytes, int *info_out,
                                                   void *stream);
+MULTIFLOATS_CUDA_API size_t mfcuda_csplit_workspace_size(int64_t m, int64_t k, int64_t n);
+MULTIFLOATS_CUDA_API int mfcuda_cmatmuldd_mm_split(const complex64x2 *a, const complex64x2 *b,
+                                                   complex64x2 *c, int64_t m, int64_t k, int64_t n,
+                                                   int slices, double target, void *workspace,
+                                                   size_t workspace_bytes, int *info_out,
+                                                   void *stream);
 
 /* Phase profiling of the split form for the calling host thread.  Between
  * begin and end, every mfcuda_matmuldd_mm_split / matmuldd_mm_split call

@@ -101,16 +101,20 @@ __global__ void init_stats_kernel(int *sig, int *mu, int *flag, int64_t n) {
 __device__ __forceinline__ int binade_above(double v) { return ilogb(v) + 1; }
 __device__ __forceinline__ int binade_below(double v) { return ilogb(v); }
 
+// Operands are read through strided views: DD element e of a view lives at
+// double2 index e * stride from its base (stride 1 for a real matrix, 2 for the
+// real or imaginary part of a complex one).
+//
 // A column-major m x k: thread per row, a chunk of columns per blockIdx.y.
 __global__ void __launch_bounds__(256) scan_a_kernel(const double *__restrict__ A, int64_t M,
-                                                     int64_t K, int kchunk, int *sig, int *mu,
-                                                     int *flag) {
+                                                     int64_t K, int64_t stride, int kchunk, int *sig,
+                                                     int *mu, int *flag) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= M) return;
   int64_t p0 = (int64_t)blockIdx.y * kchunk, p1 = p0 + kchunk < K ? p0 + kchunk : K;
   int hi_e = SENT_LO, lo_e = SENT_HI, bad = 0;
   for (int64_t p = p0; p < p1; ++p) {
-    double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i));
+    double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i) * stride);
     if (!isfinite(v.x) || !isfinite(v.y)) {
       bad = 1;
       continue;
@@ -128,14 +132,15 @@ __global__ void __launch_bounds__(256) scan_a_kernel(const double *__restrict__ 
 
 // B column-major k x n: a block per (column j, chunk of 2048 rows).
 __global__ void __launch_bounds__(256) scan_b_kernel(const double *__restrict__ B, int64_t K,
-                                                     int64_t N, int *sig, int *mu, int *flag) {
+                                                     int64_t N, int64_t stride, int *sig, int *mu,
+                                                     int *flag) {
   int64_t j = blockIdx.y;
   int64_t p0 = (int64_t)blockIdx.x * 2048;
   int hi_e = SENT_LO, lo_e = SENT_HI, bad = 0;
   for (int r = 0; r < 8; ++r) {
     int64_t p = p0 + threadIdx.x + 256 * r;
     if (p >= K) break;
-    double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p));
+    double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p) * stride);
     if (!isfinite(v.x) || !isfinite(v.y)) {
       bad = 1;
       continue;
@@ -161,16 +166,23 @@ __global__ void __launch_bounds__(256) scan_b_kernel(const double *__restrict__ 
 // ---------------------------------------------------------------------------
 // 2. plan (one block)
 // ---------------------------------------------------------------------------
-__global__ void plan_kernel(int *sigA, const int *muA, int64_t M, int *sigB, const int *muB,
-                            int64_t N, int slices, double target, Plan *plan) {
+// Exponent statistics of the operands of one call: A-side operands (rows of
+// an m x k matrix) and B-side operands (columns of a k x n matrix).
+struct StatSet {
+  int *sig[4];
+  const int *mu[4];
+  int64_t count[4];
+  int side[4];  // 0: A side, 1: B side
+  int n;
+};
+
+__global__ void plan_kernel(StatSet st, int slices, double target, Plan *plan) {
   __shared__ int red[2][32];
-  int ra = 0, rb = 0;
-  for (int64_t i = threadIdx.x; i < M; i += blockDim.x) {
-    if (sigA[i] != SENT_LO) ra = max(ra, sigA[i] - muA[i]);
-  }
-  for (int64_t j = threadIdx.x; j < N; j += blockDim.x) {
-    if (sigB[j] != SENT_LO) rb = max(rb, sigB[j] - muB[j]);
-  }
+  int r[2] = {0, 0};
+  for (int o = 0; o < st.n; ++o)
+    for (int64_t i = threadIdx.x; i < st.count[o]; i += blockDim.x)
+      if (st.sig[o][i] != SENT_LO) r[st.side[o]] = max(r[st.side[o]], st.sig[o][i] - st.mu[o][i]);
+  int ra = r[0], rb = r[1];
   for (int off = 16; off >= 1; off >>= 1) {
     ra = max(ra, __shfl_xor_sync(0xffffffffu, ra, off));
     rb = max(rb, __shfl_xor_sync(0xffffffffu, rb, off));
@@ -189,10 +201,10 @@ __global__ void plan_kernel(int *sigA, const int *muA, int64_t M, int *sigB, con
     if (S <= 0) {
       // smallest S with (S+1) 2^(106 - 8S + rho_a + rho_b) <= target
       S = SMAX;
-      for (int s = 2; s <= SMAX; ++s) {
-        double ratio = (s + 1) * ldexp(1.0, 106 - 8 * s + ra + rb);
+      for (int q = 2; q <= SMAX; ++q) {
+        double ratio = (q + 1) * ldexp(1.0, 106 - 8 * q + ra + rb);
         if (ratio <= target) {
-          S = s;
+          S = q;
           break;
         }
       }
@@ -205,10 +217,9 @@ __global__ void plan_kernel(int *sigA, const int *muA, int64_t M, int *sigB, con
   }
   // zero rows / columns: any sigma works, the digits are all zero
   __syncthreads();
-  for (int64_t i = threadIdx.x; i < M; i += blockDim.x)
-    if (sigA[i] == SENT_LO) sigA[i] = 0;
-  for (int64_t j = threadIdx.x; j < N; j += blockDim.x)
-    if (sigB[j] == SENT_LO) sigB[j] = 0;
+  for (int o = 0; o < st.n; ++o)
+    for (int64_t i = threadIdx.x; i < st.count[o]; i += blockDim.x)
+      if (st.sig[o][i] == SENT_LO) st.sig[o][i] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -268,8 +279,8 @@ __device__ __forceinline__ void dd_digits(double hi, double lo, int sigma, int W
 // that every slice row is written as contiguous 8-byte words.
 constexpr int SA_ROWS = 32, SA_COLS = 64, SA_STRIDE = 72;
 __global__ void __launch_bounds__(256) slice_a_kernel(const double *__restrict__ A, int64_t M,
-                                                      int64_t K, int64_t M_pad, int64_t K_pad,
-                                                      const int *sig, const int *flag,
+                                                      int64_t K, int64_t stride, int64_t M_pad,
+                                                      int64_t K_pad, const int *sig, const int *flag,
                                                       const Plan *plan, int8_t *__restrict__ As) {
   __shared__ __align__(16) uint8_t tile[SMAX][SA_ROWS * SA_STRIDE];
   const int S = plan->S, W = plan->W;
@@ -286,7 +297,7 @@ __global__ void __launch_bounds__(256) slice_a_kernel(const double *__restrict__
   for (int e = 0; e < 8; ++e) {
     int64_t p = p0 + grp * 8 + e;
     if (row_ok && p < K) {
-      double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i));
+      double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i) * stride);
       int8_t d[SMAX];
       dd_digits(v.x, v.y, sigma, W, d);
 #pragma unroll
@@ -309,8 +320,8 @@ __global__ void __launch_bounds__(256) slice_a_kernel(const double *__restrict__
 // consecutive entries of one column (128 contiguous bytes in, one 8-byte word
 // per slice out).
 __global__ void __launch_bounds__(256) slice_b_kernel(const double *__restrict__ B, int64_t K,
-                                                      int64_t N, int64_t N_pad, int64_t K_pad,
-                                                      const int *sig, const int *flag,
+                                                      int64_t N, int64_t stride, int64_t N_pad,
+                                                      int64_t K_pad, const int *sig, const int *flag,
                                                       const Plan *plan, int8_t *__restrict__ Bs) {
   const int S = plan->S, W = plan->W;
   const int64_t j = blockIdx.y;
@@ -325,7 +336,7 @@ __global__ void __launch_bounds__(256) slice_b_kernel(const double *__restrict__
   for (int e = 0; e < 8; ++e) {
     int64_t p = p8 + e;
     if (col_ok && p < K) {
-      double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p));
+      double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p) * stride);
       int8_t d[SMAX];
       dd_digits(v.x, v.y, tau, W, d);
 #pragma unroll
@@ -550,12 +561,16 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
 // 5. combine
 // ---------------------------------------------------------------------------
 // Thread per row i (consecutive threads -> consecutive rows: every load and
-// store is coalesced); the grid's y dimension strides over the columns.
+// store is coalesced); the grid's y dimension strides over the columns.  The
+// output is a strided view (C element (i,j) at double2 index (jM + i) cstride)
+// and `mode` stores the product P (0), or replaces C by the DD difference
+// C - P (1) or sum C + P (2), which assembles complex products.
 __global__ void __launch_bounds__(256) combine_kernel(const int32_t *__restrict__ D, const Plan *plan,
                                                       const int *sigA, const int *flagA,
                                                       const int *sigB, const int *flagB, int64_t M,
                                                       int64_t N, int64_t M_pad, int64_t N_pad,
-                                                      int nkc, double *__restrict__ C) {
+                                                      int nkc, double *__restrict__ C, int64_t cstride,
+                                                      int mode) {
   const int G = plan->G;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= M) return;
@@ -599,7 +614,14 @@ __global__ void __launch_bounds__(256) combine_kernel(const int32_t *__restrict_
         int ex = sa + sigB[j] - 12;
         out = make_double2(ldexp(h, ex), ldexp(l, ex));
       }
-      __stcs(reinterpret_cast<double2 *>(C) + (j * M + i), out);
+      double2 *dst = reinterpret_cast<double2 *>(C) + (j * M + i) * cstride;
+      if (mode != 0) {
+        double2 prev = *dst;
+        mfdev::dd p = mfdev::make(out.x, out.y), q = mfdev::make(prev.x, prev.y);
+        mfdev::dd r = mode == 1 ? mfdev::dd_sub(q, p) : mfdev::dd_add(q, p);
+        out = make_double2(r.hi, r.lo);
+      }
+      __stcs(dst, out);
     }
   }
 }
@@ -607,21 +629,26 @@ __global__ void __launch_bounds__(256) combine_kernel(const int32_t *__restrict_
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// Workspace of one call with nA A-side operands (m x k) and nB B-side
+// operands (k x n): per operand its exponent statistics and SMAX slices, one
+// INT32 diagonal scratch shared by the products, the plan and a status word.
 struct Layout {
   int64_t M_pad, N_pad, K_pad, kblocks, nkc;
-  size_t off_plan, off_sigA, off_muA, off_flagA, off_sigB, off_muB, off_flagB, off_As, off_Bs, off_D,
-      total;
+  int nA, nB;
+  size_t off_plan, off_stats[4], off_slices[4], off_D, total;
 };
 
 static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
-static Layout layout(int64_t m, int64_t k, int64_t n) {
+static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB) {
   Layout L;
   L.M_pad = round_up(m < 1 ? 1 : m, BM);
   L.N_pad = round_up(n < 1 ? 1 : n, BN);
   L.K_pad = round_up(k < 1 ? 1 : k, BK);
   L.kblocks = L.K_pad / BK;
   L.nkc = (L.kblocks + KC_BLOCKS - 1) / KC_BLOCKS;
+  L.nA = nA;
+  L.nB = nB;
   size_t off = 0;
   auto take = [&](size_t bytes) {
     size_t o = off;
@@ -629,14 +656,11 @@ static Layout layout(int64_t m, int64_t k, int64_t n) {
     return o;
   };
   L.off_plan = take(sizeof(Plan));
-  L.off_sigA = take(sizeof(int) * L.M_pad);
-  L.off_muA = take(sizeof(int) * L.M_pad);
-  L.off_flagA = take(sizeof(int) * L.M_pad);
-  L.off_sigB = take(sizeof(int) * L.N_pad);
-  L.off_muB = take(sizeof(int) * L.N_pad);
-  L.off_flagB = take(sizeof(int) * L.N_pad);
-  L.off_As = take((size_t)SMAX * L.M_pad * L.K_pad);
-  L.off_Bs = take((size_t)SMAX * L.N_pad * L.K_pad);
+  for (int o = 0; o < nA + nB; ++o) {
+    int64_t rows = o < nA ? L.M_pad : L.N_pad;
+    L.off_stats[o] = take(3 * sizeof(int) * rows);
+    L.off_slices[o] = take((size_t)SMAX * rows * L.K_pad);
+  }
   L.off_D = take((size_t)SMAX * L.nkc * L.N_pad * L.M_pad * sizeof(int32_t));
   L.total = off + 256 /* status word */;
   return L;
@@ -714,29 +738,33 @@ int profile_end(double *sums, int64_t *calls) {
   return MFCUDA_OK;
 }
 
-size_t workspace_size(int64_t m, int64_t k, int64_t n) { return layout(m, k, n).total; }
+size_t workspace_size(int64_t m, int64_t k, int64_t n, bool complex_operands) {
+  int no = complex_operands ? 2 : 1;
+  return layout(m, k, n, no, no).total;
+}
 
 static std::once_flag g_attr_once;
 
-int run(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k, int64_t n,
-        int slices, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *S_used) {
-  if (m < 0 || k < 0 || n < 0 || !mul_ok(m, k) || !mul_ok(k, n) || !mul_ok(m, n))
-    return MFCUDA_ERR_INVALID_ARG;
-  if (slices < 0 || slices > SMAX || slices == 1) return MFCUDA_ERR_INVALID_ARG;
-  if (!(target > 0.0)) return MFCUDA_ERR_INVALID_ARG;
-  if (m == 0 || n == 0) return MFCUDA_OK;
-  if (!c || (k > 0 && (!a || !b))) return MFCUDA_ERR_INVALID_ARG;
-  if ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) | reinterpret_cast<uintptr_t>(c)) & 15)
-    return MFCUDA_ERR_UNSUPPORTED;  // the split form wants 16-byte aligned operands
-  MF_TRY(require_device());
-  Layout L = layout(m, k, n);
-  if (L.M_pad > INT32_MAX / 2 || L.N_pad > INT32_MAX / 2 || L.kblocks > INT32_MAX / 2)
+// A product of one A-side operand with one B-side operand, written into a
+// strided output view with the given mode (see combine_kernel).
+struct Product {
+  int a, b;
+  double *out;
+  int64_t ostride;
+  int mode;
+};
+
+// Runs the whole split pipeline for `nprod` products of the operands
+// A-side views (aview[o], stride astride[o]) and B-side views.  info (may be
+// NULL) receives {S, rho_A, rho_B}; a non-NULL info waits for completion.
+static int run_products(const double *const *aview, const int64_t *astride, int nA,
+                        const double *const *bview, const int64_t *bstride, int nB,
+                        const Product *prods, int nprod, int64_t m, int64_t k, int64_t n, int slices,
+                        double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info) {
+  Layout L = layout(m, k, n, nA, nB);
+  if (L.M_pad > INT32_MAX / 2 || L.N_pad > INT32_MAX / 2 || L.kblocks > INT32_MAX / 2 ||
+      n > 65535 || L.K_pad / 64 > 65535)
     return MFCUDA_ERR_UNSUPPORTED;
-  if (k == 0) {
-    MF_TRY_CUDA(cudaMemsetAsync(c, 0, (size_t)(m * n) * sizeof(float64x2), s));
-    if (S_used) *S_used = 0;
-    return MFCUDA_OK;
-  }
   void *own = nullptr;
   if (!ws) {
     MF_TRY(ws_alloc(&own, L.total, s));
@@ -746,73 +774,91 @@ int run(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t
   }
   uint8_t *base = static_cast<uint8_t *>(ws);
   Plan *plan = reinterpret_cast<Plan *>(base + L.off_plan);
-  int *sigA = reinterpret_cast<int *>(base + L.off_sigA);
-  int *muA = reinterpret_cast<int *>(base + L.off_muA);
-  int *flagA = reinterpret_cast<int *>(base + L.off_flagA);
-  int *sigB = reinterpret_cast<int *>(base + L.off_sigB);
-  int *muB = reinterpret_cast<int *>(base + L.off_muB);
-  int *flagB = reinterpret_cast<int *>(base + L.off_flagB);
-  int8_t *As = reinterpret_cast<int8_t *>(base + L.off_As);
-  int8_t *Bs = reinterpret_cast<int8_t *>(base + L.off_Bs);
   int32_t *D = reinterpret_cast<int32_t *>(base + L.off_D);
   int *status = reinterpret_cast<int *>(base + L.total - 256);
-  const double *Ad = reinterpret_cast<const double *>(a);
-  const double *Bd = reinterpret_cast<const double *>(b);
+  const int nops = nA + nB;
+  int *sig[4], *mu[4], *flag[4];
+  int8_t *sl[4];
+  for (int o = 0; o < nops; ++o) {
+    int64_t rows = o < nA ? L.M_pad : L.N_pad;
+    sig[o] = reinterpret_cast<int *>(base + L.off_stats[o]);
+    mu[o] = sig[o] + rows;
+    flag[o] = mu[o] + rows;
+    sl[o] = reinterpret_cast<int8_t *>(base + L.off_slices[o]);
+  }
   int rc = MFCUDA_OK;
   do {
-    CUtensorMap tmA, tmB;
-    if (!make_map(&tmA, As, L.M_pad, L.K_pad, BM) || !make_map(&tmB, Bs, L.N_pad, L.K_pad, BN)) {
-      rc = MFCUDA_ERR_CUDA;
-      break;
-    }
     std::call_once(g_attr_once, [] {
       cudaFuncSetAttribute(split_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
     });
     prof_call_begin();
     mark(0, s);
     cudaMemsetAsync(status, 0, sizeof(int), s);
-    init_stats_kernel<<<(unsigned)((L.M_pad + 255) / 256), 256, 0, s>>>(sigA, muA, flagA, L.M_pad);
-    init_stats_kernel<<<(unsigned)((L.N_pad + 255) / 256), 256, 0, s>>>(sigB, muB, flagB, L.N_pad);
     const int kch = 64;
-    scan_a_kernel<<<dim3((unsigned)((m + 255) / 256), (unsigned)((k + kch - 1) / kch)), 256, 0, s>>>(
-        Ad, m, k, kch, sigA, muA, flagA);
-    scan_b_kernel<<<dim3((unsigned)((k + 2047) / 2048), (unsigned)n), 256, 0, s>>>(Bd, k, n, sigB, muB,
-                                                                                   flagB);
-    plan_kernel<<<1, 1024, 0, s>>>(sigA, muA, m, sigB, muB, n, slices, target, plan);
+    StatSet st;
+    st.n = nops;
+    for (int o = 0; o < nops; ++o) {
+      const bool aside = o < nA;
+      int64_t rows = aside ? L.M_pad : L.N_pad;
+      init_stats_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(sig[o], mu[o], flag[o], rows);
+      if (aside)
+        scan_a_kernel<<<dim3((unsigned)((m + 255) / 256), (unsigned)((k + kch - 1) / kch)), 256, 0, s>>>(
+            aview[o], m, k, astride[o], kch, sig[o], mu[o], flag[o]);
+      else
+        scan_b_kernel<<<dim3((unsigned)((k + 2047) / 2048), (unsigned)n), 256, 0, s>>>(
+            bview[o - nA], k, n, bstride[o - nA], sig[o], mu[o], flag[o]);
+      st.sig[o] = sig[o];
+      st.mu[o] = mu[o];
+      st.count[o] = aside ? m : n;
+      st.side[o] = aside ? 0 : 1;
+    }
+    plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, plan);
     mark(1, s);
-    slice_a_kernel<<<dim3((unsigned)(L.M_pad / 32), (unsigned)(L.K_pad / 64)), 256, 0, s>>>(
-        Ad, m, k, L.M_pad, L.K_pad, sigA, flagA, plan, As);
-    slice_b_kernel<<<dim3((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad), 256, 0, s>>>(
-        Bd, k, n, L.N_pad, L.K_pad, sigB, flagB, plan, Bs);
+    for (int o = 0; o < nops; ++o) {
+      if (o < nA)
+        slice_a_kernel<<<dim3((unsigned)(L.M_pad / 32), (unsigned)(L.K_pad / 64)), 256, 0, s>>>(
+            aview[o], m, k, astride[o], L.M_pad, L.K_pad, sig[o], flag[o], plan, sl[o]);
+      else
+        slice_b_kernel<<<dim3((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad), 256, 0, s>>>(
+            bview[o - nA], k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o], flag[o], plan, sl[o]);
+    }
     int items_max = SMAX * (int)L.nkc * (int)((L.M_pad / BM) * (L.N_pad / BN));
     int grid = sm_count();
     if (grid > items_max) grid = items_max;
+    unsigned gx = (unsigned)((m + 255) / 256);
+    int64_t want = ((int64_t)sm_count() * 32 + gx - 1) / gx;  // ~32 CTAs per SM in total
+    unsigned gy = (unsigned)(n < want ? n : want);
+    if (gy > 65535u) gy = 65535u;
     mark(2, s);
-    split_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad, (int)L.N_pad,
-                                                         (int)L.nkc, (int)L.kblocks, status);
-    mark(3, s);
-    {
-      unsigned gx = (unsigned)((m + 255) / 256);
-      int64_t want = ((int64_t)sm_count() * 32 + gx - 1) / gx;  // ~32 CTAs per SM in total
-      unsigned gy = (unsigned)(n < want ? n : want);
-      if (gy > 65535u) gy = 65535u;
-      combine_kernel<<<dim3(gx, gy), 256, 0, s>>>(D, plan, sigA, flagA, sigB, flagB, m, n, L.M_pad,
-                                                  L.N_pad, (int)L.nkc, reinterpret_cast<double *>(c));
+    for (int q = 0; q < nprod && rc == MFCUDA_OK; ++q) {
+      const int ia = prods[q].a, ib = nA + prods[q].b;
+      CUtensorMap tmA, tmB;
+      if (!make_map(&tmA, sl[ia], L.M_pad, L.K_pad, BM) || !make_map(&tmB, sl[ib], L.N_pad, L.K_pad, BN)) {
+        rc = MFCUDA_ERR_CUDA;
+        break;
+      }
+      split_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad,
+                                                           (int)L.N_pad, (int)L.nkc, (int)L.kblocks,
+                                                           status);
+      if (q == nprod - 1) mark(3, s);
+      combine_kernel<<<dim3(gx, gy), 256, 0, s>>>(D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n,
+                                                  L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,
+                                                  prods[q].ostride, prods[q].mode);
     }
     mark(4, s);
-    if (cudaGetLastError() != cudaSuccess) rc = MFCUDA_ERR_CUDA;
-    if (S_used && rc == MFCUDA_OK) {
+    if (rc == MFCUDA_OK && cudaGetLastError() != cudaSuccess) rc = MFCUDA_ERR_CUDA;
+    if (info && rc == MFCUDA_OK) {
       Plan hp;
       if (cudaMemcpyAsync(&hp, plan, sizeof(Plan), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
           cudaStreamSynchronize(s) != cudaSuccess) {
         rc = MFCUDA_ERR_CUDA;
       } else {
-        int st = 0;
-        cudaMemcpy(&st, status, sizeof(int), cudaMemcpyDeviceToHost);
-        if (st) rc = MFCUDA_ERR_TIMEOUT;
-        *S_used = hp.S;
-        S_used[1] = hp.rho_a;
-        S_used[2] = hp.rho_b;
+        int stv = 0;
+        cudaMemcpy(&stv, status, sizeof(int), cudaMemcpyDeviceToHost);
+        if (stv) rc = MFCUDA_ERR_TIMEOUT;
+        info[0] = hp.S;
+        info[1] = hp.rho_a;
+        info[2] = hp.rho_b;
       }
     }
   } while (0);
@@ -820,27 +866,92 @@ int run(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t
   return rc;
 }
 
+static int check_args(const void *a, const void *b, const void *c, int64_t m, int64_t k, int64_t n,
+                      int slices, double target) {
+  if (m < 0 || k < 0 || n < 0 || !mul_ok(m, k) || !mul_ok(k, n) || !mul_ok(m, n))
+    return MFCUDA_ERR_INVALID_ARG;
+  if (slices < 0 || slices > SMAX || slices == 1) return MFCUDA_ERR_INVALID_ARG;
+  if (!(target > 0.0)) return MFCUDA_ERR_INVALID_ARG;
+  if (m == 0 || n == 0) return -1;  // nothing to do
+  if (!c || (k > 0 && (!a || !b))) return MFCUDA_ERR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) | reinterpret_cast<uintptr_t>(c)) & 15)
+    return MFCUDA_ERR_UNSUPPORTED;  // the split form wants 16-byte aligned operands
+  return MFCUDA_OK;
+}
+
+int run(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k, int64_t n,
+        int slices, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info) {
+  int rc = check_args(a, b, c, m, k, n, slices, target);
+  if (rc == -1) return MFCUDA_OK;
+  MF_TRY(rc);
+  MF_TRY(require_device());
+  if (k == 0) {
+    MF_TRY_CUDA(cudaMemsetAsync(c, 0, (size_t)(m * n) * sizeof(float64x2), s));
+    if (info) info[0] = info[1] = info[2] = 0;
+    return MFCUDA_OK;
+  }
+  const double *av[1] = {reinterpret_cast<const double *>(a)};
+  const double *bv[1] = {reinterpret_cast<const double *>(b)};
+  int64_t one[1] = {1};
+  Product p = {0, 0, reinterpret_cast<double *>(c), 1, 0};
+  return run_products(av, one, 1, bv, one, 1, &p, 1, m, k, n, slices, target, ws, ws_bytes, s, info);
+}
+
+// Complex: re = Ar Br - Ai Bi, im = Ar Bi + Ai Br (the Fortran cdd_matmul_mm
+// composition, fsrc/multifloats.fypp:2609-2621), each real product in split form
+// with one slice count S for all four; the four operands are sliced once.
+int run_complex(const complex64x2 *a, const complex64x2 *b, complex64x2 *c, int64_t m, int64_t k,
+                int64_t n, int slices, double target, void *ws, size_t ws_bytes, cudaStream_t s,
+                int *info) {
+  int rc = check_args(a, b, c, m, k, n, slices, target);
+  if (rc == -1) return MFCUDA_OK;
+  MF_TRY(rc);
+  MF_TRY(require_device());
+  if (k == 0) {
+    MF_TRY_CUDA(cudaMemsetAsync(c, 0, (size_t)(m * n) * sizeof(complex64x2), s));
+    if (info) info[0] = info[1] = info[2] = 0;
+    return MFCUDA_OK;
+  }
+  const double *A = reinterpret_cast<const double *>(a);
+  const double *B = reinterpret_cast<const double *>(b);
+  double *Cd = reinterpret_cast<double *>(c);
+  const double *av[2] = {A, A + 2};
+  const double *bv[2] = {B, B + 2};
+  int64_t two[2] = {2, 2};
+  Product p[4] = {{0, 0, Cd, 2, 0},       // re  = Ar Br
+                  {1, 1, Cd, 2, 1},       // re -= Ai Bi
+                  {0, 1, Cd + 2, 2, 0},   // im  = Ar Bi
+                  {1, 0, Cd + 2, 2, 2}};  // im += Ai Br
+  return run_products(av, two, 2, bv, two, 2, p, 4, m, k, n, slices, target, ws, ws_bytes, s, info);
+}
+
 }  // namespace split
 
-static int split_host(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k,
-                      int64_t n, int slices, double *bound_out) {
+template <bool CPLX>
+static int split_host(const void *a, const void *b, void *c, int64_t m, int64_t k, int64_t n, int slices,
+                      double *bound_out) {
+  const size_t elem = CPLX ? sizeof(complex64x2) : sizeof(float64x2);
   if (m < 0 || k < 0 || n < 0 || !mul_ok(m, k) || !mul_ok(k, n) || !mul_ok(m, n))
     return MFCUDA_ERR_INVALID_ARG;
   if (m == 0 || n == 0) return MFCUDA_OK;
   if (!c || (k > 0 && (!a || !b))) return MFCUDA_ERR_INVALID_ARG;
   MF_TRY(require_device());
-  size_t ba = (size_t)(m * k) * sizeof(float64x2), bb = (size_t)(k * n) * sizeof(float64x2),
-         bc = (size_t)(m * n) * sizeof(float64x2);
-  size_t wsb = split::workspace_size(m, k, n);
+  size_t ba = (size_t)(m * k) * elem, bb = (size_t)(k * n) * elem, bc = (size_t)(m * n) * elem;
+  size_t wsb = split::workspace_size(m, k, n, CPLX);
   size_t sz[4] = {ba, bb, bc, wsb};
   Staging st;
   MF_TRY(staging_acquire(st, sz));
   if (ba) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[0], a, ba, cudaMemcpyHostToDevice, st.stream));
   if (bb) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[1], b, bb, cudaMemcpyHostToDevice, st.stream));
   int info[3] = {0, 0, 0};
-  MF_TRY(split::run(static_cast<float64x2 *>(st.buf[0]), static_cast<float64x2 *>(st.buf[1]),
-                    static_cast<float64x2 *>(st.buf[2]), m, k, n, slices, 8.0, st.buf[3], wsb,
-                    st.stream, info));
+  if (CPLX)
+    MF_TRY(split::run_complex(static_cast<complex64x2 *>(st.buf[0]), static_cast<complex64x2 *>(st.buf[1]),
+                              static_cast<complex64x2 *>(st.buf[2]), m, k, n, slices, 8.0, st.buf[3],
+                              wsb, st.stream, info));
+  else
+    MF_TRY(split::run(static_cast<float64x2 *>(st.buf[0]), static_cast<float64x2 *>(st.buf[1]),
+                      static_cast<float64x2 *>(st.buf[2]), m, k, n, slices, 8.0, st.buf[3], wsb,
+                      st.stream, info));
   MF_TRY_CUDA(cudaMemcpyAsync(c, st.buf[2], bc, cudaMemcpyDeviceToHost, st.stream));
   MF_TRY_CUDA(cudaStreamSynchronize(st.stream));
   if (bound_out) {
@@ -862,7 +973,24 @@ MULTIFLOATS_CUDA_API int mfcuda_phase_profile_end(double *phase_ms_sum, int64_t 
 
 MULTIFLOATS_CUDA_API size_t mfcuda_split_workspace_size(int64_t m, int64_t k, int64_t n) {
   if (m < 0 || k < 0 || n < 0) return 0;
-  return mfcuda::split::workspace_size(m, k, n);
+  return mfcuda::split::workspace_size(m, k, n, false);
+}
+MULTIFLOATS_CUDA_API size_t mfcuda_csplit_workspace_size(int64_t m, int64_t k, int64_t n) {
+  if (m < 0 || k < 0 || n < 0) return 0;
+  return mfcuda::split::workspace_size(m, k, n, true);
+}
+MULTIFLOATS_CUDA_API int mfcuda_cmatmuldd_mm_split(const complex64x2 *a, const complex64x2 *b,
+                                                   complex64x2 *c, int64_t m, int64_t k, int64_t n,
+                                                   int slices, double target, void *workspace,
+                                                   size_t workspace_bytes, int *info_out,
+                                                   void *stream) {
+  return mfcuda::split::run_complex(a, b, c, m, k, n, slices, target, workspace, workspace_bytes,
+                                    mfcuda::as_stream(stream), info_out);
+}
+MULTIFLOATS_CUDA_API void cmatmuldd_mm_split(const complex64x2 *a, const complex64x2 *b,
+                                             complex64x2 *c, int64_t m, int64_t k, int64_t n,
+                                             int slices, double *max_err_bound_out) {
+  mfcuda::set_last_error(mfcuda::split_host<true>(a, b, c, m, k, n, slices, max_err_bound_out));
 }
 
 MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_split(const float64x2 *a, const float64x2 *b,
@@ -877,7 +1005,7 @@ MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_split(const float64x2 *a, const floa
 MULTIFLOATS_CUDA_API void matmuldd_mm_split(const float64x2 *a, const float64x2 *b, float64x2 *c,
                                             int64_t m, int64_t k, int64_t n, int slices,
                                             double *max_err_bound_out) {
-  mfcuda::set_last_error(mfcuda::split_host(a, b, c, m, k, n, slices, max_err_bound_out));
+  mfcuda::set_last_error(mfcuda::split_host<false>(a, b, c, m, k, n, slices, max_err_bound_out));
 }
 
 }  // extern "C"

@@ -935,3 +935,52 @@ void orc_split_gemm(const double *a, const double *b, double *c, int64_t m, int6
     }
   free(sa); free(ma); free(fa); free(sb); free(mb); free(fb); free(da); free(db);
 }
+
+/* Complex split GEMM: re = Ar Br - Ai Bi, im = Ar Bi + Ai Br, each real
+ * product by orc_split_gemm with one slice count S chosen from the exponent
+ * spreads of all four operands (A side: Ar, Ai rows; B side: Br, Bi columns). */
+void orc_split_cgemm(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
+                     int S_req, double target, int *info) {
+  double *ar = malloc(sizeof(double) * 2 * m * k), *ai = malloc(sizeof(double) * 2 * m * k);
+  double *br = malloc(sizeof(double) * 2 * k * n), *bi = malloc(sizeof(double) * 2 * k * n);
+  for (int64_t e = 0; e < m * k; ++e) {
+    ar[2 * e] = a[4 * e]; ar[2 * e + 1] = a[4 * e + 1];
+    ai[2 * e] = a[4 * e + 2]; ai[2 * e + 1] = a[4 * e + 3];
+  }
+  for (int64_t e = 0; e < k * n; ++e) {
+    br[2 * e] = b[4 * e]; br[2 * e + 1] = b[4 * e + 1];
+    bi[2 * e] = b[4 * e + 2]; bi[2 * e + 1] = b[4 * e + 3];
+  }
+  int ra = 0, rb = 0;
+  for (int part = 0; part < 2; ++part) {
+    const double *x = part ? ai : ar, *y = part ? bi : br;
+    for (int64_t i = 0; i < m; ++i) {
+      int sg, mu, bad;
+      split_stats(x + 2 * i, k, m, &sg, &mu, &bad);
+      if (sg != -100000 && sg - mu > ra) ra = sg - mu;
+    }
+    for (int64_t j = 0; j < n; ++j) {
+      int sg, mu, bad;
+      split_stats(y + 2 * j * k, k, 1, &sg, &mu, &bad);
+      if (sg != -100000 && sg - mu > rb) rb = sg - mu;
+    }
+  }
+  int S = orc_split_plan(S_req, target, ra, rb);
+  if (info) {
+    info[0] = S;
+    info[1] = ra;
+    info[2] = rb;
+  }
+  double *rr = malloc(sizeof(double) * 2 * m * n), *ii = malloc(sizeof(double) * 2 * m * n);
+  double *ri = malloc(sizeof(double) * 2 * m * n), *ir = malloc(sizeof(double) * 2 * m * n);
+  orc_split_gemm(ar, br, rr, m, k, n, S, target, NULL);
+  orc_split_gemm(ai, bi, ii, m, k, n, S, target, NULL);
+  orc_split_gemm(ar, bi, ri, m, k, n, S, target, NULL);
+  orc_split_gemm(ai, br, ir, m, k, n, S, target, NULL);
+  for (int64_t e = 0; e < m * n; ++e) {
+    dd re = dd_sub(mk(rr[2 * e], rr[2 * e + 1]), mk(ii[2 * e], ii[2 * e + 1]));
+    dd im = dd_add(mk(ri[2 * e], ri[2 * e + 1]), mk(ir[2 * e], ir[2 * e + 1]));
+    c[4 * e] = re.hi; c[4 * e + 1] = re.lo; c[4 * e + 2] = im.hi; c[4 * e + 3] = im.lo;
+  }
+  free(ar); free(ai); free(br); free(bi); free(rr); free(ii); free(ri); free(ir);
+}

@@ -62,6 +62,7 @@ def orc():
         L.orc_reduce_error.argtypes = [C.c_int, P, P, I64, P, P, P]
         L.orc_split_gemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
         L.orc_split_plan.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int]
+        L.orc_split_cgemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
         _orc = L
     return _orc
 
@@ -190,6 +191,15 @@ def split_gemm(a, b, m, k, n, slices=0, target=8.0):
     c = np.empty(2 * m * n)
     info = np.zeros(3, dtype=np.int32)
     orc().orc_split_gemm(_p(a), _p(b), _p(c), m, k, n, slices, target, info.ctypes.data)
+    return c, tuple(int(v) for v in info)
+
+
+def split_cgemm(a, b, m, k, n, slices=0, target=8.0):
+    """Complex split-INT8 product restated on the CPU; returns (C, (S, rho_a, rho_b))."""
+    a, b = _c(a), _c(b)
+    c = np.empty(4 * m * n)
+    info = np.zeros(3, dtype=np.int32)
+    orc().orc_split_cgemm(_p(a), _p(b), _p(c), m, k, n, slices, target, info.ctypes.data)
     return c, tuple(int(v) for v in info)
 
 

@@ -130,3 +130,72 @@ def test_invalid_split_arguments(cuda_lib):
     assert cuda_lib.mfcuda_matmuldd_mm_split(None, None, None, -1, 2, 2, 0, 8.0, None, 0, None, None) == 1
     assert cuda_lib.mfcuda_matmuldd_mm_split(None, None, None, 2, 2, 2, 15, 8.0, None, 0, None, None) == 1
     assert cuda_lib.mfcuda_matmuldd_mm_split(None, None, None, 2, 2, 2, 0, 0.0, None, 0, None, None) == 1
+
+
+# ---- complex64x2 split form (four real products, Fortran composition) ----
+def _cplx(m, k, R, per, seed):
+    return W.complex_from_parts(W.dd_rowcol_scaled(m, k, R, per, seed),
+                                W.dd_rowcol_scaled(m, k, R, per, seed + 1000))
+
+
+def dev_csplit(L, dev, A, B, m, k, n, slices=0):
+    import torch
+
+    a, b = to_dev(A, dev), to_dev(B, dev)
+    c = torch.empty(4 * m * n, dtype=torch.float64, device=dev)
+    info = (C.c_int * 3)()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = L.mfcuda_cmatmuldd_mm_split(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, k, n, slices, 8.0,
+                                     None, 0, info, stream)
+    assert rc == 0, rc
+    return to_host(c), tuple(info)
+
+
+def _embed(A, B, m, k, n):
+    """Exact real embeddings: Re(AB) = [Ar | -Ai][Br; Bi], Im(AB) = [Ar | Ai][Bi; Br]
+    (column-major, DD interleaved)."""
+    a = A.reshape(k, m, 4)
+    b = B.reshape(n, k, 4)
+    ar, ai = a[..., 0:2], a[..., 2:4]
+    br, bi = b[..., 0:2], b[..., 2:4]
+    a_re = np.concatenate([ar, -ai], axis=0).reshape(-1)
+    a_im = np.concatenate([ar, ai], axis=0).reshape(-1)
+    b_re = np.concatenate([br, bi], axis=1).reshape(-1)
+    b_im = np.concatenate([bi, br], axis=1).reshape(-1)
+    return (a_re, b_re), (a_im, b_im)
+
+
+@pytest.mark.parametrize("shape", [(64, 100, 48), (130, 200, 257), (1, 3, 1)])
+def test_complex_split_bit_exact(cuda_lib, dev, shape):
+    m, k, n = shape
+    A, B = _cplx(m, k, 16, "row", 1), _cplx(k, n, 16, "col", 2)
+    got, info = dev_csplit(cuda_lib, dev, A, B, m, k, n)
+    want, winfo = O.split_cgemm(A, B, m, k, n)
+    assert info == winfo
+    assert O.same_bits(got, want).all()
+
+
+def test_complex_split_error_bound(cuda_lib, dev):
+    m, k, n = 256, 512, 192
+    A, B = _cplx(m, k, 16, "row", 3), _cplx(k, n, 16, "col", 4)
+    got, _ = dev_csplit(cuda_lib, dev, A, B, m, k, n)
+    g = got.reshape(n, m, 4)
+    rng = np.random.default_rng(0)
+    ii, jj = rng.integers(0, m, 200), rng.integers(0, n, 200)
+    for part, (ae, be) in enumerate(_embed(A, B, m, k, n)):
+        cpart = np.ascontiguousarray(g[..., 2 * part: 2 * part + 2]).reshape(-1)
+        err, ab = O.gemm_errors(ae, be, cpart, m, 2 * k, n, ii, jj)
+        assert (np.abs(err) / (k * ULP * ab)).max() <= 8.0
+        assert (np.abs(err) / (ULP * ab)).max() <= 1.0
+
+
+def test_complex_split_host_dropin(cuda_lib):
+    m, k, n = 70, 90, 50
+    A, B = _cplx(m, k, 4, "row", 5), _cplx(k, n, 4, "col", 6)
+    c = np.empty(4 * m * n)
+    bound = C.c_double(-1.0)
+    cuda_lib.cmatmuldd_mm_split(A.ctypes.data, B.ctypes.data, c.ctypes.data, m, k, n, 0, C.byref(bound))
+    assert cuda_lib.mfcuda_last_error() == 0
+    want, _ = O.split_cgemm(A, B, m, k, n)
+    assert O.same_bits(c, want).all()
+    assert 0.0 < bound.value <= 8.0
