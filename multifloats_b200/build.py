@@ -30,7 +30,7 @@ SOURCES = [
     "reduce_dd.cu",
     "split_gemm.cu",
 ]
-HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh"]
+HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh", "split_device.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
