@@ -246,6 +246,57 @@ MULTIFLOATS_CUDA_API int mfcuda_dotdd_noalloc(const float64x2 *a, const float64x
                                               int64_t renorm_interval, float64x2 *out,
                                               void *stream);
 
+/* ---- batched ragged work ---------------------------------------------------
+ * Many independent problems in grouped launches captured once in a CUDA graph
+ * (no reference counterpart; each problem computes what the single call
+ * computes, bit for bit).  A plan binds the problems' DEVICE pointers at
+ * creation; mfcuda_batch_run replays the graph on a stream (refill the same
+ * buffers between runs, or create a new plan for new buffers).
+ *   form MFCUDA_FORM_PLAIN: one persistent grouped kernel over every output
+ *     tile of every problem (longest K first, dynamic scheduling); per problem a
+ *     tile shape of 64x64, 32x32 or 16x16 outputs.  renorm_interval as in
+ *     matmuldd_mm; slices/target unused.
+ *   form MFCUDA_FORM_SPLIT: the split-INT8 pipeline, each phase one grouped
+ *     launch; one persistent tcgen05 kernel over every (diagonal, K chunk, tile)
+ *     item of every problem; per problem a tile width N of 256, 128 or 64 and a
+ *     shared K chunk (split-K when the batch is too small to fill the GPU);
+ *     slices/target as in mfcuda_matmuldd_mm_split.  Operands 16-byte aligned.
+ * tune != 0 times the candidate tile shapes of every new shape bucket on
+ * synthetic problems and caches the winners in MFCUDA_AUTOTUNE_CACHE (default
+ * $HOME/.cache/multifloats_b200/autotune.txt); tune == 0 uses cached winners or
+ * a built-in heuristic. */
+typedef struct mfcuda_gemm_desc {
+  const void *a; /* float64x2, column-major m x k */
+  const void *b; /* float64x2, column-major k x n */
+  void *c;       /* float64x2, column-major m x n (overwritten) */
+  int64_t m, k, n;
+} mfcuda_gemm_desc;
+typedef struct mfcuda_batch mfcuda_batch;
+enum { MFCUDA_FORM_PLAIN = 0, MFCUDA_FORM_SPLIT = 1 };
+MULTIFLOATS_CUDA_API int mfcuda_batch_create_gemm(const mfcuda_gemm_desc *descs, int64_t count,
+                                                  int form, int64_t renorm_interval, int slices,
+                                                  double target, int tune, mfcuda_batch **plan);
+/* Ragged elementwise batch: y_a[i] = op(x_a[i]) for every array a (lengths
+ * ns[a], device pointers), one grid-stride launch over all elements. */
+MULTIFLOATS_CUDA_API int mfcuda_batch_create_unary(int op, const float64x2 *const *xs,
+                                                   float64x2 *const *ys, const int64_t *ns,
+                                                   int64_t count, mfcuda_batch **plan);
+MULTIFLOATS_CUDA_API int mfcuda_batch_run(mfcuda_batch *plan, void *stream);
+/* Waits for the device and reports MFCUDA_ERR_TIMEOUT if a bounded device-side
+ * wait of the plan's last run expired. */
+MULTIFLOATS_CUDA_API int mfcuda_batch_status(mfcuda_batch *plan);
+/* Tile edge (plain) or tile width N (split) chosen for problem i; -1 if none. */
+MULTIFLOATS_CUDA_API int64_t mfcuda_batch_config(const mfcuda_batch *plan, int64_t i);
+/* Work items of the plan's main grouped launch (tiles, diagonal items or elements). */
+MULTIFLOATS_CUDA_API int64_t mfcuda_batch_work_items(const mfcuda_batch *plan);
+/* Split form: the K chunk (elements) whose INT32 partials are summed in DD; -1 otherwise. */
+MULTIFLOATS_CUDA_API int64_t mfcuda_batch_kchunk(const mfcuda_batch *plan);
+MULTIFLOATS_CUDA_API void mfcuda_batch_destroy(mfcuda_batch *plan);
+/* One-shot ragged elementwise call on a stream (no plan, no graph). */
+MULTIFLOATS_CUDA_API int mfcuda_unary_dd_ragged(int op, const float64x2 *const *xs,
+                                                float64x2 *const *ys, const int64_t *ns,
+                                                int64_t count, void *stream);
+
 /* Fixed launch geometry of the reductions for a given n (it depends on n only,
  * never on the device), exposed so a CPU restatement can follow the same order:
  * *blocks = number of thread blocks, *threads = threads per block. */

@@ -23,6 +23,13 @@ class complex64x2(C.Structure):
     _fields_ = [("re", float64x2), ("im", float64x2)]
 
 
+class gemm_desc(C.Structure):
+    """mfcuda_gemm_desc: device pointers and sizes of one batched product."""
+
+    _fields_ = [("a", C.c_void_p), ("b", C.c_void_p), ("c", C.c_void_p),
+                ("m", C.c_int64), ("k", C.c_int64), ("n", C.c_int64)]
+
+
 class MFCudaError(RuntimeError):
     def __init__(self, code: int, where: str):
         self.code = code
@@ -63,6 +70,15 @@ SIGNATURES = {
     "mfcuda_cmatmuldd_mm_split": (C.c_int, [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, C.c_size_t,
                                             P, P]),
     "cmatmuldd_mm_split": (None, [P, P, P, I64, I64, I64, C.c_int, C.POINTER(C.c_double)]),
+    "mfcuda_batch_create_gemm": (C.c_int, [P, I64, C.c_int, I64, C.c_int, C.c_double, C.c_int, C.POINTER(P)]),
+    "mfcuda_batch_create_unary": (C.c_int, [C.c_int, P, P, P, I64, C.POINTER(P)]),
+    "mfcuda_batch_run": (C.c_int, [P, P]),
+    "mfcuda_batch_status": (C.c_int, [P]),
+    "mfcuda_batch_config": (I64, [P, I64]),
+    "mfcuda_batch_work_items": (I64, [P]),
+    "mfcuda_batch_kchunk": (I64, [P]),
+    "mfcuda_batch_destroy": (None, [P]),
+    "mfcuda_unary_dd_ragged": (C.c_int, [C.c_int, P, P, P, I64, P]),
     "mfcuda_phase_profile_begin": (None, []),
     "mfcuda_phase_profile_end": (C.c_int, [C.POINTER(C.c_double), C.POINTER(I64)]),
     "mfcuda_matmuldd_mm_split": (C.c_int, [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, C.c_size_t,

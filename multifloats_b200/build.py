@@ -29,8 +29,9 @@ SOURCES = [
     "gemm_dd.cu",
     "reduce_dd.cu",
     "split_gemm.cu",
+    "batched.cu",
 ]
-HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh", "split_device.cuh"]
+HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh", "split_device.cuh", "gemm_tile.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [

@@ -19,151 +19,28 @@
 // 13 FP64 instructions per MAC plus 6 per renormalisation.
 #include "common.cuh"
 #include "dd_device.cuh"
+#include "gemm_tile.cuh"
 
 namespace mfcuda {
 
-namespace {
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-// 16-byte async copy; src_bytes = 0 zero-fills the destination.
-__device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
-               "r"(src_bytes));
-}
-__device__ __forceinline__ void cp_async8(void *dst, const void *src, int src_bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
-               "r"(src_bytes));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
-
-// Copy one DD (16 bytes) or zero-fill it.  `safe` is an in-bounds address
-// (the matrix base) handed to the copy when nothing is read.
-template <bool ALIGNED>
-__device__ __forceinline__ void load_dd(double2 *dst, const double *src, bool valid,
-                                        const double *safe) {
-  if constexpr (ALIGNED) {
-    cp_async16(dst, valid ? src : safe, valid ? 16 : 0);
-  } else {
-    double *d = reinterpret_cast<double *>(dst);
-    cp_async8(d, valid ? src : safe, valid ? 8 : 0);
-    cp_async8(d + 1, valid ? src + 1 : safe, valid ? 8 : 0);
-  }
-}
-
-}  // namespace
+using gtile::load_dd;
+using gtile::cp_async_commit;
+using gtile::cp_async_wait_all;
 
 // ---------------------------------------------------------------------------
-// Real GEMM.  Thread t owns rows tx + 16*i (i < TM) and columns ty + 16*j
-// (j < TN) of the CTA tile, tx = t % 16, ty = t / 16.
+// Real GEMM: one 64 x 64 tile per CTA (4 x 4 outputs per thread).
 // ---------------------------------------------------------------------------
-constexpr int kThreads = 256;
+constexpr int kThreads = gtile::kThreads;
 constexpr int kTM = 4, kTN = 4;
-constexpr int kBM = 16 * kTM, kBN = 16 * kTN, kBK = 8;
+constexpr int kBM = 16 * kTM, kBN = 16 * kTN;
 
 template <bool ALIGNED>
 __global__ void __launch_bounds__(kThreads, 2)
     gemm_dd_kernel(const double *__restrict__ A, const double *__restrict__ B,
                    double *__restrict__ C, int64_t M, int64_t K, int64_t N, int64_t ri) {
-  __shared__ double2 As[2][kBK][kBM];
-  __shared__ double2 Bs[2][kBK][kBN];
-  const int t = threadIdx.x;
-  const int tx = t % 16, ty = t / 16;
-  const int64_t m0 = (int64_t)blockIdx.x * kBM;
-  const int64_t n0 = (int64_t)blockIdx.y * kBN;
-
-  double s_hi[kTM][kTN], s_lo[kTM][kTN];
-#pragma unroll
-  for (int i = 0; i < kTM; ++i)
-#pragma unroll
-    for (int j = 0; j < kTN; ++j) s_hi[i][j] = s_lo[i][j] = 0.0;
-
-  auto issue = [&](int stage, int64_t k0) {
-#pragma unroll
-    for (int r = 0; r < (kBK * kBM) / kThreads; ++r) {
-      int idx = t + r * kThreads;
-      int row = idx % kBM, kk = idx / kBM;
-      int64_t gi = m0 + row, gk = k0 + kk;
-      bool v = gi < M && gk < K;
-      load_dd<ALIGNED>(&As[stage][kk][row], A + 2 * (gk * M + gi), v, A);
-    }
-#pragma unroll
-    for (int r = 0; r < (kBK * kBN) / kThreads; ++r) {
-      int idx = t + r * kThreads;
-      int kk = idx % kBK, col = idx / kBK;
-      int64_t gj = n0 + col, gk = k0 + kk;
-      bool v = gj < N && gk < K;
-      load_dd<ALIGNED>(&Bs[stage][kk][col], B + 2 * (gj * K + gk), v, B);
-    }
-    cp_async_commit();
-  };
-
-  const int64_t ntiles = (K + kBK - 1) / kBK;
-  int64_t cnt = 0;
-  if (ntiles > 0) issue(0, 0);
-  for (int64_t kt = 0; kt < ntiles; ++kt) {
-    const int stage = (int)(kt & 1);
-    cp_async_wait_all();
-    __syncthreads();
-    if (kt + 1 < ntiles) issue(stage ^ 1, (kt + 1) * kBK);
-    const int64_t k0 = kt * kBK;
-    const int kmax = (K - k0) < kBK ? (int)(K - k0) : kBK;
-#pragma unroll
-    for (int kk = 0; kk < kBK; ++kk) {
-      if (kk < kmax) {
-        double ah[kTM], al[kTM], bh[kTN], bl[kTN];
-#pragma unroll
-        for (int i = 0; i < kTM; ++i) {
-          double2 v = As[stage][kk][tx + 16 * i];
-          ah[i] = v.x;
-          al[i] = v.y;
-        }
-#pragma unroll
-        for (int j = 0; j < kTN; ++j) {
-          double2 v = Bs[stage][kk][ty + 16 * j];
-          bh[j] = v.x;
-          bl[j] = v.y;
-        }
-#pragma unroll
-        for (int j = 0; j < kTN; ++j)
-#pragma unroll
-          for (int i = 0; i < kTM; ++i) mfdev::mac(ah[i], al[i], bh[j], bl[j], s_hi[i][j], s_lo[i][j]);
-        if (ri > 0) {
-          if (++cnt == ri) {
-            cnt = 0;
-            if (k0 + kk + 1 < K) {
-#pragma unroll
-              for (int i = 0; i < kTM; ++i)
-#pragma unroll
-                for (int j = 0; j < kTN; ++j) mfdev::renorm(s_hi[i][j], s_lo[i][j]);
-            }
-          }
-        }
-      }
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int j = 0; j < kTN; ++j) {
-    int64_t gj = n0 + ty + 16 * j;
-#pragma unroll
-    for (int i = 0; i < kTM; ++i) {
-      int64_t gi = m0 + tx + 16 * i;
-      double h = s_hi[i][j], l = s_lo[i][j];
-      mfdev::renorm(h, l);
-      if (gi < M && gj < N) {
-        double *dst = C + 2 * (gj * M + gi);
-        if constexpr (ALIGNED) {
-          *reinterpret_cast<double2 *>(dst) = make_double2(h, l);
-        } else {
-          dst[0] = h;
-          dst[1] = l;
-        }
-      }
-    }
-  }
+  __shared__ gtile::Smem sm;
+  gtile::gemm_tile<kTM, kTN, ALIGNED>(A, B, C, M, K, N, ri, (int64_t)blockIdx.x * kBM,
+                                      (int64_t)blockIdx.y * kBN, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -171,7 +48,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 // per output (rr, ii, ri, ir).
 // ---------------------------------------------------------------------------
 constexpr int kCTM = 2, kCTN = 2;
-constexpr int kCBM = 16 * kCTM, kCBN = 16 * kCTN, kCBK = 8;
+constexpr int kCBM = 16 * kCTM, kCBN = 16 * kCTN, kCBK = gtile::kBK;
 
 template <bool ALIGNED>
 __global__ void __launch_bounds__(kThreads, 2)

@@ -4,6 +4,7 @@
 #pragma once
 #include <cstdint>
 
+#include "dd_device.cuh"
 #include "tcgen05.cuh"
 
 namespace mfcuda {
@@ -105,6 +106,268 @@ __device__ __forceinline__ void dd_digits(double hi, double lo, int sigma, int W
     v = (v ^ 0x80) - 0x80;
     d[q] = (int8_t)v;
     xh = (xh - v) >> 8;
+  }
+}
+
+// Operands are read through strided views: DD element e of a view lives at
+// double2 index e * stride from its base (stride 1 for a real matrix, 2 for the
+// real or imaginary part of a complex one).
+//
+// A column-major m x k: thread per row, a chunk of columns per blockIdx.y.
+__device__ __forceinline__ void scan_a_body(const double *__restrict__ A, int64_t M,
+                                                     int64_t K, int64_t stride, int kchunk, int *sig,
+                                                     int *mu, int *flag, int64_t bx, int64_t by) {
+  int64_t i = bx * blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  int64_t p0 = by * kchunk, p1 = p0 + kchunk < K ? p0 + kchunk : K;
+  int hi_e = SENT_LO, lo_e = SENT_HI, bad = 0;
+  for (int64_t p = p0; p < p1; ++p) {
+    double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i) * stride);
+    if (!isfinite(v.x) || !isfinite(v.y)) {
+      bad = 1;
+      continue;
+    }
+    double a = fabs(v.x) + fabs(v.y);
+    if (a != 0.0) {
+      hi_e = max(hi_e, binade_above(a));
+      lo_e = min(lo_e, binade_below(a));
+    }
+  }
+  if (hi_e != SENT_LO) atomicMax(&sig[i], hi_e);
+  if (lo_e != SENT_HI) atomicMin(&mu[i], lo_e);
+  if (bad) atomicOr(&flag[i], 1);
+}
+
+// B column-major k x n: a block per (column j, chunk of 2048 rows).
+__device__ __forceinline__ void scan_b_body(const double *__restrict__ B, int64_t K,
+                                                     int64_t N, int64_t stride, int *sig, int *mu,
+                                                     int *flag, int64_t bx, int64_t by) {
+  int64_t j = by;
+  int64_t p0 = bx * 2048;
+  int hi_e = SENT_LO, lo_e = SENT_HI, bad = 0;
+  for (int r = 0; r < 8; ++r) {
+    int64_t p = p0 + threadIdx.x + 256 * r;
+    if (p >= K) break;
+    double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p) * stride);
+    if (!isfinite(v.x) || !isfinite(v.y)) {
+      bad = 1;
+      continue;
+    }
+    double a = fabs(v.x) + fabs(v.y);
+    if (a != 0.0) {
+      hi_e = max(hi_e, binade_above(a));
+      lo_e = min(lo_e, binade_below(a));
+    }
+  }
+  for (int off = 16; off >= 1; off >>= 1) {
+    hi_e = max(hi_e, __shfl_xor_sync(0xffffffffu, hi_e, off));
+    lo_e = min(lo_e, __shfl_xor_sync(0xffffffffu, lo_e, off));
+    bad |= __shfl_xor_sync(0xffffffffu, bad, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (hi_e != SENT_LO) atomicMax(&sig[j], hi_e);
+    if (lo_e != SENT_HI) atomicMin(&mu[j], lo_e);
+    if (bad) atomicOr(&flag[j], 1);
+  }
+}
+
+// Exponent statistics of the operands of one call: A-side operands (rows of
+// an m x k matrix) and B-side operands (columns of a k x n matrix).
+struct StatSet {
+  int *sig[4];
+  const int *mu[4];
+  int64_t count[4];
+  int side[4];  // 0: A side, 1: B side
+  int n;
+};
+
+__device__ __forceinline__ void plan_body(const StatSet &st, int slices, double target, Plan *plan) {
+  __shared__ int red[2][32];
+  int r[2] = {0, 0};
+  for (int o = 0; o < st.n; ++o)
+    for (int64_t i = threadIdx.x; i < st.count[o]; i += blockDim.x)
+      if (st.sig[o][i] != SENT_LO) r[st.side[o]] = max(r[st.side[o]], st.sig[o][i] - st.mu[o][i]);
+  int ra = r[0], rb = r[1];
+  for (int off = 16; off >= 1; off >>= 1) {
+    ra = max(ra, __shfl_xor_sync(0xffffffffu, ra, off));
+    rb = max(rb, __shfl_xor_sync(0xffffffffu, rb, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = ra;
+    red[1][threadIdx.x >> 5] = rb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      ra = max(ra, red[0][w]);
+      rb = max(rb, red[1][w]);
+    }
+    int S = slices;
+    if (S <= 0) {
+      // smallest S with (S+1) 2^(106 - 8S + rho_a + rho_b) <= target
+      S = SMAX;
+      for (int q = 2; q <= SMAX; ++q) {
+        double ratio = (q + 1) * ldexp(1.0, 106 - 8 * q + ra + rb);
+        if (ratio <= target) {
+          S = q;
+          break;
+        }
+      }
+    }
+    plan->S = S;
+    plan->G = S - 1;
+    plan->W = 8 * S - 2;
+    plan->rho_a = ra;
+    plan->rho_b = rb;
+  }
+  // zero rows / columns: any sigma works, the digits are all zero
+  __syncthreads();
+  for (int o = 0; o < st.n; ++o)
+    for (int64_t i = threadIdx.x; i < st.count[o]; i += blockDim.x)
+      if (st.sig[o][i] == SENT_LO) st.sig[o][i] = 0;
+}
+
+// A (m x k column-major) -> As[s][i][p]: a block covers 32 rows x 64
+// columns; thread (i = t % 32, group = t / 32) rounds and slices the 8
+// consecutive entries A[i, p0 + 8 group .. + 7] (coalesced across i), packs
+// the 8 digits of each slice into one 64-bit word, and the tile is transposed
+// through shared memory (row stride padded to 72 bytes: conflict-free) so
+// that every slice row is written as contiguous 8-byte words.
+constexpr int SA_ROWS = 32, SA_COLS = 64, SA_STRIDE = 72;
+__device__ __forceinline__ void slice_a_body(const double *__restrict__ A, int64_t M,
+                                                      int64_t K, int64_t stride, int64_t M_pad,
+                                                      int64_t K_pad, const int *sig, const int *flag,
+                                                      const Plan *plan, int8_t *__restrict__ As, int64_t bx, int64_t by) {
+  __shared__ __align__(16) uint8_t tile[SMAX][SA_ROWS * SA_STRIDE];
+  const int S = plan->S, W = plan->W;
+  const int64_t i0 = bx * SA_ROWS, p0 = by * SA_COLS;
+  const int t = threadIdx.x;
+  const int ii = t % SA_ROWS, grp = t / SA_ROWS;
+  const int64_t i = i0 + ii;
+  const bool row_ok = i < M && !flag[i < M ? i : 0];
+  const int sigma = i < M ? sig[i] : 0;
+  uint64_t words[SMAX];
+#pragma unroll
+  for (int q = 0; q < SMAX; ++q) words[q] = 0;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int64_t p = p0 + grp * 8 + e;
+    if (row_ok && p < K) {
+      double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i) * stride);
+      int8_t d[SMAX];
+      dd_digits(v.x, v.y, sigma, W, d);
+#pragma unroll
+      for (int q = 0; q < SMAX; ++q) words[q] |= (uint64_t)(uint8_t)d[q] << (8 * e);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < SMAX; ++q)
+    if (q >= SMAX - S)
+      *reinterpret_cast<uint64_t *>(&tile[q - (SMAX - S)][ii * SA_STRIDE + grp * 8]) = words[q];
+  __syncthreads();
+  const int row = t / 8, seg = (t % 8) * 8;
+  for (int s = 0; s < S; ++s) {
+    uint64_t v = *reinterpret_cast<const uint64_t *>(&tile[s][row * SA_STRIDE + seg]);
+    *reinterpret_cast<uint64_t *>(As + ((s * M_pad + i0 + row) * K_pad + p0 + seg)) = v;
+  }
+}
+
+// B (k x n column-major) -> Bs[s][j][p]: each thread rounds and slices 8
+// consecutive entries of one column (128 contiguous bytes in, one 8-byte word
+// per slice out).
+__device__ __forceinline__ void slice_b_body(const double *__restrict__ B, int64_t K,
+                                                      int64_t N, int64_t stride, int64_t N_pad,
+                                                      int64_t K_pad, const int *sig, const int *flag,
+                                                      const Plan *plan, int8_t *__restrict__ Bs, int64_t bx, int64_t by) {
+  const int S = plan->S, W = plan->W;
+  const int64_t j = by;
+  const int64_t p8 = (bx * blockDim.x + threadIdx.x) * 8;
+  if (p8 >= K_pad) return;
+  const bool col_ok = j < N && !flag[j < N ? j : 0];
+  const int tau = j < N ? sig[j] : 0;
+  uint64_t words[SMAX];
+#pragma unroll
+  for (int q = 0; q < SMAX; ++q) words[q] = 0;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int64_t p = p8 + e;
+    if (col_ok && p < K) {
+      double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p) * stride);
+      int8_t d[SMAX];
+      dd_digits(v.x, v.y, tau, W, d);
+#pragma unroll
+      for (int q = 0; q < SMAX; ++q) words[q] |= (uint64_t)(uint8_t)d[q] << (8 * e);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < SMAX; ++q)
+    if (q >= SMAX - S)
+      *reinterpret_cast<uint64_t *>(Bs + (((int64_t)(q - (SMAX - S)) * N_pad + j) * K_pad + p8)) = words[q];
+}
+
+// Thread per row i (consecutive threads -> consecutive rows: every load and
+// store is coalesced); the grid's y dimension strides over the columns.  The
+// output is a strided view (C element (i,j) at double2 index (jM + i) cstride)
+// and `mode` stores the product P (0), or replaces C by the DD difference
+// C - P (1) or sum C + P (2), which assembles complex products.
+__device__ __forceinline__ void combine_body(const int32_t *__restrict__ D, const Plan *plan,
+                                                      const int *sigA, const int *flagA,
+                                                      const int *sigB, const int *flagB, int64_t M,
+                                                      int64_t N, int64_t M_pad, int64_t N_pad,
+                                                      int nkc, double *__restrict__ C, int64_t cstride,
+                                                      int mode, int64_t bx, int64_t by, int64_t ny) {
+  const int G = plan->G;
+  const int64_t i = bx * blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  const int64_t gstride = (int64_t)nkc * N_pad * M_pad;  // distance between diagonals
+  const int sa = sigA[i], fa = flagA[i];
+  // two columns per pass: 2 x (G+1) independent loads in flight per thread
+  for (int64_t j0 = by; j0 < N; j0 += 2 * ny) {
+    const int64_t jj[2] = {j0, j0 + ny};
+    double hi[2] = {0.0, 0.0}, lo[2] = {0.0, 0.0};
+    for (int kc = 0; kc < nkc; ++kc) {
+      int32_t v[2][SMAX];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int32_t *src = D + ((int64_t)kc * N_pad + (jj[c] < N ? jj[c] : j0)) * M_pad + i;
+#pragma unroll
+        for (int g = 0; g < SMAX; ++g) v[c][g] = g <= G ? __ldcs(src + g * gstride) : 0;
+      }
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int g = SMAX - 1; g >= 0; --g) {
+          if (g <= G) {
+            double tv = mfdev::mul((double)v[c][g], ldexp(1.0, -8 * g));  // exact
+            double s_, err;
+            mfdev::two_sum(hi[c], tv, s_, err);
+            hi[c] = s_;
+            lo[c] = mfdev::add(lo[c], err);
+          }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int64_t j = jj[c];
+      if (j >= N) break;
+      double h, l;
+      mfdev::two_sum(hi[c], lo[c], h, l);
+      double2 out;
+      if (fa | flagB[j]) {
+        out = make_double2(CUDART_NAN, 0.0);
+      } else {
+        int ex = sa + sigB[j] - 12;
+        out = make_double2(ldexp(h, ex), ldexp(l, ex));
+      }
+      double2 *dst = reinterpret_cast<double2 *>(C) + (j * M + i) * cstride;
+      if (mode != 0) {
+        double2 prev = *dst;
+        mfdev::dd p = mfdev::make(out.x, out.y), q = mfdev::make(prev.x, prev.y);
+        mfdev::dd r = mode == 1 ? mfdev::dd_sub(q, p) : mfdev::dd_add(q, p);
+        out = make_double2(r.hi, r.lo);
+      }
+      __stcs(dst, out);
+    }
   }
 }
 

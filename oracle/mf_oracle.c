@@ -860,9 +860,15 @@ int orc_split_plan(int S_req, double target, int rho_a, int rho_b) {
     if ((s + 1) * ldexp(1.0, 106 - 8 * s + rho_a + rho_b) <= target) return s;
   return SPLIT_SMAX;
 }
-/* info[0..2] = S, rho_a, rho_b */
+/* info[0..2] = S, rho_a, rho_b; kc = K chunk length in elements (<= SPLIT_KC) */
+void orc_split_gemm_kc(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
+                       int S_req, double target, int *info, int64_t kc_len);
 void orc_split_gemm(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
                     int S_req, double target, int *info) {
+  orc_split_gemm_kc(a, b, c, m, k, n, S_req, target, info, SPLIT_KC);
+}
+void orc_split_gemm_kc(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
+                       int S_req, double target, int *info, int64_t kc_len) {
   int *sa = malloc(sizeof(int) * m), *ma = malloc(sizeof(int) * m), *fa = malloc(sizeof(int) * m);
   int *sb = malloc(sizeof(int) * n), *mb = malloc(sizeof(int) * n), *fb = malloc(sizeof(int) * n);
   int ra = 0, rb = 0;
@@ -899,7 +905,7 @@ void orc_split_gemm(const double *a, const double *b, double *c, int64_t m, int6
       split_digits(b[2 * (j * k + p)], b[2 * (j * k + p) + 1], sb[j], S, W, d);
       for (int s = 0; s < S; ++s) db[((size_t)s * n + j) * k + p] = d[s];
     }
-  int64_t nkc = (k + SPLIT_KC - 1) / SPLIT_KC;
+  int64_t nkc = (k + kc_len - 1) / kc_len;
   if (nkc < 1) nkc = 1;
   for (int64_t j = 0; j < n; ++j)
     for (int64_t i = 0; i < m; ++i) {
@@ -907,7 +913,7 @@ void orc_split_gemm(const double *a, const double *b, double *c, int64_t m, int6
       for (int64_t kc = 0; kc < nkc; ++kc) {
         for (int g = G; g >= 0; --g) {
           double scale = ldexp(1.0, -8 * g);
-          int64_t p0 = kc * SPLIT_KC, p1 = p0 + SPLIT_KC < k ? p0 + SPLIT_KC : k;
+          int64_t p0 = kc * kc_len, p1 = p0 + kc_len < k ? p0 + kc_len : k;
           int64_t D = 0;
           for (int s = 0; s <= g; ++s) {
             const int8_t *ra_ = da + ((size_t)s * m + i) * k;

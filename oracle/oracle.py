@@ -63,6 +63,7 @@ def orc():
         L.orc_split_gemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
         L.orc_split_plan.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int]
         L.orc_split_cgemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
+        L.orc_split_gemm_kc.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64]
         _orc = L
     return _orc
 
@@ -185,12 +186,13 @@ def reduce_blocked(kind: str, x, y=None, ri=8) -> np.ndarray:
     return out[:4] if kind in ("csum", "cdot") else out[:2]
 
 
-def split_gemm(a, b, m, k, n, slices=0, target=8.0):
-    """The split-INT8 algorithm restated on the CPU; returns (C, (S, rho_a, rho_b))."""
+def split_gemm(a, b, m, k, n, slices=0, target=8.0, kc=73 * 128):
+    """The split-INT8 algorithm restated on the CPU with K chunks of `kc`
+    elements; returns (C, (S, rho_a, rho_b))."""
     a, b = _c(a), _c(b)
     c = np.empty(2 * m * n)
     info = np.zeros(3, dtype=np.int32)
-    orc().orc_split_gemm(_p(a), _p(b), _p(c), m, k, n, slices, target, info.ctypes.data)
+    orc().orc_split_gemm_kc(_p(a), _p(b), _p(c), m, k, n, slices, target, info.ctypes.data, kc)
     return c, tuple(int(v) for v in info)
 
 

@@ -10,6 +10,12 @@ if ROOT not in sys.path:
 
 GOLDEN = os.path.join(ROOT, "tests", "golden", "golden.npz")
 
+# the batch autotuner's cache goes to a per-session temporary file
+if "MFCUDA_AUTOTUNE_CACHE" not in os.environ:
+    import tempfile
+
+    os.environ["MFCUDA_AUTOTUNE_CACHE"] = os.path.join(tempfile.mkdtemp(prefix="mfcuda_tune_"), "autotune.txt")
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs an sm_100 GPU (B200)")
