@@ -356,6 +356,243 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- secondary workloads
+# `--workload` lines other than the default report the other configurations of
+# the hot path (same JSON conventions; the default line is the headline).
+def _events_time(fn, steps, warmup, stream):
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _dev_dd_uniform(n, seed, dev, lo=-1.0, hi=1.0):
+    """Device-side DD uniform[lo, hi) with lo-limb hi*2^-53*U[-1,1) (then two_sum)."""
+    import torch
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    h = torch.empty(n, dtype=torch.float64, device=dev).uniform_(lo, hi, generator=g)
+    l = h * 2.0 ** -53 * torch.empty(n, dtype=torch.float64, device=dev).uniform_(-1.0, 1.0, generator=g)
+    s = h + l
+    bb = s - h
+    e = (h - (s - bb)) + (l - bb)
+    return torch.stack([s, e], dim=1).reshape(-1)
+
+
+def _line(args, workload, metric, value, unit, extra):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+         "data": "synthetic (seeded)", "config": {"workload": workload}}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def run_elementwise(args):
+    import torch
+
+    from multifloats_b200 import _lib, api
+    from multifloats_b200 import workloads as W
+    from oracle import oracle as O
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    n = 1 << 26
+    res, cpu = {}, {}
+    threads = cpu_threads()
+    for op, gen in W.ELEMENTWISE_INPUTS.items():
+        x = torch.from_numpy(gen(n, seed=1)).to(dev)
+        y = torch.empty_like(x)
+        ms = _events_time(lambda: api.unary(op, x, out=y), args.steps, args.warmup, stream)
+        res[op] = {"ms": ms, "gelem_per_s": n / ms / 1e6, "hbm_gbs": 32.0 * n / ms / 1e6}
+        del x, y
+        xs = gen(1 << 21, seed=2)
+        if O.ref_available():
+            t0 = time.perf_counter()
+            O.ref_unary(op, xs, threads=threads)
+            dt = time.perf_counter() - t0
+            cpu[op] = {"gelem_per_s": (1 << 21) / dt / 1e9, "kind": "reference", "cores": threads}
+    _line(args, "dd_elementwise_2^26", "DD elementwise G elem/s, 2^26 elements (exp/log/sin/cos/sqrt)",
+          res["exp"]["gelem_per_s"], "G elem/s (exp)",
+          {"dtype": "f64", "per_op": res, "cpu_baseline_per_op": cpu,
+           "roofline": {"bound": "fp64 (exp/log/sin/cos), hbm (sqrt)", "hbm_peak_gbs": 6546.2,
+                        "sqrt_frac_hbm": res["sqrt"]["hbm_gbs"] / 6546.2}})
+
+
+def run_reductions(args):
+    import torch
+
+    from multifloats_b200 import api
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    n = 1 << 26
+    x, y = _dev_dd_uniform(n, 1, dev), _dev_dd_uniform(n, 2, dev)
+    res = {}
+    for kind, fn, bpe in [("sum", lambda: api.sum_dd(x), 16), ("dot", lambda: api.dot_product(x, y), 32),
+                          ("norm2", lambda: api.norm2(x), 16)]:
+        ms = _events_time(fn, args.steps, args.warmup, stream)
+        res[kind] = {"ms": ms, "gbs": bpe * n / ms / 1e6, "frac_hbm": bpe * n / ms / 1e6 / 6546.2}
+    nc = 1 << 24
+    cx, cy = x[: 4 * nc], y[: 4 * nc]
+    for kind, fn, bpe in [("csum", lambda: api.csum_dd(cx), 32), ("cdot", lambda: api.cdot_product(cx, cy), 64),
+                          ("cnorm2", lambda: api.cnorm2(cx), 32)]:
+        ms = _events_time(fn, args.steps, args.warmup, stream)
+        res[kind] = {"ms": ms, "gbs": bpe * nc / ms / 1e6, "frac_hbm": bpe * nc / ms / 1e6 / 6546.2}
+    _line(args, "dd_reductions_2^26", "DD reductions GB/s (dot 2^26)", res["dot"]["gbs"], "GB/s",
+          {"dtype": "f64", "per_kind": res,
+           "roofline": {"bound": "hbm", "peak": 6546.2, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs"}})
+
+
+def _batch_descs(shapes, dev, seed):
+    import torch
+
+    from multifloats_b200 import _lib
+
+    tot = sum(m * k + k * n for m, k, n in shapes)
+    buf = _dev_dd_uniform(tot, seed, dev)
+    out = torch.empty(2 * sum(m * n for m, _, n in shapes), dtype=torch.float64, device=dev)
+    descs = (_lib.gemm_desc * len(shapes))()
+    off = oc = 0
+    for i, (m, k, n) in enumerate(shapes):
+        descs[i].a = buf[2 * off:].data_ptr()
+        off += m * k
+        descs[i].b = buf[2 * off:].data_ptr()
+        off += k * n
+        descs[i].c = out[2 * oc:].data_ptr()
+        oc += m * n
+        descs[i].m, descs[i].k, descs[i].n = m, k, n
+    return descs, (buf, out)
+
+
+def run_batched(args):
+    import torch
+
+    from multifloats_b200 import _lib
+
+    L = _lib.lib()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    rng = np.random.default_rng(2024)
+    shapes = [tuple(int(v) for v in s) for s in np.exp(rng.uniform(np.log(16), np.log(1024), (2000, 3)))]
+    flops = sum(2.0 * m * k * n for m, k, n in shapes)
+    descs, keep = _batch_descs(shapes, dev, 7)
+    res = {}
+    for form, name in ((0, "plain"), (1, "split")):
+        p = C.c_void_p()
+        t0 = time.perf_counter()
+        _lib.check(L.mfcuda_batch_create_gemm(descs, len(shapes), form, RI, 0, 8.0, 1, C.byref(p)), "batch")
+        t_create = time.perf_counter() - t0
+        ms = _events_time(lambda: _lib.check(L.mfcuda_batch_run(p, sp), "run"), max(1, args.steps // 3),
+                          args.warmup, stream)
+        _lib.check(L.mfcuda_batch_status(p), "status")
+        res[name] = {"ms": ms, "dd_gflops": flops / ms / 1e6, "work_items": L.mfcuda_batch_work_items(p),
+                     "plan_create_s": t_create}
+        L.mfcuda_batch_destroy(p)
+    del keep
+    torch.cuda.empty_cache()
+    # 10^4 ragged exp / log arrays, lengths log-uniform in [64, 2^20]
+    lens = [int(v) for v in np.exp(rng.uniform(np.log(64), np.log(1 << 20), 10000))]
+    tot = sum(lens)
+    x = _dev_dd_uniform(tot, 9, dev, 0.5, 2.0)
+    yv = torch.empty_like(x)
+    offs = np.concatenate([[0], np.cumsum(lens)])
+    X = (C.c_void_p * len(lens))(*[x[2 * int(o):].data_ptr() for o in offs[:-1]])
+    Y = (C.c_void_p * len(lens))(*[yv[2 * int(o):].data_ptr() for o in offs[:-1]])
+    N = (C.c_int64 * len(lens))(*lens)
+    for op, code in (("exp", 0), ("log", 1)):
+        p = C.c_void_p()
+        _lib.check(L.mfcuda_batch_create_unary(code, X, Y, N, len(lens), C.byref(p)), "ragged")
+        ms = _events_time(lambda: _lib.check(L.mfcuda_batch_run(p, sp), "run"), max(1, args.steps // 3),
+                          args.warmup, stream)
+        res["ragged_" + op] = {"ms": ms, "arrays": len(lens), "elements": tot, "gelem_per_s": tot / ms / 1e6}
+        L.mfcuda_batch_destroy(p)
+    _line(args, "dd_batched_2000_gemms_16_1024", "Batched DD-GEMM DD-GFLOP/s, 2000 problems M,N,K log-uniform [16,1024]",
+          res["split"]["dd_gflops"], "DD-GFLOP/s",
+          {"dtype": "int8+f64", "plain_vs_split": res, "speedup_split_vs_plain": res["split"]["dd_gflops"] / res["plain"]["dd_gflops"],
+           "launch": "one CUDA graph per batch (grouped persistent kernels); autotuned tiles"})
+
+
+def run_complex(args):
+    import torch
+
+    from multifloats_b200 import _lib, api
+    from multifloats_b200 import workloads as W
+
+    L = _lib.lib()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    m = 4096
+    A = torch.from_numpy(W.complex_from_parts(W.dd_rowcol_scaled(m, m, 16, "row", 1), W.dd_rowcol_scaled(m, m, 16, "row", 2))).to(dev)
+    B = torch.from_numpy(W.complex_from_parts(W.dd_rowcol_scaled(m, m, 16, "col", 3), W.dd_rowcol_scaled(m, m, 16, "col", 4))).to(dev)
+    Cm = torch.empty_like(A)
+    wsb = L.mfcuda_csplit_workspace_size(m, m, m)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    ms_s = _events_time(lambda: _lib.check(L.mfcuda_cmatmuldd_mm_split(A.data_ptr(), B.data_ptr(), Cm.data_ptr(), m, m, m, 0, 8.0, ws.data_ptr(), wsb, None, sp), "cs"),
+                        max(1, args.steps // 3), args.warmup, stream)
+    ms_p = _events_time(lambda: _lib.check(L.mfcuda_cmatmuldd_mm(A.data_ptr(), B.data_ptr(), Cm.data_ptr(), m, m, m, RI, sp), "cp"), 1, 1, stream)
+    flops = 8.0 * m ** 3  # four real products
+    del A, B, Cm, ws
+    nc = 1 << 24
+    x, y = _dev_dd_uniform(2 * nc, 5, dev), _dev_dd_uniform(2 * nc, 6, dev)
+    ms_dot = _events_time(lambda: api.cdot_product(x, y), args.steps, args.warmup, stream)
+    ms_n2 = _events_time(lambda: api.cnorm2(x), args.steps, args.warmup, stream)
+    _line(args, "complex_dd_gemm_4096_split", "complex64x2 GEMM 4096^3 real DD-GFLOP/s (8mnk), split-INT8 vs plain",
+          flops / ms_s / 1e6, "DD-GFLOP/s",
+          {"dtype": "int8+f64", "split_ms": ms_s, "plain_ms": ms_p, "plain_dd_gflops": flops / ms_p / 1e6,
+           "speedup_split_vs_plain": ms_p / ms_s,
+           "cdot_2^24": {"ms": ms_dot, "gbs": 64 * nc / ms_dot / 1e6},
+           "cnorm2_2^24": {"ms": ms_n2, "gbs": 32 * nc / ms_n2 / 1e6}})
+
+
+def run_gemm8192(args):
+    import torch
+
+    from multifloats_b200 import _lib
+    from multifloats_b200 import workloads as W
+    from oracle import oracle as O
+
+    L = _lib.lib()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    res = {}
+    for n in (4096, 8192):
+        for R in (0, 16, 64):
+            A = W.dd_rowcol_scaled(n, n, R, "row", 31 + R)
+            B = W.dd_rowcol_scaled(n, n, R, "col", 41 + R)
+            dA, dB = torch.from_numpy(A).to(dev), torch.from_numpy(B).to(dev)
+            dC = torch.empty_like(dA)
+            wsb = L.mfcuda_split_workspace_size(n, n, n)
+            ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+            info = (C.c_int * 3)()
+            _lib.check(L.mfcuda_matmuldd_mm_split(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), n, n, n, 0, 8.0, ws.data_ptr(), wsb, info, sp), "s")
+            ms = _events_time(lambda: _lib.check(L.mfcuda_matmuldd_mm_split(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), n, n, n, 0, 8.0, ws.data_ptr(), wsb, None, sp), "s"),
+                              max(1, args.steps // 5), args.warmup, stream)
+            Ch = dC.cpu().numpy()
+            rng = np.random.default_rng(R)
+            ii, jj = rng.integers(0, n, 128), rng.integers(0, n, 128)
+            err, ab = O.gemm_errors(A, B, Ch, n, n, n, ii, jj)
+            res[f"{n}_R{R}"] = {"ms": ms, "dd_gflops": 2.0 * n ** 3 / ms / 1e6, "slices": info[0],
+                                "max_err_over_k_ulp_absab": float(np.max(np.abs(err) / (n * 2.0 ** -104 * ab))),
+                                "max_err_over_ulp_absab": float(np.max(np.abs(err) / (2.0 ** -104 * ab)))}
+            log(n, R, res[f"{n}_R{R}"])
+            del dA, dB, dC, ws
+            torch.cuda.empty_cache()
+    _line(args, "dd_gemm_split_4096_8192_R", "split-INT8 DD-GEMM DD-GFLOP/s 8192^3 (R=16)", res["8192_R16"]["dd_gflops"],
+          "DD-GFLOP/s", {"dtype": "int8+f64", "per_config": res, "ulp": "1 DD ulp = 2^-104"})
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
@@ -391,12 +628,18 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="gemm4096",
+                    choices=["gemm4096", "elementwise", "reductions", "batched", "complex", "gemm8192"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         # CPU-only arm: rank 0 measures, the other ranks exit without work
         run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    if args.workload != "gemm4096":
+        {"elementwise": run_elementwise, "reductions": run_reductions, "batched": run_batched,
+         "complex": run_complex, "gemm8192": run_gemm8192}[args.workload](args)
         return
     ws, rank, local = dist_init()
     try:

@@ -882,8 +882,12 @@ static int tune_bucket(int form, const Bucket &bk, int64_t ri) {
   std::vector<int> cands = form == 0 ? std::vector<int>{0, 1, 2} : std::vector<int>{256, 128, 64};
   const int64_t tiles16 = ((m + 15) / 16) * ((n + 15) / 16);
   int64_t copies = std::max<int64_t>(bk.population, 1);
-  copies = std::max<int64_t>(copies, (int64_t)sm_count() * 4 * 16 / std::max<int64_t>(tiles16, 1));
-  copies = std::min<int64_t>(std::max<int64_t>(copies, 1), 256);
+  if (form == 0) {
+    copies = std::max<int64_t>(copies, (int64_t)sm_count() * 4 * 16 / std::max<int64_t>(tiles16, 1));
+    copies = std::min<int64_t>(copies, 256);
+  } else {
+    copies = std::min<int64_t>(copies, 16);
+  }
   void *buf = nullptr;
   const int64_t per = 2 * (m * k + k * n + m * n);
   if (cudaMalloc(&buf, sizeof(double) * per * copies) != cudaSuccess) {
@@ -906,7 +910,7 @@ static int tune_bucket(int form, const Bucket &bk, int64_t ri) {
     int rc = form == 0 ? create_plain(descs.data(), copies, ri, cfg, &b)
                        : create_split(descs.data(), copies, 0, 8.0, cfg, KC_BLOCKS, &b);
     if (rc != MFCUDA_OK) continue;
-    double ms = time_plan(b, 3);
+    double ms = time_plan(b, 2);
     destroy(b);
     if (ms < best_ms) {
       best_ms = ms;
@@ -936,10 +940,12 @@ static std::string bucket_key(int form, const Bucket &b) {
 static std::vector<int> choose(int form, const mfcuda_gemm_desc *d, int64_t count, int tune, int64_t ri) {
   std::vector<int> cfg(count);
   std::map<std::tuple<int, int, int>, Bucket> buckets;
+  // plain: the tile edge depends on m and n; split: the tile width N on n and
+  // a coarse K class (m only changes the number of 128-row tiles)
   auto bucket_of = [&](const mfcuda_gemm_desc &g) {
-    int bm = std::min(std::max(clog2(g.m), 4), 10), bn = std::min(std::max(clog2(g.n), 4), 10);
-    int bk = form == 0 ? 8 : std::min(std::max(clog2(g.k), 4), 12);  // plain: k does not change the tile choice
-    return std::make_tuple(bm, bn, bk);
+    int bn = std::min(std::max(clog2(g.n), 4), 10);
+    if (form == 0) return std::make_tuple(std::min(std::max(clog2(g.m), 4), 10), bn, 8);
+    return std::make_tuple(bn, bn, std::min(std::max(clog2(g.k), 7), 10));
   };
   for (int64_t p = 0; p < count; ++p) {
     auto t = bucket_of(d[p]);
