@@ -246,6 +246,34 @@ MULTIFLOATS_CUDA_API int mfcuda_dotdd_noalloc(const float64x2 *a, const float64x
                                               int64_t renorm_interval, float64x2 *out,
                                               void *stream);
 
+/* ---- reductions sharded over several devices --------------------------------
+ * No reference counterpart (the reference is single-process).  Each device
+ * reduces its contiguous shard with mfcuda_reduce_partial, which runs the same
+ * two kernels as the single-device call but stops before the final step and
+ * writes mfcuda_reduce_partial_values(kind) DD values to `out` (sum, dot: the
+ * DD sum; norm2, cnorm2: the sum of squares before the square root; csum: re,
+ * im; cdot: the four component dots rr, ii, ri, ir).  After an all-gather of
+ * those partials in rank order, mfcuda_reduce_combine folds them left to
+ * right with DD addition and applies the final step, writing the result in
+ * the single call's format.  The result is deterministic for a given shard
+ * split and within the single call's error bound (not bit-identical to it,
+ * whose fold order differs).  kind: MFCUDA_RED_*; x, y, parts, out: device
+ * pointers; y only for the dot kinds. */
+enum {
+  MFCUDA_RED_SUM = 0,
+  MFCUDA_RED_DOT = 1,
+  MFCUDA_RED_NORM2 = 2,
+  MFCUDA_RED_CSUM = 3,
+  MFCUDA_RED_CDOT = 4,
+  MFCUDA_RED_CNORM2 = 5
+};
+MULTIFLOATS_CUDA_API int mfcuda_reduce_partial_values(int kind);
+MULTIFLOATS_CUDA_API int mfcuda_reduce_partial(int kind, const void *x, const void *y, int64_t n,
+                                               int64_t renorm_interval, void *out, void *workspace,
+                                               size_t workspace_bytes, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_reduce_combine(int kind, const void *parts, int64_t count, void *out,
+                                               void *stream);
+
 /* ---- batched ragged work ---------------------------------------------------
  * Many independent problems in grouped launches captured once in a CUDA graph
  * (no reference counterpart; each problem computes what the single call

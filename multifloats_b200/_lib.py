@@ -94,6 +94,9 @@ SIGNATURES = {
     "mfcuda_sumdd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
     "mfcuda_dotdd": (C.c_int, [P, P, I64, I64, P, P, C.c_size_t, P]),
     "mfcuda_dotdd_noalloc": (C.c_int, [P, P, I64, I64, P, P]),
+    "mfcuda_reduce_partial_values": (C.c_int, [C.c_int]),
+    "mfcuda_reduce_partial": (C.c_int, [C.c_int, P, P, I64, I64, P, P, C.c_size_t, P]),
+    "mfcuda_reduce_combine": (C.c_int, [C.c_int, P, I64, P, P]),
     "mfcuda_norm2dd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
     "mfcuda_csumdd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
     "mfcuda_cdotdd": (C.c_int, [P, P, I64, I64, P, P, C.c_size_t, P]),

@@ -220,9 +220,26 @@ __global__ void __launch_bounds__(kRThreads) reduce_stage1(const double *__restr
     for (int q = 0; q < NV; ++q) partials[(int64_t)blockIdx.x * NV + q] = v[q];
 }
 
-// Stage 2: one block folds the block partials (thread t: p[t], p[t+256], ...
-// in order with DD add), same tree, then the final combination.
+// The final step of each kind, applied to the fully combined NV values.
 template <int KIND>
+__device__ __forceinline__ void finish_kind(const dd *v, dd *out) {
+  if constexpr (KIND == 0 || KIND == 1) {
+    out[0] = v[0];
+  } else if constexpr (KIND == 2 || KIND == 5) {
+    out[0] = mfdev::dd_sqrt(v[0]);
+  } else if constexpr (KIND == 3) {
+    out[0] = v[0];
+    out[1] = v[1];
+  } else {
+    out[0] = mfdev::dd_add(v[0], v[1]);  // re = rr + ii
+    out[1] = mfdev::dd_sub(v[2], v[3]);  // im = ri - ir
+  }
+}
+
+// Stage 2: one block folds the block partials (thread t: p[t], p[t+256], ...
+// in order with DD add), same tree, then the final combination (FINAL) or the
+// NV combined values themselves (a partial for a later cross-device combine).
+template <int KIND, bool FINAL = true>
 __global__ void __launch_bounds__(kRThreads) reduce_stage2(const dd *__restrict__ partials,
                                                            int64_t nblocks, dd *__restrict__ out) {
   constexpr int NV = KindInfo<KIND>::NV;
@@ -238,18 +255,27 @@ __global__ void __launch_bounds__(kRThreads) reduce_stage2(const dd *__restrict_
   }
   block_combine<NV>(v);
   if (threadIdx.x == 0) {
-    if constexpr (KIND == 0 || KIND == 1) {
-      out[0] = v[0];
-    } else if constexpr (KIND == 2 || KIND == 5) {
-      out[0] = mfdev::dd_sqrt(v[0]);
-    } else if constexpr (KIND == 3) {
-      out[0] = v[0];
-      out[1] = v[1];
+    if constexpr (FINAL) {
+      finish_kind<KIND>(v, out);
     } else {
-      out[0] = mfdev::dd_add(v[0], v[1]);  // re = rr + ii
-      out[1] = mfdev::dd_sub(v[2], v[3]);  // im = ri - ir
+#pragma unroll
+      for (int q = 0; q < NV; ++q) out[q] = v[q];
     }
   }
+}
+
+// Cross-device combine: the partials of `count` devices (NV values each, in
+// rank order) folded left to right with DD add, then the final step.
+template <int KIND>
+__global__ void combine_ranks_kernel(const dd *__restrict__ parts, int64_t count, dd *__restrict__ out) {
+  constexpr int NV = KindInfo<KIND>::NV;
+  dd v[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = parts[q];
+  for (int64_t r = 1; r < count; ++r)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = mfdev::dd_add(v[q], parts[r * NV + q]);
+  finish_kind<KIND>(v, out);
 }
 
 size_t reduce_ws_size(int64_t n) {
@@ -258,7 +284,7 @@ size_t reduce_ws_size(int64_t n) {
   return (size_t)b * 4 * sizeof(dd);
 }
 
-template <int KIND>
+template <int KIND, bool FINAL = true>
 static int reduce_dev(const double *x, const double *y, int64_t n, int64_t ri, void *out,
                       void *ws, size_t ws_bytes, cudaStream_t s) {
   constexpr int E = KindInfo<KIND>::ELEM;
@@ -283,7 +309,7 @@ static int reduce_dev(const double *x, const double *y, int64_t n, int64_t ri, v
     reduce_stage1<KIND, false><<<(unsigned)blocks, (unsigned)threads, 0, s>>>(x, y, n, ri, part);
   cudaError_t e1 = cudaGetLastError();
   if (e1 == cudaSuccess) {
-    reduce_stage2<KIND><<<1, kRThreads, 0, s>>>(part, blocks, static_cast<dd *>(out));
+    reduce_stage2<KIND, FINAL><<<1, kRThreads, 0, s>>>(part, blocks, static_cast<dd *>(out));
     e1 = cudaGetLastError();
   }
   if (own) ws_free(own, s);
@@ -312,6 +338,47 @@ static int reduce_host(const void *x, const void *y, int64_t n, int64_t ri, void
   size_t rbytes = (KIND == 3 || KIND == 4) ? 2 * sizeof(dd) : sizeof(dd);
   MF_TRY_CUDA(cudaMemcpyAsync(result, st.buf[3], rbytes, cudaMemcpyDeviceToHost, st.stream));
   MF_TRY_CUDA(cudaStreamSynchronize(st.stream));
+  return MFCUDA_OK;
+}
+
+// Kind-dispatched partial and cross-device combine.
+static int reduce_partial(int kind, const double *x, const double *y, int64_t n, int64_t ri, void *out,
+                          void *ws, size_t wsb, cudaStream_t s) {
+  switch (kind) {
+    case 0: return reduce_dev<0, false>(x, nullptr, n, 0, out, ws, wsb, s);
+    case 1: return reduce_dev<1, false>(x, y, n, ri, out, ws, wsb, s);
+    case 2: return reduce_dev<2, false>(x, nullptr, n, 0, out, ws, wsb, s);
+    case 3: return reduce_dev<3, false>(x, nullptr, n, 0, out, ws, wsb, s);
+    case 4: return reduce_dev<4, false>(x, y, n, ri, out, ws, wsb, s);
+    case 5: return reduce_dev<5, false>(x, nullptr, n, 0, out, ws, wsb, s);
+    default: return MFCUDA_ERR_INVALID_ARG;
+  }
+}
+static int partial_values(int kind) {
+  switch (kind) {
+    case 0: return KindInfo<0>::NV;
+    case 1: return KindInfo<1>::NV;
+    case 2: return KindInfo<2>::NV;
+    case 3: return KindInfo<3>::NV;
+    case 4: return KindInfo<4>::NV;
+    case 5: return KindInfo<5>::NV;
+    default: return 0;
+  }
+}
+static int reduce_combine(int kind, const void *parts, int64_t count, void *out, cudaStream_t s) {
+  if (kind < 0 || kind > 5 || count < 1 || !parts || !out) return MFCUDA_ERR_INVALID_ARG;
+  MF_TRY(require_device());
+  const dd *p = static_cast<const dd *>(parts);
+  dd *o = static_cast<dd *>(out);
+  switch (kind) {
+    case 0: combine_ranks_kernel<0><<<1, 1, 0, s>>>(p, count, o); break;
+    case 1: combine_ranks_kernel<1><<<1, 1, 0, s>>>(p, count, o); break;
+    case 2: combine_ranks_kernel<2><<<1, 1, 0, s>>>(p, count, o); break;
+    case 3: combine_ranks_kernel<3><<<1, 1, 0, s>>>(p, count, o); break;
+    case 4: combine_ranks_kernel<4><<<1, 1, 0, s>>>(p, count, o); break;
+    default: combine_ranks_kernel<5><<<1, 1, 0, s>>>(p, count, o); break;
+  }
+  MF_TRY_CUDA(cudaGetLastError());
   return MFCUDA_OK;
 }
 
@@ -424,6 +491,17 @@ MULTIFLOATS_CUDA_API int mfcuda_cdotdd(const complex64x2 *a, const complex64x2 *
 MULTIFLOATS_CUDA_API int mfcuda_cnorm2dd(const complex64x2 *x, int64_t n, float64x2 *out, void *ws,
                                          size_t wsb, void *stream) {
   return mfcuda::reduce_dev<5>(MF_D(x), nullptr, n, 0, out, ws, wsb, mfcuda::as_stream(stream));
+}
+MULTIFLOATS_CUDA_API int mfcuda_reduce_partial_values(int kind) { return mfcuda::partial_values(kind); }
+MULTIFLOATS_CUDA_API int mfcuda_reduce_partial(int kind, const void *x, const void *y, int64_t n,
+                                               int64_t renorm_interval, void *out, void *ws, size_t wsb,
+                                               void *stream) {
+  return mfcuda::reduce_partial(kind, MF_D(x), MF_D(y), n, renorm_interval, out, ws, wsb,
+                                mfcuda::as_stream(stream));
+}
+MULTIFLOATS_CUDA_API int mfcuda_reduce_combine(int kind, const void *parts, int64_t count, void *out,
+                                               void *stream) {
+  return mfcuda::reduce_combine(kind, parts, count, out, mfcuda::as_stream(stream));
 }
 #undef MF_D
 

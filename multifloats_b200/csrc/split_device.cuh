@@ -59,18 +59,44 @@ static __global__ void init_stats_kernel(int *sig, int *mu, int *flag, int64_t n
   }
 }
 
+// floor(log2 v) for a finite v > 0, read from the IEEE-754 fields (subnormals
+// from the position of the leading fraction bit).
+__device__ __forceinline__ int floor_log2(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  const int E = (int)((b >> 52) & 0x7FF);
+  if (E) return E - 1023;
+  return (63 - __clzll((long long)(b & ((1ull << 52) - 1)))) - 1074;
+}
 // binade of |hi| + |lo|: v < 2^e (frexp convention); 0 for v == 0 (unused)
-__device__ __forceinline__ int binade_above(double v) { return ilogb(v) + 1; }
-__device__ __forceinline__ int binade_below(double v) { return ilogb(v); }
+__device__ __forceinline__ int binade_above(double v) { return floor_log2(v) + 1; }
+__device__ __forceinline__ int binade_below(double v) { return floor_log2(v); }
 
-// x * 2^t for the double x = m 2^e as a fixed-point integer with F fractional
-// bits (floor for the bits below).
+// Exact power of two 2^e for -1022 <= e <= 1023.
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+// x 2^e, correctly rounded like ldexp: a multiplication by an exact power of
+// two when 2^e is a normal double, ldexp otherwise.
+__device__ __forceinline__ double scale2(double x, int e) {
+  return (e >= -1022 && e <= 1023) ? x * pow2(e) : ldexp(x, e);
+}
+
+// x * 2^t for the finite double x = m 2^e (integer m, |m| < 2^53, read from
+// the IEEE-754 fields) as a fixed-point integer with FRAC fractional bits,
+// floor for the bits below.
 constexpr int FRAC = 16;
 __device__ __forceinline__ __int128 scaled_fixed(double x, int t) {
   if (x == 0.0) return 0;
-  int e = ilogb(x);
-  long long m = (long long)ldexp(x, 52 - e);  // exact: |m| < 2^53
-  int sh = e - 52 + t + FRAC;
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  const int E = (int)((b >> 52) & 0x7FF);
+  long long m = (long long)(b & ((1ull << 52) - 1));
+  int e;
+  if (E) {
+    m |= 1ll << 52;
+    e = E - 1075;
+  } else {
+    e = -1074;
+  }
+  if (b >> 63) m = -m;
+  int sh = e + t + FRAC;
   if (sh >= 0) return (__int128)m << sh;
   if (sh <= -64) return m < 0 ? (__int128)-1 : (__int128)0;
   return (__int128)(m >> (-sh));
@@ -338,7 +364,7 @@ __device__ __forceinline__ void combine_body(const int32_t *__restrict__ D, cons
 #pragma unroll
         for (int g = SMAX - 1; g >= 0; --g) {
           if (g <= G) {
-            double tv = mfdev::mul((double)v[c][g], ldexp(1.0, -8 * g));  // exact
+            double tv = mfdev::mul((double)v[c][g], pow2(-8 * g));  // exact
             double s_, err;
             mfdev::two_sum(hi[c], tv, s_, err);
             hi[c] = s_;
@@ -357,7 +383,7 @@ __device__ __forceinline__ void combine_body(const int32_t *__restrict__ D, cons
         out = make_double2(CUDART_NAN, 0.0);
       } else {
         int ex = sa + sigB[j] - 12;
-        out = make_double2(ldexp(h, ex), ldexp(l, ex));
+        out = make_double2(scale2(h, ex), scale2(l, ex));
       }
       double2 *dst = reinterpret_cast<double2 *>(C) + (j * M + i) * cstride;
       if (mode != 0) {

@@ -290,6 +290,257 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// 4b. the same work on CTA pairs: 256 x 256 or 256 x 512 output tiles
+// ---------------------------------------------------------------------------
+// A cluster of two CTAs (neighbouring SMs) owns a 256 x (256 nsub) tile,
+// nsub = 1 or 2.  Per pipeline stage each CTA loads its own 128 rows of the A
+// slice and its own 128 rows (output columns) of each 256-column half of the
+// B slice, and one thread of the even CTA issues, per K step, nsub M = 256,
+// N = 256 MMAs that read both CTAs' shared memory; each CTA's tensor memory
+// holds its 128 rows of the accumulator, and each CTA drains its own rows.
+// Bytes loaded per SM per unit of tensor work: 2/3 (nsub = 1) or 1/2
+// (nsub = 2) of the single-CTA kernel's, and the deeper ring in flight per
+// byte of work hides more L2 / DRAM latency.  nsub = 1 keeps two 256-column
+// accumulators (the drain of one item overlaps the next item's MMAs); nsub = 2
+// uses all 512 columns for one accumulator, so the MMAs of the next item wait
+// for the drain (~1% of an item's tensor time) while the loads run ahead.
+//
+// Barriers: every TMA load of both CTAs completes on the even CTA's full[s]
+// (armed by the even CTA with both CTAs' bytes); each stage's MMAs are
+// committed to empty[s] of both CTAs and each accumulator to tfull[a] of both
+// CTAs (commit arrive fan-out, mask 0b11); the eight epilogue warps of the
+// pair arrive on the even CTA's tempty[a].  All waits are bounded.
+//
+// Items (anti-diagonal, K chunk, tile) are dealt to the pairs in snake order
+// (round r: pair p takes item r P + p, or r P + P-1-p for odd r) over the
+// heaviest-first list, which evens out the per-pair work.
+constexpr int P_STAGE_A = 128 * BK;  // 16 KiB: this CTA's 128 rows of A
+constexpr int P_HALF_B = 128 * BK;   // 16 KiB: this CTA's 128 rows of one B half
+constexpr int BM_PAIR = 256;
+constexpr int PAIR_SMEM = 6 * (P_STAGE_A + P_HALF_B) + 1024 + 256;  // >= 4 * (16 + 32) KiB + extras
+
+__host__ __device__ constexpr int pair_stages(int nsub) { return nsub == 1 ? 6 : 4; }
+
+__device__ __forceinline__ int snake_item(int r, int p, int np) { return r * np + ((r & 1) ? np - 1 - p : p); }
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
+    split_mma_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                          const Plan *plan, int32_t *__restrict__ D, int M_pad, int N_pad, int nkc,
+                          int kblocks, int nsub, int *status) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int nst = pair_stages(nsub);
+  const int stage_b = nsub * P_HALF_B;
+  const int stage_bytes = P_STAGE_A + stage_b;
+  uint8_t *sA = smem;
+  uint8_t *sB = smem + nst * P_STAGE_A;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + nst * stage_bytes);
+  uint64_t *empty = full + 6;
+  uint64_t *tfull = empty + 6;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = mftc::cluster_rank();
+  const bool leader = rank == 0;
+  const int pair_id = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  const int S = plan->S, G = S - 1;
+  const int tn_cols = BN * nsub;
+  const int ntm = M_pad / BM_PAIR, ntn = N_pad / tn_cols, ntiles = ntm * ntn;
+  const int items = (G + 1) * nkc * ntiles;
+  const int nacc = 2 / nsub;             // accumulators
+  const int acc_cols = BN * nsub;        // columns per accumulator
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < nst; ++s) {
+      mftc::mbar_init(&full[s], 1);
+      mftc::mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mftc::mbar_init(&tfull[a], 1);
+      mftc::mbar_init(&tempty[a], 8);
+    }
+    mftc::mbar_init(drain, 1);
+    *abort_flag = 0;
+    mftc::fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    mftc::prefetch_tmap(&tmA);
+    mftc::prefetch_tmap(&tmB);
+  }
+  if (warp == 1) {
+    mftc::tmem_alloc_pair(tmem_slot, TMEM_COLS);
+    mftc::tmem_relinquish_pair();
+  }
+  __syncwarp();
+  mftc::tc_fence_before();
+  mftc::cluster_sync();  // both CTAs' barriers are initialised before any cross-CTA signal
+  mftc::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  auto fail = [&](int code) {
+    *abort_flag = 1;
+    atomicOr(status, code);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer (both CTAs) ----
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t armed_parity[6];
+      bool armed[6];
+      for (int s = 0; s < 6; ++s) armed[s] = false;
+      bool ok = true;
+      for (int r = 0; ok; ++r) {
+        const int w = snake_item(r, pair_id, npairs);
+        if (w >= items) break;
+        Item it = decode(w, G, nkc, ntm, ntiles);
+        int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
+        const int arow = it.tm * BM_PAIR + (int)rank * 128;
+        const int brow = it.tn * tn_cols + (int)rank * 128;
+        for (int s = 0; s <= it.g && ok; ++s) {
+          int t = it.g - s;
+          for (int kb = kb0; kb < kb1; ++kb) {
+            if (!wait_bar(&empty[stage], phase ^ 1, abort_flag)) {
+              fail(1);
+              ok = false;
+              break;
+            }
+            if (leader) {
+              mftc::mbar_arrive_expect_tx(&full[stage], 2 * stage_bytes);
+              armed[stage] = true;
+              armed_parity[stage] = phase;
+            }
+            const uint32_t fb = mftc::cluster_addr(&full[stage], 0);
+            mftc::tma_load_3d_pair(sA + stage * P_STAGE_A, &tmA, fb, kb * BK, arow, s);
+            for (int h = 0; h < nsub; ++h)
+              mftc::tma_load_3d_pair(sB + stage * stage_b + h * P_HALF_B, &tmB, fb, kb * BK, brow + h * BN, t);
+            if (++stage == nst) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+        }
+      }
+      if (!ok) {
+        // The even CTA waits for the copies of both CTAs that complete on its
+        // barriers; neither CTA leaves before the closing cluster barrier.
+        for (int s = 0; s < nst; ++s)
+          if (armed[s]) {
+            uint64_t t0 = globaltimer();
+            while (!mftc::mbar_try_wait(&full[s], armed_parity[s]) && globaltimer() - t0 < WAIT_NS) {
+            }
+          }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && leader) {
+      // ---- MMA issuer (even CTA) ----
+      const uint32_t idesc = mftc::idesc_i8(BM_PAIR, BN);
+      int stage = 0;
+      uint32_t phase = 0;
+      int acc = 0;
+      uint32_t acc_phase = 0;
+      bool ok = true;
+      for (int r = 0; ok; ++r) {
+        const int w = snake_item(r, pair_id, npairs);
+        if (w >= items) break;
+        Item it = decode(w, G, nkc, ntm, ntiles);
+        int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
+        if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag)) {
+          fail(2);
+          break;
+        }
+        mftc::tc_fence_after();
+        const uint32_t d_tmem = tmem_base + (uint32_t)(acc * acc_cols);
+        uint32_t accumulate = 0;
+        for (int s = 0; s <= it.g && ok; ++s) {
+          for (int kb = kb0; kb < kb1; ++kb) {
+            if (!wait_bar(&full[stage], phase, abort_flag)) {
+              fail(4);
+              ok = false;
+              break;
+            }
+            mftc::tc_fence_after();
+            const uint32_t a0 = mftc::smem_u32(sA + stage * P_STAGE_A);
+            const uint32_t b0 = mftc::smem_u32(sB + stage * stage_b);
+#pragma unroll
+            for (int kk = 0; kk < BK / UMMA_K; ++kk) {
+              const uint64_t adesc = mftc::smem_desc_k_sw128(a0 + kk * UMMA_K);
+              for (int h = 0; h < nsub; ++h)
+                mftc::umma_i8_pair(d_tmem + (uint32_t)(h * BN), adesc,
+                                   mftc::smem_desc_k_sw128(b0 + h * P_HALF_B + kk * UMMA_K), idesc, accumulate);
+              accumulate = 1;
+            }
+            mftc::umma_commit_pair(&empty[stage], 0x3);
+            if (++stage == nst) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+        }
+        if (!ok) break;
+        mftc::umma_commit_pair(&tfull[acc], 0x3);
+        if (++acc == nacc) {
+          acc = 0;
+          acc_phase ^= 1;
+        }
+      }
+      // every MMA issued by this thread has finished once `drain` flips; the
+      // odd CTA is held by the closing cluster barrier until then
+      mftc::umma_commit_pair(drain, 0x1);
+      uint64_t t0 = globaltimer();
+      while (!mftc::mbar_try_wait(drain, 0) && globaltimer() - t0 < WAIT_NS) {
+      }
+    }
+  } else {
+    // ---- epilogue: warps 2..5 of both CTAs, TMEM lane quadrant = warp % 4 ----
+    const int quad = warp & 3;
+    const int row = quad * 32 + lane;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    for (int r = 0;; ++r) {
+      const int w = snake_item(r, pair_id, npairs);
+      if (w >= items) break;
+      Item it = decode(w, G, nkc, ntm, ntiles);
+      bool got = wait_bar(&tfull[acc], acc_phase, abort_flag);
+      if (!__all_sync(0xffffffffu, got)) {
+        if (lane == 0) fail(8);
+        break;
+      }
+      mftc::tc_fence_after();
+      int32_t *dst_base = D + (((int64_t)(it.g * nkc + it.kc) * N_pad + (int64_t)it.tn * tn_cols) * M_pad +
+                               (int64_t)it.tm * BM_PAIR + (int64_t)rank * 128 + row);
+#pragma unroll 1
+      for (int chunk = 0; chunk < acc_cols / 32; ++chunk) {
+        uint32_t v[32];
+        mftc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * acc_cols + chunk * 32), v);
+        mftc::tmem_wait_ld();
+        int32_t *dst = dst_base + (int64_t)chunk * 32 * M_pad;
+#pragma unroll
+        for (int q = 0; q < 32; ++q) dst[(int64_t)q * M_pad] = (int32_t)v[q];
+      }
+      mftc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mftc::mbar_arrive_cluster(mftc::cluster_addr(&tempty[acc], 0));
+      if (++acc == nacc) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+  }
+
+  __syncwarp();
+  mftc::tc_fence_before();
+  mftc::cluster_sync();  // no CTA leaves while its peer may still signal it or read its shared memory
+  mftc::tc_fence_after();
+  if (warp == 1) mftc::tmem_dealloc_pair(tmem_base, TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
 // 5. combine
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) combine_kernel(const int32_t *__restrict__ D, const Plan *plan,
@@ -310,15 +561,29 @@ __global__ void __launch_bounds__(256) combine_kernel(const int32_t *__restrict_
 struct Layout {
   int64_t M_pad, N_pad, K_pad, kblocks, nkc;
   int nA, nB;
+  bool pair;  // 256 x (256 nsub) tiles on CTA pairs (m > 128), else 128 x 256 tiles
+  int nsub;   // 256-column halves per pair tile: 2 when n > 256
   size_t off_plan, off_stats[4], off_slices[4], off_D, total;
 };
 
 static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
+// CTA pairs unless m fits one 128-row tile; MFCUDA_SPLIT_PAIR=0 selects the
+// single-CTA kernel for every shape (same results, bit for bit).
+static bool use_pair(int64_t m) {
+  static const bool enabled = [] {
+    const char *e = getenv("MFCUDA_SPLIT_PAIR");
+    return !(e && e[0] == '0');
+  }();
+  return enabled && m > BM;
+}
+
 static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB) {
   Layout L;
-  L.M_pad = round_up(m < 1 ? 1 : m, BM);
-  L.N_pad = round_up(n < 1 ? 1 : n, BN);
+  L.pair = use_pair(m);
+  L.nsub = L.pair && n > BN ? 2 : 1;
+  L.M_pad = round_up(m < 1 ? 1 : m, L.pair ? BM_PAIR : BM);
+  L.N_pad = round_up(n < 1 ? 1 : n, BN * L.nsub);
   L.K_pad = round_up(k < 1 ? 1 : k, BK);
   L.kblocks = L.K_pad / BK;
   L.nkc = (L.kblocks + KC_BLOCKS - 1) / KC_BLOCKS;
@@ -420,6 +685,23 @@ size_t workspace_size(int64_t m, int64_t k, int64_t n, bool complex_operands) {
 
 static std::once_flag g_attr_once;
 
+// Persistent grid of the pair kernel: two CTAs per co-resident cluster.
+static int pair_grid() {
+  static int grid = [] {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * (unsigned)sm_count(), 1, 1);
+    cfg.blockDim = dim3(MMA_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = PAIR_SMEM;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, split_mma_pair_kernel, &cfg) != cudaSuccess || clusters < 1) {
+      cudaGetLastError();
+      clusters = sm_count() / 2;
+    }
+    return 2 * clusters;
+  }();
+  return grid;
+}
+
 // A product of one A-side operand with one B-side operand, written into a
 // strided output view with the given mode (see combine_kernel).
 struct Product {
@@ -438,7 +720,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                         double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info) {
   Layout L = layout(m, k, n, nA, nB);
   if (L.M_pad > INT32_MAX / 2 || L.N_pad > INT32_MAX / 2 || L.kblocks > INT32_MAX / 2 ||
-      n > 65535 || L.K_pad / 64 > 65535)
+      L.N_pad > 65535 || L.K_pad / 64 > 65535)
     return MFCUDA_ERR_UNSUPPORTED;
   void *own = nullptr;
   if (!ws) {
@@ -465,6 +747,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
   do {
     std::call_once(g_attr_once, [] {
       cudaFuncSetAttribute(split_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
+      cudaFuncSetAttribute(split_mma_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM);
     });
     prof_call_begin();
     mark(0, s);
@@ -497,9 +780,15 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
         slice_b_kernel<<<dim3((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad), 256, 0, s>>>(
             bview[o - nA], k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o], flag[o], plan, sl[o]);
     }
-    int items_max = SMAX * (int)L.nkc * (int)((L.M_pad / BM) * (L.N_pad / BN));
+    const int tile_m = L.pair ? BM_PAIR : BM;
+    int items_max = SMAX * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
     int grid = sm_count();
-    if (grid > items_max) grid = items_max;
+    if (L.pair) {
+      grid = pair_grid();
+      if (grid > 2 * items_max) grid = 2 * items_max;
+    } else if (grid > items_max) {
+      grid = items_max;
+    }
     unsigned gx = (unsigned)((m + 255) / 256);
     int64_t want = ((int64_t)sm_count() * 32 + gx - 1) / gx;  // ~32 CTAs per SM in total
     unsigned gy = (unsigned)(n < want ? n : want);
@@ -508,13 +797,19 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     for (int q = 0; q < nprod && rc == MFCUDA_OK; ++q) {
       const int ia = prods[q].a, ib = nA + prods[q].b;
       CUtensorMap tmA, tmB;
-      if (!make_map(&tmA, sl[ia], L.M_pad, L.K_pad, BM) || !make_map(&tmB, sl[ib], L.N_pad, L.K_pad, BN)) {
+      if (!make_map(&tmA, sl[ia], L.M_pad, L.K_pad, BM) ||
+          !make_map(&tmB, sl[ib], L.N_pad, L.K_pad, L.pair ? 128 : BN)) {
         rc = MFCUDA_ERR_CUDA;
         break;
       }
-      split_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad,
-                                                           (int)L.N_pad, (int)L.nkc, (int)L.kblocks,
-                                                           status);
+      if (L.pair)
+        split_mma_pair_kernel<<<grid, MMA_THREADS, PAIR_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad,
+                                                                   (int)L.N_pad, (int)L.nkc,
+                                                                   (int)L.kblocks, L.nsub, status);
+      else
+        split_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad,
+                                                             (int)L.N_pad, (int)L.nkc, (int)L.kblocks,
+                                                             status);
       if (q == nprod - 1) mark(3, s);
       combine_kernel<<<dim3(gx, gy), 256, 0, s>>>(D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n,
                                                   L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,

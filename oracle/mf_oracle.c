@@ -593,8 +593,54 @@ static void block_tree(dd *v, int nv) {
   for (int q = 0; q < nv; ++q) v[q] = wp[0][q];
 }
 /* kind: 0 sum, 1 dot, 2 norm2, 3 csum, 4 cdot, 5 cnorm2 (same as the device) */
+/* The final step of each kind on the fully combined values (reduce_dd.cu
+ * finish_kind). */
+static void reduce_finish(int kind, const dd *v, double *out) {
+  dd r0 = v[0], r1 = mk(0.0, 0.0);
+  if (kind == 2 || kind == 5) r0 = dd_sqrt(v[0]);
+  if (kind == 3) r1 = v[1];
+  if (kind == 4) {
+    r0 = dd_add(v[0], v[1]);
+    r1 = dd_sub(v[2], v[3]);
+  }
+  out[0] = r0.hi;
+  out[1] = r0.lo;
+  if (kind == 3 || kind == 4) {
+    out[2] = r1.hi;
+    out[3] = r1.lo;
+  }
+}
+
+static void reduce_blocked_impl(int kind, const double *x, const double *y, int64_t n, int64_t ri,
+                                double *out, int final);
+
 void orc_reduce_blocked(int kind, const double *x, const double *y, int64_t n, int64_t ri,
                         double *out) {
+  reduce_blocked_impl(kind, x, y, n, ri, out, 1);
+}
+
+/* The device's partial for a cross-device combine (mfcuda_reduce_partial):
+ * the NV combined values before the final step, as hi/lo pairs. */
+void orc_reduce_blocked_partial(int kind, const double *x, const double *y, int64_t n, int64_t ri,
+                                double *out) {
+  reduce_blocked_impl(kind, x, y, n, ri, out, 0);
+}
+
+/* mfcuda_reduce_combine: partials of `count` devices (NV hi/lo pairs each, in
+ * rank order) folded left to right with DD add, then the final step. */
+void orc_reduce_combine(int kind, const double *parts, int64_t count, double *out) {
+  static const int NV[6] = {1, 1, 1, 2, 4, 1};
+  int nv = NV[kind];
+  dd v[4];
+  for (int q = 0; q < nv; ++q) v[q] = mk(parts[2 * q], parts[2 * q + 1]);
+  for (int64_t r = 1; r < count; ++r)
+    for (int q = 0; q < nv; ++q)
+      v[q] = dd_add(v[q], mk(parts[2 * (r * nv + q)], parts[2 * (r * nv + q) + 1]));
+  reduce_finish(kind, v, out);
+}
+
+static void reduce_blocked_impl(int kind, const double *x, const double *y, int64_t n, int64_t ri,
+                                double *out, int final) {
   static const int NV[6] = {1, 1, 1, 2, 4, 1};
   static const int E[6] = {2, 2, 2, 4, 4, 4};
   int nv = NV[kind], e = E[kind];
@@ -658,18 +704,13 @@ void orc_reduce_blocked(int kind, const double *x, const double *y, int64_t n, i
         v[(int64_t)t * nv + q] = (b == t) ? p : dd_add(v[(int64_t)t * nv + q], p);
       }
   block_tree(v, nv);
-  dd r0 = v[0], r1 = mk(0.0, 0.0);
-  if (kind == 2 || kind == 5) r0 = dd_sqrt(v[0]);
-  if (kind == 3) r1 = v[1];
-  if (kind == 4) {
-    r0 = dd_add(v[0], v[1]);
-    r1 = dd_sub(v[2], v[3]);
-  }
-  out[0] = r0.hi;
-  out[1] = r0.lo;
-  if (kind == 3 || kind == 4) {
-    out[2] = r1.hi;
-    out[3] = r1.lo;
+  if (final) {
+    reduce_finish(kind, v, out);
+  } else {
+    for (int q = 0; q < nv; ++q) {
+      out[2 * q] = v[q].hi;
+      out[2 * q + 1] = v[q].lo;
+    }
   }
   free(part);
   free(v);

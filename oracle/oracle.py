@@ -58,6 +58,8 @@ def orc():
             getattr(L, f).argtypes = [P, P, I64, I64, P]
         L.orc_reduce_geometry.argtypes = [I64, C.POINTER(I64), C.POINTER(I64)]
         L.orc_reduce_blocked.argtypes = [C.c_int, P, P, I64, I64, P]
+        L.orc_reduce_blocked_partial.argtypes = [C.c_int, P, P, I64, I64, P]
+        L.orc_reduce_combine.argtypes = [C.c_int, P, I64, P]
         L.orc_gemm_errors.argtypes = [P, P, P, I64, I64, I64, P, P, I64, P, P]
         L.orc_reduce_error.argtypes = [C.c_int, P, P, I64, P, P, P]
         L.orc_split_gemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
@@ -183,6 +185,30 @@ def reduce_blocked(kind: str, x, y=None, ri=8) -> np.ndarray:
     yy = _c(y) if y is not None else x
     out = np.zeros(4)
     orc().orc_reduce_blocked(KINDS[kind], _p(x), _p(yy), n, ri, _p(out))
+    return out[:4] if kind in ("csum", "cdot") else out[:2]
+
+
+PARTIAL_VALUES = {"sum": 1, "dot": 1, "norm2": 1, "csum": 2, "cdot": 4, "cnorm2": 1}
+
+
+def reduce_partial(kind: str, x, y=None, ri=8) -> np.ndarray:
+    """The device's per-shard partial (mfcuda_reduce_partial), restated:
+    PARTIAL_VALUES[kind] DD values as hi/lo pairs."""
+    x = _c(x)
+    cplx = kind.startswith("c")
+    n = x.size // (4 if cplx else 2)
+    yy = _c(y) if y is not None else x
+    out = np.zeros(8)
+    orc().orc_reduce_blocked_partial(KINDS[kind], _p(x), _p(yy), n, ri, _p(out))
+    return out[: 2 * PARTIAL_VALUES[kind]]
+
+
+def reduce_combine(kind: str, parts) -> np.ndarray:
+    """Rank-order fold of gathered partials (mfcuda_reduce_combine), restated."""
+    parts = _c(parts)
+    count = parts.size // (2 * PARTIAL_VALUES[kind])
+    out = np.zeros(4)
+    orc().orc_reduce_combine(KINDS[kind], _p(parts), count, _p(out))
     return out[:4] if kind in ("csum", "cdot") else out[:2]
 
 

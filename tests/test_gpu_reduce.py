@@ -86,3 +86,34 @@ def test_nonfinite_inputs(dev):
     x[2 * 99] = np.nan
     got = _dev_reduce("norm2", x, None, dev)
     assert np.isnan(got[0])
+
+
+@pytest.mark.parametrize("kind", ["sum", "dot", "norm2", "csum", "cdot", "cnorm2"])
+def test_shard_partials_and_rank_combine(dev, kind):
+    """mfcuda_reduce_partial over shards, then mfcuda_reduce_combine in shard
+    order: bit-identical to the CPU restatement of the same order; one shard
+    reproduces the single call."""
+    import torch
+
+    from multifloats_b200 import dist as D
+
+    cplx = kind.startswith("c")
+    e = 4 if cplx else 2
+    n = 3 * 4096 * 5 + 17
+    x = W.dd_uniform(2 * n if cplx else n, seed=71)
+    y = W.dd_uniform(2 * n if cplx else n, seed=72) if "dot" in kind else None
+    be = D.CudaBackend()
+    for world in (1, 3, 4):
+        parts_dev, parts_cpu = [], []
+        for r in range(world):
+            a, b = D.shard_bounds(n, r, world)
+            xl = to_dev(x[e * a: e * b], dev)
+            yl = to_dev(y[e * a: e * b], dev) if y is not None else None
+            parts_dev.append(be.partial(kind, xl, yl, 8))
+            parts_cpu.append(O.reduce_partial(kind, x[e * a: e * b], y[e * a: e * b] if y is not None else None, 8))
+        got = to_host(be.combine(kind, torch.cat(parts_dev)))
+        assert O.same_bits(to_host(torch.cat(parts_dev)), np.concatenate(parts_cpu)).all()
+        want = O.reduce_combine(kind, np.concatenate(parts_cpu))
+        assert O.same_bits(got, want).all(), (world, got, want)
+        if world == 1:
+            assert O.same_bits(got, O.reduce_blocked(kind, x, y, ri=8)).all()
