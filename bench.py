@@ -41,6 +41,19 @@ FP64_INSTR_PER_MAC = 13 + 6 / RI  # mac_inl (matmul.inc:6-19) + renorm_inl every
 METRIC = "DD-GEMM DD-GFLOP/s 4096^3: split-INT8 vs plain FP64-DD, 1 B200, err<=8 DD ulp"
 
 
+def _measured_hbm() -> float:
+    """Measured HBM copy bandwidth of this pool's B200s (GB/s), from
+    MEASURED_PEAKS.json when present, else the earlier pool measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+HBM_GBS = _measured_hbm()
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -194,6 +207,39 @@ def load_peaks_lib():
     return p
 
 
+def int8_peaks(pk, sp, seconds: float = 1.5):
+    """(burst, sustained, clocks) INT8 tensor throughput in ops/s: one probe
+    launch after the warm-up, then probe launches back to back for `seconds`
+    with the median over the second half and the NVML clocks seen there."""
+    ms, ops = C.c_double(), C.c_double()
+    if pk.mfpeak_int8(20000, sp, C.byref(ms), C.byref(ops)) != 0:
+        return None, None, None
+    burst = ops.value / (ms.value * 1e-3)
+    rates = []
+    t0 = time.perf_counter()
+    with NvmlClocks(gpu_uuid()) as clk:
+        while time.perf_counter() - t0 < seconds:
+            if pk.mfpeak_int8(20000, sp, C.byref(ms), C.byref(ops)) != 0:
+                return burst, None, None
+            rates.append(ops.value / (ms.value * 1e-3))
+    late = rates[len(rates) // 2:]
+    return burst, statistics.median(late) if late else None, clk.summary()
+
+
+def profile_traffic(kernel: str, workload: str):
+    """DRAM bytes (read + write) per launch of `kernel` on `workload` from the
+    committed ncu summary profiles/traffic_per_launch.txt, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic_per_launch.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and parts[1] == workload:
+                    return int(parts[2])
+    except OSError:
+        pass
+    return None
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
@@ -245,9 +291,8 @@ def run_ours(args, ws, rank, local):
     ms_p, ins_p = C.c_double(), C.c_double()
     pk.mfpeak_fp64(200000, sp, C.byref(ms_p), C.byref(ins_p))
     fp64_peak = ins_p.value / (ms_p.value * 1e-3)
-    ms_i, ops_i = C.c_double(), C.c_double()
-    rc_i = pk.mfpeak_int8(20000, sp, C.byref(ms_i), C.byref(ops_i))
-    int8_peak = ops_i.value / (ms_i.value * 1e-3) if rc_i == 0 else None
+    int8_burst, int8_sustained, int8_clk = int8_peaks(pk, sp)
+    int8_peak = int8_sustained
 
     # ---- timed region: K split steps, every launch's phases recorded ----
     for _ in range(args.warmup):
@@ -320,14 +365,19 @@ def run_ours(args, ws, rank, local):
     t_e2e = max_over_ranks(ws, (time.perf_counter() - t0) / e2e_steps)
     _lib.check_last("matmuldd_mm_split")
 
-    # roofline of the dominant kernel: split_mma_kernel on the INT8 tensor pipe
+    # roofline of the dominant kernel: split_mma_pair_kernel on the INT8 tensor pipe
     int8_ops = (S * (S + 1) // 2) * 2.0 * M * N * K  # algorithmic INT8 ops per launch
     achieved = int8_ops / (phase["mma"] * 1e-3)
     roof = {"bound": "tensor", "achieved": achieved / 1e12,
             "peak": int8_peak / 1e12 if int8_peak else None, "unit": "TFLOP/s",
-            "frac": achieved / int8_peak if int8_peak else None, "traffic": None,
-            "kernel": "split_mma_kernel", "op_kind": "INT8 tensor ops (multiply + add), S(S+1)/2 slice products",
-            "peak_source": "own tcgen05 kind::i8 M=128 N=256 probe (multifloats_b200/csrc/peaks.cu), same process"}
+            "frac": achieved / int8_peak if int8_peak else None,
+            "traffic": profile_traffic("split_mma_pair_kernel", "dd_gemm_4096"),
+            "kernel": "split_mma_pair_kernel", "op_kind": "INT8 tensor ops (multiply + add), S(S+1)/2 slice products",
+            "peak_source": "own tcgen05 kind::i8 probe (multifloats_b200/csrc/peaks.cu), same process, "
+                           "sustained: back-to-back launches for 1.5 s (the kernel is timed inside a "
+                           "long step loop); of measured",
+            "peak_burst": int8_burst / 1e12 if int8_burst else None, "peak_sustained_clocks": int8_clk,
+            "algorithmic_bytes": {"slices_read": 2 * 14 * M * K, "diagonals_written": 14 * M * N * 4}}
 
     if rank == 0:
         line = {
@@ -359,18 +409,32 @@ def run_ours(args, ws, rank, local):
 # ------------------------------------------------------- secondary workloads
 # `--workload` lines other than the default report the other configurations of
 # the hot path (same JSON conventions; the default line is the headline).
-def _events_time(fn, steps, warmup, stream):
+_CLOCKS = []  # NVML clock summaries of every timed region of a secondary workload
+
+
+def _events_time(fn, steps, warmup, stream, min_warm_s=0.3):
+    """Mean CUDA-event time of `steps` calls after `warmup` calls and, for
+    short kernels, more untimed calls until the GPU has been busy for at least
+    min_warm_s seconds (clocks ramped up before the first timed call).  The
+    SM clock is sampled during the timed region."""
     import torch
 
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < min_warm_s:
+        for _ in range(max(1, warmup)):
+            fn()
+        torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        fn()
-    e1.record(stream)
-    e1.synchronize()
+    with NvmlClocks(gpu_uuid()) as clk:
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+    _CLOCKS.append(clk.summary())
     return e0.elapsed_time(e1) / steps
 
 
@@ -393,6 +457,11 @@ def _line(args, workload, metric, value, unit, extra):
          "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
          "data": "synthetic (seeded)", "config": {"workload": workload}}
     d.update(extra)
+    if _CLOCKS:
+        sm = [c["sm_mhz"] for c in _CLOCKS if c.get("sm_mhz")]
+        d["clocks"] = {"sm_mhz_min_median": min(sm) if sm else None, "sm_max_mhz": _CLOCKS[0].get("sm_max_mhz"),
+                       "reasons": sorted({r for c in _CLOCKS for r in c.get("reasons", [])}),
+                       "timed_regions": len(_CLOCKS)}
     print(json.dumps(d), flush=True)
 
 
@@ -420,11 +489,25 @@ def run_elementwise(args):
             O.ref_unary(op, xs, threads=threads)
             dt = time.perf_counter() - t0
             cpu[op] = {"gelem_per_s": (1 << 21) / dt / 1e9, "kind": "reference", "cores": threads}
+    # FP64 thread instructions (DADD + DMUL + DFMA) per element, from ncu counters
+    # on these distributions (profiles/unary_kernel_fp64_instructions_2^24.md)
+    fp64_per_elem = {"exp": 323.0, "log": 316.0, "sin": 827.5, "cos": 827.5, "sqrt": 25.4}
+    pk = load_peaks_lib()
+    ms_p, ins_p = C.c_double(), C.c_double()
+    pk.mfpeak_fp64(200000, C.c_void_p(stream.cuda_stream), C.byref(ms_p), C.byref(ins_p))
+    fp64_peak = ins_p.value / (ms_p.value * 1e-3)
+    for op, r in res.items():
+        r["fp64_instr_per_s"] = fp64_per_elem[op] * n / (r["ms"] * 1e-3)
+        r["frac_fp64"] = r["fp64_instr_per_s"] / fp64_peak
+        r["frac_hbm"] = r["hbm_gbs"] / HBM_GBS
     _line(args, "dd_elementwise_2^26", "DD elementwise G elem/s, 2^26 elements (exp/log/sin/cos/sqrt)",
           res["exp"]["gelem_per_s"], "G elem/s (exp)",
           {"dtype": "f64", "per_op": res, "cpu_baseline_per_op": cpu,
-           "roofline": {"bound": "fp64 (exp/log/sin/cos), hbm (sqrt)", "hbm_peak_gbs": 6546.2,
-                        "sqrt_frac_hbm": res["sqrt"]["hbm_gbs"] / 6546.2}})
+           "roofline": {"bound": "fp64 (exp/log/sin/cos), hbm (sqrt)", "kernel": "unary_kernel<exp>",
+                        "achieved": res["exp"]["fp64_instr_per_s"] / 1e12, "peak": fp64_peak / 1e12,
+                        "unit": "T FP64-instr/s", "frac": res["exp"]["frac_fp64"], "traffic": None,
+                        "peak_source": "own FP64 FMA probe (multifloats_b200/csrc/peaks.cu), same process",
+                        "hbm_peak_gbs": HBM_GBS, "sqrt_frac_hbm": res["sqrt"]["frac_hbm"]}})
 
 
 def run_reductions(args):
@@ -440,16 +523,18 @@ def run_reductions(args):
     for kind, fn, bpe in [("sum", lambda: api.sum_dd(x), 16), ("dot", lambda: api.dot_product(x, y), 32),
                           ("norm2", lambda: api.norm2(x), 16)]:
         ms = _events_time(fn, args.steps, args.warmup, stream)
-        res[kind] = {"ms": ms, "gbs": bpe * n / ms / 1e6, "frac_hbm": bpe * n / ms / 1e6 / 6546.2}
+        res[kind] = {"ms": ms, "gbs": bpe * n / ms / 1e6, "frac_hbm": bpe * n / ms / 1e6 / HBM_GBS}
     nc = 1 << 24
     cx, cy = x[: 4 * nc], y[: 4 * nc]
     for kind, fn, bpe in [("csum", lambda: api.csum_dd(cx), 32), ("cdot", lambda: api.cdot_product(cx, cy), 64),
                           ("cnorm2", lambda: api.cnorm2(cx), 32)]:
         ms = _events_time(fn, args.steps, args.warmup, stream)
-        res[kind] = {"ms": ms, "gbs": bpe * nc / ms / 1e6, "frac_hbm": bpe * nc / ms / 1e6 / 6546.2}
+        res[kind] = {"ms": ms, "gbs": bpe * nc / ms / 1e6, "frac_hbm": bpe * nc / ms / 1e6 / HBM_GBS}
     _line(args, "dd_reductions_2^26", "DD reductions GB/s (dot 2^26)", res["dot"]["gbs"], "GB/s",
           {"dtype": "f64", "per_kind": res,
-           "roofline": {"bound": "hbm", "peak": 6546.2, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs"}})
+           "roofline": {"bound": "hbm", "kernel": "reduce_stage1<dot>", "achieved": res["dot"]["gbs"],
+                        "peak": HBM_GBS, "unit": "GB/s", "frac": res["dot"]["frac_hbm"], "traffic": None,
+                        "peak_source": "MEASURED_PEAKS.json hbm_gbs"}})
 
 
 def _batch_descs(shapes, dev, seed):

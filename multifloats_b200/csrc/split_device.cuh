@@ -397,5 +397,71 @@ __device__ __forceinline__ void combine_body(const int32_t *__restrict__ D, cons
   }
 }
 
+// Same result as combine_body, element for element (same operations in the
+// same order), with a thread per 4 consecutive rows of one column: each
+// diagonal is one 16-byte load per thread (512 contiguous bytes per warp), all
+// G+1 of them in flight before the DD accumulation.  Requires M_pad % 4 == 0
+// and a 16-byte aligned D.  Thread (q = blockIdx.x * blockDim.x + t) owns rows
+// 4q..4q+3 of column j = column index given by the caller.
+__device__ __forceinline__ void combine4_body(const int32_t *__restrict__ D, const Plan *plan,
+                                              const int *sigA, const int *flagA, const int *sigB,
+                                              const int *flagB, int64_t M, int64_t N, int64_t M_pad,
+                                              int64_t N_pad, int nkc, double *__restrict__ C, int64_t cstride,
+                                              int mode, int64_t quad, int64_t j) {
+  const int G = plan->G;
+  const int64_t i0 = quad * 4;
+  if (i0 >= M || j >= N) return;
+  const int64_t gstride = (int64_t)nkc * N_pad * M_pad;  // int32 elements between diagonals
+  double hi[4] = {0.0, 0.0, 0.0, 0.0}, lo[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int kc = 0; kc < nkc; ++kc) {
+    const int4 *src = reinterpret_cast<const int4 *>(D + ((int64_t)kc * N_pad + j) * M_pad + i0);
+    const int64_t gs4 = gstride / 4;
+    int4 v[SMAX];
+#pragma unroll
+    for (int g = 0; g < SMAX; ++g) v[g] = g <= G ? __ldcs(src + g * gs4) : make_int4(0, 0, 0, 0);
+#pragma unroll
+    for (int g = SMAX - 1; g >= 0; --g) {
+      if (g <= G) {
+        const double sc = pow2(-8 * g);
+        const int d[4] = {v[g].x, v[g].y, v[g].z, v[g].w};
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          double tv = mfdev::mul((double)d[r], sc);  // exact
+          double s_, err;
+          mfdev::two_sum(hi[r], tv, s_, err);
+          hi[r] = s_;
+          lo[r] = mfdev::add(lo[r], err);
+        }
+      }
+    }
+  }
+  const int4 sa = *reinterpret_cast<const int4 *>(sigA + i0);
+  const int4 fa = *reinterpret_cast<const int4 *>(flagA + i0);
+  const int sav[4] = {sa.x, sa.y, sa.z, sa.w}, fav[4] = {fa.x, fa.y, fa.z, fa.w};
+  const int sb = sigB[j], fb = flagB[j];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int64_t i = i0 + r;
+    if (i >= M) break;
+    double h, l;
+    mfdev::two_sum(hi[r], lo[r], h, l);
+    double2 out;
+    if (fav[r] | fb) {
+      out = make_double2(CUDART_NAN, 0.0);
+    } else {
+      int ex = sav[r] + sb - 12;
+      out = make_double2(scale2(h, ex), scale2(l, ex));
+    }
+    double2 *dst = reinterpret_cast<double2 *>(C) + (j * M + i) * cstride;
+    if (mode != 0) {
+      double2 prev = *dst;
+      mfdev::dd p = mfdev::make(out.x, out.y), q = mfdev::make(prev.x, prev.y);
+      mfdev::dd res = mode == 1 ? mfdev::dd_sub(q, p) : mfdev::dd_add(q, p);
+      out = make_double2(res.hi, res.lo);
+    }
+    __stcs(dst, out);
+  }
+}
+
 }  // namespace split
 }  // namespace mfcuda

@@ -311,9 +311,13 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
 // CTAs (commit arrive fan-out, mask 0b11); the eight epilogue warps of the
 // pair arrive on the even CTA's tempty[a].  All waits are bounded.
 //
-// Items (anti-diagonal, K chunk, tile) are dealt to the pairs in snake order
-// (round r: pair p takes item r P + p, or r P + P-1-p for odd r) over the
-// heaviest-first list, which evens out the per-pair work.
+// Work is dealt in super-items of equal length: (q, K chunk, tile) runs the
+// diagonal G-q and then the diagonal q of its tile ((G-q+1) + (q+1) = S+1
+// slice products; a single diagonal when G-q == q).  Round r gives pair p the
+// super-item r P + p of a q-major list, so all pairs start and finish their
+// super-items together and, at any moment, multiply the same slice pair (s,
+// t) of different tiles: the slices they read are shared through L2 instead
+// of being fetched from DRAM once per pair.
 constexpr int P_STAGE_A = 128 * BK;  // 16 KiB: this CTA's 128 rows of A
 constexpr int P_HALF_B = 128 * BK;   // 16 KiB: this CTA's 128 rows of one B half
 constexpr int BM_PAIR = 256;
@@ -321,7 +325,38 @@ constexpr int PAIR_SMEM = 6 * (P_STAGE_A + P_HALF_B) + 1024 + 256;  // >= 4 * (1
 
 __host__ __device__ constexpr int pair_stages(int nsub) { return nsub == 1 ? 6 : 4; }
 
-__device__ __forceinline__ int snake_item(int r, int p, int np) { return r * np + ((r & 1) ? np - 1 - p : p); }
+// Sequence of (diagonal, K chunk, tile) items of one pair (see above).
+struct PairSched {
+  int p, np, G, nkc, ntm, ntiles, nsuper;
+  int r = 0, half = 0;
+  __device__ PairSched(int p_, int np_, int G_, int nkc_, int ntm_, int ntiles_)
+      : p(p_), np(np_), G(G_), nkc(nkc_), ntm(ntm_), ntiles(ntiles_), nsuper(((G_ + 2) / 2) * nkc_ * ntiles_) {}
+  __device__ bool next(Item &it) {
+    while (true) {
+      const int u = r * np + p;
+      if (u >= nsuper) return false;
+      const int per_q = nkc * ntiles;
+      const int q = u / per_q, rem = u % per_q;
+      if (half == 1 && q == G - q) {  // the middle diagonal stands alone
+        half = 0;
+        ++r;
+        continue;
+      }
+      it.g = half == 0 ? G - q : q;
+      it.kc = rem / ntiles;
+      const int tile = rem % ntiles;
+      it.tm = tile % ntm;
+      it.tn = tile / ntm;
+      if (half == 0) {
+        half = 1;
+      } else {
+        half = 0;
+        ++r;
+      }
+      return true;
+    }
+  }
+};
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
     split_mma_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -349,7 +384,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
   const int S = plan->S, G = S - 1;
   const int tn_cols = BN * nsub;
   const int ntm = M_pad / BM_PAIR, ntn = N_pad / tn_cols, ntiles = ntm * ntn;
-  const int items = (G + 1) * nkc * ntiles;
   const int nacc = 2 / nsub;             // accumulators
   const int acc_cols = BN * nsub;        // columns per accumulator
 
@@ -394,10 +428,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
       bool armed[6];
       for (int s = 0; s < 6; ++s) armed[s] = false;
       bool ok = true;
-      for (int r = 0; ok; ++r) {
-        const int w = snake_item(r, pair_id, npairs);
-        if (w >= items) break;
-        Item it = decode(w, G, nkc, ntm, ntiles);
+      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles);
+      Item it;
+      while (ok && sched.next(it)) {
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
         const int arow = it.tm * BM_PAIR + (int)rank * 128;
         const int brow = it.tn * tn_cols + (int)rank * 128;
@@ -445,10 +478,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
       int acc = 0;
       uint32_t acc_phase = 0;
       bool ok = true;
-      for (int r = 0; ok; ++r) {
-        const int w = snake_item(r, pair_id, npairs);
-        if (w >= items) break;
-        Item it = decode(w, G, nkc, ntm, ntiles);
+      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles);
+      Item it;
+      while (ok && sched.next(it)) {
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
         if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag)) {
           fail(2);
@@ -502,10 +534,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
     const int row = quad * 32 + lane;
     int acc = 0;
     uint32_t acc_phase = 0;
-    for (int r = 0;; ++r) {
-      const int w = snake_item(r, pair_id, npairs);
-      if (w >= items) break;
-      Item it = decode(w, G, nkc, ntm, ntiles);
+    PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles);
+    Item it;
+    while (sched.next(it)) {
       bool got = wait_bar(&tfull[acc], acc_phase, abort_flag);
       if (!__all_sync(0xffffffffu, got)) {
         if (lane == 0) fail(8);
@@ -543,14 +574,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
 // ---------------------------------------------------------------------------
 // 5. combine
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) combine_kernel(const int32_t *__restrict__ D, const Plan *plan,
+__global__ void __launch_bounds__(128) combine_kernel(const int32_t *__restrict__ D, const Plan *plan,
                                                       const int *sigA, const int *flagA, const int *sigB,
                                                       const int *flagB, int64_t M, int64_t N,
                                                       int64_t M_pad, int64_t N_pad, int nkc,
                                                       double *__restrict__ C, int64_t cstride, int mode) {
-  combine_body(D, plan, sigA, flagA, sigB, flagB, M, N, M_pad, N_pad, nkc, C, cstride, mode, blockIdx.x,
-               blockIdx.y, gridDim.y);
+  combine4_body(D, plan, sigA, flagA, sigB, flagB, M, N, M_pad, N_pad, nkc, C, cstride, mode,
+                (int64_t)blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
+constexpr int COMBINE_THREADS = 128;
 
 // ---------------------------------------------------------------------------
 // host side
@@ -578,10 +610,20 @@ static bool use_pair(int64_t m) {
   return enabled && m > BM;
 }
 
+// Output columns per pair tile in 256-column halves (1 or 2; 2 halves the
+// operand bytes per tensor op).  MFCUDA_SPLIT_NSUB=1 or 2 overrides.
+static int pair_nsub() {
+  static const int v = [] {
+    const char *e = getenv("MFCUDA_SPLIT_NSUB");
+    return (e && e[0] == '1') ? 1 : 2;
+  }();
+  return v;
+}
+
 static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB) {
   Layout L;
   L.pair = use_pair(m);
-  L.nsub = L.pair && n > BN ? 2 : 1;
+  L.nsub = L.pair && n > BN ? pair_nsub() : 1;
   L.M_pad = round_up(m < 1 ? 1 : m, L.pair ? BM_PAIR : BM);
   L.N_pad = round_up(n < 1 ? 1 : n, BN * L.nsub);
   L.K_pad = round_up(k < 1 ? 1 : k, BK);
@@ -784,15 +826,14 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     int items_max = SMAX * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
     int grid = sm_count();
     if (L.pair) {
+      // super-items (pairs of diagonals) of the largest plan, SMAX slices
+      const int supers_max = ((SMAX + 1) / 2) * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
       grid = pair_grid();
-      if (grid > 2 * items_max) grid = 2 * items_max;
+      if (grid > 2 * supers_max) grid = 2 * supers_max;
     } else if (grid > items_max) {
       grid = items_max;
     }
-    unsigned gx = (unsigned)((m + 255) / 256);
-    int64_t want = ((int64_t)sm_count() * 32 + gx - 1) / gx;  // ~32 CTAs per SM in total
-    unsigned gy = (unsigned)(n < want ? n : want);
-    if (gy > 65535u) gy = 65535u;
+    const unsigned cgx = (unsigned)(((m + 3) / 4 + COMBINE_THREADS - 1) / COMBINE_THREADS);
     mark(2, s);
     for (int q = 0; q < nprod && rc == MFCUDA_OK; ++q) {
       const int ia = prods[q].a, ib = nA + prods[q].b;
@@ -811,7 +852,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                                                              (int)L.N_pad, (int)L.nkc, (int)L.kblocks,
                                                              status);
       if (q == nprod - 1) mark(3, s);
-      combine_kernel<<<dim3(gx, gy), 256, 0, s>>>(D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n,
+      combine_kernel<<<dim3(cgx, (unsigned)n), COMBINE_THREADS, 0, s>>>(D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n,
                                                   L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,
                                                   prods[q].ostride, prods[q].mode);
     }
