@@ -102,38 +102,56 @@ __device__ __forceinline__ __int128 scaled_fixed(double x, int t) {
   return (__int128)(m >> (-sh));
 }
 
-// Balanced digits of round((hi + lo) 2^(W - sigma)) in SMAX positions, most
-// significant first (fully unrolled, so the digits stay in registers).  Since
-// |X| < 2^(8S-2), the top SMAX-S digits are zero and slice s of the S-slice
-// representation is d[SMAX - S + s]; the digit left in position SMAX-S lies in
-// [-64, 64].
-__device__ __forceinline__ void dd_digits(double hi, double lo, int sigma, int W, int8_t (&d)[SMAX]) {
-  int t = W - sigma;
-  __int128 xf = scaled_fixed(hi, t) + scaled_fixed(lo, t);
+// The entry rounded to the fixed-point grid of its row / column:
+// X = round((hi + lo) 2^(W - sigma)) (each limb floored at FRAC fractional
+// bits, summed, rounded half up), clamped to |X| <= 2^W - 1 (W = 8S-2 <= 110).
+// Returned as the four 32-bit words of Y = X + sum_{q<14} 128 * 256^q.  The
+// balanced base-256 representation X = sum_q d_q 256^q with d_q in
+// [-128, 127] is unique, and 0 <= Y < 256^14, so byte q of Y is exactly
+// d_q + 128: digit q as a signed byte is byte q of Y xor 0x80, with no carry
+// chain.  Slice s of the S-slice representation (most significant first) is
+// digit q = S-1-s; digits q >= S are zero.
+// Word w of the bias (X = 0 gives all digits zero).
+__host__ __device__ constexpr uint32_t bias_word(int w) { return w < 3 ? 0x80808080u : 0x00008080u; }
+__device__ __forceinline__ void biased_bytes(double hi, double lo, int sigma, int W, uint32_t (&y)[4]) {
+  const int t = W - sigma;
+  const __int128 xf = scaled_fixed(hi, t) + scaled_fixed(lo, t);
   __int128 X = (xf + ((__int128)1 << (FRAC - 1))) >> FRAC;
   const __int128 lim = ((__int128)1 << W) - 1;
   if (X > lim) X = lim;
   if (X < -lim) X = -lim;
-  // X = xh 2^56 + xl with 0 <= xl < 2^56: the low seven digits come from xl,
-  // the carry (0 or 1) moves into xh, the high seven digits come from xh.
-  long long xl = (long long)((unsigned long long)X & ((1ull << 56) - 1));
-  long long xh = (long long)(X >> 56);
-#pragma unroll
-  for (int q = SMAX - 1; q >= SMAX - 7; --q) {
-    int v = (int)(xl & 0xFF);
-    v = (v ^ 0x80) - 0x80;
-    d[q] = (int8_t)v;
-    xl = (xl - v) >> 8;
-  }
-  xh += xl;
-#pragma unroll
-  for (int q = SMAX - 8; q >= 0; --q) {
-    int v = (int)(xh & 0xFF);
-    v = (v ^ 0x80) - 0x80;
-    d[q] = (int8_t)v;
-    xh = (xh - v) >> 8;
-  }
+  const unsigned __int128 bias =
+      (unsigned __int128)0x8080808080808080ull | ((unsigned __int128)0x808080808080ull << 64);
+  const unsigned __int128 Y = (unsigned __int128)X + bias;
+  const uint64_t ylo = (uint64_t)Y, yhi = (uint64_t)(Y >> 64);
+  y[0] = (uint32_t)ylo;
+  y[1] = (uint32_t)(ylo >> 32);
+  y[2] = (uint32_t)yhi;
+  y[3] = (uint32_t)(yhi >> 32);
 }
+// Byte k of each of a, b, c, d packed as bytes 0..3.
+__device__ __forceinline__ uint32_t gather_byte(uint32_t a, uint32_t b, uint32_t c, uint32_t d, int k) {
+  const uint32_t sel = (uint32_t)k | ((uint32_t)(k + 4) << 4);
+  return __byte_perm(__byte_perm(a, b, sel), __byte_perm(c, d, sel), 0x5410);
+}
+// Digit q (signed bytes) of 8 entries packed in entry order into one word.
+template <int Q>
+__device__ __forceinline__ uint64_t digit_word(const uint32_t (&y)[8][4]) {
+  constexpr int w = Q >> 2, k = Q & 3;
+  const uint32_t lo = gather_byte(y[0][w], y[1][w], y[2][w], y[3][w], k) ^ 0x80808080u;
+  const uint32_t hi = gather_byte(y[4][w], y[5][w], y[6][w], y[7][w], k) ^ 0x80808080u;
+  return (uint64_t)lo | ((uint64_t)hi << 32);
+}
+// Calls f(slice index, word) for the S slices of 8 entries.
+template <class F>
+__device__ __forceinline__ void for_each_slice_word(const uint32_t (&y)[8][4], int S, F f) {
+#define MF_SLICE_Q(Q) \
+  if (Q < S) f(S - 1 - Q, digit_word<Q>(y));
+  MF_SLICE_Q(0) MF_SLICE_Q(1) MF_SLICE_Q(2) MF_SLICE_Q(3) MF_SLICE_Q(4) MF_SLICE_Q(5) MF_SLICE_Q(6)
+  MF_SLICE_Q(7) MF_SLICE_Q(8) MF_SLICE_Q(9) MF_SLICE_Q(10) MF_SLICE_Q(11) MF_SLICE_Q(12) MF_SLICE_Q(13)
+#undef MF_SLICE_Q
+}
+static_assert(SMAX == 14, "for_each_slice_word unrolls 14 digit positions");
 
 // Operands are read through strided views: DD element e of a view lives at
 // double2 index e * stride from its base (stride 1 for a real matrix, 2 for the
@@ -272,24 +290,21 @@ __device__ __forceinline__ void slice_a_body(const double *__restrict__ A, int64
   const int64_t i = i0 + ii;
   const bool row_ok = i < M && !flag[i < M ? i : 0];
   const int sigma = i < M ? sig[i] : 0;
-  uint64_t words[SMAX];
-#pragma unroll
-  for (int q = 0; q < SMAX; ++q) words[q] = 0;
+  uint32_t y[8][4];
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     int64_t p = p0 + grp * 8 + e;
     if (row_ok && p < K) {
       double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i) * stride);
-      int8_t d[SMAX];
-      dd_digits(v.x, v.y, sigma, W, d);
+      biased_bytes(v.x, v.y, sigma, W, y[e]);
+    } else {
 #pragma unroll
-      for (int q = 0; q < SMAX; ++q) words[q] |= (uint64_t)(uint8_t)d[q] << (8 * e);
+      for (int w = 0; w < 4; ++w) y[e][w] = bias_word(w);  // X = 0: all digits zero
     }
   }
-#pragma unroll
-  for (int q = 0; q < SMAX; ++q)
-    if (q >= SMAX - S)
-      *reinterpret_cast<uint64_t *>(&tile[q - (SMAX - S)][ii * SA_STRIDE + grp * 8]) = words[q];
+  for_each_slice_word(y, S, [&](int sl, uint64_t word) {
+    *reinterpret_cast<uint64_t *>(&tile[sl][ii * SA_STRIDE + grp * 8]) = word;
+  });
   __syncthreads();
   const int row = t / 8, seg = (t % 8) * 8;
   for (int s = 0; s < S; ++s) {
@@ -311,24 +326,21 @@ __device__ __forceinline__ void slice_b_body(const double *__restrict__ B, int64
   if (p8 >= K_pad) return;
   const bool col_ok = j < N && !flag[j < N ? j : 0];
   const int tau = j < N ? sig[j] : 0;
-  uint64_t words[SMAX];
-#pragma unroll
-  for (int q = 0; q < SMAX; ++q) words[q] = 0;
+  uint32_t y[8][4];
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     int64_t p = p8 + e;
     if (col_ok && p < K) {
       double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p) * stride);
-      int8_t d[SMAX];
-      dd_digits(v.x, v.y, tau, W, d);
+      biased_bytes(v.x, v.y, tau, W, y[e]);
+    } else {
 #pragma unroll
-      for (int q = 0; q < SMAX; ++q) words[q] |= (uint64_t)(uint8_t)d[q] << (8 * e);
+      for (int w = 0; w < 4; ++w) y[e][w] = bias_word(w);
     }
   }
-#pragma unroll
-  for (int q = 0; q < SMAX; ++q)
-    if (q >= SMAX - S)
-      *reinterpret_cast<uint64_t *>(Bs + (((int64_t)(q - (SMAX - S)) * N_pad + j) * K_pad + p8)) = words[q];
+  for_each_slice_word(y, S, [&](int sl, uint64_t word) {
+    *reinterpret_cast<uint64_t *>(Bs + (((int64_t)sl * N_pad + j) * K_pad + p8)) = word;
+  });
 }
 
 // Thread per row i (consecutive threads -> consecutive rows: every load and
