@@ -510,26 +510,44 @@ def run_elementwise(args):
                         "hbm_peak_gbs": HBM_GBS, "sqrt_frac_hbm": res["sqrt"]["frac_hbm"]}})
 
 
+def _reduction_fns(L, x, y, n, nc, out, ws, wsb, sp):
+    """Device-pointer reduction calls on preallocated output and workspace
+    (no per-call allocation): {kind: (call, bytes per element, elements)}."""
+    def chk(rc):
+        if rc:
+            raise RuntimeError(f"reduction failed: {rc}")
+
+    X, Y, O, WS = x.data_ptr(), y.data_ptr(), out.data_ptr(), ws.data_ptr()
+    return {
+        "sum": (lambda: chk(L.mfcuda_sumdd(X, n, O, WS, wsb, sp)), 16, n),
+        "dot": (lambda: chk(L.mfcuda_dotdd(X, Y, n, RI, O, WS, wsb, sp)), 32, n),
+        "norm2": (lambda: chk(L.mfcuda_norm2dd(X, n, O, WS, wsb, sp)), 16, n),
+        "csum": (lambda: chk(L.mfcuda_csumdd(X, nc, O, WS, wsb, sp)), 32, nc),
+        "cdot": (lambda: chk(L.mfcuda_cdotdd(X, Y, nc, RI, O, WS, wsb, sp)), 64, nc),
+        "cnorm2": (lambda: chk(L.mfcuda_cnorm2dd(X, nc, O, WS, wsb, sp)), 32, nc),
+    }
+
+
 def run_reductions(args):
     import torch
 
-    from multifloats_b200 import api
+    from multifloats_b200 import _lib
 
+    L = _lib.lib()
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
     n = 1 << 26
+    nc = 1 << 24  # complex elements: the first 2^25 DD of the same arrays
     x, y = _dev_dd_uniform(n, 1, dev), _dev_dd_uniform(n, 2, dev)
+    out = torch.empty(4, dtype=torch.float64, device=dev)
+    wsb = L.mfcuda_reduce_workspace_size(n)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
     res = {}
-    for kind, fn, bpe in [("sum", lambda: api.sum_dd(x), 16), ("dot", lambda: api.dot_product(x, y), 32),
-                          ("norm2", lambda: api.norm2(x), 16)]:
+    for kind, (fn, bpe, cnt) in _reduction_fns(L, x, y, n, nc, out, ws, wsb, sp).items():
         ms = _events_time(fn, args.steps, args.warmup, stream)
-        res[kind] = {"ms": ms, "gbs": bpe * n / ms / 1e6, "frac_hbm": bpe * n / ms / 1e6 / HBM_GBS}
-    nc = 1 << 24
-    cx, cy = x[: 4 * nc], y[: 4 * nc]
-    for kind, fn, bpe in [("csum", lambda: api.csum_dd(cx), 32), ("cdot", lambda: api.cdot_product(cx, cy), 64),
-                          ("cnorm2", lambda: api.cnorm2(cx), 32)]:
-        ms = _events_time(fn, args.steps, args.warmup, stream)
-        res[kind] = {"ms": ms, "gbs": bpe * nc / ms / 1e6, "frac_hbm": bpe * nc / ms / 1e6 / HBM_GBS}
+        res[kind] = {"ms": ms, "gbs": bpe * cnt / ms / 1e6, "frac_hbm": bpe * cnt / ms / 1e6 / HBM_GBS,
+                     "elements": cnt}
     _line(args, "dd_reductions_2^26", "DD reductions GB/s (dot 2^26)", res["dot"]["gbs"], "GB/s",
           {"dtype": "f64", "per_kind": res,
            "roofline": {"bound": "hbm", "kernel": "reduce_stage1<dot>", "achieved": res["dot"]["gbs"],
@@ -628,16 +646,51 @@ def run_complex(args):
     ms_p = _events_time(lambda: _lib.check(L.mfcuda_cmatmuldd_mm(A.data_ptr(), B.data_ptr(), Cm.data_ptr(), m, m, m, RI, sp), "cp"), 1, 1, stream)
     flops = 8.0 * m ** 3  # four real products
     del A, B, Cm, ws
+    torch.cuda.empty_cache()
+    # complex dot / norm2 over 2^24 elements (device calls, preallocated workspace)
     nc = 1 << 24
     x, y = _dev_dd_uniform(2 * nc, 5, dev), _dev_dd_uniform(2 * nc, 6, dev)
-    ms_dot = _events_time(lambda: api.cdot_product(x, y), args.steps, args.warmup, stream)
-    ms_n2 = _events_time(lambda: api.cnorm2(x), args.steps, args.warmup, stream)
+    out = torch.empty(4, dtype=torch.float64, device=dev)
+    wsb_r = L.mfcuda_reduce_workspace_size(nc)
+    wsr = torch.empty(wsb_r, dtype=torch.uint8, device=dev)
+    fns = _reduction_fns(L, x, y, 0, nc, out, wsr, wsb_r, sp)
+    ms_dot = _events_time(fns["cdot"][0], args.steps, args.warmup, stream)
+    ms_n2 = _events_time(fns["cnorm2"][0], args.steps, args.warmup, stream)
+    del x, y, wsr
+    # batch of 512 complex GEMMs, M, N, K log-uniform in [32, 512]: plain and split plans
+    rng = np.random.default_rng(512)
+    shapes = [tuple(int(v) for v in s_) for s_ in np.exp(rng.uniform(np.log(32), np.log(512), (512, 3)))]
+    bflops = sum(8.0 * mm * kk * nn for mm, kk, nn in shapes)
+    tot = sum(mm * kk + kk * nn for mm, kk, nn in shapes)
+    buf = _dev_dd_uniform(2 * tot, 8, dev)  # 2 DD per complex element
+    cout = torch.empty(4 * sum(mm * nn for mm, _, nn in shapes), dtype=torch.float64, device=dev)
+    descs = (_lib.gemm_desc * len(shapes))()
+    off = oc = 0
+    for i, (mm, kk, nn) in enumerate(shapes):
+        descs[i].a = buf[4 * off:].data_ptr()
+        off += mm * kk
+        descs[i].b = buf[4 * off:].data_ptr()
+        off += kk * nn
+        descs[i].c = cout[4 * oc:].data_ptr()
+        oc += mm * nn
+        descs[i].m, descs[i].k, descs[i].n = mm, kk, nn
+    batch = {}
+    for form, name in ((0, "plain"), (1, "split")):
+        p = C.c_void_p()
+        _lib.check(L.mfcuda_batch_create_cgemm(descs, len(shapes), form, RI, 0, 8.0, 1, C.byref(p)), "cbatch")
+        bms = _events_time(lambda: _lib.check(L.mfcuda_batch_run(p, sp), "run"), max(1, args.steps // 2),
+                           args.warmup, stream)
+        _lib.check(L.mfcuda_batch_status(p), "status")
+        batch[name] = {"ms": bms, "dd_gflops": bflops / bms / 1e6, "work_items": L.mfcuda_batch_work_items(p)}
+        L.mfcuda_batch_destroy(p)
     _line(args, "complex_dd_gemm_4096_split", "complex64x2 GEMM 4096^3 real DD-GFLOP/s (8mnk), split-INT8 vs plain",
           flops / ms_s / 1e6, "DD-GFLOP/s",
           {"dtype": "int8+f64", "split_ms": ms_s, "plain_ms": ms_p, "plain_dd_gflops": flops / ms_p / 1e6,
            "speedup_split_vs_plain": ms_p / ms_s,
-           "cdot_2^24": {"ms": ms_dot, "gbs": 64 * nc / ms_dot / 1e6},
-           "cnorm2_2^24": {"ms": ms_n2, "gbs": 32 * nc / ms_n2 / 1e6}})
+           "cdot_2^24": {"ms": ms_dot, "gbs": 64 * nc / ms_dot / 1e6, "frac_hbm": 64 * nc / ms_dot / 1e6 / HBM_GBS},
+           "cnorm2_2^24": {"ms": ms_n2, "gbs": 32 * nc / ms_n2 / 1e6, "frac_hbm": 32 * nc / ms_n2 / 1e6 / HBM_GBS},
+           "batch_512_complex_32_512": {**batch, "speedup_split_vs_plain": batch["plain"]["ms"] / batch["split"]["ms"],
+                                        "real_dd_gflop_per_step": bflops / 1e9}})
 
 
 def run_gemm8192(args):

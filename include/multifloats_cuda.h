@@ -304,6 +304,17 @@ enum { MFCUDA_FORM_PLAIN = 0, MFCUDA_FORM_SPLIT = 1 };
 MULTIFLOATS_CUDA_API int mfcuda_batch_create_gemm(const mfcuda_gemm_desc *descs, int64_t count,
                                                   int form, int64_t renorm_interval, int slices,
                                                   double target, int tune, mfcuda_batch **plan);
+/* The same for complex64x2 problems (a, b, c of each descriptor point to
+ * complex64x2 matrices): MFCUDA_FORM_PLAIN runs every 32 x 32 output tile with
+ * the tile code of mfcuda_cmatmuldd_mm (bit-identical to it);
+ * MFCUDA_FORM_SPLIT runs each problem as the four real products of
+ * mfcuda_cmatmuldd_mm_split (one slice count from all four operands, each
+ * operand sliced once, re = ArBr - AiBi and im = ArBi + AiBr combined in that
+ * order), bit-identical to it when the plan's K chunk (mfcuda_batch_kchunk)
+ * is the single call's 73 x 128. */
+MULTIFLOATS_CUDA_API int mfcuda_batch_create_cgemm(const mfcuda_gemm_desc *descs, int64_t count,
+                                                   int form, int64_t renorm_interval, int slices,
+                                                   double target, int tune, mfcuda_batch **plan);
 /* Ragged elementwise batch: y_a[i] = op(x_a[i]) for every array a (lengths
  * ns[a], device pointers), one grid-stride launch over all elements. */
 MULTIFLOATS_CUDA_API int mfcuda_batch_create_unary(int op, const float64x2 *const *xs,

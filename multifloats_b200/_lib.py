@@ -71,6 +71,7 @@ SIGNATURES = {
                                             P, P]),
     "cmatmuldd_mm_split": (None, [P, P, P, I64, I64, I64, C.c_int, C.POINTER(C.c_double)]),
     "mfcuda_batch_create_gemm": (C.c_int, [P, I64, C.c_int, I64, C.c_int, C.c_double, C.c_int, C.POINTER(P)]),
+    "mfcuda_batch_create_cgemm": (C.c_int, [P, I64, C.c_int, I64, C.c_int, C.c_double, C.c_int, C.POINTER(P)]),
     "mfcuda_batch_create_unary": (C.c_int, [C.c_int, P, P, P, I64, C.POINTER(P)]),
     "mfcuda_batch_run": (C.c_int, [P, P]),
     "mfcuda_batch_status": (C.c_int, [P]),

@@ -93,6 +93,27 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
+// Complex problems (complex64x2): every 32 x 32 output tile runs the
+// single-problem complex tile code (gtile::cgemm_tile).
+template <bool ALIGNED>
+__global__ void __launch_bounds__(256, 2)
+    cplain_grouped_kernel(const PProb *__restrict__ probs, const PItem *__restrict__ items, int nitems,
+                          int64_t ri, int *counter) {
+  __shared__ gtile::CSmem sm;
+  __shared__ int next;
+  for (;;) {
+    if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+    __syncthreads();
+    const int w = next;
+    __syncthreads();
+    if (w >= nitems) break;
+    const PItem it = items[w];
+    const PProb p = probs[it.prob];
+    gtile::cgemm_tile<ALIGNED>(p.A, p.B, p.C, p.m, p.k, p.n, ri, (int64_t)it.tm * gtile::kCBM,
+                               (int64_t)it.tn * gtile::kCBN, sm);
+  }
+}
+
 // ===========================================================================
 // ragged elementwise
 // ===========================================================================
@@ -143,18 +164,29 @@ __global__ void __launch_bounds__(256) ragged_unary_kernel(const RArr *__restric
 // ===========================================================================
 using namespace split;
 
+// One real product of the grouped split pipeline: a real problem, or one of
+// the four real products of a complex problem (re = ArBr - AiBi,
+// im = ArBi + AiBr).  Operands and the output are strided views (DD element e
+// at double2 index e * stride); a product may reuse the statistics and slices
+// of another product's A or B operand and share its plan (the four products
+// of a complex problem use one slice count, planned from all four operands).
 struct SProb {
   const double *A, *B;
   double *C;
+  int64_t astride, bstride, cstride;
+  int mode;  // recombination: 0 store, 1 C - P, 2 C + P
+  int own_a, own_b, own_plan;
   int64_t m, k, n, M_pad, N_pad, K_pad;
   int bn, kcb, nkc, kblocks, ntm, ntn;
   int *sigA, *muA, *flagA, *sigB, *muB, *flagB;
+  int *sigA2, *muA2, *sigB2, *muB2;  // the plan's second A and B operands (complex), or null
   int8_t *As, *Bs;
   int32_t *D;
   Plan *plan;
 };
-// phases with a per-problem block count (prefix sums in a table)
-enum { PH_SCAN_A, PH_SCAN_B, PH_SLICE_A, PH_SLICE_B, PH_COMBINE, PH_ITEMS, PH_COUNT };
+// phases with a per-problem block count (prefix sums in a table); the
+// recombination runs in two launches: stores first, then the - / + updates
+enum { PH_SCAN_A, PH_SCAN_B, PH_SLICE_A, PH_SLICE_B, PH_COMBINE, PH_COMBINE2, PH_ITEMS, PH_COUNT };
 
 __device__ __forceinline__ int find_prob(const int64_t *prefix, int nprob, int64_t b) {
   int lo = 0, hi = nprob - 1;
@@ -173,27 +205,31 @@ __global__ void __launch_bounds__(256) g_scan_a(const SProb *probs, const int64_
   const SProb &P = probs[p];
   const int64_t l = blockIdx.x - prefix[p];
   const int64_t nbx = (P.m + 255) / 256;
-  scan_a_body(P.A, P.m, P.k, 1, 64, P.sigA, P.muA, P.flagA, l % nbx, l / nbx);
+  scan_a_body(P.A, P.m, P.k, P.astride, 64, P.sigA, P.muA, P.flagA, l % nbx, l / nbx);
 }
 __global__ void __launch_bounds__(256) g_scan_b(const SProb *probs, const int64_t *prefix, int nprob) {
   const int p = find_prob(prefix, nprob, blockIdx.x);
   const SProb &P = probs[p];
   const int64_t l = blockIdx.x - prefix[p];
   const int64_t nbx = (P.k + 2047) / 2048;
-  scan_b_body(P.B, P.k, P.n, 1, P.sigB, P.muB, P.flagB, l % nbx, l / nbx);
+  scan_b_body(P.B, P.k, P.n, P.bstride, P.sigB, P.muB, P.flagB, l % nbx, l / nbx);
 }
 __global__ void __launch_bounds__(256) g_plan(const SProb *probs, int slices, double target) {
   const SProb &P = probs[blockIdx.x];
+  if (!P.own_plan) return;
   StatSet st;
-  st.n = 2;
-  st.sig[0] = P.sigA;
-  st.mu[0] = P.muA;
-  st.count[0] = P.m;
-  st.side[0] = 0;
-  st.sig[1] = P.sigB;
-  st.mu[1] = P.muB;
-  st.count[1] = P.n;
-  st.side[1] = 1;
+  st.n = 0;
+  auto add = [&](int *sig, const int *mu, int64_t count, int side) {
+    st.sig[st.n] = sig;
+    st.mu[st.n] = mu;
+    st.count[st.n] = count;
+    st.side[st.n] = side;
+    ++st.n;
+  };
+  add(P.sigA, P.muA, P.m, 0);
+  if (P.sigA2) add(P.sigA2, P.muA2, P.m, 0);
+  add(P.sigB, P.muB, P.n, 1);
+  if (P.sigB2) add(P.sigB2, P.muB2, P.n, 1);
   plan_body(st, slices, target, P.plan);
 }
 __global__ void __launch_bounds__(256) g_slice_a(const SProb *probs, const int64_t *prefix, int nprob) {
@@ -201,24 +237,25 @@ __global__ void __launch_bounds__(256) g_slice_a(const SProb *probs, const int64
   const SProb &P = probs[p];
   const int64_t l = blockIdx.x - prefix[p];
   const int64_t nbx = P.M_pad / 32;
-  slice_a_body(P.A, P.m, P.k, 1, P.M_pad, P.K_pad, P.sigA, P.flagA, P.plan, P.As, l % nbx, l / nbx);
+  slice_a_body(P.A, P.m, P.k, P.astride, P.M_pad, P.K_pad, P.sigA, P.flagA, P.plan, P.As, l % nbx, l / nbx);
 }
 __global__ void __launch_bounds__(256) g_slice_b(const SProb *probs, const int64_t *prefix, int nprob) {
   const int p = find_prob(prefix, nprob, blockIdx.x);
   const SProb &P = probs[p];
   const int64_t l = blockIdx.x - prefix[p];
   const int64_t nbx = (P.K_pad / 8 + 255) / 256;
-  slice_b_body(P.B, P.k, P.n, 1, P.N_pad, P.K_pad, P.sigB, P.flagB, P.plan, P.Bs, l % nbx, l / nbx);
+  slice_b_body(P.B, P.k, P.n, P.bstride, P.N_pad, P.K_pad, P.sigB, P.flagB, P.plan, P.Bs, l % nbx, l / nbx);
 }
-constexpr int64_t kCombineCols = 8;  // columns per combine block (2 per pass)
-__global__ void __launch_bounds__(256) g_combine(const SProb *probs, const int64_t *prefix, int nprob) {
+// a block covers 128 x 4 rows of one column (combine4_body)
+constexpr int kCombineThreads = 128;
+static int64_t combine_row_blocks(int64_t m) { return ((m + 3) / 4 + kCombineThreads - 1) / kCombineThreads; }
+__global__ void __launch_bounds__(kCombineThreads) g_combine(const SProb *probs, const int64_t *prefix, int nprob) {
   const int p = find_prob(prefix, nprob, blockIdx.x);
   const SProb &P = probs[p];
   const int64_t l = blockIdx.x - prefix[p];
-  const int64_t nbx = (P.m + 255) / 256;
-  const int64_t ny = (P.n + kCombineCols - 1) / kCombineCols;
-  combine_body(P.D, P.plan, P.sigA, P.flagA, P.sigB, P.flagB, P.m, P.n, P.M_pad, P.N_pad, P.nkc, P.C, 1,
-               0, l % nbx, l / nbx, ny);
+  const int64_t nbx = ((P.m + 3) / 4 + kCombineThreads - 1) / kCombineThreads;
+  combine4_body(P.D, P.plan, P.sigA, P.flagA, P.sigB, P.flagB, P.m, P.n, P.M_pad, P.N_pad, P.nkc, P.C,
+                P.cstride, P.mode, (l % nbx) * kCombineThreads + threadIdx.x, l / nbx);
 }
 
 struct GItem {
@@ -553,8 +590,9 @@ static int capture(mfcuda_batch *b, F enqueue) {
 }
 
 // ---- plain ------------------------------------------------------------------
+// complex = true: complex64x2 problems, 32 x 32 tiles (cfg ignored).
 static int create_plain(const mfcuda_gemm_desc *d, int64_t count, int64_t ri, const std::vector<int> &cfg,
-                        mfcuda_batch **out) {
+                        mfcuda_batch **out, bool complex = false) {
   std::vector<int64_t> order;
   bool aligned = true;
   for (int64_t p = 0; p < count; ++p) {
@@ -568,10 +606,10 @@ static int create_plain(const mfcuda_gemm_desc *d, int64_t count, int64_t ri, co
     probs[p] = {static_cast<const double *>(d[p].a), static_cast<const double *>(d[p].b),
                 static_cast<double *>(d[p].c), d[p].m, d[p].k, d[p].n};
   for (int64_t p : order) {
-    const int e = cfg_edge(cfg[p]);
+    const int e = complex ? gtile::kCBM : cfg_edge(cfg[p]);
     for (int64_t tn = 0; tn < (d[p].n + e - 1) / e; ++tn)
       for (int64_t tm = 0; tm < (d[p].m + e - 1) / e; ++tm)
-        items.push_back({(int)p, cfg[p], (int)tm, (int)tn});
+        items.push_back({(int)p, complex ? 1 : cfg[p], (int)tm, (int)tn});
   }
   if (items.size() > (size_t)INT32_MAX) return MFCUDA_ERR_UNSUPPORTED;
   auto *b = new mfcuda_batch;
@@ -605,10 +643,16 @@ static int create_plain(const mfcuda_gemm_desc *d, int64_t count, int64_t ri, co
   if (grid > nitems) grid = nitems > 0 ? nitems : 1;
   int rc = capture(b, [&](cudaStream_t cs) {
     cudaMemsetAsync(ctr, 0, sizeof(int), cs);
-    if (aligned)
+    if (complex) {
+      if (aligned)
+        cplain_grouped_kernel<true><<<grid, 256, 0, cs>>>(dp, di, nitems, ri, ctr);
+      else
+        cplain_grouped_kernel<false><<<grid, 256, 0, cs>>>(dp, di, nitems, ri, ctr);
+    } else if (aligned) {
       plain_grouped_kernel<true><<<grid, 256, 0, cs>>>(dp, di, nitems, ri, ctr);
-    else
+    } else {
       plain_grouped_kernel<false><<<grid, 256, 0, cs>>>(dp, di, nitems, ri, ctr);
+    }
   });
   if (rc != MFCUDA_OK) {
     destroy(b);
@@ -644,38 +688,63 @@ static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, 
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// cfg[p] = tile width N (256, 128 or 64); kcb: K chunk in blocks of 128 (shared).
-static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, double target,
-                        const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out) {
-  std::vector<int64_t> order;
-  for (int64_t p = 0; p < count; ++p) {
-    if (!aligned16(d[p].a) || !aligned16(d[p].b) || !aligned16(d[p].c)) return MFCUDA_ERR_UNSUPPORTED;
-    if (d[p].n > 65535) return MFCUDA_ERR_UNSUPPORTED;
-    if (d[p].m > 0 && d[p].n > 0) order.push_back(p);
+// One real product to plan (host side of SProb): operand / output views, its
+// tile width, and where its A operand, B operand and plan come from (-1: its
+// own; else the index of the product that provides them).  A plan owner lists
+// in plan_a2 / plan_b2 the products whose A / B statistics also enter its plan.
+struct Spec {
+  const double *A, *B;
+  double *C;
+  int64_t astride, bstride, cstride;
+  int mode;
+  int64_t m, k, n;
+  int bn;
+  int a_src, b_src, plan_src, plan_a2, plan_b2;
+};
+
+// kcb: K chunk in blocks of 128 (shared by all products).
+static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices, double target,
+                              const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out) {
+  // longest K first (stable: the products of one complex problem stay together)
+  const int np = (int)specs.size();
+  std::vector<int> order(np), pos(np);
+  for (int q = 0; q < np; ++q) order[q] = q;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return specs[x].k > specs[y].k; });
+  for (int q = 0; q < np; ++q) pos[order[q]] = q;
+  std::vector<Spec> sp(np);
+  for (int q = 0; q < np; ++q) {
+    sp[q] = specs[order[q]];
+    for (int *r : {&sp[q].a_src, &sp[q].b_src, &sp[q].plan_src, &sp[q].plan_a2, &sp[q].plan_b2})
+      if (*r >= 0) *r = pos[*r];
   }
-  std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return d[x].k > d[y].k; });
-  const int np = (int)order.size();
   std::vector<SProb> probs(np);
   Arena ar;
   size_t o_probs = ar.take(sizeof(SProb) * std::max(np, 1));
   size_t o_prefix = ar.take(sizeof(int64_t) * PH_COUNT * std::max(np, 1));
   size_t o_maps = ar.take(sizeof(CUtensorMap) * 2 * std::max(np, 1), 128);
   size_t o_status = ar.take(sizeof(int));
-  std::vector<size_t> o_plan(np), o_as(np), o_bs(np), o_d(np);
-  std::vector<int64_t> rowoff(np);  // offset of the problem's statistics rows (A rows, then B columns)
+  std::vector<size_t> o_plan(np, 0), o_as(np, 0), o_bs(np, 0), o_d(np);
+  std::vector<int64_t> rowA(np, -1), rowB(np, -1);  // statistics rows of owned operands
   int64_t rows_total = 0;
   std::vector<int64_t> prefix(PH_COUNT * (size_t)std::max(np, 1), 0);
-  int64_t total[PH_COUNT] = {0, 0, 0, 0, 0, 0};
+  int64_t total[PH_COUNT] = {0, 0, 0, 0, 0, 0, 0};
   for (int q = 0; q < np; ++q) {
-    const mfcuda_gemm_desc &g = d[order[q]];
+    const Spec &g = sp[q];
     SProb &P = probs[q];
-    P.A = static_cast<const double *>(g.a);
-    P.B = static_cast<const double *>(g.b);
-    P.C = static_cast<double *>(g.c);
+    P.A = g.A;
+    P.B = g.B;
+    P.C = g.C;
+    P.astride = g.astride;
+    P.bstride = g.bstride;
+    P.cstride = g.cstride;
+    P.mode = g.mode;
+    P.own_a = g.a_src < 0;
+    P.own_b = g.b_src < 0;
+    P.own_plan = g.plan_src < 0;
     P.m = g.m;
     P.k = g.k;
     P.n = g.n;
-    P.bn = cfg[order[q]];
+    P.bn = g.bn;
     P.M_pad = ru(g.m, BM);
     P.N_pad = ru(g.n, P.bn);
     P.K_pad = ru(g.k < 1 ? 1 : g.k, BK);
@@ -684,16 +753,26 @@ static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, do
     P.nkc = (P.kblocks + P.kcb - 1) / P.kcb;
     P.ntm = (int)(P.M_pad / BM);
     P.ntn = (int)(P.N_pad / P.bn);
-    o_plan[q] = ar.take(sizeof(Plan));
-    rowoff[q] = rows_total;
-    rows_total += P.M_pad + P.N_pad;
-    o_as[q] = ar.take((size_t)SMAX * P.M_pad * P.K_pad, 1024);
-    o_bs[q] = ar.take((size_t)SMAX * P.N_pad * P.K_pad, 1024);
+    if (P.own_plan) o_plan[q] = ar.take(sizeof(Plan));
+    if (P.own_a) {
+      rowA[q] = rows_total;
+      rows_total += P.M_pad;
+      o_as[q] = ar.take((size_t)SMAX * P.M_pad * P.K_pad, 1024);
+    }
+    if (P.own_b) {
+      rowB[q] = rows_total;
+      rows_total += P.N_pad;
+      o_bs[q] = ar.take((size_t)SMAX * P.N_pad * P.K_pad, 1024);
+    }
     o_d[q] = ar.take((size_t)SMAX * P.nkc * P.N_pad * P.M_pad * sizeof(int32_t));
+    const int64_t comb = combine_row_blocks(P.m) * P.n;
     const int64_t blocks[PH_COUNT] = {
-        ((P.m + 255) / 256) * ((P.k + 63) / 64),  (P.k > 0 ? (P.k + 2047) / 2048 : 0) * P.n,
-        (P.M_pad / 32) * (P.K_pad / 64),          ((P.K_pad / 8 + 255) / 256) * P.N_pad,
-        ((P.m + 255) / 256) * ((P.n + kCombineCols - 1) / kCombineCols),
+        P.own_a ? ((P.m + 255) / 256) * ((P.k + 63) / 64) : 0,
+        P.own_b ? (P.k > 0 ? (P.k + 2047) / 2048 : 0) * P.n : 0,
+        P.own_a ? (P.M_pad / 32) * (P.K_pad / 64) : 0,
+        P.own_b ? ((P.K_pad / 8 + 255) / 256) * P.N_pad : 0,
+        P.mode == 0 ? comb : 0,
+        P.mode != 0 ? comb : 0,
         (int64_t)SMAX * P.nkc * P.ntm * P.ntn};
     for (int ph = 0; ph < PH_COUNT; ++ph) {
       prefix[(size_t)ph * np + q] = total[ph];
@@ -702,7 +781,7 @@ static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, do
   }
   for (int ph = 0; ph < PH_COUNT; ++ph)
     if (total[ph] > INT32_MAX) return MFCUDA_ERR_UNSUPPORTED;
-  // exponent statistics of all problems in three contiguous arrays
+  // exponent statistics of all owned operands in three contiguous arrays
   const size_t o_sig = ar.take(sizeof(int) * std::max<int64_t>(rows_total, 1));
   const size_t o_mu = ar.take(sizeof(int) * std::max<int64_t>(rows_total, 1));
   const size_t o_flag = ar.take(sizeof(int) * std::max<int64_t>(rows_total, 1));
@@ -720,19 +799,49 @@ static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, do
     return MFCUDA_ERR_ALLOC;
   }
   uint8_t *base = static_cast<uint8_t *>(b->mem);
+  int *sig0 = reinterpret_cast<int *>(base + o_sig), *mu0 = reinterpret_cast<int *>(base + o_mu),
+      *flag0 = reinterpret_cast<int *>(base + o_flag);
+  // owned storage first, then the borrowed pointers
+  for (int q = 0; q < np; ++q) {
+    SProb &P = probs[q];
+    if (P.own_plan) P.plan = reinterpret_cast<Plan *>(base + o_plan[q]);
+    if (P.own_a) {
+      P.sigA = sig0 + rowA[q];
+      P.muA = mu0 + rowA[q];
+      P.flagA = flag0 + rowA[q];
+      P.As = reinterpret_cast<int8_t *>(base + o_as[q]);
+    }
+    if (P.own_b) {
+      P.sigB = sig0 + rowB[q];
+      P.muB = mu0 + rowB[q];
+      P.flagB = flag0 + rowB[q];
+      P.Bs = reinterpret_cast<int8_t *>(base + o_bs[q]);
+    }
+    P.D = reinterpret_cast<int32_t *>(base + o_d[q]);
+  }
   std::vector<CUtensorMap> maps(2 * (size_t)std::max(np, 1));
   for (int q = 0; q < np; ++q) {
     SProb &P = probs[q];
-    P.plan = reinterpret_cast<Plan *>(base + o_plan[q]);
-    P.sigA = reinterpret_cast<int *>(base + o_sig) + rowoff[q];
-    P.muA = reinterpret_cast<int *>(base + o_mu) + rowoff[q];
-    P.flagA = reinterpret_cast<int *>(base + o_flag) + rowoff[q];
-    P.sigB = P.sigA + P.M_pad;
-    P.muB = P.muA + P.M_pad;
-    P.flagB = P.flagA + P.M_pad;
-    P.As = reinterpret_cast<int8_t *>(base + o_as[q]);
-    P.Bs = reinterpret_cast<int8_t *>(base + o_bs[q]);
-    P.D = reinterpret_cast<int32_t *>(base + o_d[q]);
+    const Spec &g = sp[q];
+    if (!P.own_plan) P.plan = probs[g.plan_src].plan;
+    if (!P.own_a) {
+      const SProb &S = probs[g.a_src];
+      P.sigA = S.sigA;
+      P.muA = S.muA;
+      P.flagA = S.flagA;
+      P.As = S.As;
+    }
+    if (!P.own_b) {
+      const SProb &S = probs[g.b_src];
+      P.sigB = S.sigB;
+      P.muB = S.muB;
+      P.flagB = S.flagB;
+      P.Bs = S.Bs;
+    }
+    P.sigA2 = g.plan_a2 >= 0 ? probs[g.plan_a2].sigA : nullptr;
+    P.muA2 = g.plan_a2 >= 0 ? probs[g.plan_a2].muA : nullptr;
+    P.sigB2 = g.plan_b2 >= 0 ? probs[g.plan_b2].sigB : nullptr;
+    P.muB2 = g.plan_b2 >= 0 ? probs[g.plan_b2].muB : nullptr;
     if (!make_map(&maps[2 * q], P.As, P.M_pad, P.K_pad, BM) ||
         !make_map(&maps[2 * q + 1], P.Bs, P.N_pad, P.K_pad, (uint32_t)P.bn)) {
       destroy(b);
@@ -760,17 +869,22 @@ static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, do
     cudaMemsetAsync(b->status, 0, sizeof(int), cs);
     if (np == 0) return;
     const unsigned fb = (unsigned)((rows_total + 255) / 256);
-    fill_kernel<<<fb, 256, 0, cs>>>(reinterpret_cast<int *>(base + o_sig), rows_total, SENT_LO);
-    fill_kernel<<<fb, 256, 0, cs>>>(reinterpret_cast<int *>(base + o_mu), rows_total, SENT_HI);
-    fill_kernel<<<fb, 256, 0, cs>>>(reinterpret_cast<int *>(base + o_flag), rows_total, 0);
-    if (total[PH_SCAN_A]) g_scan_a<<<(unsigned)total[PH_SCAN_A], 256, 0, cs>>>(dp, dprefix + 0 * np, np);
-    if (total[PH_SCAN_B]) g_scan_b<<<(unsigned)total[PH_SCAN_B], 256, 0, cs>>>(dp, dprefix + 1 * np, np);
+    fill_kernel<<<fb, 256, 0, cs>>>(sig0, rows_total, SENT_LO);
+    fill_kernel<<<fb, 256, 0, cs>>>(mu0, rows_total, SENT_HI);
+    fill_kernel<<<fb, 256, 0, cs>>>(flag0, rows_total, 0);
+    if (total[PH_SCAN_A]) g_scan_a<<<(unsigned)total[PH_SCAN_A], 256, 0, cs>>>(dp, dprefix + PH_SCAN_A * np, np);
+    if (total[PH_SCAN_B]) g_scan_b<<<(unsigned)total[PH_SCAN_B], 256, 0, cs>>>(dp, dprefix + PH_SCAN_B * np, np);
     g_plan<<<np, 256, 0, cs>>>(dp, slices, target);
-    g_slice_a<<<(unsigned)total[PH_SLICE_A], 256, 0, cs>>>(dp, dprefix + 2 * np, np);
-    g_slice_b<<<(unsigned)total[PH_SLICE_B], 256, 0, cs>>>(dp, dprefix + 3 * np, np);
-    g_mma<<<mma_grid, MMA_THREADS, MMA_SMEM, cs>>>(dp, dmaps, dprefix + 5 * np, np, total[PH_ITEMS],
+    if (total[PH_SLICE_A])
+      g_slice_a<<<(unsigned)total[PH_SLICE_A], 256, 0, cs>>>(dp, dprefix + PH_SLICE_A * np, np);
+    if (total[PH_SLICE_B])
+      g_slice_b<<<(unsigned)total[PH_SLICE_B], 256, 0, cs>>>(dp, dprefix + PH_SLICE_B * np, np);
+    g_mma<<<mma_grid, MMA_THREADS, MMA_SMEM, cs>>>(dp, dmaps, dprefix + PH_ITEMS * np, np, total[PH_ITEMS],
                                                    b->status);
-    g_combine<<<(unsigned)total[PH_COMBINE], 256, 0, cs>>>(dp, dprefix + 4 * np, np);
+    if (total[PH_COMBINE])
+      g_combine<<<(unsigned)total[PH_COMBINE], kCombineThreads, 0, cs>>>(dp, dprefix + PH_COMBINE * np, np);
+    if (total[PH_COMBINE2])
+      g_combine<<<(unsigned)total[PH_COMBINE2], kCombineThreads, 0, cs>>>(dp, dprefix + PH_COMBINE2 * np, np);
   });
   if (rc != MFCUDA_OK) {
     destroy(b);
@@ -778,6 +892,47 @@ static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, do
   }
   *out = b;
   return MFCUDA_OK;
+}
+
+static bool split_args_ok(const mfcuda_gemm_desc &g) {
+  return aligned16(g.a) && aligned16(g.b) && aligned16(g.c) && g.n <= 65535;
+}
+
+// Real problems: one product each.  cfg[p] = tile width N (256, 128 or 64).
+static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, double target,
+                        const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out) {
+  std::vector<Spec> specs;
+  for (int64_t p = 0; p < count; ++p) {
+    if (!split_args_ok(d[p])) return MFCUDA_ERR_UNSUPPORTED;
+    if (d[p].m <= 0 || d[p].n <= 0) continue;
+    specs.push_back({static_cast<const double *>(d[p].a), static_cast<const double *>(d[p].b),
+                     static_cast<double *>(d[p].c), 1, 1, 1, 0, d[p].m, d[p].k, d[p].n, cfg[p], -1, -1, -1, -1,
+                     -1});
+  }
+  return create_split_specs(std::move(specs), count, slices, target, cfg, kcb_all, out);
+}
+
+// Complex problems (complex64x2 operands): four real products each, in the
+// order and with the combination of mfcuda_cmatmuldd_mm_split (re = ArBr, then
+// re - AiBi; im = ArBi, then im + AiBr), one plan from all four operands, each
+// operand sliced once.
+static int create_csplit(const mfcuda_gemm_desc *d, int64_t count, int slices, double target,
+                         const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out) {
+  std::vector<Spec> specs;
+  for (int64_t p = 0; p < count; ++p) {
+    if (!split_args_ok(d[p])) return MFCUDA_ERR_UNSUPPORTED;
+    if (d[p].m <= 0 || d[p].n <= 0) continue;
+    const double *A = static_cast<const double *>(d[p].a), *B = static_cast<const double *>(d[p].b);
+    double *Cm = static_cast<double *>(d[p].c);
+    const int64_t m = d[p].m, k = d[p].k, n = d[p].n;
+    const int q = (int)specs.size();
+    //           A      B      C       strides  mode  shape    bn      a_src  b_src  plan_src plan_a2 plan_b2
+    specs.push_back({A, B, Cm, 2, 2, 2, 0, m, k, n, cfg[p], -1, -1, -1, q + 1, q + 1});          // re  = Ar Br
+    specs.push_back({A + 2, B + 2, Cm, 2, 2, 2, 1, m, k, n, cfg[p], -1, -1, q, -1, -1});          // re -= Ai Bi
+    specs.push_back({A, B + 2, Cm + 2, 2, 2, 2, 0, m, k, n, cfg[p], q, q + 1, q, -1, -1});        // im  = Ar Bi
+    specs.push_back({A + 2, B, Cm + 2, 2, 2, 2, 2, m, k, n, cfg[p], q + 1, q, q, -1, -1});        // im += Ai Br
+  }
+  return create_split_specs(std::move(specs), count, slices, target, cfg, kcb_all, out);
 }
 
 // ---- ragged elementwise -------------------------------------------------------
@@ -990,13 +1145,14 @@ static std::vector<int> choose(int form, const mfcuda_gemm_desc *d, int64_t coun
 // Split-K rule: K chunks of at most KC_BLOCKS blocks (the INT32 bound); when
 // the whole batch has fewer items than four per SM, shorter chunks raise the
 // item count (the chunks' INT32 partials are summed exactly in the combine).
-static int choose_kcb(const mfcuda_gemm_desc *d, int64_t count, const std::vector<int> &cfg) {
+static int choose_kcb(const mfcuda_gemm_desc *d, int64_t count, const std::vector<int> &cfg, int prods = 1) {
   int64_t items = 0, kmax = 1;
   for (int64_t p = 0; p < count; ++p) {
     if (d[p].m <= 0 || d[p].n <= 0) continue;
     int64_t kb = (ru(std::max<int64_t>(d[p].k, 1), BK)) / BK;
     kmax = std::max(kmax, kb);
-    items += (int64_t)SMAX * ((kb + KC_BLOCKS - 1) / KC_BLOCKS) * (ru(d[p].m, BM) / BM) * (ru(d[p].n, cfg[p]) / cfg[p]);
+    items += (int64_t)prods * SMAX * ((kb + KC_BLOCKS - 1) / KC_BLOCKS) * (ru(d[p].m, BM) / BM) *
+             (ru(d[p].n, cfg[p]) / cfg[p]);
   }
   const int64_t want = (int64_t)sm_count() * 4;
   if (items >= want || items == 0) return KC_BLOCKS;
@@ -1010,9 +1166,8 @@ static int choose_kcb(const mfcuda_gemm_desc *d, int64_t count, const std::vecto
 
 extern "C" {
 
-MULTIFLOATS_CUDA_API int mfcuda_batch_create_gemm(const mfcuda_gemm_desc *descs, int64_t count, int form,
-                                                  int64_t renorm_interval, int slices, double target, int tune,
-                                                  mfcuda_batch **plan) {
+static int batch_create(const mfcuda_gemm_desc *descs, int64_t count, int form, int64_t renorm_interval,
+                        int slices, double target, int tune, mfcuda_batch **plan, bool complex) {
   using namespace mfcuda;
   if (!plan || count < 0 || (count > 0 && !descs)) return MFCUDA_ERR_INVALID_ARG;
   *plan = nullptr;
@@ -1026,10 +1181,25 @@ MULTIFLOATS_CUDA_API int mfcuda_batch_create_gemm(const mfcuda_gemm_desc *descs,
     if (g.m > 0 && g.n > 0 && (!g.c || (g.k > 0 && (!g.a || !g.b)))) return MFCUDA_ERR_INVALID_ARG;
   }
   MF_TRY(require_device());
+  if (complex && form == MFCUDA_FORM_PLAIN)
+    return batch::create_plain(descs, count, renorm_interval, std::vector<int>(count, 1), plan, true);
   std::vector<int> cfg = batch::choose(form, descs, count, tune, renorm_interval);
   if (form == MFCUDA_FORM_PLAIN) return batch::create_plain(descs, count, renorm_interval, cfg, plan);
-  int kcb = batch::choose_kcb(descs, count, cfg);
+  int kcb = batch::choose_kcb(descs, count, cfg, complex ? 4 : 1);
+  if (complex) return batch::create_csplit(descs, count, slices, target, cfg, kcb, plan);
   return batch::create_split(descs, count, slices, target, cfg, kcb, plan);
+}
+
+MULTIFLOATS_CUDA_API int mfcuda_batch_create_gemm(const mfcuda_gemm_desc *descs, int64_t count, int form,
+                                                  int64_t renorm_interval, int slices, double target, int tune,
+                                                  mfcuda_batch **plan) {
+  return batch_create(descs, count, form, renorm_interval, slices, target, tune, plan, false);
+}
+
+MULTIFLOATS_CUDA_API int mfcuda_batch_create_cgemm(const mfcuda_gemm_desc *descs, int64_t count, int form,
+                                                   int64_t renorm_interval, int slices, double target, int tune,
+                                                   mfcuda_batch **plan) {
+  return batch_create(descs, count, form, renorm_interval, slices, target, tune, plan, true);
 }
 
 MULTIFLOATS_CUDA_API int mfcuda_batch_create_unary(int op, const float64x2 *const *xs,

@@ -986,8 +986,16 @@ void orc_split_gemm_kc(const double *a, const double *b, double *c, int64_t m, i
 /* Complex split GEMM: re = Ar Br - Ai Bi, im = Ar Bi + Ai Br, each real
  * product by orc_split_gemm with one slice count S chosen from the exponent
  * spreads of all four operands (A side: Ar, Ai rows; B side: Br, Bi columns). */
+void orc_split_cgemm_kc(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
+                        int S_req, double target, int *info, int64_t kc);
 void orc_split_cgemm(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
                      int S_req, double target, int *info) {
+  orc_split_cgemm_kc(a, b, c, m, k, n, S_req, target, info, SPLIT_KC);
+}
+/* Complex split product with K chunks of kc elements in each real product
+ * (the batched form may use shorter chunks than the single call). */
+void orc_split_cgemm_kc(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
+                        int S_req, double target, int *info, int64_t kc) {
   double *ar = malloc(sizeof(double) * 2 * m * k), *ai = malloc(sizeof(double) * 2 * m * k);
   double *br = malloc(sizeof(double) * 2 * k * n), *bi = malloc(sizeof(double) * 2 * k * n);
   for (int64_t e = 0; e < m * k; ++e) {
@@ -1020,10 +1028,10 @@ void orc_split_cgemm(const double *a, const double *b, double *c, int64_t m, int
   }
   double *rr = malloc(sizeof(double) * 2 * m * n), *ii = malloc(sizeof(double) * 2 * m * n);
   double *ri = malloc(sizeof(double) * 2 * m * n), *ir = malloc(sizeof(double) * 2 * m * n);
-  orc_split_gemm(ar, br, rr, m, k, n, S, target, NULL);
-  orc_split_gemm(ai, bi, ii, m, k, n, S, target, NULL);
-  orc_split_gemm(ar, bi, ri, m, k, n, S, target, NULL);
-  orc_split_gemm(ai, br, ir, m, k, n, S, target, NULL);
+  orc_split_gemm_kc(ar, br, rr, m, k, n, S, target, NULL, kc);
+  orc_split_gemm_kc(ai, bi, ii, m, k, n, S, target, NULL, kc);
+  orc_split_gemm_kc(ar, bi, ri, m, k, n, S, target, NULL, kc);
+  orc_split_gemm_kc(ai, br, ir, m, k, n, S, target, NULL, kc);
   for (int64_t e = 0; e < m * n; ++e) {
     dd re = dd_sub(mk(rr[2 * e], rr[2 * e + 1]), mk(ii[2 * e], ii[2 * e + 1]));
     dd im = dd_add(mk(ri[2 * e], ri[2 * e + 1]), mk(ir[2 * e], ir[2 * e + 1]));

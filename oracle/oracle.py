@@ -66,6 +66,7 @@ def orc():
         L.orc_split_plan.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int]
         L.orc_split_cgemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
         L.orc_split_gemm_kc.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64]
+        L.orc_split_cgemm_kc.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64]
         _orc = L
     return _orc
 
@@ -222,12 +223,13 @@ def split_gemm(a, b, m, k, n, slices=0, target=8.0, kc=73 * 128):
     return c, tuple(int(v) for v in info)
 
 
-def split_cgemm(a, b, m, k, n, slices=0, target=8.0):
-    """Complex split-INT8 product restated on the CPU; returns (C, (S, rho_a, rho_b))."""
+def split_cgemm(a, b, m, k, n, slices=0, target=8.0, kc=73 * 128):
+    """Complex split-INT8 product restated on the CPU (K chunks of `kc` in
+    each real product); returns (C, (S, rho_a, rho_b))."""
     a, b = _c(a), _c(b)
     c = np.empty(4 * m * n)
     info = np.zeros(3, dtype=np.int32)
-    orc().orc_split_cgemm(_p(a), _p(b), _p(c), m, k, n, slices, target, info.ctypes.data)
+    orc().orc_split_cgemm_kc(_p(a), _p(b), _p(c), m, k, n, slices, target, info.ctypes.data, kc)
     return c, tuple(int(v) for v in info)
 
 

@@ -187,3 +187,98 @@ def test_batch_invalid_arguments(cuda_lib):
     assert cuda_lib.mfcuda_batch_create_gemm(d, 1, 7, 8, 0, 8.0, 0, C.byref(p)) == 1  # bad form
     assert cuda_lib.mfcuda_batch_create_gemm(d, 1, 0, 8, 0, 8.0, 0, C.byref(p)) == 1  # NULL pointers
     assert cuda_lib.mfcuda_batch_run(None, None) == 1
+
+
+# ---- complex64x2 batches (the complex configuration's batch of uneven products) ----
+class CBatch:
+    """Complex problems: A (m x k), B (k x n), C (m x n) complex64x2, column-major."""
+
+    def __init__(self, L, dev, shapes, seed, R=0):
+        self.L, self.shapes = L, shapes
+        self.A, self.B, self.C, self.hA, self.hB = [], [], [], [], []
+        for i, (m, k, n) in enumerate(shapes):
+            a = W.complex_from_parts(W.dd_rowcol_scaled(m, k, R, "row", seed + 4 * i) if m * k else np.zeros(0),
+                                     W.dd_rowcol_scaled(m, k, R, "row", seed + 4 * i + 1) if m * k else np.zeros(0))
+            b = W.complex_from_parts(W.dd_rowcol_scaled(k, n, R, "col", seed + 4 * i + 2) if k * n else np.zeros(0),
+                                     W.dd_rowcol_scaled(k, n, R, "col", seed + 4 * i + 3) if k * n else np.zeros(0))
+            self.hA.append(a)
+            self.hB.append(b)
+            self.A.append(to_dev(a, dev) if a.size else None)
+            self.B.append(to_dev(b, dev) if b.size else None)
+            self.C.append(to_dev(np.full(4 * m * n, np.nan), dev) if m * n else None)
+        descs = (_lib.gemm_desc * len(shapes))()
+        for i, (m, k, n) in enumerate(shapes):
+            descs[i].a = self.A[i].data_ptr() if self.A[i] is not None else None
+            descs[i].b = self.B[i].data_ptr() if self.B[i] is not None else None
+            descs[i].c = self.C[i].data_ptr() if self.C[i] is not None else None
+            descs[i].m, descs[i].k, descs[i].n = m, k, n
+        self.descs = descs
+
+    def plan(self, form, ri=8, tune=0):
+        p = C.c_void_p()
+        rc = self.L.mfcuda_batch_create_cgemm(self.descs, len(self.shapes), form, ri, 0, 8.0, tune, C.byref(p))
+        assert rc == 0, self.L.mfcuda_error_string(rc)
+        return p
+
+    def run(self, p):
+        import torch
+
+        assert self.L.mfcuda_batch_run(p, C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+        assert self.L.mfcuda_batch_status(p) == 0
+
+
+def test_complex_plain_batch_bit_exact(cuda_lib, dev):
+    rng = np.random.default_rng(11)
+    shapes = _shapes(rng, 30, 1, 160)
+    bt = CBatch(cuda_lib, dev, shapes, 900)
+    p = bt.plan(0, ri=8)
+    try:
+        assert {cuda_lib.mfcuda_batch_config(p, i) for i in range(len(shapes))} == {32}
+        bt.run(p)
+        for i, (m, k, n) in enumerate(shapes):
+            if m * n == 0:
+                continue
+            want = O.cmatmul_mm(bt.hA[i], bt.hB[i], m, k, n, 8)
+            assert O.same_bits(to_host(bt.C[i]), want).all(), (i, m, k, n)
+    finally:
+        cuda_lib.mfcuda_batch_destroy(p)
+
+
+@pytest.mark.parametrize("tune", [0, 1])
+def test_complex_split_batch_bit_exact(cuda_lib, dev, tune):
+    rng = np.random.default_rng(12 + tune)
+    shapes = _shapes(rng, 14, 4, 260)
+    bt = CBatch(cuda_lib, dev, shapes, 1300, R=8)
+    p = bt.plan(1, tune=tune)
+    try:
+        kc = cuda_lib.mfcuda_batch_kchunk(p)
+        assert kc > 0 and kc % 128 == 0
+        bt.run(p)
+        for i, (m, k, n) in enumerate(shapes):
+            if m * n == 0:
+                continue
+            want, _ = O.split_cgemm(bt.hA[i], bt.hB[i], m, k, n, kc=kc)
+            assert O.same_bits(to_host(bt.C[i]), want).all(), (i, m, k, n, kc)
+    finally:
+        cuda_lib.mfcuda_batch_destroy(p)
+
+
+def test_complex_split_batch_matches_single_call(cuda_lib, dev):
+    """With the single call's K chunk the batch reproduces mfcuda_cmatmuldd_mm_split."""
+    import torch
+
+    shapes = [(200, 300, 150)] * 40  # enough items that the plan keeps full K chunks
+    bt = CBatch(cuda_lib, dev, shapes, 1700, R=16)
+    p = bt.plan(1)
+    try:
+        assert cuda_lib.mfcuda_batch_kchunk(p) == 73 * 128
+        bt.run(p)
+        m, k, n = shapes[0]
+        c = torch.empty(4 * m * n, dtype=torch.float64, device=dev)
+        rc = cuda_lib.mfcuda_cmatmuldd_mm_split(bt.A[0].data_ptr(), bt.B[0].data_ptr(), c.data_ptr(), m, k, n, 0,
+                                                8.0, None, 0, None,
+                                                C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == 0
+        assert O.same_bits(to_host(bt.C[0]), to_host(c)).all()
+    finally:
+        cuda_lib.mfcuda_batch_destroy(p)
