@@ -207,12 +207,12 @@ __global__ void __launch_bounds__(256) g_scan_a(const SProb *probs, const int64_
   const int64_t nbx = (P.m + 255) / 256;
   scan_a_body(P.A, P.m, P.k, P.astride, 64, P.sigA, P.muA, P.flagA, l % nbx, l / nbx);
 }
+// a warp per column, 8 columns per block
 __global__ void __launch_bounds__(256) g_scan_b(const SProb *probs, const int64_t *prefix, int nprob) {
   const int p = find_prob(prefix, nprob, blockIdx.x);
   const SProb &P = probs[p];
-  const int64_t l = blockIdx.x - prefix[p];
-  const int64_t nbx = (P.k + 2047) / 2048;
-  scan_b_body(P.B, P.k, P.n, P.bstride, P.sigB, P.muB, P.flagB, l % nbx, l / nbx);
+  const int64_t j = (int64_t)(blockIdx.x - prefix[p]) * 8 + (threadIdx.x >> 5);
+  if (j < P.n) scan_b_warp(P.B, P.k, P.bstride, P.sigB, P.muB, P.flagB, j);
 }
 __global__ void __launch_bounds__(256) g_plan(const SProb *probs, int slices, double target) {
   const SProb &P = probs[blockIdx.x];
@@ -239,23 +239,29 @@ __global__ void __launch_bounds__(256) g_slice_a(const SProb *probs, const int64
   const int64_t nbx = P.M_pad / 32;
   slice_a_body(P.A, P.m, P.k, P.astride, P.M_pad, P.K_pad, P.sigA, P.flagA, P.plan, P.As, l % nbx, l / nbx);
 }
+// flat: thread t of the problem takes column t / (K_pad / 8), entries 8 (t % (K_pad / 8)) .. + 7
 __global__ void __launch_bounds__(256) g_slice_b(const SProb *probs, const int64_t *prefix, int nprob) {
   const int p = find_prob(prefix, nprob, blockIdx.x);
   const SProb &P = probs[p];
-  const int64_t l = blockIdx.x - prefix[p];
-  const int64_t nbx = (P.K_pad / 8 + 255) / 256;
-  slice_b_body(P.B, P.k, P.n, P.bstride, P.N_pad, P.K_pad, P.sigB, P.flagB, P.plan, P.Bs, l % nbx, l / nbx);
+  const int64_t t = (int64_t)(blockIdx.x - prefix[p]) * 256 + threadIdx.x;
+  const int64_t per_col = P.K_pad / 8;
+  const int64_t j = t / per_col;
+  if (j < P.N_pad)
+    slice_b_one(P.B, P.k, P.n, P.bstride, P.N_pad, P.K_pad, P.sigB, P.flagB, P.plan, P.Bs, j, (t % per_col) * 8);
 }
-// a block covers 128 x 4 rows of one column (combine4_body)
+// flat: thread t of the problem owns rows 4 (t % q) .. + 3 of column t / q,
+// q = ceil(m / 4) (combine4_body)
 constexpr int kCombineThreads = 128;
-static int64_t combine_row_blocks(int64_t m) { return ((m + 3) / 4 + kCombineThreads - 1) / kCombineThreads; }
+static int64_t combine_blocks(int64_t m, int64_t n) {
+  return (((m + 3) / 4) * n + kCombineThreads - 1) / kCombineThreads;
+}
 __global__ void __launch_bounds__(kCombineThreads) g_combine(const SProb *probs, const int64_t *prefix, int nprob) {
   const int p = find_prob(prefix, nprob, blockIdx.x);
   const SProb &P = probs[p];
-  const int64_t l = blockIdx.x - prefix[p];
-  const int64_t nbx = ((P.m + 3) / 4 + kCombineThreads - 1) / kCombineThreads;
+  const int64_t t = (int64_t)(blockIdx.x - prefix[p]) * kCombineThreads + threadIdx.x;
+  const int64_t q = (P.m + 3) / 4;
   combine4_body(P.D, P.plan, P.sigA, P.flagA, P.sigB, P.flagB, P.m, P.n, P.M_pad, P.N_pad, P.nkc, P.C,
-                P.cstride, P.mode, (l % nbx) * kCombineThreads + threadIdx.x, l / nbx);
+                P.cstride, P.mode, t % q, t / q);
 }
 
 struct GItem {
@@ -451,7 +457,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         mftc::tmem_wait_ld();
         int32_t *dst = dst_base + (int64_t)chunk * 32 * P.M_pad;
 #pragma unroll
-        for (int q = 0; q < 32; ++q) dst[(int64_t)q * P.M_pad] = (int32_t)r[q];
+        for (int q = 0; q < 32; ++q) __stcs(dst + (int64_t)q * P.M_pad, (int32_t)r[q]);  // evict-first: keep L2 for the slices
       }
       mftc::tc_fence_before();
       __syncwarp();
@@ -765,12 +771,12 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
       o_bs[q] = ar.take((size_t)SMAX * P.N_pad * P.K_pad, 1024);
     }
     o_d[q] = ar.take((size_t)SMAX * P.nkc * P.N_pad * P.M_pad * sizeof(int32_t));
-    const int64_t comb = combine_row_blocks(P.m) * P.n;
+    const int64_t comb = combine_blocks(P.m, P.n);
     const int64_t blocks[PH_COUNT] = {
         P.own_a ? ((P.m + 255) / 256) * ((P.k + 63) / 64) : 0,
-        P.own_b ? (P.k > 0 ? (P.k + 2047) / 2048 : 0) * P.n : 0,
+        P.own_b && P.k > 0 ? (P.n + 7) / 8 : 0,
         P.own_a ? (P.M_pad / 32) * (P.K_pad / 64) : 0,
-        P.own_b ? ((P.K_pad / 8 + 255) / 256) * P.N_pad : 0,
+        P.own_b ? (P.N_pad * (P.K_pad / 8) + 255) / 256 : 0,
         P.mode == 0 ? comb : 0,
         P.mode != 0 ? comb : 0,
         (int64_t)SMAX * P.nkc * P.ntm * P.ntn};

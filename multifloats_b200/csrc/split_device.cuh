@@ -316,14 +316,12 @@ __device__ __forceinline__ void slice_a_body(const double *__restrict__ A, int64
 // B (k x n column-major) -> Bs[s][j][p]: each thread rounds and slices 8
 // consecutive entries of one column (128 contiguous bytes in, one 8-byte word
 // per slice out).
-__device__ __forceinline__ void slice_b_body(const double *__restrict__ B, int64_t K,
-                                                      int64_t N, int64_t stride, int64_t N_pad,
-                                                      int64_t K_pad, const int *sig, const int *flag,
-                                                      const Plan *plan, int8_t *__restrict__ Bs, int64_t bx, int64_t by) {
+// Entries p8 .. p8+7 of column j (0 <= j < N_pad, p8 a multiple of 8 below K_pad).
+__device__ __forceinline__ void slice_b_one(const double *__restrict__ B, int64_t K, int64_t N,
+                                            int64_t stride, int64_t N_pad, int64_t K_pad, const int *sig,
+                                            const int *flag, const Plan *plan, int8_t *__restrict__ Bs,
+                                            int64_t j, int64_t p8) {
   const int S = plan->S, W = plan->W;
-  const int64_t j = by;
-  const int64_t p8 = (bx * blockDim.x + threadIdx.x) * 8;
-  if (p8 >= K_pad) return;
   const bool col_ok = j < N && !flag[j < N ? j : 0];
   const int tau = j < N ? sig[j] : 0;
   uint32_t y[8][4];
@@ -341,6 +339,47 @@ __device__ __forceinline__ void slice_b_body(const double *__restrict__ B, int64
   for_each_slice_word(y, S, [&](int sl, uint64_t word) {
     *reinterpret_cast<uint64_t *>(Bs + (((int64_t)sl * N_pad + j) * K_pad + p8)) = word;
   });
+}
+// A block per (column by, range of K): thread t of block bx takes entries
+// (bx * blockDim.x + t) * 8 .. + 7.
+__device__ __forceinline__ void slice_b_body(const double *__restrict__ B, int64_t K,
+                                             int64_t N, int64_t stride, int64_t N_pad,
+                                             int64_t K_pad, const int *sig, const int *flag,
+                                             const Plan *plan, int8_t *__restrict__ Bs, int64_t bx, int64_t by) {
+  const int64_t p8 = (bx * blockDim.x + threadIdx.x) * 8;
+  if (p8 >= K_pad) return;
+  slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, by, p8);
+}
+
+// Column j of B (k x n column-major view) scanned by one warp: lane l reads
+// entries l, l+32, ...; the warp's max / min / or is written by lane 0 (no
+// other warp touches column j).
+__device__ __forceinline__ void scan_b_warp(const double *__restrict__ B, int64_t K, int64_t stride, int *sig,
+                                            int *mu, int *flag, int64_t j) {
+  const int lane = threadIdx.x & 31;
+  int hi_e = SENT_LO, lo_e = SENT_HI, bad = 0;
+  for (int64_t p = lane; p < K; p += 32) {
+    double2 v = __ldg(reinterpret_cast<const double2 *>(B) + (j * K + p) * stride);
+    if (!isfinite(v.x) || !isfinite(v.y)) {
+      bad = 1;
+      continue;
+    }
+    double a = fabs(v.x) + fabs(v.y);
+    if (a != 0.0) {
+      hi_e = max(hi_e, binade_above(a));
+      lo_e = min(lo_e, binade_below(a));
+    }
+  }
+  for (int off = 16; off >= 1; off >>= 1) {
+    hi_e = max(hi_e, __shfl_xor_sync(0xffffffffu, hi_e, off));
+    lo_e = min(lo_e, __shfl_xor_sync(0xffffffffu, lo_e, off));
+    bad |= __shfl_xor_sync(0xffffffffu, bad, off);
+  }
+  if (lane == 0) {
+    sig[j] = hi_e;
+    mu[j] = lo_e;
+    flag[j] = bad;
+  }
 }
 
 // Thread per row i (consecutive threads -> consecutive rows: every load and

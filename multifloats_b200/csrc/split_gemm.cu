@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         mftc::tmem_wait_ld();
         int32_t *dst = dst_base + (int64_t)chunk * 32 * M_pad;
 #pragma unroll
-        for (int q = 0; q < 32; ++q) dst[(int64_t)q * M_pad] = (int32_t)r[q];
+        for (int q = 0; q < 32; ++q) __stcs(dst + (int64_t)q * M_pad, (int32_t)r[q]);  // evict-first: keep L2 for the slices
       }
       mftc::tc_fence_before();
       __syncwarp();
@@ -552,7 +552,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
         mftc::tmem_wait_ld();
         int32_t *dst = dst_base + (int64_t)chunk * 32 * M_pad;
 #pragma unroll
-        for (int q = 0; q < 32; ++q) dst[(int64_t)q * M_pad] = (int32_t)v[q];
+        for (int q = 0; q < 32; ++q) __stcs(dst + (int64_t)q * M_pad, (int32_t)v[q]);  // evict-first: keep L2 for the slices
       }
       mftc::tc_fence_before();
       __syncwarp();

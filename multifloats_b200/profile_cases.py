@@ -24,7 +24,7 @@ def main() -> int:
     from multifloats_b200 import workloads as W
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["split", "plain", "elementwise", "reduce", "all"])
+    ap.add_argument("case", choices=["split", "plain", "elementwise", "reduce", "batched", "all"])
     ap.add_argument("--n", type=int, default=2048, help="matrix size for split / plain")
     args = ap.parse_args()
     dev = torch.device("cuda:0")
@@ -57,6 +57,32 @@ def main() -> int:
         api.dot_product(x, y)
         api.sum_dd(x)
         api.norm2(x)
+    if args.case == "batched":
+        # the batched configuration: 2000 GEMMs, M, N, K log-uniform in [16, 1024],
+        # plain and split plans (built-in tile choice), each run once
+        import numpy as np
+
+        rng = np.random.default_rng(2024)
+        shapes = [tuple(int(v) for v in s) for s in np.exp(rng.uniform(np.log(16), np.log(1024), (2000, 3)))]
+        tot = sum(m * k + k * n for m, k, n in shapes)
+        buf = d(W.dd_uniform(tot, 7))
+        out = torch.empty(2 * sum(m * n for m, _, n in shapes), dtype=torch.float64, device=dev)
+        descs = (_lib.gemm_desc * len(shapes))()
+        off = oc = 0
+        for i, (m, k, n) in enumerate(shapes):
+            descs[i].a = buf[2 * off:].data_ptr()
+            off += m * k
+            descs[i].b = buf[2 * off:].data_ptr()
+            off += k * n
+            descs[i].c = out[2 * oc:].data_ptr()
+            oc += m * n
+            descs[i].m, descs[i].k, descs[i].n = m, k, n
+        for form in (0, 1):
+            p = C.c_void_p()
+            _lib.check(L.mfcuda_batch_create_gemm(descs, len(shapes), form, 8, 0, 8.0, 0, C.byref(p)), "batch")
+            _lib.check(L.mfcuda_batch_run(p, sp), "run")
+            _lib.check(L.mfcuda_batch_status(p), "status")
+            L.mfcuda_batch_destroy(p)
     torch.cuda.synchronize()
     print("ok")
     return 0
