@@ -748,8 +748,13 @@ def run_reference(args, ws, rank):
     line = {
         "metric": METRIC, "value": value, "unit": "DD-GFLOP/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": "dd_gemm_4096", "M": M, "N": N, "K": K, "renorm_interval": RI},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded; hi = +-u 2^e, u~U[1,2), e~U{-16..16} per row of A / column of B)",
+        "impl": "reference",
+        "config": {"workload": "dd_gemm_4096_split_int8", "M": M, "N": N, "K": K, "R": 16,
+                   "renorm_interval": RI, "parallelism": f"independent problem per GPU x{ws}",
+                   "form": "the reference library's CPU matmuldd_mm (plain compensated form; the "
+                           "reference has no split form), built from its sources, all host cores"},
         "cpu_baseline": {"value": value, "unit": "DD-GFLOP/s", "cores": threads, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "DD-GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
