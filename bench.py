@@ -693,6 +693,44 @@ def run_complex(args):
                                         "real_dd_gflop_per_step": bflops / 1e9}})
 
 
+def run_gemv(args):
+    """matmuldd_mv / matmuldd_vm device paths (HBM-bound: 16 bytes of the
+    matrix per MAC), bit-identical to the reference's sequential MAC."""
+    import torch
+
+    from multifloats_b200 import _lib
+
+    L = _lib.lib()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    res = {}
+    for m in (4096, 16384):
+        A = _dev_dd_uniform(m * m, 3, dev)
+        x = _dev_dd_uniform(m, 4, dev)
+        yv = torch.empty(2 * m, dtype=torch.float64, device=dev)
+
+        def mv():
+            _lib.check(L.mfcuda_matmuldd_mv(A.data_ptr(), x.data_ptr(), yv.data_ptr(), m, m, RI, sp), "mv")
+
+        def vm():
+            _lib.check(L.mfcuda_matmuldd_vm(x.data_ptr(), A.data_ptr(), yv.data_ptr(), m, m, RI, sp), "vm")
+
+        for name, fn in (("mv", mv), ("vm", vm)):
+            ms = _events_time(fn, args.steps, args.warmup, stream)
+            gbs = 16.0 * m * m / ms / 1e6
+            res[f"{name}_{m}"] = {"ms": ms, "gbs": gbs, "frac_hbm": gbs / HBM_GBS,
+                                  "dd_gflops": 2.0 * m * m / ms / 1e6}
+        del A, x, yv
+        torch.cuda.empty_cache()
+    _line(args, "dd_gemv_4096_16384", "DD matrix-vector GB/s (matrix bytes / time), mv 16384^2",
+          res["mv_16384"]["gbs"], "GB/s",
+          {"dtype": "f64", "per_case": res,
+           "roofline": {"bound": "hbm", "kernel": "gemv_dd_kernel", "achieved": res["mv_16384"]["gbs"],
+                        "peak": HBM_GBS, "unit": "GB/s", "frac": res["mv_16384"]["frac_hbm"], "traffic": None,
+                        "peak_source": "MEASURED_PEAKS.json hbm_gbs"}})
+
+
 def run_gemm8192(args):
     import torch
 
@@ -772,7 +810,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="gemm4096",
-                    choices=["gemm4096", "elementwise", "reductions", "batched", "complex", "gemm8192"])
+                    choices=["gemm4096", "elementwise", "reductions", "batched", "complex", "gemm8192", "gemv"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -782,7 +820,7 @@ def main():
         return
     if args.workload != "gemm4096":
         {"elementwise": run_elementwise, "reductions": run_reductions, "batched": run_batched,
-         "complex": run_complex, "gemm8192": run_gemm8192}[args.workload](args)
+         "complex": run_complex, "gemm8192": run_gemm8192, "gemv": run_gemv}[args.workload](args)
         return
     ws, rank, local = dist_init()
     try:

@@ -17,6 +17,8 @@
 // depth BK are staged in shared memory with cp.async (16-byte copies,
 // zero-filled past the matrix edge) in a two-stage ring.  Bound: FP64 pipe,
 // 13 FP64 instructions per MAC plus 6 per renormalisation.
+#include <mutex>
+
 #include "common.cuh"
 #include "dd_device.cuh"
 #include "gemm_tile.cuh"
@@ -57,73 +59,236 @@ __global__ void __launch_bounds__(kThreads, 2)
 }
 
 // ---------------------------------------------------------------------------
-// y(m) = A(m,k) x(k): one thread per row, k sequential (gaxpy_mv_panel,
-// matmul.inc:47-88, A is the MAC's first operand).
+// Matrix-vector forms.  Every output keeps the reference's sequential MAC over
+// p = 0..k-1, so there is one dependency chain per output and only a few
+// thousand of them; a CTA owns 32 outputs and splits each MAC
+// (matmul.inc:6-19) in two:
+//   * three producer warps stream the matrix through a 4-stage cp.async ring
+//     (32 outputs x 32 k per stage) and compute the accumulator-independent
+//     part of every MAC, p = ah*bh and q = fma(ah,bh,-p) + fma(ah,bl,al*bh),
+//     into a double-buffered shared array;
+//   * one warp runs the accumulator chain (two_sum of s_hi with p, then
+//     s_lo += q + (aerr + berr)) and the renorm cadence, lane = output.
+// The operations and their order per output are the reference's, so results
+// are bit-identical; the producers and the chain hand over through
+// __syncthreads once per stage.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) gemv_dd_kernel(const double *__restrict__ A,
-                                                      const double *__restrict__ x,
-                                                      double *__restrict__ y, int64_t M,
-                                                      int64_t K, int64_t ri) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= M) return;
-  double sh = 0.0, sl = 0.0;
-  int64_t cnt = 0;
-  for (int64_t p = 0; p < K; ++p) {
-    double ah = A[2 * (p * M + i)], al = A[2 * (p * M + i) + 1];
-    double xh = __ldg(x + 2 * p), xl = __ldg(x + 2 * p + 1);
-    mfdev::mac(ah, al, xh, xl, sh, sl);
-    if (ri > 0 && ++cnt == ri) {
-      cnt = 0;
-      if (p + 1 < K) mfdev::renorm(sh, sl);
-    }
-  }
-  mfdev::renorm(sh, sl);
-  y[2 * i] = sh;
-  y[2 * i + 1] = sl;
+constexpr int kGvN = 32, kGvK = 32, kGvStages = 4, kGvPitch = 33, kGvProd = 3;
+constexpr int kGvThreads = 32 * (1 + kGvProd);
+constexpr size_t kGvRingBytes = sizeof(double2) * kGvStages * kGvN * kGvPitch;
+constexpr size_t kGvSmem = kGvRingBytes + sizeof(double2) * 2 * kGvK * kGvPitch;
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait_n() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// y(n) = x(k) B(k,n): one thread per column, k sequential, x is the MAC's
-// first operand (vm_impl, matmul.inc:213-239).  B k-slices are staged in
-// shared memory so the column reads coalesce.
-constexpr int kVmP = 8;
-__global__ void __launch_bounds__(256) gevm_dd_kernel(const double *__restrict__ x,
-                                                      const double *__restrict__ B,
-                                                      double *__restrict__ y, int64_t K,
-                                                      int64_t N, int64_t ri) {
-  __shared__ double2 Bs[256][kVmP + 1];
-  const int t = threadIdx.x;
-  const int64_t j0 = (int64_t)blockIdx.x * 256;
-  const int64_t j = j0 + t;
-  double sh = 0.0, sl = 0.0;
-  int64_t cnt = 0;
-  for (int64_t p0 = 0; p0 < K; p0 += kVmP) {
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < kVmP; ++r) {
-      int idx = t + r * 256;
-      int col = idx / kVmP, pp = idx % kVmP;
-      int64_t gj = j0 + col, gp = p0 + pp;
-      double2 v = make_double2(0.0, 0.0);
-      if (gj < N && gp < K) {
-        const double *src = B + 2 * (gj * K + gp);
-        v = make_double2(src[0], src[1]);
-      }
-      Bs[col][pp] = v;
-    }
-    __syncthreads();
-    int pmax = (K - p0) < kVmP ? (int)(K - p0) : kVmP;
-    for (int pp = 0; pp < pmax; ++pp) {
-      int64_t p = p0 + pp;
-      double xh = __ldg(x + 2 * p), xl = __ldg(x + 2 * p + 1);
-      double2 b = Bs[t][pp];
-      mfdev::mac(xh, xl, b.x, b.y, sh, sl);
-      if (ri > 0 && ++cnt == ri) {
+// The accumulator half of mac_inl for one output: p and q from the producers.
+__device__ __forceinline__ void mac_chain(double p, double q, double &s_hi, double &s_lo) {
+  double t = mfdev::add(s_hi, p);
+  double bp = mfdev::sub(t, s_hi);
+  double ap = mfdev::sub(t, bp);
+  double aerr = mfdev::sub(s_hi, ap);
+  double berr = mfdev::sub(p, bp);
+  s_lo = mfdev::add(s_lo, mfdev::add(q, mfdev::add(aerr, berr)));
+  s_hi = t;
+}
+// The accumulator-independent half: p = ah bh, q = e + cross (same operations as mac).
+__device__ __forceinline__ double2 mac_terms(double ah, double al, double bh, double bl) {
+  double p = mfdev::mul(ah, bh);
+  double e = mfdev::fma_(ah, bh, -p);
+  double cross = mfdev::fma_(ah, bl, mfdev::mul(al, bh));
+  return make_double2(p, mfdev::add(e, cross));
+}
+
+// Runs the chain over stage st's terms (lane = output), renorm cadence as in
+// the reference: after each full chunk of ri steps when more remain.  The
+// MACs between two renorm points run as one branch-free loop, so the
+// compiler can start a MAC's t = s_hi + p while the previous MAC's error
+// terms are still in flight (same operations, same order).
+__device__ __forceinline__ void chain_stage(const double2 *__restrict__ pq, int cmax, int64_t p0, int64_t K,
+                                            int64_t ri, int lane, double &sh, double &sl, int64_t &cnt) {
+  int c = 0;
+  while (c < cmax) {
+    const int run = ri > 0 ? (int)min((int64_t)(cmax - c), ri - cnt) : cmax - c;
+    const double2 *v = pq + (size_t)c * kGvPitch + lane;
+#pragma unroll 8
+    for (int r = 0; r < run; ++r) mac_chain(v[r * kGvPitch].x, v[r * kGvPitch].y, sh, sl);
+    c += run;
+    if (ri > 0) {
+      cnt += run;
+      if (cnt == ri) {
         cnt = 0;
-        if (p + 1 < K) mfdev::renorm(sh, sl);
+        if (p0 + c < K) mfdev::renorm(sh, sl);
       }
     }
   }
-  if (j < N) {
+}
+
+// y(m) = A(m,k) x(k) (gaxpy_mv_panel, matmul.inc:47-88; A is the MAC's first
+// operand).  Producer warp w copies and evaluates the stage columns c with
+// c % 3 == w - 1, lane l = row i0 + l (each copy instruction moves one
+// 512-byte segment of column-major A; a thread reads only what it copied).
+template <bool ALIGNED>
+__global__ void __launch_bounds__(kGvThreads) gemv_dd_kernel(const double *__restrict__ A,
+                                                             const double *__restrict__ x,
+                                                             double *__restrict__ y, int64_t M,
+                                                             int64_t K, int64_t ri) {
+  extern __shared__ double2 smem_gv[];
+  double2 *ring = smem_gv;                                   // [stage][k][row pitch]
+  double2 *pq = smem_gv + (size_t)kGvStages * kGvK * kGvPitch;  // [2][k][row pitch]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t i = (int64_t)blockIdx.x * kGvN + lane;
+  const bool row_ok = i < M;
+  const int64_t nst = (K + kGvK - 1) / kGvK;
+  const int w = warp - 1;  // producer index
+  auto issue = [&](int64_t st) {
+    if (st < nst) {
+      double2 *dst = ring + (size_t)(st % kGvStages) * kGvK * kGvPitch;
+      const int64_t p0 = st * kGvK;
+      const double *src = A + 2 * ((p0 + w) * M + i);
+#pragma unroll
+      for (int c = w; c < kGvK; c += kGvProd, src += 2 * kGvProd * M)
+        load_dd<ALIGNED>(&dst[c * kGvPitch + lane], src, row_ok && p0 + c < K, A);
+    }
+    cp_async_commit();
+  };
+  auto load_x = [&](int64_t st) {  // lane l: x[st * 32 + l] (zero past k), one stage ahead of use
+    double2 v = make_double2(0.0, 0.0);
+    const int64_t p = st * kGvK + lane;
+    if (st < nst && p < K) {
+      const double *xp = x + 2 * p;
+      v = ALIGNED ? *reinterpret_cast<const double2 *>(xp) : make_double2(xp[0], xp[1]);
+    }
+    return v;
+  };
+  auto produce = [&](int64_t st, double2 xv) {  // terms of stage st into pq[st % 2]
+    if (st >= nst) return;
+    const int64_t p0 = st * kGvK;
+    const int cmax = (K - p0) < kGvK ? (int)(K - p0) : kGvK;
+    const double2 *src = ring + (size_t)(st % kGvStages) * kGvK * kGvPitch;
+    double2 *out = pq + (size_t)(st & 1) * kGvK * kGvPitch;
+#pragma unroll
+    for (int c0 = 0; c0 < kGvK; c0 += kGvProd) {
+      const int c = c0 + w;
+      const double xh = __shfl_sync(0xffffffffu, xv.x, c & 31), xl = __shfl_sync(0xffffffffu, xv.y, c & 31);
+      if (c < cmax) {
+        const double2 av = src[c * kGvPitch + lane];
+        out[c * kGvPitch + lane] = mac_terms(av.x, av.y, xh, xl);
+      }
+    }
+  };
+  double2 xnext = make_double2(0.0, 0.0);
+  if (warp > 0) {
+    for (int s0 = 0; s0 < kGvStages - 1; ++s0) issue(s0);
+    const double2 x0 = load_x(0);
+    xnext = load_x(1);
+    cp_async_wait_n<kGvStages - 2>();  // stage 0 landed
+    produce(0, x0);
+  }
+  __syncthreads();
+  double sh = 0.0, sl = 0.0;
+  int64_t cnt = 0;
+  for (int64_t st = 0; st < nst; ++st) {
+    if (warp == 0) {
+      const int64_t p0 = st * kGvK;
+      const int cmax = (K - p0) < kGvK ? (int)(K - p0) : kGvK;
+      chain_stage(pq + (size_t)(st & 1) * kGvK * kGvPitch, cmax, p0, K, ri, lane, sh, sl, cnt);
+    } else {
+      issue(st + kGvStages - 1);        // into the slot of stage st - 1, consumed already
+      const double2 xcur = xnext;
+      xnext = load_x(st + 2);
+      cp_async_wait_n<kGvStages - 2>();  // stage st + 1 landed
+      produce(st + 1, xcur);
+    }
+    __syncthreads();
+  }
+  if (warp > 0) cp_async_wait_n<0>();
+  if (warp == 0 && row_ok) {
+    mfdev::renorm(sh, sl);
+    y[2 * i] = sh;
+    y[2 * i + 1] = sl;
+  }
+}
+
+// y(n) = x(k) B(k,n) (vm_impl, matmul.inc:213-239; x is the MAC's first
+// operand).  Producer warp w copies the stage's columns jj with
+// jj % 3 == w - 1, lane l taking k = p0 + l (one 512-byte segment of
+// column-major B per copy instruction), and evaluates exactly the entries it
+// copied; the chain warp's lane j owns column j0 + j.
+template <bool ALIGNED>
+__global__ void __launch_bounds__(kGvThreads) gevm_dd_kernel(const double *__restrict__ x,
+                                                             const double *__restrict__ B,
+                                                             double *__restrict__ y, int64_t K,
+                                                             int64_t N, int64_t ri) {
+  extern __shared__ double2 smem_gv[];
+  double2 *ring = smem_gv;                                   // [stage][column][k pitch]
+  double2 *pq = smem_gv + (size_t)kGvStages * kGvN * kGvPitch;  // [2][k][column pitch]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t j0 = (int64_t)blockIdx.x * kGvN;
+  const int64_t nst = (K + kGvK - 1) / kGvK;
+  const int w = warp - 1;
+  auto issue = [&](int64_t st) {
+    if (st < nst) {
+      double2 *dst = ring + (size_t)(st % kGvStages) * kGvN * kGvPitch;
+      const int64_t p = st * kGvK + lane;
+      const double *src = B + 2 * ((j0 + w) * K + p);
+#pragma unroll
+      for (int jj = w; jj < kGvN; jj += kGvProd, src += 2 * kGvProd * K)
+        load_dd<ALIGNED>(&dst[jj * kGvPitch + lane], src, j0 + jj < N && p < K, B);
+    }
+    cp_async_commit();
+  };
+  auto load_x = [&](int64_t st) {  // lane l: x[st * 32 + l] (zero past k), one stage ahead of use
+    double2 v = make_double2(0.0, 0.0);
+    const int64_t p = st * kGvK + lane;
+    if (st < nst && p < K) {
+      const double *xp = x + 2 * p;
+      v = ALIGNED ? *reinterpret_cast<const double2 *>(xp) : make_double2(xp[0], xp[1]);
+    }
+    return v;
+  };
+  auto produce = [&](int64_t st, double2 xv) {
+    if (st >= nst) return;
+    const int64_t p0 = st * kGvK;
+    const int cmax = (K - p0) < kGvK ? (int)(K - p0) : kGvK;
+    if (lane >= cmax) return;  // k = p0 + lane past the end: never read
+    const double2 *src = ring + (size_t)(st % kGvStages) * kGvN * kGvPitch;
+    double2 *out = pq + (size_t)(st & 1) * kGvK * kGvPitch;
+#pragma unroll
+    for (int jj = w; jj < kGvN; jj += kGvProd) {
+      const double2 bv = src[jj * kGvPitch + lane];
+      out[lane * kGvPitch + jj] = mac_terms(xv.x, xv.y, bv.x, bv.y);  // pitch 33: conflict-free
+    }
+  };
+  double2 xnext = make_double2(0.0, 0.0);
+  if (warp > 0) {
+    for (int s0 = 0; s0 < kGvStages - 1; ++s0) issue(s0);
+    const double2 x0 = load_x(0);
+    xnext = load_x(1);
+    cp_async_wait_n<kGvStages - 2>();
+    produce(0, x0);
+  }
+  __syncthreads();
+  double sh = 0.0, sl = 0.0;
+  int64_t cnt = 0;
+  for (int64_t st = 0; st < nst; ++st) {
+    if (warp == 0) {
+      const int64_t p0 = st * kGvK;
+      const int cmax = (K - p0) < kGvK ? (int)(K - p0) : kGvK;
+      chain_stage(pq + (size_t)(st & 1) * kGvK * kGvPitch, cmax, p0, K, ri, lane, sh, sl, cnt);
+    } else {
+      issue(st + kGvStages - 1);
+      const double2 xcur = xnext;
+      xnext = load_x(st + 2);
+      cp_async_wait_n<kGvStages - 2>();
+      produce(st + 1, xcur);
+    }
+    __syncthreads();
+  }
+  if (warp > 0) cp_async_wait_n<0>();
+  const int64_t j = j0 + lane;
+  if (warp == 0 && j < N) {
     mfdev::renorm(sh, sl);
     y[2 * j] = sh;
     y[2 * j + 1] = sl;
@@ -198,17 +363,32 @@ int cgemm_dev(const complex64x2 *a, const complex64x2 *b, complex64x2 *c, int64_
   return MFCUDA_OK;
 }
 
+// dynamic shared memory above the 48 KB default, set once per process
+static void gv_attrs() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(gemv_dd_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGvSmem);
+    cudaFuncSetAttribute(gemv_dd_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGvSmem);
+    cudaFuncSetAttribute(gevm_dd_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGvSmem);
+    cudaFuncSetAttribute(gevm_dd_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGvSmem);
+  });
+}
+
 int gemv_dev(const float64x2 *a, const float64x2 *x, float64x2 *y, int64_t m, int64_t k,
              int64_t ri, cudaStream_t s) {
   if (!shape_ok(m, k, 1, sizeof(float64x2))) return MFCUDA_ERR_INVALID_ARG;
   if (m == 0) return MFCUDA_OK;
   if (!y || (k > 0 && (!a || !x))) return MFCUDA_ERR_INVALID_ARG;
   MF_TRY(require_device());
-  int64_t blocks = (m + 255) / 256;
+  int64_t blocks = (m + kGvN - 1) / kGvN;
   if (blocks > INT32_MAX) return MFCUDA_ERR_UNSUPPORTED;
-  gemv_dd_kernel<<<(unsigned)blocks, 256, 0, s>>>(reinterpret_cast<const double *>(a),
-                                                   reinterpret_cast<const double *>(x),
-                                                   reinterpret_cast<double *>(y), m, k, ri);
+  gv_attrs();
+  const double *A = reinterpret_cast<const double *>(a), *X = reinterpret_cast<const double *>(x);
+  double *Y = reinterpret_cast<double *>(y);
+  if (aligned16(a, x, y))
+    gemv_dd_kernel<true><<<(unsigned)blocks, kGvThreads, kGvSmem, s>>>(A, X, Y, m, k, ri);
+  else
+    gemv_dd_kernel<false><<<(unsigned)blocks, kGvThreads, kGvSmem, s>>>(A, X, Y, m, k, ri);
   MF_TRY_CUDA(cudaGetLastError());
   return MFCUDA_OK;
 }
@@ -219,11 +399,15 @@ int gevm_dev(const float64x2 *x, const float64x2 *b, float64x2 *y, int64_t k, in
   if (n == 0) return MFCUDA_OK;
   if (!y || (k > 0 && (!b || !x))) return MFCUDA_ERR_INVALID_ARG;
   MF_TRY(require_device());
-  int64_t blocks = (n + 255) / 256;
+  int64_t blocks = (n + kGvN - 1) / kGvN;
   if (blocks > INT32_MAX) return MFCUDA_ERR_UNSUPPORTED;
-  gevm_dd_kernel<<<(unsigned)blocks, 256, 0, s>>>(reinterpret_cast<const double *>(x),
-                                                   reinterpret_cast<const double *>(b),
-                                                   reinterpret_cast<double *>(y), k, n, ri);
+  gv_attrs();
+  const double *X = reinterpret_cast<const double *>(x), *Bm = reinterpret_cast<const double *>(b);
+  double *Y = reinterpret_cast<double *>(y);
+  if (aligned16(x, b, y))
+    gevm_dd_kernel<true><<<(unsigned)blocks, kGvThreads, kGvSmem, s>>>(X, Bm, Y, k, n, ri);
+  else
+    gevm_dd_kernel<false><<<(unsigned)blocks, kGvThreads, kGvSmem, s>>>(X, Bm, Y, k, n, ri);
   MF_TRY_CUDA(cudaGetLastError());
   return MFCUDA_OK;
 }

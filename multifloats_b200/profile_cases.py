@@ -24,7 +24,7 @@ def main() -> int:
     from multifloats_b200 import workloads as W
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["split", "plain", "elementwise", "reduce", "batched", "all"])
+    ap.add_argument("case", choices=["split", "plain", "elementwise", "reduce", "batched", "gemv", "all"])
     ap.add_argument("--n", type=int, default=2048, help="matrix size for split / plain")
     args = ap.parse_args()
     dev = torch.device("cuda:0")
@@ -57,6 +57,11 @@ def main() -> int:
         api.dot_product(x, y)
         api.sum_dd(x)
         api.norm2(x)
+    if args.case in ("gemv", "all"):
+        m = 4096
+        a, x = d(W.dd_uniform(m * m, 8)), d(W.dd_uniform(m, 9))
+        api.matmuldd_mv(a, x, m, m, 8)
+        api.matmuldd_vm(x, a, m, m, 8)
     if args.case == "batched":
         # the batched configuration: 2000 GEMMs, M, N, K log-uniform in [16, 1024],
         # plain and split plans (built-in tile choice), each run once

@@ -122,3 +122,24 @@ def test_mv_vm_large(dev):
     xv = W.dd_uniform(m, seed=19)
     y = to_host(api.matmuldd_vm(to_dev(xv, dev), to_dev(a, dev), m, k, 8))
     assert O.same_bits(y, O.matmul_vm(xv, a, m, k, 8)).all()
+
+
+@pytest.mark.parametrize("ri", [0, 3, 8])
+@pytest.mark.parametrize("m,k", [(1, 1), (77, 45), (33, 65), (1000, 97)])
+def test_mv_vm_ragged_and_unaligned(dev, m, k, ri):
+    """Sizes off the 32-row / 32-k staging grid, every renorm cadence, and
+    8-byte-offset (not 16-byte-aligned) operand views."""
+    import torch
+
+    a, x, xv = W.dd_uniform(m * k, seed=m + k), W.dd_uniform(k, seed=m + 1), W.dd_uniform(m, seed=k + 2)
+    want_mv, want_vm = O.matmul_mv(a, x, m, k, ri), O.matmul_vm(xv, a, m, k, ri)
+    for offset in (0, 1):
+        def view(v):
+            buf = torch.empty(v.size + offset, dtype=torch.float64, device=dev)
+            buf[offset:] = torch.from_numpy(v).to(dev)
+            return buf[offset:]
+
+        y = to_host(api.matmuldd_mv(view(a), view(x), m, k, ri))
+        assert O.same_bits(y, want_mv).all(), ("mv", offset)
+        y = to_host(api.matmuldd_vm(view(xv), view(a), m, k, ri))
+        assert O.same_bits(y, want_vm).all(), ("vm", offset)
