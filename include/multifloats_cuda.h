@@ -114,6 +114,20 @@ MULTIFLOATS_CUDA_API void logdd_array(const float64x2 *x, float64x2 *y, int64_t 
 MULTIFLOATS_CUDA_API void sindd_array(const float64x2 *x, float64x2 *y, int64_t n);
 MULTIFLOATS_CUDA_API void cosdd_array(const float64x2 *x, float64x2 *y, int64_t n);
 MULTIFLOATS_CUDA_API void sqrtdd_array(const float64x2 *x, float64x2 *y, int64_t n);
+/* exp2dd / log2dd / log10dd (src/float64x2/exp_log.inc:109-128, :311-326,
+ * :344-353) per element; bit-identical. */
+MULTIFLOATS_CUDA_API void exp2dd_array(const float64x2 *x, float64x2 *y, int64_t n);
+MULTIFLOATS_CUDA_API void log2dd_array(const float64x2 *x, float64x2 *y, int64_t n);
+MULTIFLOATS_CUDA_API void log10dd_array(const float64x2 *x, float64x2 *y, int64_t n);
+/* Fused sine and cosine: sincosdd (src/float64x2/abi.inc:123-125,
+ * trig.inc:216-236) per element, one range reduction for both outputs;
+ * equal bit for bit to sindd / cosdd. */
+MULTIFLOATS_CUDA_API void sincosdd_array(const float64x2 *x, float64x2 *s, float64x2 *c, int64_t n);
+/* z[i] = cos x[i] + i sin x[i]: cexpidd (abi.inc:226-229). */
+MULTIFLOATS_CUDA_API void cexpidd_array(const float64x2 *x, complex64x2 *z, int64_t n);
+/* w[i] = exp(z[i]): cexpdd (src/complex64x2/abi.inc:189, the std::exp
+ * specialisation of src/complex64x2/std.inc:20-74, C99 Annex G special values). */
+MULTIFLOATS_CUDA_API void cexpdd_array(const complex64x2 *z, complex64x2 *w, int64_t n);
 
 /* Reductions: the Fortran-only sum / dot_product / norm2 generics
  * (fsrc/multifloats.fypp:1980-2019, :2094-2158, :2254-2331, :2338-2352) as
@@ -202,7 +216,21 @@ MULTIFLOATS_CUDA_API void mfcuda_phase_profile_begin(void);
 MULTIFLOATS_CUDA_API int mfcuda_phase_profile_end(double *phase_ms_sum, int64_t *calls);
 
 /* op: 0 exp, 1 log, 2 sin, 3 cos, 4 sqrt */
-enum { MFCUDA_EXP = 0, MFCUDA_LOG = 1, MFCUDA_SIN = 2, MFCUDA_COS = 3, MFCUDA_SQRT = 4 };
+enum {
+  MFCUDA_EXP = 0,
+  MFCUDA_LOG = 1,
+  MFCUDA_SIN = 2,
+  MFCUDA_COS = 3,
+  MFCUDA_SQRT = 4,
+  MFCUDA_EXP2 = 5,  /* exp2dd, src/float64x2/exp_log.inc:109-128 */
+  MFCUDA_LOG2 = 6,  /* log2dd, exp_log.inc:311-326 */
+  MFCUDA_LOG10 = 7  /* log10dd, exp_log.inc:344-353 */
+};
+/* Device forms of sincosdd_array, cexpidd_array, cexpdd_array. */
+MULTIFLOATS_CUDA_API int mfcuda_sincos_dd(const float64x2 *x, float64x2 *s, float64x2 *c, int64_t n,
+                                          void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_cexpi_dd(const float64x2 *x, complex64x2 *z, int64_t n, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_cexp_dd(const complex64x2 *z, complex64x2 *w, int64_t n, void *stream);
 MULTIFLOATS_CUDA_API int mfcuda_unary_dd(int op, const float64x2 *x, float64x2 *y, int64_t n,
                                          void *stream);
 

@@ -90,6 +90,15 @@ SIGNATURES = {
     "mfcuda_matmuldd_vm": (C.c_int, [P, P, P, I64, I64, I64, P]),
     "mfcuda_cmatmuldd_mm": (C.c_int, [P, P, P, I64, I64, I64, I64, P]),
     "mfcuda_unary_dd": (C.c_int, [C.c_int, P, P, I64, P]),
+    "mfcuda_sincos_dd": (C.c_int, [P, P, P, I64, P]),
+    "mfcuda_cexpi_dd": (C.c_int, [P, P, I64, P]),
+    "mfcuda_cexp_dd": (C.c_int, [P, P, I64, P]),
+    "exp2dd_array": (None, [P, P, I64]),
+    "log2dd_array": (None, [P, P, I64]),
+    "log10dd_array": (None, [P, P, I64]),
+    "sincosdd_array": (None, [P, P, P, I64]),
+    "cexpidd_array": (None, [P, P, I64]),
+    "cexpdd_array": (None, [P, P, I64]),
     "mfcuda_reduce_workspace_size": (C.c_size_t, [I64]),
     "mfcuda_reduce_geometry": (None, [I64, C.POINTER(I64), C.POINTER(I64)]),
     "mfcuda_sumdd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),

@@ -18,7 +18,7 @@ import numpy as np
 
 from ._lib import check, check_last, complex64x2, float64x2, lib
 
-OP = {"exp": 0, "log": 1, "sin": 2, "cos": 3, "sqrt": 4}
+OP = {"exp": 0, "log": 1, "sin": 2, "cos": 3, "sqrt": 4, "exp2": 5, "log2": 6, "log10": 7}
 
 
 def _is_dev(x) -> bool:
@@ -125,7 +125,7 @@ def cmatmuldd_mm(a, b, m: int, k: int, n: int, renorm_interval: int = 8, out=Non
 
 # ---- elementwise ---------------------------------------------------------------
 def unary(op: str, x, out=None):
-    """y[i] = op(x[i]) for op in exp, log, sin, cos, sqrt."""
+    """y[i] = op(x[i]) for op in exp, log, sin, cos, sqrt, exp2, log2, log10."""
     L = lib()
     code = OP[op]
     n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 2
@@ -139,6 +139,56 @@ def unary(op: str, x, out=None):
     getattr(L, f"{op}dd_array")(_ptr(x), _ptr(y), n)
     check_last(f"{op}dd_array")
     return y
+
+
+def sincos(x, s=None, c=None):
+    """(sin x, cos x) elementwise in one pass (sincosdd); device tensors or numpy."""
+    L = lib()
+    n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 2
+    if _is_dev(x):
+        x = _dev_check(x, 2 * n, "x")
+        s = s if s is not None else _empty_like_kind(x, 2 * n)
+        c = c if c is not None else _empty_like_kind(x, 2 * n)
+        check(L.mfcuda_sincos_dd(_ptr(x), _ptr(s), _ptr(c), n, _stream()), "mfcuda_sincos_dd")
+        return s, c
+    x = _host(x, 2 * n, "x")
+    s = s if s is not None else np.empty(2 * n)
+    c = c if c is not None else np.empty(2 * n)
+    L.sincosdd_array(_ptr(x), _ptr(s), _ptr(c), n)
+    check_last("sincosdd_array")
+    return s, c
+
+
+def cexpi(x, out=None):
+    """cos x + i sin x as complex64x2 (cexpidd); device tensors or numpy."""
+    L = lib()
+    n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 2
+    if _is_dev(x):
+        x = _dev_check(x, 2 * n, "x")
+        z = out if out is not None else _empty_like_kind(x, 4 * n)
+        check(L.mfcuda_cexpi_dd(_ptr(x), _ptr(z), n, _stream()), "mfcuda_cexpi_dd")
+        return z
+    x = _host(x, 2 * n, "x")
+    z = out if out is not None else np.empty(4 * n)
+    L.cexpidd_array(_ptr(x), _ptr(z), n)
+    check_last("cexpidd_array")
+    return z
+
+
+def cexp(z, out=None):
+    """exp of complex64x2 elements (cexpdd); device tensors or numpy."""
+    L = lib()
+    n = (z.numel() if _is_dev(z) else np.asarray(z).size) // 4
+    if _is_dev(z):
+        z = _dev_check(z, 4 * n, "z")
+        w = out if out is not None else _empty_like_kind(z, 4 * n)
+        check(L.mfcuda_cexp_dd(_ptr(z), _ptr(w), n, _stream()), "mfcuda_cexp_dd")
+        return w
+    z = _host(z, 4 * n, "z")
+    w = out if out is not None else np.empty(4 * n)
+    L.cexpdd_array(_ptr(z), _ptr(w), n)
+    check_last("cexpdd_array")
+    return w
 
 
 def exp(x, out=None):

@@ -51,6 +51,9 @@ __device__ __forceinline__ void two_prod(double a, double b, double& p, double& 
 }
 
 __device__ __forceinline__ dd make(double h, double l) { dd r; r.hi = h; r.lo = l; return r; }
+// The quiet NaN of std::numeric_limits<double>::quiet_NaN() (sign bit clear),
+// which the reference returns; its sign is visible through copysign (complex exp).
+__device__ __forceinline__ double qnan() { return __longlong_as_double(0x7ff8000000000000ll); }
 __device__ __forceinline__ dd neg(dd a) { return make(-a.hi, -a.lo); }
 
 // ---- DD operators (float64x2.h:203-311) -----------------------------------
@@ -246,7 +249,7 @@ __device__ __forceinline__ dd log2_kernel(dd x) {
   return dd_add(dd_add(make((double)e, 0.0), v), dd_mul(t, p));
 }
 __device__ __forceinline__ dd dd_log2(dd x) {
-  if (isnan(x.hi) || x.hi < 0.0) return make(CUDART_NAN, 0.0);
+  if (isnan(x.hi) || x.hi < 0.0) return make(qnan(), 0.0);
   if (x.hi == 0.0) return make(-CUDART_INF, 0.0);
   if (!isfinite(x.hi)) return make(CUDART_INF, 0.0);
   return log2_kernel(x);
@@ -345,7 +348,7 @@ __device__ __forceinline__ bool trig_arg_too_large(double a) { return !(fabs(a) 
 
 __device__ __forceinline__ dd dd_sin(dd x) {
   if (x.hi == 0.0 && x.lo == 0.0) return x;
-  if (!isfinite(x.hi) || trig_arg_too_large(x.hi)) return make(CUDART_NAN, 0.0);
+  if (!isfinite(x.hi) || trig_arg_too_large(x.hi)) return make(qnan(), 0.0);
   int q;
   dd r = reduce_pi_half(x, q);
   // q=0: sin, q=1: cos, q=2: -sin, q=3: -cos
@@ -353,12 +356,138 @@ __device__ __forceinline__ dd dd_sin(dd x) {
   return (q & 2) ? neg(v) : v;
 }
 __device__ __forceinline__ dd dd_cos(dd x) {
-  if (!isfinite(x.hi) || trig_arg_too_large(x.hi)) return make(CUDART_NAN, 0.0);
+  if (!isfinite(x.hi) || trig_arg_too_large(x.hi)) return make(qnan(), 0.0);
   int q;
   dd r = reduce_pi_half(x, q);
   // q=0: cos, q=1: -sin, q=2: -cos, q=3: sin
   dd v = sincos_eval_one(r, (q & 1) == 1);
   return (q == 1 || q == 2) ? neg(v) : v;
+}
+
+// ---- fused sin / cos (trig.inc:189-236): one reduction, both evaluations ----
+// sincos_eval: the same two Taylor kernels and pi/4 shift as sin_eval and
+// cos_eval, so each output equals the separate call bit for bit.
+__device__ __forceinline__ void sincos_eval_both(dd r, dd &s, dd &c) {
+  const double pi8 = 0.392699081698724;
+  const bool small = fabs(r.hi) <= pi8;
+  const bool pos = r.hi > 0.0;
+  dd pi4 = make(mf_pi_quarter_hi[0], mf_pi_quarter_lo[0]);
+  dd arg = small ? r : (pos ? dd_sub(r, pi4) : dd_add(r, pi4));
+  dd x2 = dd_mul(arg, arg);
+  dd y2 = dd_mul(x2, x2);
+  dd y4 = dd_mul(y2, y2);
+  dd y8 = dd_mul(y4, y4);
+  dd sk = dd_mul(neval12_pow(x2, y2, y4, y8, mf_sin_taylor_hi, mf_sin_taylor_lo), arg);
+  dd ck = neval12_pow(x2, y2, y4, y8, mf_cos_taylor_hi, mf_cos_taylor_lo);
+  if (small) {
+    s = sk;
+    c = ck;
+    return;
+  }
+  dd is2 = make(mf_inv_sqrt2_hi[0], mf_inv_sqrt2_lo[0]);
+  s = pos ? dd_mul(dd_add(sk, ck), is2) : dd_mul(dd_sub(sk, ck), is2);
+  c = pos ? dd_mul(dd_sub(ck, sk), is2) : dd_mul(dd_add(ck, sk), is2);
+}
+// sincos(x, s, c) (trig.inc:216-236)
+__device__ __forceinline__ void dd_sincos(dd x, dd &s, dd &c) {
+  if (!isfinite(x.hi) || trig_arg_too_large(x.hi)) {
+    s = c = make(qnan(), 0.0);
+    return;
+  }
+  if (x.hi == 0.0 && x.lo == 0.0) {  // sin(+-0) = +-0, cos(+-0) = 1
+    s = x;
+    c = make(1.0, 0.0);
+    return;
+  }
+  int q;
+  dd r = reduce_pi_half(x, q);
+  dd ss, cc;
+  sincos_eval_both(r, ss, cc);
+  switch (q) {
+    case 0: s = ss; c = cc; break;
+    case 1: s = cc; c = neg(ss); break;
+    case 2: s = neg(ss); c = neg(cc); break;
+    default: s = neg(cc); c = ss; break;
+  }
+}
+
+// ---- exp2 (exp_log.inc:109-128) ------------------------------------------
+__device__ __forceinline__ dd dd_exp2(dd x) {
+  const double h = x.hi;
+  if (!isfinite(h)) return make(h < 0.0 ? 0.0 : h, 0.0);  // +inf, -inf -> 0, NaN
+  if (h < mf_exp2_min[0]) return make(0.0, 0.0);
+  if (h > mf_exp2_max[0]) return make(CUDART_INF, 0.0);
+  double n_d = rint(h);
+  double rh, rl, t;
+  two_sum(h, -n_d, rh, t);
+  rl = add(t, x.lo);
+  fast_two_sum(rh, rl, rh, rl);
+  return exp2_from_reduced(n_d, rh, rl);
+}
+
+// ---- log10 (exp_log.inc:344-353) -------------------------------------------
+__device__ __forceinline__ dd dd_log10(dd x) {
+  if (!isfinite(x.hi)) return make(log10(x.hi), 0.0);
+  dd l2 = dd_log2(x);
+  if (!isfinite(l2.hi)) return l2;
+  return dd_mul(l2, make(mf_log10_2_hi[0], mf_log10_2_lo[0]));
+}
+
+// ---- complex exp (src/complex64x2/std.inc:20-74) ------------------------------
+// exp(a + bi) = e^a (cos b + i sin b), with the C99 Annex G.6.3.1 special
+// values handled first, as the reference does.
+__device__ __forceinline__ void dd_cexp(dd a, dd b, dd &re, dd &im) {
+  const double a_hi = a.hi, b_hi = b.hi;
+  const bool b_zero = b_hi == 0.0 && b.lo == 0.0;
+  if (!isfinite(a_hi) || !isfinite(b_hi)) {
+    const dd nan2 = make(qnan(), 0.0), zero = make(0.0, 0.0), pinf = make(CUDART_INF, 0.0);
+    if (isnan(a_hi)) {
+      re = nan2;
+      im = b_zero ? b : nan2;
+      return;
+    }
+    if (isinf(b_hi)) {
+      if (isinf(a_hi)) {
+        if (a_hi > 0.0) {
+          re = pinf;
+          im = nan2;
+        } else {
+          re = zero;
+          im = zero;
+        }
+        return;
+      }
+      re = im = nan2;
+      return;
+    }
+    if (isnan(b_hi)) {
+      if (a_hi > 0.0) {
+        re = pinf;
+        im = nan2;
+      } else {
+        re = zero;
+        im = zero;
+      }
+      return;
+    }
+    // a = +-inf, b finite
+    if (b_zero) {
+      re = a_hi > 0.0 ? pinf : zero;
+      im = b;
+      return;
+    }
+    dd s, c;
+    dd_sincos(b, s, c);
+    const double mag = a_hi > 0.0 ? CUDART_INF : 0.0;
+    re = make(copysign(mag, c.hi), 0.0);
+    im = make(copysign(mag, s.hi), 0.0);
+    return;
+  }
+  dd ea = dd_exp(a);
+  dd s, c;
+  dd_sincos(b, s, c);
+  re = dd_mul(ea, c);
+  im = dd_mul(ea, s);
 }
 
 // ---- compensated matmul MAC (src/float64x2/matmul.inc:6-39) ----------------

@@ -19,6 +19,7 @@ Closed forms (reference section in ``src/dd_constants.hh``):
 * ``exp2_coefs[k]`` = (ln 2)^k / k!, k = 0..15                (EXP2 section)
 * ``exp2_table[k]`` = 2^((k-128)/256), k = 0..256
 * ``exp_max`` = RN(1024 ln 2), ``exp_min`` = -750
+* ``exp2_max`` = 1024 - 2^-42, ``exp2_min`` = -1080, ``log10_2`` = log10(2)
 * ``log2_narrow[k]`` (k<7), ``log2_wide[k]`` (k<11) = 2 / ((2k+1) ln 2)   (LOG2 section)
 * ``log2_centers[i]`` = 1 + (2i+1)/64, ``log2_values[i]`` = log2(centers[i]), i < 32
 * ``sin_taylor[k]`` = (-1)^k/(2k+1)!, ``cos_taylor[k]`` = (-1)^k/(2k)!, k < 13
@@ -89,6 +90,9 @@ def build() -> dict[str, list[float]]:
     put_dd("exp2_table", [mpf(2) ** (mpf(k - 128) / 256) for k in range(257)])
     t["exp_max"] = [rn(1024 * ln2)]
     t["exp_min"] = [-750.0]
+    t["exp2_max"] = [1024.0 - 2.0 ** -42]
+    t["exp2_min"] = [-1080.0]
+    put_dd("log10_2", [log(2, 10)])
 
     put_dd("log2_narrow", [2 / ((2 * k + 1) * ln2) for k in range(7)])
     put_dd("log2_wide", [2 / ((2 * k + 1) * ln2) for k in range(11)])
@@ -110,6 +114,8 @@ REF_NAMES = {
     "ln2_cw": ["ln2_cw1", "ln2_cw2", "ln2_cw3"],
     "pi_half_cw": ["pi_half_cw1", "pi_half_cw2", "pi_half_cw3"],
     "exp_max": ["exp_max"], "exp_min": ["exp_min"],
+    "exp2_max": ["exp2_max"], "exp2_min": ["exp2_min"],
+    "log10_2_hi": ["log10_2_hi"], "log10_2_lo": ["log10_2_lo"],
 }
 
 

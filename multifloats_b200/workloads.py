@@ -85,3 +85,13 @@ ELEMENTWISE_INPUTS = {
     "cos": dd_trig_inputs,
     "sqrt": dd_pow2_inputs,
 }
+
+
+def dd_exp2_inputs(n: int, seed: int = 0) -> np.ndarray:
+    """exp2 arguments across its whole range: hi ~ U[-1100, 1030] (past both
+    clamps, exp_log.inc:119-128), lo as elsewhere."""
+    return with_lo(np.random.default_rng(seed).uniform(-1100.0, 1030.0, n), np.random.default_rng(seed + 1))
+
+
+# the adjacent elementwise functions (exp2 / log2 / log10), not in the benchmark configs
+EXTRA_ELEMENTWISE_INPUTS = {"exp2": dd_exp2_inputs, "log2": dd_pow2_inputs, "log10": dd_pow2_inputs}

@@ -327,6 +327,129 @@ static dd orc_cos1(dd x) {
   }
 }
 
+/* ---- exp2 (exp_log.inc:109-128), log10 (exp_log.inc:344-353) ----------- */
+static dd orc_exp2_1(dd x) {
+  double h = x.hi;
+  if (!isfinite(h)) return mk(h > 0.0 ? h : (h < 0.0 ? 0.0 : h), 0.0);
+  if (h < mf_exp2_min[0]) return mk(0.0, 0.0);
+  if (h > mf_exp2_max[0]) return mk(INFINITY, 0.0);
+  double n_d = nearbyint(h);
+  double rh, rl, t;
+  two_sum(h, -n_d, &rh, &t);
+  rl = t + x.lo;
+  fast_two_sum(rh, rl, &rh, &rl);
+  return exp2_from_reduced(n_d, rh, rl);
+}
+static dd orc_log10_1(dd x) {
+  if (!isfinite(x.hi)) return mk(log10(x.hi), 0.0);
+  dd l2 = orc_log2(x);
+  if (!isfinite(l2.hi)) return l2;
+  return dd_mul(l2, mk(mf_log10_2_hi[0], mf_log10_2_lo[0]));
+}
+
+/* ---- sincos (trig.inc:189-236): sincos_eval shares the kernels of the
+ * pi/4-shifted argument between both outputs ----------------------------- */
+static void sincos_eval(dd r, dd *s, dd *c) {
+  const double pi8 = 0.392699081698724;
+  if (fabs(r.hi) <= pi8) {
+    *s = sin_kernel(r);
+    *c = cos_kernel(r);
+    return;
+  }
+  dd pi4 = mk(mf_pi_quarter_hi[0], mf_pi_quarter_lo[0]);
+  dd is2 = mk(mf_inv_sqrt2_hi[0], mf_inv_sqrt2_lo[0]);
+  int pos = r.hi > 0.0;
+  dd rp = pos ? dd_sub(r, pi4) : dd_add(r, pi4);
+  dd sk = sin_kernel(rp), ck = cos_kernel(rp);
+  if (pos) {
+    *s = dd_mul(dd_add(sk, ck), is2);
+    *c = dd_mul(dd_sub(ck, sk), is2);
+  } else {
+    *s = dd_mul(dd_sub(sk, ck), is2);
+    *c = dd_mul(dd_add(ck, sk), is2);
+  }
+}
+static void orc_sincos1(dd x, dd *s, dd *c) {
+  if (!isfinite(x.hi) || trig_too_large(x.hi)) {
+    *s = *c = mk(NAN, 0.0);
+    return;
+  }
+  if (x.hi == 0.0 && x.lo == 0.0) {
+    *s = x;
+    *c = mk(1.0, 0.0);
+    return;
+  }
+  int q;
+  dd r = reduce_pi_half(x, &q), ss, cc;
+  sincos_eval(r, &ss, &cc);
+  switch (q) {
+    case 0: *s = ss; *c = cc; break;
+    case 1: *s = cc; *c = dd_neg(ss); break;
+    case 2: *s = dd_neg(ss); *c = dd_neg(cc); break;
+    default: *s = dd_neg(cc); *c = ss; break;
+  }
+}
+
+/* ---- complex exp (src/complex64x2/std.inc:20-74) ------------------------ */
+static void orc_cexp1(dd a, dd b, dd *re, dd *im) {
+  int b_zero = b.hi == 0.0 && b.lo == 0.0;
+  if (!isfinite(a.hi) || !isfinite(b.hi)) {
+    dd nan2 = mk(NAN, 0.0), zero = mk(0.0, 0.0), pinf = mk(INFINITY, 0.0);
+    if (isnan(a.hi)) {
+      *re = nan2;
+      *im = b_zero ? b : nan2;
+      return;
+    }
+    if (isinf(b.hi)) {
+      if (isinf(a.hi)) {
+        *re = a.hi > 0.0 ? pinf : zero;
+        *im = a.hi > 0.0 ? nan2 : zero;
+      } else {
+        *re = *im = nan2;
+      }
+      return;
+    }
+    if (isnan(b.hi)) {
+      *re = a.hi > 0.0 ? pinf : zero;
+      *im = a.hi > 0.0 ? nan2 : zero;
+      return;
+    }
+    if (b_zero) {
+      *re = a.hi > 0.0 ? pinf : zero;
+      *im = b;
+      return;
+    }
+    dd sn, cs;
+    orc_sincos1(b, &sn, &cs);
+    double mag = a.hi > 0.0 ? INFINITY : 0.0;
+    *re = mk(copysign(mag, cs.hi), 0.0);
+    *im = mk(copysign(mag, sn.hi), 0.0);
+    return;
+  }
+  dd ea = orc_exp1(a), sn, cs;
+  orc_sincos1(b, &sn, &cs);
+  *re = dd_mul(ea, cs);
+  *im = dd_mul(ea, sn);
+}
+
+/* kind 0: sincos (s, c arrays); 1: cexpi (complex z = c + i s); 2: cexp */
+void orc_pair(int kind, const double *x, double *y0, double *y1, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) {
+    dd a, b;
+    if (kind == 2) {
+      orc_cexp1(mk(x[4 * i], x[4 * i + 1]), mk(x[4 * i + 2], x[4 * i + 3]), &a, &b);
+      y0[4 * i] = a.hi; y0[4 * i + 1] = a.lo; y0[4 * i + 2] = b.hi; y0[4 * i + 3] = b.lo;
+    } else {
+      orc_sincos1(mk(x[2 * i], x[2 * i + 1]), &a, &b);
+      if (kind == 0) {
+        y0[2 * i] = a.hi; y0[2 * i + 1] = a.lo; y1[2 * i] = b.hi; y1[2 * i + 1] = b.lo;
+      } else {
+        y0[4 * i] = b.hi; y0[4 * i + 1] = b.lo; y0[4 * i + 2] = a.hi; y0[4 * i + 3] = a.lo;
+      }
+    }
+  }
+}
+
 /* ---- elementwise array maps (Fortran elemental, fypp:792-798) ---------- */
 void orc_unary(int op, const double *x, double *y, int64_t n) {
   for (int64_t i = 0; i < n; ++i) {
@@ -336,6 +459,9 @@ void orc_unary(int op, const double *x, double *y, int64_t n) {
       case 1: r = orc_log1(v); break;
       case 2: r = orc_sin1(v); break;
       case 3: r = orc_cos1(v); break;
+      case 5: r = orc_exp2_1(v); break;
+      case 6: r = orc_log2(v); break;
+      case 7: r = orc_log10_1(v); break;
       default: r = dd_sqrt(v); break;
     }
     y[2 * i] = r.hi;

@@ -20,7 +20,8 @@ REF_SO = os.path.join(HERE, "_ref", "libmfref.so")
 
 P = C.c_void_p
 I64 = C.c_int64
-OPS = {"exp": 0, "log": 1, "sin": 2, "cos": 3, "sqrt": 4}
+OPS = {"exp": 0, "log": 1, "sin": 2, "cos": 3, "sqrt": 4, "exp2": 5, "log2": 6, "log10": 7}
+PAIRS = {"sincos": 0, "cexpi": 1, "cexp": 2}
 KINDS = {"sum": 0, "dot": 1, "norm2": 2, "csum": 3, "cdot": 4, "cnorm2": 5}
 
 _orc = None
@@ -46,6 +47,7 @@ def orc():
             build()
         L = C.CDLL(ORACLE_SO)
         L.orc_unary.argtypes = [C.c_int, P, P, I64]
+        L.orc_pair.argtypes = [C.c_int, P, P, P, I64]
         L.orc_binary.argtypes = [C.c_int, P, P, P, I64]
         L.orc_matmul_mm.argtypes = [P, P, P, I64, I64, I64, I64]
         L.orc_matmul_mm_block.argtypes = [P, P, P, I64, I64, I64, I64, I64, I64, I64, I64]
@@ -83,6 +85,7 @@ def ref():
         L.ref_unary_array.argtypes = [C.c_int, P, P, I64]
         L.ref_unary_array_mt.argtypes = [C.c_int, P, P, I64, C.c_int]
         L.ref_binary_array.argtypes = [C.c_int, P, P, P, I64]
+        L.ref_pair_array.argtypes = [C.c_int, P, P, P, I64]
         L.matmuldd_mm.argtypes = [P, P, P, I64, I64, I64, I64]
         L.matmuldd_mv.argtypes = [P, P, P, I64, I64, I64]
         L.matmuldd_vm.argtypes = [P, P, P, I64, I64, I64]
@@ -104,6 +107,14 @@ def _c(a) -> np.ndarray:
 
 
 # ---- C restatement ------------------------------------------------------------
+def pair(kind: str, x):
+    """sincos / cexpi / cexp restated (orc_pair): (s, c) for sincos, else the
+    complex output."""
+    x, n, y0, y1 = _pair_out(kind, x)
+    orc().orc_pair(PAIRS[kind], _p(x), _p(y0), _p(y1) if y1.size else None, n)
+    return (y0, y1) if kind == "sincos" else y0
+
+
 def unary(op: str, x) -> np.ndarray:
     x = _c(x)
     y = np.empty_like(x)
@@ -271,6 +282,22 @@ def ref_unary(op: str, x, threads: int = 1) -> np.ndarray:
     else:
         ref().ref_unary_array(OPS[op], _p(x), _p(y), x.size // 2)
     return y
+
+
+def _pair_out(kind: str, x):
+    x = _c(x)
+    n = x.size // (4 if kind == "cexp" else 2)
+    y0 = np.empty(2 * n if kind == "sincos" else 4 * n)
+    y1 = np.empty(2 * n) if kind == "sincos" else np.empty(0)
+    return x, n, y0, y1
+
+
+def ref_pair(kind: str, x):
+    """The reference's sincosdd / cexpidd / cexpdd over an array: (s, c) for
+    sincos, else the complex output."""
+    x, n, y0, y1 = _pair_out(kind, x)
+    ref().ref_pair_array(PAIRS[kind], _p(x), _p(y0), _p(y1) if y1.size else None, n)
+    return (y0, y1) if kind == "sincos" else y0
 
 
 def ref_binary(op: int, a, b) -> np.ndarray:

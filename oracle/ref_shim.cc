@@ -23,7 +23,24 @@ void ref_unary_array(int op, const float64x2 *x, float64x2 *y, int64_t n) {
       case 1: y[i] = logdd(x[i]); break;
       case 2: y[i] = sindd(x[i]); break;
       case 3: y[i] = cosdd(x[i]); break;
+      case 5: y[i] = exp2dd(x[i]); break;
+      case 6: y[i] = log2dd(x[i]); break;
+      case 7: y[i] = log10dd(x[i]); break;
       default: y[i] = sqrtdd(x[i]); break;
+    }
+  }
+}
+
+// kind 0: sincosdd into s, c; 1: cexpidd into complex z; 2: cexpdd over complex z.
+void ref_pair_array(int kind, const void *x, void *y0, void *y1, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) {
+    if (kind == 0) {
+      sincosdd(static_cast<const float64x2 *>(x)[i], static_cast<float64x2 *>(y0) + i,
+               static_cast<float64x2 *>(y1) + i);
+    } else if (kind == 1) {
+      static_cast<complex64x2 *>(y0)[i] = cexpidd(static_cast<const float64x2 *>(x)[i]);
+    } else {
+      static_cast<complex64x2 *>(y0)[i] = cexpdd(static_cast<const complex64x2 *>(x)[i]);
     }
   }
 }

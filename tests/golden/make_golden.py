@@ -6,7 +6,8 @@ oracle/_ref/libmfref.so (``make -C oracle``):
     python tests/golden/make_golden.py
 
 Every output stored here was computed by the reference's own exported
-functions (expdd, logdd, sindd, cosdd, sqrtdd, adddd..divdd, matmuldd_mm/mv/vm)
+functions (expdd, logdd, sindd, cosdd, sqrtdd, exp2dd, log2dd, log10dd,
+sincosdd, cexpidd, cexpdd, adddd..divdd, matmuldd_mm/mv/vm)
 or by compositions of them that mirror the Fortran layer (complex matmul from
 four matmuldd_mm calls and the DD operators; norm2 from the DD operators and
 sqrtdd).  Inputs are seeded and regenerable.  The fixtures let the tests pin
@@ -84,7 +85,28 @@ def edge_inputs() -> dict[str, np.ndarray]:
     d["sin"] = d["cos"] = np.concatenate([base, W.with_lo(np.array(tr), np.random.default_rng(9)), tr_dd])
     d["sqrt"] = np.concatenate([base, W.with_lo(np.array([4.0, 2.0, 1e-310, 1e308, 0.25, 1e-320, -4.0]),
                                                  np.random.default_rng(10))])
+    # exp2: clamp rims exp2_max = 1024 - 2^-42 and exp2_min = -1080 (exp_log.inc:119-128),
+    # subnormal outputs below 2^-1022, integer and half-integer arguments
+    e2max, e2min = 1024.0 - 2.0 ** -42, -1080.0
+    e2 = [e2max, np.nextafter(e2max, 2e3), np.nextafter(e2max, 0), 1024.0, 1023.5, e2min,
+          np.nextafter(e2min, 0), np.nextafter(e2min, -2e3), -1074.0, -1074.5, -1075.0, -1022.0,
+          -1022.5, -1023.0, 0.5, -0.5, 1.5, 10.0, -10.0, 1e-20, -1e-20, 0.25, 100.49999999999999]
+    d["exp2"] = np.concatenate([base, W.with_lo(np.array(e2), np.random.default_rng(11))])
+    d["log2"] = d["log10"] = d["log"]
     return d
+
+
+def cexp_edges() -> np.ndarray:
+    """complex64x2 arguments over the special-value grid of C99 Annex G.6.3.1
+    (src/complex64x2/std.inc:20-74) plus ordinary and extreme finite ones."""
+    inf, nan = float("inf"), float("nan")
+    re_parts = [0.0, -0.0, 1.0, -1.0, 700.0, -750.0, 709.9, 1e-300, inf, -inf, nan]
+    im_parts = [0.0, -0.0, 1.0, 1.5707963267948966, 3.141592653589793, 1e6, -2.5, 2.0 ** 56, inf, -inf, nan]
+    rows = []
+    for a in re_parts:
+        for b in im_parts:
+            rows.append([a, 0.0, b, 0.0])
+    return np.array(rows, dtype=np.float64).reshape(-1)
 
 
 def fuzz_mix(n: int, seed: int) -> np.ndarray:
@@ -126,6 +148,24 @@ def main() -> int:
         x = np.concatenate([edges[op], gen(2000, seed=100 + O.OPS[op]), fuzz_mix(600, 200 + O.OPS[op])])
         g[f"unary_{op}_x"] = x
         g[f"unary_{op}_y"] = O.ref_unary(op, x)
+    # exp2 / log2 / log10 over their edges, the config-like distributions and the fuzz mix
+    for op, gen in W.EXTRA_ELEMENTWISE_INPUTS.items():
+        x = np.concatenate([edges[op], gen(2000, seed=100 + O.OPS[op]), fuzz_mix(600, 200 + O.OPS[op])])
+        g[f"unary_{op}_x"] = x
+        g[f"unary_{op}_y"] = O.ref_unary(op, x)
+    # fused sincos and cexpi over the trig edges and distribution; cexp over the Annex G grid
+    x = np.concatenate([edges["sin"], W.ELEMENTWISE_INPUTS["sin"](2000, seed=150), fuzz_mix(600, 250)])
+    g["pair_sincos_x"] = x
+    g["pair_sincos_s"], g["pair_sincos_c"] = O.ref_pair("sincos", x)
+    g["pair_cexpi_x"] = x
+    g["pair_cexpi_z"] = O.ref_pair("cexpi", x)
+    rng = np.random.default_rng(151)
+    z = np.concatenate([cexp_edges(),
+                        W.complex_from_parts(W.with_lo(rng.uniform(-700.0, 700.0, 2000), rng),
+                                             W.ELEMENTWISE_INPUTS["sin"](2000, seed=152)),
+                        W.complex_from_parts(fuzz_mix(600, 253), fuzz_mix(600, 254))])
+    g["pair_cexp_x"] = z
+    g["pair_cexp_w"] = O.ref_pair("cexp", z)
     a = fuzz_mix(3000, 300)
     b = fuzz_mix(3000, 301)
     g["binary_a"], g["binary_b"] = a, b

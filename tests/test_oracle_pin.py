@@ -7,7 +7,7 @@ import pytest
 from multifloats_b200 import workloads as W
 from oracle import oracle as O
 
-OPS = ["exp", "log", "sin", "cos", "sqrt"]
+OPS = ["exp", "log", "sin", "cos", "sqrt", "exp2", "log2", "log10"]
 
 
 @pytest.mark.parametrize("op", OPS)
@@ -15,6 +15,18 @@ def test_unary_vs_golden(golden, op):
     x, y = golden[f"unary_{op}_x"], golden[f"unary_{op}_y"]
     ok = O.same_bits(O.unary(op, x), y)
     assert ok.all(), f"{op}: {np.count_nonzero(~ok)} of {ok.size} differ"
+
+
+def test_sincos_cexpi_cexp_vs_golden(golden):
+    s, c = O.pair("sincos", golden["pair_sincos_x"])
+    assert O.same_bits(s, golden["pair_sincos_s"]).all() and O.same_bits(c, golden["pair_sincos_c"]).all()
+    assert O.same_bits(O.pair("cexpi", golden["pair_cexpi_x"]), golden["pair_cexpi_z"]).all()
+    w = O.pair("cexp", golden["pair_cexp_x"])
+    ok = O.same_bits(w, golden["pair_cexp_w"])
+    assert ok.all(), f"cexp: {np.count_nonzero(~ok)} of {ok.size} differ"
+    # the fused form equals the separate sine and cosine, bit for bit
+    x = golden["pair_sincos_x"]
+    assert O.same_bits(s, O.unary("sin", x)).all() and O.same_bits(c, O.unary("cos", x)).all()
 
 
 @pytest.mark.parametrize("op", range(4))
@@ -47,7 +59,7 @@ needs_ref = pytest.mark.skipif(not O.ref_available(), reason="reference library 
 @needs_ref
 @pytest.mark.parametrize("op", OPS)
 def test_unary_vs_reference_fresh(op):
-    x = W.ELEMENTWISE_INPUTS[op](50000, seed=777)
+    x = {**W.ELEMENTWISE_INPUTS, **W.EXTRA_ELEMENTWISE_INPUTS}[op](50000, seed=777)
     assert O.same_bits(O.unary(op, x), O.ref_unary(op, x)).all()
 
 
