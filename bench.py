@@ -489,6 +489,29 @@ def run_elementwise(args):
             O.ref_unary(op, xs, threads=threads)
             dt = time.perf_counter() - t0
             cpu[op] = {"gelem_per_s": (1 << 21) / dt / 1e9, "kind": "reference", "cores": threads}
+    # the adjacent functions: exp2 / log2 / log10, fused sincos (one reduction for
+    # both outputs) against separate sin + cos, and the complex exp
+    extra = {}
+    for op, gen in W.EXTRA_ELEMENTWISE_INPUTS.items():
+        x = torch.from_numpy(gen(n, seed=1)).to(dev)
+        y = torch.empty_like(x)
+        ms = _events_time(lambda: api.unary(op, x, out=y), args.steps, args.warmup, stream)
+        extra[op] = {"ms": ms, "gelem_per_s": n / ms / 1e6}
+        del x, y
+    x = torch.from_numpy(W.ELEMENTWISE_INPUTS["sin"](n, seed=1)).to(dev)
+    sv, cv = torch.empty_like(x), torch.empty_like(x)
+    ms = _events_time(lambda: api.sincos(x, sv, cv), args.steps, args.warmup, stream)
+    extra["sincos"] = {"ms": ms, "gelem_per_s": n / ms / 1e6,
+                       "vs_sin_plus_cos": (res["sin"]["ms"] + res["cos"]["ms"]) / ms}
+    del x, sv, cv
+    nz = n // 2
+    rng = np.random.default_rng(3)
+    z = torch.from_numpy(W.complex_from_parts(W.with_lo(rng.uniform(-700.0, 700.0, nz), rng),
+                                              W.ELEMENTWISE_INPUTS["sin"](nz, seed=4))).to(dev)
+    w = torch.empty_like(z)
+    ms = _events_time(lambda: api.cexp(z, out=w), args.steps, args.warmup, stream)
+    extra["cexp_2^25"] = {"ms": ms, "gelem_per_s": nz / ms / 1e6}
+    del z, w
     # FP64 thread instructions (DADD + DMUL + DFMA) per element, from ncu counters
     # on these distributions (profiles/unary_kernel_fp64_instructions_2^24.md)
     fp64_per_elem = {"exp": 323.0, "log": 316.0, "sin": 827.5, "cos": 827.5, "sqrt": 25.4}
@@ -502,7 +525,7 @@ def run_elementwise(args):
         r["frac_hbm"] = r["hbm_gbs"] / HBM_GBS
     _line(args, "dd_elementwise_2^26", "DD elementwise G elem/s, 2^26 elements (exp/log/sin/cos/sqrt)",
           res["exp"]["gelem_per_s"], "G elem/s (exp)",
-          {"dtype": "f64", "per_op": res, "cpu_baseline_per_op": cpu,
+          {"dtype": "f64", "per_op": res, "cpu_baseline_per_op": cpu, "adjacent_functions": extra,
            "roofline": {"bound": "fp64 (exp/log/sin/cos), hbm (sqrt)", "kernel": "unary_kernel<exp>",
                         "achieved": res["exp"]["fp64_instr_per_s"] / 1e12, "peak": fp64_peak / 1e12,
                         "unit": "T FP64-instr/s", "frac": res["exp"]["frac_fp64"], "traffic": None,
