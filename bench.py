@@ -754,6 +754,108 @@ def run_gemv(args):
                         "peak_source": "MEASURED_PEAKS.json hbm_gbs"}})
 
 
+def _dev_triangular(n, seed, dev):
+    """n x n DD matrix, off-diagonal U[-1,1)/n, diagonal +-U[1,2) (diagonally
+    dominant: repeated solves stay bounded)."""
+    import torch
+
+    a = _dev_dd_uniform(n * n, seed, dev).view(n, n, 2)
+    a /= float(n)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 1)
+    d = torch.empty(n, dtype=torch.float64, device=dev).uniform_(1.0, 2.0, generator=g)
+    d *= torch.where(torch.rand(n, generator=g, device=dev) < 0.5, -1.0, 1.0)
+    idx = torch.arange(n, device=dev)
+    a[idx, idx, 0] = d
+    a[idx, idx, 1] = 0.0
+    return a.reshape(-1)
+
+
+# FP64 instructions per wgemm / wtrsm multiply-add: DD multiply (two_prod 2, cross
+# terms 4, fast_two_sum 3) + DD add or subtract (two two_sums 11 with the shared
+# leading sum, 2 adds, 2 fast_two_sums 6 -> 20): 29 (the zero / non-finite tests
+# are integer or predicate work).
+BLAS_FP64_PER_MAC = 29.0
+
+
+def run_blas(args):
+    """BLAS-style shims (DGEMM / DTRSM semantics over DD matrices): wgemm at
+    4096^3 in both accumulation forms and wtrsm 4096 x 4096 on the left and on
+    the right; bit-identical to the reference shims' loops (tests)."""
+    import torch
+
+    from multifloats_b200 import api
+    from multifloats_b200 import workloads as W
+    from oracle import oracle as O
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    n = 4096
+    A = _dev_dd_uniform(n * n, 11, dev)
+    B = _dev_dd_uniform(n * n, 12, dev)
+    Cm = _dev_dd_uniform(n * n, 13, dev)
+    alpha, beta = np.array([1.5, 0.0]), np.array([0.5, 0.0])
+    res = {}
+    for ta, tb in (("N", "N"), ("T", "N"), ("N", "T")):
+        ms = _events_time(lambda: api.wgemm(ta, tb, n, n, n, alpha, A, n, B, n, beta, Cm, n),
+                          args.steps, args.warmup, stream, min_warm_s=0.0)
+        res[f"wgemm_{ta}{tb}"] = {"ms": ms, "dd_gflops": 2.0 * n ** 3 / ms / 1e6,
+                                  "fp64_instr_per_s": BLAS_FP64_PER_MAC * n ** 3 / (ms * 1e-3)}
+    del A, B, Cm
+    T = _dev_triangular(n, 21, dev)
+    X = _dev_dd_uniform(n * n, 22, dev)
+    one = np.array([1.0, 0.0])
+    for side, uplo, ta in (("L", "L", "N"), ("L", "U", "T"), ("R", "U", "N"), ("R", "L", "T")):
+        ms = _events_time(lambda: api.wtrsm(side, uplo, ta, "N", n, n, one, T, n, X, n),
+                          args.steps, args.warmup, stream, min_warm_s=0.0)
+        macs = n * n * (n - 1) / 2.0
+        res[f"wtrsm_{side}{uplo}{ta}N"] = {"ms": ms, "dd_gflops": 2.0 * macs / ms / 1e6,
+                                           "fp64_instr_per_s": BLAS_FP64_PER_MAC * macs / (ms * 1e-3)}
+    del T, X
+    torch.cuda.empty_cache()
+    # end to end through the Fortran-callable host drop-in wgemm_ (host buffers,
+    # copies inside the timed region)
+    Ah, Bh = W.dd_uniform(n * n, seed=31), W.dd_uniform(n * n, seed=32)
+    Ch = W.dd_uniform(n * n, seed=33)
+    e2e_steps = max(1, min(args.steps, 3))
+    api.wgemm("N", "N", n, n, n, alpha, Ah, n, Bh, n, beta, Ch, n)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        api.wgemm("N", "N", n, n, n, alpha, Ah, n, Bh, n, beta, Ch, n)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    del Ah, Bh, Ch
+    pk = load_peaks_lib()
+    sp = C.c_void_p(stream.cuda_stream)
+    ms_p, ins_p = C.c_double(), C.c_double()
+    pk.mfpeak_fp64(200000, sp, C.byref(ms_p), C.byref(ins_p))
+    fp64_peak = ins_p.value / (ms_p.value * 1e-3)
+    for r in res.values():
+        r["frac_fp64"] = r["fp64_instr_per_s"] / fp64_peak
+    cpu = None
+    if O.ref_available() and not args.no_cpu_baseline:
+        threads = cpu_threads()
+        s = 1024
+        a, b, c = W.dd_uniform(s * s, seed=1), W.dd_uniform(s * s, seed=2), W.dd_uniform(s * s, seed=3)
+        t0 = time.perf_counter()
+        O.ref_wgemm("N", "N", s, s, s, alpha, a, s, b, s, beta, c, s, threads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": 2.0 * s ** 3 / dt / 1e9, "unit": "DD-GFLOP/s", "cores": threads, "kind": "reference",
+               "sample": f"wgemm NN {s}^3 (the reference's DD operators in wgemm.f90's loop order, "
+                         f"columns sharded over threads)"}
+    head = res["wgemm_NN"]
+    _line(args, "dd_wgemm_4096_wtrsm_4096", "DD BLAS-shim DD-GFLOP/s, wgemm NN 4096^3 (alpha, beta general)",
+          head["dd_gflops"], "DD-GFLOP/s",
+          {"dtype": "f64", "per_case": res, "cpu_baseline": cpu,
+           "e2e": {"value": 2.0 * n ** 3 / e2e_ms / 1e6, "unit": "DD-GFLOP/s", "ms": e2e_ms,
+                   "h2d_bytes_per_step": 3 * 16 * n * n, "d2h_bytes_per_step": 16 * n * n,
+                   "path": "wgemm_ (Fortran-callable host drop-in)"},
+           "roofline": {"bound": "fp64", "kernel": "wgemm_kernel<false,false,true>",
+                        "achieved": head["fp64_instr_per_s"] / 1e12, "peak": fp64_peak / 1e12,
+                        "unit": "T FP64-instr/s", "frac": head["frac_fp64"], "traffic": None,
+                        "fp64_instr_per_mac": BLAS_FP64_PER_MAC,
+                        "peak_source": "own FP64 FMA probe (multifloats_b200/csrc/peaks.cu), same process"}})
+
+
 def run_gemm8192(args):
     import torch
 
@@ -833,7 +935,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="gemm4096",
-                    choices=["gemm4096", "elementwise", "reductions", "batched", "complex", "gemm8192", "gemv"])
+                    choices=["gemm4096", "elementwise", "reductions", "batched", "complex", "gemm8192", "gemv",
+                             "blas"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -843,7 +946,8 @@ def main():
         return
     if args.workload != "gemm4096":
         {"elementwise": run_elementwise, "reductions": run_reductions, "batched": run_batched,
-         "complex": run_complex, "gemm8192": run_gemm8192, "gemv": run_gemv}[args.workload](args)
+         "complex": run_complex, "gemm8192": run_gemm8192, "gemv": run_gemv,
+         "blas": run_blas}[args.workload](args)
         return
     ws, rank, local = dist_init()
     try:

@@ -364,6 +364,49 @@ MULTIFLOATS_CUDA_API int mfcuda_unary_dd_ragged(int op, const float64x2 *const *
                                                 float64x2 *const *ys, const int64_t *ns,
                                                 int64_t count, void *stream);
 
+/* ---- BLAS-style shims over DD matrices ------------------------------------
+ * DGEMM / DTRSM argument semantics as in the reference's BLAS shims
+ * test/integration/blas/wgemm.f90 and wtrsm.f90 (the `blas-multifloat`
+ * library, CMakeLists.txt:377-380): column-major operands with leading
+ * dimensions, transposition letters 'N' / 'T' / 'C' (C = T for real DD),
+ * alpha / beta as one DD each (HOST memory), uplo 'U' / 'L', diag 'U' / 'N',
+ * letters case-insensitive.  Results are bit-identical to the Fortran loops
+ * with the DD operators, including the quick returns, the alpha = 0 / beta = 0
+ * / beta = 1 branches (C, resp. B, is not read when beta = 0, resp. alpha = 0)
+ * and the zero tests that skip a wtrsm update.
+ *
+ *   wgemm:  C := alpha op(A) op(B) + beta C,  op(A) m x k, op(B) k x n
+ *   wtrsm:  B := alpha inv(op(A)) B  (side 'L', A m x m)  or
+ *           B := alpha B inv(op(A))  (side 'R', A n x n),  A triangular
+ *
+ * Device-pointer forms: an invalid argument returns MFCUDA_ERR_INVALID_ARG
+ * without launching anything and stores the BLAS info code (the parameter
+ * position the reference hands to xerbla) in *info when info is not NULL;
+ * *info = 0 otherwise. */
+MULTIFLOATS_CUDA_API int mfcuda_wgemm_dd(char transa, char transb, int64_t m, int64_t n, int64_t k,
+                                         const float64x2 *alpha, const float64x2 *a, int64_t lda,
+                                         const float64x2 *b, int64_t ldb, const float64x2 *beta,
+                                         float64x2 *c, int64_t ldc, int *info, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_wtrsm_dd(char side, char uplo, char transa, char diag, int64_t m,
+                                         int64_t n, const float64x2 *alpha, const float64x2 *a,
+                                         int64_t lda, float64x2 *b, int64_t ldb, int *info,
+                                         void *stream);
+/* Fortran-callable drop-ins for the shim library's SUBROUTINE wgemm / wtrsm
+ * (gfortran calling convention: every argument by reference, default INTEGER,
+ * hidden CHARACTER lengths appended), HOST pointers, synchronous.  On an
+ * invalid argument they call the caller's xerbla_ when one is linked (as the
+ * reference does) and latch MFCUDA_ERR_INVALID_ARG in mfcuda_last_error(). */
+MULTIFLOATS_CUDA_API void wgemm_(const char *transa, const char *transb, const int *m, const int *n,
+                                 const int *k, const float64x2 *alpha, const float64x2 *a,
+                                 const int *lda, const float64x2 *b, const int *ldb,
+                                 const float64x2 *beta, float64x2 *c, const int *ldc,
+                                 size_t transa_len, size_t transb_len);
+MULTIFLOATS_CUDA_API void wtrsm_(const char *side, const char *uplo, const char *transa,
+                                 const char *diag, const int *m, const int *n,
+                                 const float64x2 *alpha, const float64x2 *a, const int *lda,
+                                 float64x2 *b, const int *ldb, size_t side_len, size_t uplo_len,
+                                 size_t transa_len, size_t diag_len);
+
 /* Fixed launch geometry of the reductions for a given n (it depends on n only,
  * never on the device), exposed so a CPU restatement can follow the same order:
  * *blocks = number of thread blocks, *threads = threads per block. */

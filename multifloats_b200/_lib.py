@@ -111,6 +111,12 @@ SIGNATURES = {
     "mfcuda_csumdd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
     "mfcuda_cdotdd": (C.c_int, [P, P, I64, I64, P, P, C.c_size_t, P]),
     "mfcuda_cnorm2dd": (C.c_int, [P, I64, P, P, C.c_size_t, P]),
+    # BLAS-style shims
+    "mfcuda_wgemm_dd": (C.c_int, [C.c_char, C.c_char, I64, I64, I64, P, P, I64, P, I64, P, P, I64, P, P]),
+    "mfcuda_wtrsm_dd": (C.c_int, [C.c_char, C.c_char, C.c_char, C.c_char, I64, I64, P, P, I64, P, I64,
+                                  P, P]),
+    "wgemm_": (None, [P, P, P, P, P, P, P, P, P, P, P, P, P, C.c_size_t, C.c_size_t]),
+    "wtrsm_": (None, [P, P, P, P, P, P, P, P, P, P, P, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t]),
 }
 
 _lib = None

@@ -299,3 +299,110 @@ __all__ = [
     "sum_dd", "dot_product", "norm2", "csum_dd", "cdot_product", "cnorm2",
     "reduce_geometry", "float64x2", "complex64x2",
 ]
+
+
+# ---- BLAS-style shims (wgemm / wtrsm) ---------------------------------------------
+class BlasArgumentError(ValueError):
+    """An invalid wgemm / wtrsm argument: `info` is the BLAS parameter position
+    (the code the reference shims hand to xerbla)."""
+
+    def __init__(self, name: str, info: int):
+        self.info = info
+        super().__init__(f"{name}: parameter number {info} had an illegal value")
+
+
+def _dd_scalar(v) -> np.ndarray:
+    s = np.zeros(2, dtype=np.float64)
+    a = np.asarray(v, dtype=np.float64).reshape(-1)
+    s[: a.size] = a[:2]
+    return s
+
+
+def _span(ld: int, rows: int, cols: int) -> int:
+    """Doubles a column-major rows x cols DD operand spans at leading dimension ld."""
+    return 0 if rows <= 0 or cols <= 0 else 2 * (ld * (cols - 1) + rows)
+
+
+def _need(x, doubles: int, name: str):
+    if doubles == 0:
+        return x
+    if x is None:
+        raise ValueError(f"{name}: operand missing")
+    if _is_dev(x):
+        import torch
+
+        if x.dtype != torch.float64 or not x.is_contiguous() or x.numel() < doubles:
+            raise ValueError(f"{name}: expected a contiguous float64 CUDA tensor of >= {doubles} doubles")
+    elif not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous and x.size >= doubles):
+        raise ValueError(f"{name}: expected a contiguous float64 array of >= {doubles} doubles")
+    return x
+
+
+def _ch(x: str) -> bytes:
+    return str(x).encode()[:1]
+
+
+def wgemm(transa: str, transb: str, m: int, n: int, k: int, alpha, a, lda: int, b, ldb: int, beta,
+          c, ldc: int):
+    """C := alpha op(A) op(B) + beta C in place, DGEMM argument semantics
+    (test/integration/blas/wgemm.f90): column-major DD operands with leading
+    dimensions, op = 'N' | 'T' | 'C'; alpha / beta are one DD each ((hi, lo) or
+    a float).  CUDA tensors go through mfcuda_wgemm_dd on torch's current
+    stream, numpy arrays through the Fortran-callable wgemm_ (host pointers).
+    Returns c."""
+    L = lib()
+    al, be = _dd_scalar(alpha), _dd_scalar(beta)
+    info = C.c_int(0)
+    scalars = (_ch(transa), _ch(transb), m, n, k)
+    nota, notb = _ch(transa).upper() == b"N", _ch(transb).upper() == b"N"
+    # argument check only: with no operands the call returns before any device work
+    L.mfcuda_wgemm_dd(*scalars, al.ctypes.data, None, lda, None, ldb, be.ctypes.data, None, ldc,
+                      C.byref(info), None)
+    if info.value:
+        raise BlasArgumentError("wgemm", info.value)
+    if m == 0 or n == 0:
+        return c  # wgemm.f90:49
+    uses_ab = not (al[0] == 0.0 and al[1] == 0.0)  # alpha = 0: A and B are not read
+    a = _need(a, _span(lda, m if nota else k, k if nota else m) if uses_ab else 0, "a")
+    b = _need(b, _span(ldb, k if notb else n, n if notb else k) if uses_ab else 0, "b")
+    c = _need(c, _span(ldc, m, n), "c")
+    if _is_dev(c):
+        check(L.mfcuda_wgemm_dd(*scalars, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb, be.ctypes.data, _ptr(c),
+                                ldc, C.byref(info), _stream()), "mfcuda_wgemm_dd")
+        return c
+    ints = [C.c_int(v) for v in (m, n, k, lda, ldb, ldc)]
+    ta, tb = C.c_char(_ch(transa)), C.c_char(_ch(transb))
+    L.wgemm_(C.byref(ta), C.byref(tb), C.byref(ints[0]), C.byref(ints[1]), C.byref(ints[2]), al.ctypes.data,
+             _ptr(a), C.byref(ints[3]), _ptr(b), C.byref(ints[4]), be.ctypes.data, _ptr(c), C.byref(ints[5]), 1, 1)
+    check_last("wgemm_")
+    return c
+
+
+def wtrsm(side: str, uplo: str, transa: str, diag: str, m: int, n: int, alpha, a, lda: int, b, ldb: int):
+    """B := alpha inv(op(A)) B (side 'L') or alpha B inv(op(A)) (side 'R') in
+    place, DTRSM argument semantics (test/integration/blas/wtrsm.f90): A
+    triangular ('U' | 'L'), unit or non-unit diagonal ('U' | 'N').  CUDA tensors
+    go through mfcuda_wtrsm_dd, numpy arrays through wtrsm_.  Returns b."""
+    L = lib()
+    al = _dd_scalar(alpha)
+    info = C.c_int(0)
+    scalars = (_ch(side), _ch(uplo), _ch(transa), _ch(diag), m, n)
+    # argument check only: with no operands the call returns before any device work
+    L.mfcuda_wtrsm_dd(*scalars, al.ctypes.data, None, lda, None, ldb, C.byref(info), None)
+    if info.value:
+        raise BlasArgumentError("wtrsm", info.value)
+    if m == 0 or n == 0:
+        return b
+    na = m if _ch(side).upper() == b"L" else n
+    a = _need(a, _span(lda, na, na) if not (al[0] == 0.0 and al[1] == 0.0) else 0, "a")
+    b = _need(b, _span(ldb, m, n), "b")
+    if _is_dev(b):
+        check(L.mfcuda_wtrsm_dd(*scalars, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb, C.byref(info), _stream()),
+              "mfcuda_wtrsm_dd")
+        return b
+    ints = [C.c_int(v) for v in (m, n, lda, ldb)]
+    ch = [C.c_char(_ch(v)) for v in (side, uplo, transa, diag)]
+    L.wtrsm_(*(C.byref(x) for x in ch), C.byref(ints[0]), C.byref(ints[1]), al.ctypes.data, _ptr(a),
+             C.byref(ints[2]), _ptr(b), C.byref(ints[3]), 1, 1, 1, 1)
+    check_last("wtrsm_")
+    return b

@@ -30,6 +30,7 @@ SOURCES = [
     "reduce_dd.cu",
     "split_gemm.cu",
     "batched.cu",
+    "blas_dd.cu",
 ]
 HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh", "split_device.cuh", "gemm_tile.cuh"]
 

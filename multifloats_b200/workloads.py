@@ -95,3 +95,34 @@ def dd_exp2_inputs(n: int, seed: int = 0) -> np.ndarray:
 
 # the adjacent elementwise functions (exp2 / log2 / log10), not in the benchmark configs
 EXTRA_ELEMENTWISE_INPUTS = {"exp2": dd_exp2_inputs, "log2": dd_pow2_inputs, "log10": dd_pow2_inputs}
+
+
+# ---- BLAS-style shims (wgemm / wtrsm) ------------------------------------------
+def dd_padded(rows: int, cols: int, ld: int, seed: int, zeros: float = 0.0,
+              pad: float = np.nan) -> np.ndarray:
+    """Column-major rows x cols DD matrix (hi ~ U[-1, 1)) stored with leading
+    dimension ld >= rows; the ld - rows padding rows of every column hold `pad`
+    (NaN by default, so a kernel that reads or writes padding shows it).  A
+    fraction `zeros` of the entries is exactly (0, 0)."""
+    rng = np.random.default_rng(seed)
+    v = with_lo(rng.uniform(-1.0, 1.0, rows * cols), rng).reshape(cols, rows, 2)
+    if zeros > 0:
+        v[rng.random((cols, rows)) < zeros] = 0.0
+    out = np.full((max(cols, 1), max(ld, 1), 2), pad, dtype=np.float64)
+    out[:cols, :rows] = v
+    return out[: max(cols, 1)].reshape(-1).copy()
+
+
+def dd_triangular(n: int, ld: int, seed: int, zeros: float = 0.0) -> np.ndarray:
+    """n x n matrix for triangular solves: every entry filled (both triangles,
+    so a solve that reads the wrong triangle shows), off-diagonal hi ~ U[-1, 1)/n,
+    diagonal hi = +-U[1, 2) (diagonally dominant: no growth), padding NaN.  A
+    fraction `zeros` of the off-diagonal entries is exactly (0, 0)."""
+    a = dd_padded(n, n, ld, seed, zeros=zeros).reshape(max(n, 1), max(ld, 1), 2)
+    if n > 0:
+        a[:n, :n] /= float(n)
+        rng = np.random.default_rng(seed + 7)
+        d = rng.uniform(1.0, 2.0, n) * rng.choice([-1.0, 1.0], n)
+        idx = np.arange(n)
+        a[idx, idx] = with_lo(d, rng).reshape(n, 2)
+    return a.reshape(-1).copy()

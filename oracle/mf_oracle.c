@@ -1165,3 +1165,176 @@ void orc_split_cgemm_kc(const double *a, const double *b, double *c, int64_t m, 
   }
   free(ar); free(ai); free(br); free(bi); free(rr); free(ii); free(ri); free(ir);
 }
+
+/* ---- BLAS-style shims: test/integration/blas/wgemm.f90, wtrsm.f90 --------
+ * DGEMM / DTRSM over DD values, column-major with leading dimensions, in the
+ * exact loop order of the Fortran (its DD operators are bit-identical to the
+ * C++ ones restated above, test/integration/crosscheck.cc).  Argument checks
+ * return the BLAS info code the reference hands to xerbla, 0 when valid;
+ * nothing is written when it is non-zero.  alpha and beta point at one DD. */
+static int lsame1(char a, char b) {
+  if (a >= 'a' && a <= 'z') a = (char)(a - 32);
+  if (b >= 'a' && b <= 'z') b = (char)(b - 32);
+  return a == b;
+}
+/* DD == / /=: both limbs compared (fsrc/multifloats.fypp:2920-2928). */
+static int dd_eq(dd x, dd y) { return x.hi == y.hi && x.lo == y.lo; }
+#define ODD(p, i, j, ld) mk((p)[2 * ((i) + (j) * (ld))], (p)[2 * ((i) + (j) * (ld)) + 1])
+#define OSET(p, i, j, ld, v)                   \
+  do {                                         \
+    dd v_ = (v);                               \
+    (p)[2 * ((i) + (j) * (ld))] = v_.hi;       \
+    (p)[2 * ((i) + (j) * (ld)) + 1] = v_.lo;   \
+  } while (0)
+static int64_t max1(int64_t x) { return x > 1 ? x : 1; }
+
+int orc_wgemm_info(char transa, char transb, int64_t m, int64_t n, int64_t k, int64_t lda,
+                   int64_t ldb, int64_t ldc) { /* wgemm.f90:16-48 */
+  int nota = lsame1(transa, 'N'), notb = lsame1(transb, 'N');
+  int64_t nrowa = nota ? m : k, nrowb = notb ? k : n;
+  if (!nota && !lsame1(transa, 'C') && !lsame1(transa, 'T')) return 1;
+  if (!notb && !lsame1(transb, 'C') && !lsame1(transb, 'T')) return 2;
+  if (m < 0) return 3;
+  if (n < 0) return 4;
+  if (k < 0) return 5;
+  if (lda < max1(nrowa)) return 8;
+  if (ldb < max1(nrowb)) return 10;
+  if (ldc < max1(m)) return 13;
+  return 0;
+}
+
+int orc_wgemm(char transa, char transb, int64_t m, int64_t n, int64_t k, const double *alpha_,
+              const double *a, int64_t lda, const double *b, int64_t ldb, const double *beta_,
+              double *c, int64_t ldc) {
+  int info = orc_wgemm_info(transa, transb, m, n, k, lda, ldb, ldc);
+  if (info) return info;
+  const dd one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
+  dd alpha = mk(alpha_[0], alpha_[1]), beta = mk(beta_[0], beta_[1]);
+  int nota = lsame1(transa, 'N'), notb = lsame1(transb, 'N');
+  if (m == 0 || n == 0 || ((dd_eq(alpha, zero) || k == 0) && dd_eq(beta, one))) return 0; /* :49 */
+  if (dd_eq(alpha, zero)) { /* :50-65 */
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t i = 0; i < m; ++i)
+        OSET(c, i, j, ldc, dd_eq(beta, zero) ? zero : dd_mul(beta, ODD(c, i, j, ldc)));
+    return 0;
+  }
+  if (nota) { /* :68-84 and :106-122: C := beta C, then C += (alpha b_lj) A(:,l) */
+    for (int64_t j = 0; j < n; ++j) {
+      if (dd_eq(beta, zero)) {
+        for (int64_t i = 0; i < m; ++i) OSET(c, i, j, ldc, zero);
+      } else if (!dd_eq(beta, one)) {
+        for (int64_t i = 0; i < m; ++i) OSET(c, i, j, ldc, dd_mul(beta, ODD(c, i, j, ldc)));
+      }
+      for (int64_t l = 0; l < k; ++l) {
+        dd temp = dd_mul(alpha, notb ? ODD(b, l, j, ldb) : ODD(b, j, l, ldb));
+        for (int64_t i = 0; i < m; ++i)
+          OSET(c, i, j, ldc, dd_add(ODD(c, i, j, ldc), dd_mul(temp, ODD(a, i, l, lda))));
+      }
+    }
+  } else { /* :86-99 and :124-137: dot products down the columns of A */
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t i = 0; i < m; ++i) {
+        dd temp = zero;
+        for (int64_t l = 0; l < k; ++l)
+          temp = dd_add(temp, dd_mul(ODD(a, l, i, lda), notb ? ODD(b, l, j, ldb) : ODD(b, j, l, ldb)));
+        if (dd_eq(beta, zero))
+          OSET(c, i, j, ldc, dd_mul(alpha, temp));
+        else
+          OSET(c, i, j, ldc, dd_add(dd_mul(alpha, temp), dd_mul(beta, ODD(c, i, j, ldc))));
+      }
+  }
+  return 0;
+}
+
+int orc_wtrsm_info(char side, char uplo, char transa, char diag, int64_t m, int64_t n,
+                   int64_t lda, int64_t ldb) { /* wtrsm.f90:16-44 */
+  int lside = lsame1(side, 'L');
+  int64_t nrowa = lside ? m : n;
+  int upper = lsame1(uplo, 'U');
+  if (!lside && !lsame1(side, 'R')) return 1;
+  if (!upper && !lsame1(uplo, 'L')) return 2;
+  if (!lsame1(transa, 'N') && !lsame1(transa, 'T') && !lsame1(transa, 'C')) return 3;
+  if (!lsame1(diag, 'U') && !lsame1(diag, 'N')) return 4;
+  if (m < 0) return 5;
+  if (n < 0) return 6;
+  if (lda < max1(nrowa)) return 9;
+  if (ldb < max1(m)) return 11;
+  return 0;
+}
+
+int orc_wtrsm(char side, char uplo, char transa, char diag, int64_t m, int64_t n,
+              const double *alpha_, const double *a, int64_t lda, double *b, int64_t ldb) {
+  int info = orc_wtrsm_info(side, uplo, transa, diag, m, n, lda, ldb);
+  if (info) return info;
+  const dd one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
+  dd alpha = mk(alpha_[0], alpha_[1]), temp;
+  int lside = lsame1(side, 'L'), nounit = lsame1(diag, 'N'), upper = lsame1(uplo, 'U');
+  int notr = lsame1(transa, 'N');
+  if (m == 0 || n == 0) return 0;
+  if (dd_eq(alpha, zero)) { /* :46-53 */
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t i = 0; i < m; ++i) OSET(b, i, j, ldb, zero);
+    return 0;
+  }
+  if (lside && notr) { /* :55-102: B := alpha inv(A) B, column by column */
+    for (int64_t j = 0; j < n; ++j) {
+      if (!dd_eq(alpha, one))
+        for (int64_t i = 0; i < m; ++i) OSET(b, i, j, ldb, dd_mul(alpha, ODD(b, i, j, ldb)));
+      for (int64_t q = 0; q < m; ++q) {
+        int64_t kk = upper ? m - 1 - q : q;
+        if (!dd_eq(ODD(b, kk, j, ldb), zero)) {
+          if (nounit) OSET(b, kk, j, ldb, dd_div(ODD(b, kk, j, ldb), ODD(a, kk, kk, lda)));
+          int64_t i0 = upper ? 0 : kk + 1, i1 = upper ? kk : m;
+          for (int64_t i = i0; i < i1; ++i)
+            OSET(b, i, j, ldb, dd_sub(ODD(b, i, j, ldb), dd_mul(ODD(b, kk, j, ldb), ODD(a, i, kk, lda))));
+        }
+      }
+    }
+  } else if (lside) { /* :103-132: B := alpha inv(A^T) B */
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t q = 0; q < m; ++q) {
+        int64_t i = upper ? q : m - 1 - q;
+        temp = dd_mul(alpha, ODD(b, i, j, ldb));
+        int64_t k0 = upper ? 0 : i + 1, k1 = upper ? i : m;
+        for (int64_t kk = k0; kk < k1; ++kk)
+          temp = dd_sub(temp, dd_mul(ODD(a, kk, i, lda), ODD(b, kk, j, ldb)));
+        if (nounit) temp = dd_div(temp, ODD(a, i, i, lda));
+        OSET(b, i, j, ldb, temp);
+      }
+  } else if (notr) { /* :135-177: B := alpha B inv(A) */
+    for (int64_t q = 0; q < n; ++q) {
+      int64_t j = upper ? q : n - 1 - q;
+      if (!dd_eq(alpha, one))
+        for (int64_t i = 0; i < m; ++i) OSET(b, i, j, ldb, dd_mul(alpha, ODD(b, i, j, ldb)));
+      int64_t k0 = upper ? 0 : j + 1, k1 = upper ? j : n;
+      for (int64_t kk = k0; kk < k1; ++kk)
+        if (!dd_eq(ODD(a, kk, j, lda), zero))
+          for (int64_t i = 0; i < m; ++i)
+            OSET(b, i, j, ldb, dd_sub(ODD(b, i, j, ldb), dd_mul(ODD(a, kk, j, lda), ODD(b, i, kk, ldb))));
+      if (nounit) {
+        temp = dd_div(one, ODD(a, j, j, lda));
+        for (int64_t i = 0; i < m; ++i) OSET(b, i, j, ldb, dd_mul(temp, ODD(b, i, j, ldb)));
+      }
+    }
+  } else { /* :178-207: B := alpha B inv(A^T) */
+    for (int64_t q = 0; q < n; ++q) {
+      int64_t kk = upper ? n - 1 - q : q;
+      if (nounit) {
+        temp = dd_div(one, ODD(a, kk, kk, lda));
+        for (int64_t i = 0; i < m; ++i) OSET(b, i, kk, ldb, dd_mul(temp, ODD(b, i, kk, ldb)));
+      }
+      int64_t j0 = upper ? 0 : kk + 1, j1 = upper ? kk : n;
+      for (int64_t j = j0; j < j1; ++j)
+        if (!dd_eq(ODD(a, j, kk, lda), zero)) {
+          temp = ODD(a, j, kk, lda);
+          for (int64_t i = 0; i < m; ++i)
+            OSET(b, i, j, ldb, dd_sub(ODD(b, i, j, ldb), dd_mul(temp, ODD(b, i, kk, ldb))));
+        }
+      if (!dd_eq(alpha, one))
+        for (int64_t i = 0; i < m; ++i) OSET(b, i, kk, ldb, dd_mul(alpha, ODD(b, i, kk, ldb)));
+    }
+  }
+  return 0;
+}
+#undef ODD
+#undef OSET

@@ -69,6 +69,10 @@ def orc():
         L.orc_split_cgemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
         L.orc_split_gemm_kc.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64]
         L.orc_split_cgemm_kc.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64]
+        L.orc_wgemm.argtypes = [C.c_char, C.c_char, I64, I64, I64, P, P, I64, P, I64, P, P, I64]
+        L.orc_wgemm_info.argtypes = [C.c_char, C.c_char, I64, I64, I64, I64, I64, I64]
+        L.orc_wtrsm.argtypes = [C.c_char, C.c_char, C.c_char, C.c_char, I64, I64, P, P, I64, P, I64]
+        L.orc_wtrsm_info.argtypes = [C.c_char, C.c_char, C.c_char, C.c_char, I64, I64, I64, I64]
         _orc = L
     return _orc
 
@@ -92,6 +96,11 @@ def ref():
         L.ref_matmul_mm_mt.argtypes = [P, P, P, I64, I64, I64, I64, C.c_int]
         L.ref_cmatmul_mm.argtypes = [P, P, P, I64, I64, I64, I64]
         L.ref_norm2_serial.argtypes = [P, I64]
+        L.ref_wgemm.argtypes = [C.c_char, C.c_char, I64, I64, I64, P, P, I64, P, I64, P, P, I64]
+        L.ref_wtrsm.argtypes = [C.c_char, C.c_char, C.c_char, C.c_char, I64, I64, P, P, I64, P, I64]
+        L.ref_wgemm_mt.argtypes = [C.c_char, C.c_char, I64, I64, I64, P, P, I64, P, I64, P, P, I64, C.c_int]
+        L.ref_wtrsm_mt.argtypes = [C.c_char, C.c_char, C.c_char, C.c_char, I64, I64, P, P, I64, P, I64,
+                                   C.c_int]
         L.ref_norm2_serial.restype = _DD
         _ref = L
     return _ref
@@ -163,6 +172,37 @@ def cmatmul_mm(a, b, m, k, n, ri=8) -> np.ndarray:
     c = np.empty(4 * m * n)
     orc().orc_cmatmul_mm(_p(a), _p(b), _p(c), m, k, n, ri)
     return c
+
+
+def _ch(x: str) -> bytes:
+    return x.encode()[:1]
+
+
+def wgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """wgemm.f90 restated (orc_wgemm): returns (info, C after the call); the
+    input C is not modified."""
+    a, b, c = _c(a), _c(b), _c(c).copy()
+    al, be = _c(alpha).copy(), _c(beta).copy()
+    info = orc().orc_wgemm(_ch(transa), _ch(transb), m, n, k, _p(al), _p(a), lda, _p(b), ldb,
+                           _p(be), _p(c), ldc)
+    return info, c
+
+
+def wgemm_info(transa, transb, m, n, k, lda, ldb, ldc) -> int:
+    return orc().orc_wgemm_info(_ch(transa), _ch(transb), m, n, k, lda, ldb, ldc)
+
+
+def wtrsm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """wtrsm.f90 restated (orc_wtrsm): returns (info, B after the call)."""
+    a, b = _c(a), _c(b).copy()
+    al = _c(alpha).copy()
+    info = orc().orc_wtrsm(_ch(side), _ch(uplo), _ch(transa), _ch(diag), m, n, _p(al), _p(a), lda,
+                           _p(b), ldb)
+    return info, b
+
+
+def wtrsm_info(side, uplo, transa, diag, m, n, lda, ldb) -> int:
+    return orc().orc_wtrsm_info(_ch(side), _ch(uplo), _ch(transa), _ch(diag), m, n, lda, ldb)
 
 
 def reduce_serial(kind: str, x, y=None, ri=8) -> np.ndarray:
@@ -325,6 +365,27 @@ def ref_norm2(x) -> np.ndarray:
     x = _c(x)
     r = ref().ref_norm2_serial(_p(x), x.size // 2)
     return np.array([r.hi, r.lo])
+
+
+def ref_wgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, threads: int = 1) -> np.ndarray:
+    """wgemm.f90's loops on the reference's own operators (valid arguments only),
+    columns of C sharded over `threads` threads (bit-identical to one thread)."""
+    a, b, c = _c(a), _c(b), _c(c).copy()
+    al, be = _c(alpha).copy(), _c(beta).copy()
+    ta, tb = transa.upper().replace("C", "T"), transb.upper().replace("C", "T")
+    ref().ref_wgemm_mt(_ch(ta), _ch(tb), m, n, k, _p(al), _p(a), lda, _p(b), ldb, _p(be), _p(c), ldc, threads)
+    return c
+
+
+def ref_wtrsm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, threads: int = 1) -> np.ndarray:
+    """wtrsm.f90's loops on the reference's own operators (valid arguments only),
+    independent vectors of B sharded over `threads` threads."""
+    a, b = _c(a), _c(b).copy()
+    al = _c(alpha).copy()
+    t = transa.upper().replace("C", "T")
+    ref().ref_wtrsm_mt(_ch(side.upper()), _ch(uplo.upper()), _ch(t), _ch(diag.upper()), m, n, _p(al),
+                       _p(a), lda, _p(b), ldb, threads)
+    return b
 
 
 def ref_matmul_mv(a, x, m, k, ri=8) -> np.ndarray:

@@ -93,6 +93,150 @@ void ref_matmul_mm_mt(const float64x2 *a, const float64x2 *b, float64x2 *c, int6
   for (auto &th : pool) th.join();
 }
 
+// BLAS-style shims test/integration/blas/wgemm.f90 and wtrsm.f90 (Fortran, not
+// buildable here: no Fortran compiler) written out on the reference's own
+// float64x2 operators, which are bit-identical to the Fortran ones
+// (test/integration/crosscheck.cc).  Column-major with leading dimensions,
+// transposition and diagonal flags as upper-case letters; the argument checks
+// are left to the caller.  Same loop order as the Fortran.
+void ref_wgemm(char ta, char tb, int64_t m, int64_t n, int64_t k, const float64x2 *alpha_,
+               const float64x2 *a, int64_t lda, const float64x2 *b, int64_t ldb,
+               const float64x2 *beta_, float64x2 *c, int64_t ldc) {
+  const float64x2 one(1.0), zero(0.0), alpha = *alpha_, beta = *beta_;
+  auto A = [&](int64_t i, int64_t j) { return a[i + j * lda]; };
+  auto B = [&](int64_t i, int64_t j) { return b[i + j * ldb]; };
+  auto C = [&](int64_t i, int64_t j) -> float64x2 & { return c[i + j * ldc]; };
+  const bool nota = ta == 'N', notb = tb == 'N';
+  if (m == 0 || n == 0 || ((alpha == zero || k == 0) && beta == one)) return;
+  if (alpha == zero) {
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t i = 0; i < m; ++i) C(i, j) = beta == zero ? zero : beta * C(i, j);
+    return;
+  }
+  for (int64_t j = 0; j < n; ++j) {
+    if (nota) {
+      if (beta == zero) {
+        for (int64_t i = 0; i < m; ++i) C(i, j) = zero;
+      } else if (beta != one) {
+        for (int64_t i = 0; i < m; ++i) C(i, j) = beta * C(i, j);
+      }
+      for (int64_t l = 0; l < k; ++l) {
+        float64x2 temp = alpha * (notb ? B(l, j) : B(j, l));
+        for (int64_t i = 0; i < m; ++i) C(i, j) = C(i, j) + temp * A(i, l);
+      }
+    } else {
+      for (int64_t i = 0; i < m; ++i) {
+        float64x2 temp = zero;
+        for (int64_t l = 0; l < k; ++l) temp = temp + A(l, i) * (notb ? B(l, j) : B(j, l));
+        C(i, j) = beta == zero ? alpha * temp : alpha * temp + beta * C(i, j);
+      }
+    }
+  }
+}
+
+void ref_wtrsm(char side, char uplo, char ta, char diag, int64_t m, int64_t n,
+               const float64x2 *alpha_, const float64x2 *a, int64_t lda, float64x2 *b,
+               int64_t ldb) {
+  const float64x2 one(1.0), zero(0.0), alpha = *alpha_;
+  auto A = [&](int64_t i, int64_t j) { return a[i + j * lda]; };
+  auto B = [&](int64_t i, int64_t j) -> float64x2 & { return b[i + j * ldb]; };
+  const bool lside = side == 'L', upper = uplo == 'U', nounit = diag == 'N', notr = ta == 'N';
+  if (m == 0 || n == 0) return;
+  if (alpha == zero) {
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t i = 0; i < m; ++i) B(i, j) = zero;
+    return;
+  }
+  float64x2 temp;
+  if (lside && notr) {
+    for (int64_t j = 0; j < n; ++j) {
+      if (alpha != one)
+        for (int64_t i = 0; i < m; ++i) B(i, j) = alpha * B(i, j);
+      for (int64_t s = 0; s < m; ++s) {
+        const int64_t k = upper ? m - 1 - s : s;
+        if (B(k, j) != zero) {
+          if (nounit) B(k, j) = B(k, j) / A(k, k);
+          for (int64_t i = upper ? 0 : k + 1; i < (upper ? k : m); ++i)
+            B(i, j) = B(i, j) - B(k, j) * A(i, k);
+        }
+      }
+    }
+  } else if (lside) {
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t s = 0; s < m; ++s) {
+        const int64_t i = upper ? s : m - 1 - s;
+        temp = alpha * B(i, j);
+        for (int64_t k = upper ? 0 : i + 1; k < (upper ? i : m); ++k) temp = temp - A(k, i) * B(k, j);
+        if (nounit) temp = temp / A(i, i);
+        B(i, j) = temp;
+      }
+  } else if (notr) {
+    for (int64_t s = 0; s < n; ++s) {
+      const int64_t j = upper ? s : n - 1 - s;
+      if (alpha != one)
+        for (int64_t i = 0; i < m; ++i) B(i, j) = alpha * B(i, j);
+      for (int64_t k = upper ? 0 : j + 1; k < (upper ? j : n); ++k)
+        if (A(k, j) != zero)
+          for (int64_t i = 0; i < m; ++i) B(i, j) = B(i, j) - A(k, j) * B(i, k);
+      if (nounit) {
+        temp = one / A(j, j);
+        for (int64_t i = 0; i < m; ++i) B(i, j) = temp * B(i, j);
+      }
+    }
+  } else {
+    for (int64_t s = 0; s < n; ++s) {
+      const int64_t k = upper ? n - 1 - s : s;
+      if (nounit) {
+        temp = one / A(k, k);
+        for (int64_t i = 0; i < m; ++i) B(i, k) = temp * B(i, k);
+      }
+      for (int64_t j = upper ? 0 : k + 1; j < (upper ? k : n); ++j)
+        if (A(j, k) != zero) {
+          temp = A(j, k);
+          for (int64_t i = 0; i < m; ++i) B(i, j) = B(i, j) - temp * B(i, k);
+        }
+      if (alpha != one)
+        for (int64_t i = 0; i < m; ++i) B(i, k) = alpha * B(i, k);
+    }
+  }
+}
+
+// Column-sharded (wgemm; wtrsm on the left) or row-sharded (wtrsm on the
+// right) drivers over `threads` threads: the shims' outputs are independent
+// per column of C / per vector of B, so each shard runs exactly the loops of a
+// single call and the result is bit-identical to it.
+void ref_wgemm_mt(char ta, char tb, int64_t m, int64_t n, int64_t k, const float64x2 *alpha,
+                  const float64x2 *a, int64_t lda, const float64x2 *b, int64_t ldb,
+                  const float64x2 *beta, float64x2 *c, int64_t ldc, int threads) {
+  if (threads < 1) threads = 1;
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t) {
+    const int64_t j0 = n * t / threads, j1 = n * (t + 1) / threads;
+    if (j1 <= j0) continue;
+    const float64x2 *bs = tb == 'N' ? b + j0 * ldb : b + j0;
+    pool.emplace_back(ref_wgemm, ta, tb, m, j1 - j0, k, alpha, a, lda, bs, ldb, beta, c + j0 * ldc, ldc);
+  }
+  for (auto &th : pool) th.join();
+}
+
+void ref_wtrsm_mt(char side, char uplo, char ta, char diag, int64_t m, int64_t n,
+                  const float64x2 *alpha, const float64x2 *a, int64_t lda, float64x2 *b,
+                  int64_t ldb, int threads) {
+  if (threads < 1) threads = 1;
+  const bool lside = side == 'L';
+  const int64_t nv = lside ? n : m;
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t) {
+    const int64_t v0 = nv * t / threads, v1 = nv * (t + 1) / threads;
+    if (v1 <= v0) continue;
+    if (lside)
+      pool.emplace_back(ref_wtrsm, side, uplo, ta, diag, m, v1 - v0, alpha, a, lda, b + v0 * ldb, ldb);
+    else
+      pool.emplace_back(ref_wtrsm, side, uplo, ta, diag, v1 - v0, n, alpha, a, lda, b + v0, ldb);
+  }
+  for (auto &th : pool) th.join();
+}
+
 }  // extern "C"
 
 extern "C" {

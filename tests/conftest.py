@@ -62,3 +62,28 @@ def to_host(t):
 
     torch.cuda.synchronize()
     return t.cpu().numpy()
+
+
+def wgemm_golden(golden):
+    """(case index, args for wgemm(...), expected C) for every stored wgemm case;
+    args = (transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)."""
+    i = 0
+    while f"wgemm{i}_p" in golden.files:
+        p = golden[f"wgemm{i}_p"]
+        m, n, k, lda, ldb, ldc = (int(v) for v in p[2:])
+        s = golden[f"wgemm{i}_s"]
+        yield i, (chr(p[0]), chr(p[1]), m, n, k, s[:2], golden[f"wgemm{i}_a"], lda,
+                  golden[f"wgemm{i}_b"], ldb, s[2:], golden[f"wgemm{i}_c"], ldc), golden[f"wgemm{i}_out"]
+        i += 1
+
+
+def wtrsm_golden(golden):
+    """(case index, args for wtrsm(...), expected B) for every stored wtrsm case;
+    args = (side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb)."""
+    i = 0
+    while f"wtrsm{i}_p" in golden.files:
+        p = golden[f"wtrsm{i}_p"]
+        m, n, lda, ldb = (int(v) for v in p[4:])
+        yield i, (chr(p[0]), chr(p[1]), chr(p[2]), chr(p[3]), m, n, golden[f"wtrsm{i}_s"],
+                  golden[f"wtrsm{i}_a"], lda, golden[f"wtrsm{i}_b"], ldb), golden[f"wtrsm{i}_out"]
+        i += 1

@@ -10,7 +10,8 @@ functions (expdd, logdd, sindd, cosdd, sqrtdd, exp2dd, log2dd, log10dd,
 sincosdd, cexpidd, cexpdd, adddd..divdd, matmuldd_mm/mv/vm)
 or by compositions of them that mirror the Fortran layer (complex matmul from
 four matmuldd_mm calls and the DD operators; norm2 from the DD operators and
-sqrtdd).  Inputs are seeded and regenerable.  The fixtures let the tests pin
+sqrtdd; the BLAS-style shims wgemm / wtrsm from the DD operators in the
+Fortran's loop order).  Inputs are seeded and regenerable.  The fixtures let the tests pin
 the oracle and the GPU kernels on machines where the reference is absent.
 """
 from __future__ import annotations
@@ -138,6 +139,100 @@ GEMM_SHAPES = [
 ]
 
 
+# BLAS-style shim cases: every branch of wgemm.f90 / wtrsm.f90 (quick returns,
+# alpha = 0, beta = 0 / 1 / other, k = 0, both transpositions, padded leading
+# dimensions, zero and non-finite entries).
+_DDK = {"rand": None, "one": (1.0, 0.0), "zero": (0.0, 0.0), "negzero": (-0.0, 0.0),
+        "onelo": (1.0, 2.0 ** -60), "two": (2.0, 0.0), "nan": (float("nan"), 0.0)}
+
+
+def _dd_scalar(kind: str, rng) -> np.ndarray:
+    if _DDK[kind] is None:
+        return W.with_lo(rng.uniform(-2.0, 2.0, 1), rng)
+    return np.array(_DDK[kind], dtype=np.float64)
+
+
+def _sprinkle(x: np.ndarray, rng, count: int) -> None:
+    """Put inf / -inf / NaN into `count` random (non-padding) entries."""
+    v = x.reshape(-1, 2)
+    ok = np.flatnonzero(~np.isnan(v[:, 0]))
+    if ok.size == 0 or count == 0:
+        return
+    for i, val in zip(rng.choice(ok, min(count, ok.size), replace=False), [np.inf, -np.inf, np.nan] * count):
+        v[i] = (val, 0.0)
+
+
+def wgemm_cases():
+    rng = np.random.default_rng(900)
+    cases = []
+    shapes = [(5, 4, 3), (17, 9, 33), (33, 17, 8), (1, 1, 1), (0, 3, 2), (4, 0, 2), (6, 5, 0), (24, 21, 40)]
+    scal = [("rand", "rand"), ("rand", "zero"), ("rand", "one"), ("zero", "one"), ("zero", "zero"),
+            ("zero", "rand"), ("negzero", "two"), ("onelo", "onelo"), ("one", "negzero"), ("nan", "rand")]
+    idx = 0
+    for ta in "NTC":
+        for tb in "NTc":
+            for s_i, (m, n, k) in enumerate(shapes):
+                al, be = scal[(idx * 3 + s_i) % len(scal)]
+                if s_i == 0:
+                    al, be = scal[idx % len(scal)]
+                cases.append((ta, tb, m, n, k, int(rng.integers(0, 3)), int(rng.integers(0, 3)),
+                              int(rng.integers(0, 3)), al, be, 2 if s_i == 1 else 0))
+                idx += 1
+    # every scalar pair on one shape of each transposition of A
+    for ta in "NT":
+        for al, be in scal:
+            cases.append((ta, "N", 9, 7, 11, 1, 0, 2, al, be, 0))
+    return cases
+
+
+def wtrsm_cases():
+    cases = []
+    for side in "LR":
+        for uplo in "UL":
+            for ta in "NTC":
+                for diag in "NU":
+                    for (m, n, al, zeros, special) in [(23, 9, "rand", 0.2, 0), (7, 31, "one", 0.4, 0),
+                                                       (26, 19, "two", 0.0, 2), (1, 3, "onelo", 0.0, 0)]:
+                        cases.append((side, uplo, ta, diag, m, n, al, zeros, special))
+    cases += [("L", "U", "N", "N", 0, 4, "rand", 0.0, 0), ("R", "L", "T", "U", 5, 0, "rand", 0.0, 0),
+              ("L", "L", "N", "N", 6, 5, "zero", 0.0, 0), ("R", "U", "N", "N", 6, 5, "negzero", 0.0, 0),
+              ("l", "u", "t", "n", 8, 3, "nan", 0.0, 0)]
+    return cases
+
+
+def wgemm_operands(case, seed):
+    ta, tb, m, n, k, pa, pb, pc, al, be, special = case
+    rng = np.random.default_rng(seed)
+    nota, notb = ta.upper() == "N", tb.upper() == "N"
+    ra, ca = (m, k) if nota else (k, m)
+    rb, cb = (k, n) if notb else (n, k)
+    lda, ldb, ldc = max(1, ra) + pa, max(1, rb) + pb, max(1, m) + pc
+    a = W.dd_padded(ra, ca, lda, seed, zeros=0.1)
+    b = W.dd_padded(rb, cb, ldb, seed + 1, zeros=0.1)
+    c = W.dd_padded(m, n, ldc, seed + 2)
+    if special:
+        _sprinkle(a, rng, special)
+        _sprinkle(b, rng, special)
+    return (ta, tb, m, n, k, _dd_scalar(al, rng), a, lda, b, ldb, _dd_scalar(be, rng), c, ldc)
+
+
+def wtrsm_operands(case, seed):
+    side, uplo, ta, diag, m, n, al, zeros, special = case
+    rng = np.random.default_rng(seed)
+    na = m if side.upper() == "L" else n
+    lda, ldb = max(1, na) + int(rng.integers(0, 3)), max(1, m) + int(rng.integers(0, 3))
+    a = W.dd_triangular(na, lda, seed, zeros=zeros)
+    b = W.dd_padded(m, n, ldb, seed + 1, zeros=zeros)
+    if special:
+        _sprinkle(b, rng, special)
+        _sprinkle(a, rng, 1)
+    return (side, uplo, ta, diag, m, n, _dd_scalar(al, rng), a, lda, b, ldb)
+
+
+def _letters(*xs) -> np.ndarray:
+    return np.array([ord(x) for x in xs], dtype=np.int64)
+
+
 def main() -> int:
     if not O.ref_available():
         print("oracle/_ref/libmfref.so not built; run `make -C oracle` where the reference exists")
@@ -189,6 +284,18 @@ def main() -> int:
         x = W.dd_uniform(n, seed=5000 + idx)
         g[f"norm2_{idx}_x"] = x
         g[f"norm2_{idx}_y"] = O.ref_norm2(x)
+    for idx, case in enumerate(wgemm_cases()):
+        ta, tb, m, n, k, al, a, lda, b, ldb, be, c, ldc = wgemm_operands(case, 6000 + 10 * idx)
+        g[f"wgemm{idx}_p"] = np.concatenate([_letters(ta, tb), [m, n, k, lda, ldb, ldc]]).astype(np.int64)
+        g[f"wgemm{idx}_s"] = np.concatenate([al, be])
+        g[f"wgemm{idx}_a"], g[f"wgemm{idx}_b"], g[f"wgemm{idx}_c"] = a, b, c
+        g[f"wgemm{idx}_out"] = O.ref_wgemm(ta, tb, m, n, k, al, a, lda, b, ldb, be, c, ldc)
+    for idx, case in enumerate(wtrsm_cases()):
+        side, uplo, ta, diag, m, n, al, a, lda, b, ldb = wtrsm_operands(case, 7000 + 10 * idx)
+        g[f"wtrsm{idx}_p"] = np.concatenate([_letters(side, uplo, ta, diag), [m, n, lda, ldb]]).astype(np.int64)
+        g[f"wtrsm{idx}_s"] = al
+        g[f"wtrsm{idx}_a"], g[f"wtrsm{idx}_b"] = a, b
+        g[f"wtrsm{idx}_out"] = O.ref_wtrsm(side, uplo, ta, diag, m, n, al, a, lda, b, ldb)
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT} ({os.path.getsize(OUT)} bytes, {len(g)} arrays)")
     return 0

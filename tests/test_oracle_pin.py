@@ -71,3 +71,80 @@ def test_gemm_vs_reference_fresh():
         ri = int(rng.choice([0, 1, 2, 5, 8, 16]))
         a, b = W.dd_uniform(m * k, seed=m + 100 * k), W.dd_uniform(k * n, seed=n + 7 * k)
         assert O.same_bits(O.matmul_mm(a, b, m, k, n, ri), O.ref_matmul_mm(a, b, m, k, n, ri)).all()
+
+
+def test_wgemm_vs_golden(golden):
+    from conftest import wgemm_golden
+
+    n = 0
+    for i, args, want in wgemm_golden(golden):
+        info, got = O.wgemm(*args)
+        assert info == 0 and O.same_bits(got, want).all(), (i, args[:5])
+        n += 1
+    assert n >= 90
+
+
+def test_wtrsm_vs_golden(golden):
+    from conftest import wtrsm_golden
+
+    n = 0
+    for i, args, want in wtrsm_golden(golden):
+        info, got = O.wtrsm(*args)
+        assert info == 0 and O.same_bits(got, want).all(), (i, args[:6])
+        n += 1
+    assert n >= 100
+
+
+def test_blas_argument_checks():
+    """The info codes of wgemm.f90:29-48 / wtrsm.f90:24-44, first failing check wins."""
+    assert O.wgemm_info("N", "N", 2, 3, 4, 2, 4, 2) == 0
+    assert O.wgemm_info("X", "Q", -1, 3, 4, 2, 4, 2) == 1
+    assert O.wgemm_info("t", "Q", -1, 3, 4, 2, 4, 2) == 2
+    assert O.wgemm_info("c", "n", -1, -3, 4, 2, 4, 2) == 3
+    assert O.wgemm_info("N", "N", 2, -3, 4, 2, 4, 2) == 4
+    assert O.wgemm_info("N", "N", 2, 3, -4, 2, 4, 2) == 5
+    assert O.wgemm_info("N", "N", 2, 3, 4, 1, 4, 2) == 8
+    assert O.wgemm_info("T", "N", 2, 3, 4, 3, 4, 2) == 8  # lda >= k when A is transposed
+    assert O.wgemm_info("N", "N", 2, 3, 4, 2, 3, 2) == 10
+    assert O.wgemm_info("N", "T", 2, 3, 4, 2, 2, 2) == 10  # ldb >= n when B is transposed
+    assert O.wgemm_info("N", "N", 2, 3, 4, 2, 4, 1) == 13
+    assert O.wgemm_info("N", "N", 0, 0, 0, 1, 1, 1) == 0  # max(1, .) floors
+    assert O.wgemm_info("N", "N", 0, 0, 0, 0, 1, 1) == 8
+    assert O.wtrsm_info("L", "U", "N", "N", 3, 2, 3, 3) == 0
+    assert O.wtrsm_info("X", "U", "N", "N", 3, 2, 3, 3) == 1
+    assert O.wtrsm_info("r", "X", "N", "N", 3, 2, 3, 3) == 2
+    assert O.wtrsm_info("L", "l", "X", "N", 3, 2, 3, 3) == 3
+    assert O.wtrsm_info("L", "U", "c", "X", 3, 2, 3, 3) == 4
+    assert O.wtrsm_info("L", "U", "N", "u", -3, 2, 3, 3) == 5
+    assert O.wtrsm_info("L", "U", "N", "N", 3, -2, 3, 3) == 6
+    assert O.wtrsm_info("L", "U", "N", "N", 3, 2, 2, 3) == 9
+    assert O.wtrsm_info("R", "U", "N", "N", 3, 2, 2, 3) == 0  # right side: lda >= n
+    assert O.wtrsm_info("L", "U", "N", "N", 3, 2, 3, 2) == 11
+    # an invalid call writes nothing
+    c = np.full(8, 7.0)
+    info, out = O.wgemm("N", "N", 2, 2, 2, [1.0, 0.0], np.ones(8), 1, np.ones(8), 2, [0.0, 0.0], c, 2)
+    assert info == 8 and (out == 7.0).all()
+
+
+@needs_ref
+def test_blas_vs_reference_fresh():
+    import sys, os
+
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import wgemm_operands, wtrsm_operands
+
+    rng = np.random.default_rng(77)
+    for t in range(40):
+        case = (str(rng.choice(list("NTC"))), str(rng.choice(list("NTC"))), *(int(v) for v in rng.integers(0, 30, 3)),
+                *(int(v) for v in rng.integers(0, 3, 3)), str(rng.choice(["rand", "one", "zero", "two"])),
+                str(rng.choice(["rand", "one", "zero", "negzero"])), int(rng.integers(0, 2)))
+        args = wgemm_operands(case, 8000 + t)
+        info, got = O.wgemm(*args)
+        assert info == 0 and O.same_bits(got, O.ref_wgemm(*args)).all(), case
+    for t in range(48):
+        case = (str(rng.choice(list("LR"))), str(rng.choice(list("UL"))), str(rng.choice(list("NTC"))),
+                str(rng.choice(list("NU"))), *(int(v) for v in rng.integers(0, 40, 2)),
+                str(rng.choice(["rand", "one", "two"])), float(rng.choice([0.0, 0.3])), int(rng.integers(0, 2)))
+        args = wtrsm_operands(case, 9000 + t)
+        info, got = O.wtrsm(*args)
+        assert info == 0 and O.same_bits(got, O.ref_wtrsm(*args)).all(), case
