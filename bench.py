@@ -805,7 +805,11 @@ def run_blas(args):
     T = _dev_triangular(n, 21, dev)
     X = _dev_dd_uniform(n * n, 22, dev)
     one = np.array([1.0, 0.0])
-    for side, uplo, ta in (("L", "L", "N"), ("L", "U", "T"), ("R", "U", "N"), ("R", "L", "T")):
+    # six (side, uplo, trans) cases run the blocked right-looking solve; L-L-T and
+    # R-L-N are one sequential chain per vector (their update order runs against
+    # the pivot order), latency-bound
+    for side, uplo, ta in (("L", "L", "N"), ("L", "U", "T"), ("R", "U", "N"), ("R", "L", "T"),
+                           ("L", "L", "T"), ("R", "L", "N")):
         ms = _events_time(lambda: api.wtrsm(side, uplo, ta, "N", n, n, one, T, n, X, n),
                           args.steps, args.warmup, stream, min_warm_s=0.0)
         macs = n * n * (n - 1) / 2.0

@@ -117,6 +117,89 @@ __device__ __forceinline__ dd dd_div(dd x, dd y) {
   return r;
 }
 
+// ---- multiply-add forms for the long loops ----------------------------------
+// Integer tests on the bit patterns (no FP64 compares): not inf / NaN, and two
+// values both +-0.
+//
+// fmadd_dd: acc + x * y (or acc - x * y) with the DD operators, bit-identical
+// to dd_add(acc, dd_mul(x, y)) (dd_sub) for every input.  The general paths of
+// both operators are evaluated unconditionally; every short-circuit case of
+// the two operators (non-finite product -- its general-path high limb is then
+// NaN --, non-finite sum, both high limbs of the addition zero) shows as a
+// non-finite leading sum or two zero high limbs, and only then is the step
+// redone with the operators themselves.
+__device__ __forceinline__ bool finite_bits(double v) {
+  return (__double2hiint(v) & 0x7ff00000) != 0x7ff00000;
+}
+__device__ __forceinline__ bool both_zero_bits(double a, double b) {
+  return ((((unsigned)__double2hiint(a) | (unsigned)__double2hiint(b)) & 0x7fffffffu) |
+          (unsigned)__double2loint(a) | (unsigned)__double2loint(b)) == 0u;
+}
+// Branch-free forms of +, -, *: bit-identical to dd_add / dd_sub / dd_mul for
+// every input; the short-circuit results are selected instead of branched to,
+// so the compiler can interleave many independent chains (a tile of
+// accumulators) or hoist independent products ahead of a dependent chain.
+__device__ __forceinline__ dd add_parts_bf(double xh, double xl, double yh, double yl) {
+  double s, b, c, d, a2, c2, rh, rl;
+  two_sum(xh, yh, s, b);
+  two_sum(xl, yl, c, d);  // c = xl + yl, the short-circuit low limb
+  fast_two_sum(s, c, a2, c2);
+  b = add(b, d);
+  b = add(b, c2);
+  fast_two_sum(a2, b, rh, rl);
+  const bool fin = finite_bits(s), zz = both_zero_bits(xh, yh);
+  dd r;
+  r.hi = (fin && !zz) ? rh : s;
+  r.lo = fin ? (zz ? c : rl) : 0.0;
+  return r;
+}
+__device__ __forceinline__ dd dd_add_bf(dd x, dd y) { return add_parts_bf(x.hi, x.lo, y.hi, y.lo); }
+__device__ __forceinline__ dd dd_sub_bf(dd x, dd y) { return add_parts_bf(x.hi, x.lo, -y.hi, -y.lo); }
+__device__ __forceinline__ dd dd_mul_bf(dd x, dd y) {
+  double p00, e00, rh, rl;
+  two_prod(x.hi, y.hi, p00, e00);
+  double p01 = mul(x.hi, y.lo);
+  const double p10 = mul(x.lo, y.hi);
+  p01 = add(p01, p10);
+  e00 = add(e00, p01);
+  fast_two_sum(p00, e00, rh, rl);
+  const bool fin = finite_bits(p00);
+  dd r;
+  r.hi = fin ? rh : p00;
+  r.lo = fin ? rl : 0.0;
+  return r;
+}
+
+// Guarded form: the general path and a branch (not taken on ordinary data) to
+// the operators.  Fewer instructions than the select form, but each step ends a
+// basic block, so it suits loops with few chains per thread and many warps.
+template <bool SUB>
+__device__ __forceinline__ dd fmadd_dd(dd acc, dd x, dd y) {
+  double p00, e00;
+  two_prod(x.hi, y.hi, p00, e00);
+  double p01 = mul(x.hi, y.lo);
+  const double p10 = mul(x.lo, y.hi);
+  p01 = add(p01, p10);
+  e00 = add(e00, p01);
+  double ph, pl;
+  fast_two_sum(p00, e00, ph, pl);
+  if (SUB) {
+    ph = -ph;
+    pl = -pl;
+  }
+  double s, b, c, d, a2, c2;
+  two_sum(acc.hi, ph, s, b);
+  two_sum(acc.lo, pl, c, d);
+  fast_two_sum(s, c, a2, c2);
+  b = add(b, d);
+  b = add(b, c2);
+  dd r;
+  fast_two_sum(a2, b, r.hi, r.lo);
+  if (__builtin_expect(!finite_bits(s) || both_zero_bits(acc.hi, ph), 0))
+    r = SUB ? dd_sub(acc, dd_mul(x, y)) : dd_add(acc, dd_mul(x, y));
+  return r;
+}
+
 // ---- sqrt (float64x2.h:2190-2212), Karp/Markstein --------------------------
 __device__ __forceinline__ dd dd_sqrt(dd x) {
   double c = __dsqrt_rn(x.hi);

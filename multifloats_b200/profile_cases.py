@@ -24,7 +24,7 @@ def main() -> int:
     from multifloats_b200 import workloads as W
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["split", "plain", "elementwise", "reduce", "batched", "gemv", "all"])
+    ap.add_argument("case", choices=["split", "plain", "elementwise", "reduce", "batched", "gemv", "blas", "all"])
     ap.add_argument("--n", type=int, default=2048, help="matrix size for split / plain")
     args = ap.parse_args()
     dev = torch.device("cuda:0")
@@ -62,6 +62,15 @@ def main() -> int:
         a, x = d(W.dd_uniform(m * m, 8)), d(W.dd_uniform(m, 9))
         api.matmuldd_mv(a, x, m, m, 8)
         api.matmuldd_vm(x, a, m, m, 8)
+    if args.case in ("blas", "all"):
+        # wgemm in both accumulation forms and the blocked / chain wtrsm, n = 1024
+        m = 1024
+        a, b, c = d(W.dd_uniform(m * m, 10)), d(W.dd_uniform(m * m, 11)), d(W.dd_uniform(m * m, 12))
+        api.wgemm("N", "N", m, m, m, (1.5, 0.0), a, m, b, m, (0.5, 0.0), c, m)
+        api.wgemm("T", "N", m, m, m, (1.5, 0.0), a, m, b, m, (0.5, 0.0), c, m)
+        t = d(W.dd_triangular(m, m, 13))
+        api.wtrsm("L", "L", "N", "N", m, m, (1.0, 0.0), t, m, c, m)
+        api.wtrsm("L", "L", "T", "N", m, m, (1.0, 0.0), t, m, c, m)
     if args.case == "batched":
         # the batched configuration: 2000 GEMMs, M, N, K log-uniform in [16, 1024],
         # plain and split plans (built-in tile choice), each run once
