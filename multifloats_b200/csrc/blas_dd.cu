@@ -470,57 +470,80 @@ __global__ void __launch_bounds__(kTThreads)
 //   RN: x = alpha x if alpha /= one; x -= A(k,j) x_k unless A(k,j) = 0;
 //       x = (one / A(j,j)) x if non-unit.
 constexpr int kChainThreads = 32;
-constexpr int kChainBatch = 8;  // (coefficient, pivot) pairs loaded one batch ahead
+constexpr int kChainBatch = 16;  // (coefficient, pivot) pairs loaded one batch ahead
 
-template <int KIND>
+template <int KIND, bool ALIGNED>
 __global__ void __launch_bounds__(kChainThreads)
     wtrsm_chain_kernel(const double *__restrict__ A, int64_t lda, double *__restrict__ B,
                        int64_t ldb, int64_t L, int64_t NV, dd alpha, int alpha_not_one, int nounit) {
   const int64_t v = (int64_t)blockIdx.x * kChainThreads + threadIdx.x;
   if (v >= NV) return;
-  auto xptr = [&](int64_t e) -> double * {
-    return KIND == T_LT ? B + 2 * (e + v * ldb) : B + 2 * (v + e * ldb);
-  };
+  // element e of this vector at xv + e * xs (doubles)
+  const int64_t xs = KIND == T_LT ? 2 : 2 * ldb;
+  double *const xv = KIND == T_LT ? B + 2 * v * ldb : B + 2 * v;
   for (int64_t e = L - 1; e >= 0; --e) {
-    dd x = ld_dd(xptr(e));
+    dd x = ld_dd_a<ALIGNED>(xv + e * xs);
     if (KIND == T_LT || alpha_not_one) x = dd_mul(alpha, x);
-    const double *col = A + 2 * (e * lda);
-    // the chain x -= A(k,e) x_k over k = e+1 .. L-1; the loads and products of
-    // the next batch are independent of it and issued before its subtractions
+    // the chain x -= A(k,e) x_k over k = e+1 .. L-1 in batches: the loads and
+    // products of a batch do not depend on the chain and go ahead of it
+    const double *cp = A + 2 * (e * lda + e + 1);
+    const double *xp = xv + (e + 1) * xs;
+    int64_t rem = L - 1 - e;
     dd cn[kChainBatch], xn[kChainBatch];
-    auto fetch = [&](int64_t k0) {
+    auto fetch = [&]() {
 #pragma unroll
       for (int u = 0; u < kChainBatch; ++u) {
-        const bool in = k0 + u < L;
-        cn[u] = in ? ld_dd(col + 2 * (k0 + u)) : dd0();
-        xn[u] = in ? ld_dd(xptr(k0 + u)) : dd0();
+        cn[u] = ld_dd_a<ALIGNED>(cp + 2 * u);
+        xn[u] = ld_dd_a<ALIGNED>(xp + u * xs);
       }
     };
-    if (e + 1 < L) fetch(e + 1);
-    for (int64_t k0 = e + 1; k0 < L; k0 += kChainBatch) {
+    // the product's general path with only its high limb selected: when the
+    // product short-circuits (non-finite), so does the subtraction, and its low
+    // limb is never read
+    auto product = [&](dd c, dd xk, double &ph, double &pl) {
+      double p00, e00;
+      mfdev::two_prod(c.hi, xk.hi, p00, e00);
+      double p01 = __dmul_rn(c.hi, xk.lo);
+      const double p10 = __dmul_rn(c.lo, xk.hi);
+      p01 = __dadd_rn(p01, p10);
+      e00 = __dadd_rn(e00, p01);
+      mfdev::fast_two_sum(p00, e00, ph, pl);
+      ph = mfdev::finite_bits(p00) ? ph : p00;
+    };
+    auto step = [&](dd c, double ph, double pl) {
+      const dd r = mfdev::dd_sub_bf(x, mfdev::make(ph, pl));
+      const bool skip = KIND == T_RN && mfdev::both_zero_bits(c.hi, c.lo);
+      x.hi = skip ? x.hi : r.hi;
+      x.lo = skip ? x.lo : r.lo;
+    };
+    if (rem >= kChainBatch) fetch();
+    while (rem >= kChainBatch) {
       dd c[kChainBatch], xk[kChainBatch];
 #pragma unroll
       for (int u = 0; u < kChainBatch; ++u) {
         c[u] = cn[u];
         xk[u] = xn[u];
       }
-      if (k0 + kChainBatch < L) fetch(k0 + kChainBatch);
-      dd p[kChainBatch];  // the products do not depend on the chain
+      cp += 2 * kChainBatch;
+      xp += kChainBatch * xs;
+      rem -= kChainBatch;
+      if (rem >= kChainBatch) fetch();
+      double ph[kChainBatch], pl[kChainBatch];
 #pragma unroll
-      for (int u = 0; u < kChainBatch; ++u) p[u] = mfdev::dd_mul_bf(c[u], xk[u]);
+      for (int u = 0; u < kChainBatch; ++u) product(c[u], xk[u], ph[u], pl[u]);
 #pragma unroll
-      for (int u = 0; u < kChainBatch; ++u) {
-        const dd r = mfdev::dd_sub_bf(x, p[u]);
-        const bool skip = (KIND == T_RN && is_zero(c[u])) || k0 + u >= L;
-        x.hi = skip ? x.hi : r.hi;
-        x.lo = skip ? x.lo : r.lo;
-      }
+      for (int u = 0; u < kChainBatch; ++u) step(c[u], ph[u], pl[u]);
     }
-    const dd d = ld_dd(col + 2 * e);
+    for (; rem > 0; --rem, cp += 2, xp += xs) {
+      const dd c = ld_dd_a<ALIGNED>(cp);
+      double ph, pl;
+      product(c, ld_dd_a<ALIGNED>(xp), ph, pl);
+      step(c, ph, pl);
+    }
+    const dd d = ld_dd_a<ALIGNED>(A + 2 * (e * lda + e));
     if (nounit) x = KIND == T_LT ? dd_div(x, d) : dd_mul(dd_div(mfdev::make(1.0, 0.0), d), x);
-    double *p = xptr(e);
-    p[0] = x.hi;
-    p[1] = x.lo;
+    double *p = xv + e * xs;
+    st_dd<ALIGNED>(p, x);
   }
 }
 
@@ -595,10 +618,15 @@ int wtrsm_dev(char side, char uplo, char ta, char diag, int64_t m, int64_t n,
   const unsigned g = (unsigned)blocks;
   if (!upper && lside != notr) {  // LT lower / RN lower: the sequential chain form
     const int64_t cb = (NV + kChainThreads - 1) / kChainThreads;
-    if (lside)
-      wtrsm_chain_kernel<T_LT><<<(unsigned)cb, kChainThreads, 0, s>>>(A, lda, Bm, ldb, L, NV, av, ano, nounit);
+    const bool al = ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15) == 0;
+    if (lside && al)
+      wtrsm_chain_kernel<T_LT, true><<<(unsigned)cb, kChainThreads, 0, s>>>(A, lda, Bm, ldb, L, NV, av, ano, nounit);
+    else if (lside)
+      wtrsm_chain_kernel<T_LT, false><<<(unsigned)cb, kChainThreads, 0, s>>>(A, lda, Bm, ldb, L, NV, av, ano, nounit);
+    else if (al)
+      wtrsm_chain_kernel<T_RN, true><<<(unsigned)cb, kChainThreads, 0, s>>>(A, lda, Bm, ldb, L, NV, av, ano, nounit);
     else
-      wtrsm_chain_kernel<T_RN><<<(unsigned)cb, kChainThreads, 0, s>>>(A, lda, Bm, ldb, L, NV, av, ano, nounit);
+      wtrsm_chain_kernel<T_RN, false><<<(unsigned)cb, kChainThreads, 0, s>>>(A, lda, Bm, ldb, L, NV, av, ano, nounit);
     MF_TRY_CUDA(cudaGetLastError());
     return MFCUDA_OK;
   }
