@@ -168,6 +168,22 @@ MULTIFLOATS_CUDA_API void matmuldd_mm_split(const float64x2 *a, const float64x2 
 MULTIFLOATS_CUDA_API void cmatmuldd_mm_split(const complex64x2 *a, const complex64x2 *b,
                                              complex64x2 *c, int64_t m, int64_t k, int64_t n,
                                              int slices, double *max_err_bound_out);
+/* CRT (modular) split-INT8 DD matmul (no reference counterpart): the same
+ * product, to the same kind of stated bound, from fewer tensor-core products.
+ * Each row of A / column of B is scaled by a power of two and every entry
+ * rounded to a W-bit integer (as in matmuldd_mm_split); the exact integer
+ * product is recovered from its residues modulo N pairwise-coprime moduli
+ * <= 256 (one INT8 GEMM per modulus on the tcgen05 tensor cores, exact INT32
+ * accumulation) by the Chinese remainder theorem, then rounded to DD and
+ * scaled.  bits = 0 picks the smallest W whose a-priori bound meets
+ * err_ij <= 8 k 2^-104 (|A||B|)_ij (W = 92, N = 27 at k = 4096 for operands
+ * spanning one binade per row / column); 8..110 = fixed W.  *max_err_bound_out
+ * (may be NULL) receives the bound in units of k 2^-104 (|A||B|)_ij.  Inf/NaN
+ * in a row of A or column of B yields NaN in the affected outputs.  Host
+ * pointers, synchronous. */
+MULTIFLOATS_CUDA_API void matmuldd_mm_crt(const float64x2 *a, const float64x2 *b, float64x2 *c,
+                                          int64_t m, int64_t k, int64_t n, int bits,
+                                          double *max_err_bound_out);
 
 /* ==========================================================================
  * 2. Device-pointer API (asynchronous on `stream`, a cudaStream_t; NULL = legacy
@@ -194,6 +210,18 @@ MULTIFLOATS_CUDA_API int mfcuda_cmatmuldd_mm(const complex64x2 *a, const complex
  * operands' exponent spreads); a non-NULL info_out makes the call wait for the
  * result and report MFCUDA_ERR_TIMEOUT if a bounded device wait expired. */
 MULTIFLOATS_CUDA_API size_t mfcuda_split_workspace_size(int64_t m, int64_t k, int64_t n);
+/* CRT form on device pointers (16-byte aligned).  bits: 0 = W from `target`
+ * (units of k 2^-104 (|A||B|)_ij), 8..110 = fixed.  `workspace` may be NULL or
+ * hold mfcuda_crt_workspace_size(m, k, n, bits) bytes.  info_out may be NULL or
+ * point to int[4] receiving {N moduli, rho_A, rho_B, W} (waits for the result,
+ * MFCUDA_ERR_TIMEOUT if a bounded device wait expired).  mfcuda_crt_bound gives
+ * the a-priori bound for W, the spreads and k (-1 for invalid arguments). */
+MULTIFLOATS_CUDA_API size_t mfcuda_crt_workspace_size(int64_t m, int64_t k, int64_t n, int bits);
+MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_crt(const float64x2 *a, const float64x2 *b, float64x2 *c,
+                                                int64_t m, int64_t k, int64_t n, int bits, double target,
+                                                void *workspace, size_t workspace_bytes, int *info_out,
+                                                void *stream);
+MULTIFLOATS_CUDA_API double mfcuda_crt_bound(int bits, int rho_a, int rho_b, int64_t k);
 MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_split(const float64x2 *a, const float64x2 *b,
                                                   float64x2 *c, int64_t m, int64_t k, int64_t n,
                                                   int slices, double target, void *workspace,

@@ -32,7 +32,8 @@ SOURCES = [
     "batched.cu",
     "blas_dd.cu",
 ]
-HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh", "split_device.cuh", "gemm_tile.cuh"]
+HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh", "split_device.cuh", "gemm_tile.cuh",
+           "crt_device.cuh", "crt_tables.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [

@@ -1,0 +1,104 @@
+#!/usr/bin/env python3
+"""Generate ``crt_tables.h``: the moduli of the CRT (modular) split form.
+
+The moduli are the pairwise-coprime integers m <= 256 taken greedily from 256
+down (256, 255, 253, 251, 247, 241, ...): every residue fits a signed byte in
+the symmetric range [-floor(m/2), ceil(m/2) - 1], so each modulus costs one
+INT8 x INT8 -> INT32 product on the tensor cores.  Per modulus the header
+holds:
+
+* ``crt_mod[t]``       m_t
+* ``crt_lg[t]``        floor(log2(m_0 ... m_{t-1})) (exact: the product's bit
+                       length minus one), ``crt_lg[0] = 0``; the plan takes the
+                       smallest count N with crt_lg[N] >= the bits it needs
+                       (``crt_lg_host``: the same numbers for host code)
+* ``crt_digw[t][w]``   the signed bytes c_q = symmetric residue of 256^q mod m_t
+                       for q = 4w .. 4w+3 (q < 14; zero above), packed as the
+                       four bytes of a word, so that for a balanced base-256
+                       representation X = sum_q d_q 256^q (signed byte digits)
+                       the dot product sum_q d_q c_q (four dp4a) is congruent
+                       to X modulo m_t
+* ``crt_inv[t]``       1/m_t rounded to float (quotient estimate of the final
+                       reduction; the two range corrections make it exact)
+* ``crt_rlo[t]``, ``crt_rhi[t]``  the symmetric residue range
+
+Usage::
+
+    python gen_crt_tables.py     # (re)write crt_tables.h next to this file
+"""
+from __future__ import annotations
+
+import os
+import struct
+import sys
+from math import gcd
+
+NMAX = 36   # 266 bits: enough for 2W + log2(k) + 3 with W <= 110, k < 2^31
+DIGITS = 14
+
+
+def moduli(n: int) -> list[int]:
+    out: list[int] = []
+    m = 256
+    while len(out) < n:
+        if all(gcd(m, x) == 1 for x in out):
+            out.append(m)
+        m -= 1
+    return out
+
+
+def sym(v: int, m: int) -> int:
+    """Symmetric representative of v mod m in [-floor(m/2), ceil(m/2) - 1]."""
+    r = v % m
+    return r - m if r >= (m + 1) // 2 else r
+
+
+def main() -> int:
+    ms = moduli(NMAX)
+    prod, lg = 1, [0]
+    for m in ms:
+        prod *= m
+        lg.append(prod.bit_length() - 1)
+    lines = [
+        "// Generated by gen_crt_tables.py -- do not edit.",
+        "// Moduli of the CRT split form and their per-modulus constants.",
+        "#pragma once",
+        "#include <stdint.h>",
+        "#ifndef MF_TABLE",
+        "#define MF_TABLE static const",
+        "#endif",
+        f"#define CRT_NMAX {NMAX}",
+        f"MF_TABLE uint32_t crt_mod[{NMAX}] = {{" + ", ".join(str(m) for m in ms) + "};",
+        f"MF_TABLE int crt_lg[{NMAX + 1}] = {{" + ", ".join(str(v) for v in lg) + "};",
+        "#ifdef __cplusplus",
+        "// host copy of crt_lg (workspace sizing)",
+        f"static constexpr int crt_lg_host[{NMAX + 1}] = {{" + ", ".join(str(v) for v in lg) + "};",
+        "#endif",
+    ]
+    words = []
+    for m in ms:
+        cs = [sym(pow(256, q, m), m) if q < DIGITS else 0 for q in range(16)]
+        w = []
+        for k in range(4):
+            v = 0
+            for b in range(4):
+                v |= (cs[4 * k + b] & 0xFF) << (8 * b)
+            w.append(f"0x{v:08x}u")
+        words.append("{" + ", ".join(w) + "}")
+    lines.append(f"MF_TABLE uint32_t crt_digw[{NMAX}][4] = {{" + ",\n    ".join(words) + "};")
+    inv = []
+    for m in ms:
+        b = struct.unpack("<I", struct.pack("<f", 1.0 / m))[0]
+        inv.append(f"0x{b:08x}u")
+    lines.append(f"MF_TABLE uint32_t crt_inv_bits[{NMAX}] = {{" + ", ".join(inv) + "};  // float(1/m) bit patterns")
+    lines.append(f"MF_TABLE int crt_rlo[{NMAX}] = {{" + ", ".join(str(-(m // 2)) for m in ms) + "};")
+    lines.append(f"MF_TABLE int crt_rhi[{NMAX}] = {{" + ", ".join(str((m + 1) // 2 - 1) for m in ms) + "};")
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "crt_tables.h")
+    with open(out, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    print(out)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

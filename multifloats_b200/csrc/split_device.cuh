@@ -25,10 +25,13 @@ constexpr int MMA_SMEM = NSTAGE * STAGE + 1024 /*align*/ + 256 /*barriers*/;
 constexpr int KC_BLOCKS = (int)(2147483647LL / ((long long)SMAX * 16384LL * BK));
 constexpr uint64_t WAIT_NS = 2000000000ull;  // bounded waits: 2 s
 
+// S: slices per operand (CRT form: moduli), G = S - 1, W: bits of the fixed-point
+// operands; crt = 1 selects the CRT form (one product per item, slice t of A
+// with slice t of B); nl: 32-bit limbs of its reconstruction.
 struct Plan {
   int S, G, W;
   int rho_a, rho_b;
-  int pad[3];
+  int crt, nl, pad;
 };
 
 __device__ __forceinline__ uint64_t globaltimer() {
@@ -263,6 +266,8 @@ __device__ __forceinline__ void plan_body(const StatSet &st, int slices, double 
     plan->W = 8 * S - 2;
     plan->rho_a = ra;
     plan->rho_b = rb;
+    plan->crt = 0;
+    plan->nl = 0;
   }
   // zero rows / columns: any sigma works, the digits are all zero
   __syncthreads();

@@ -39,6 +39,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "crt_device.cuh"
 #include "dd_device.cuh"
 #include "split_device.cuh"
 #include "tcgen05.cuh"
@@ -117,6 +118,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = plan->S, G = S - 1;
+  const bool crt = plan->crt != 0;  // CRT form: item g is the single product A_g B_g
   const int ntm = M_pad / BM, ntn = N_pad / BN, ntiles = ntm * ntn;
   const int items = (G + 1) * nkc * ntiles;
 
@@ -163,8 +165,8 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
       for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
         Item it = decode(w, G, nkc, ntm, ntiles);
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
-        for (int s = 0; s <= it.g && ok; ++s) {
-          int t = it.g - s;
+        for (int s = crt ? it.g : 0; s <= it.g && ok; ++s) {
+          int t = crt ? s : it.g - s;
           for (int kb = kb0; kb < kb1; ++kb) {
             if (!wait_bar(&empty[stage], phase ^ 1, abort_flag)) {
               fail(1);
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         mftc::tc_fence_after();
         const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
         uint32_t accumulate = 0;
-        for (int s = 0; s <= it.g && ok; ++s) {
+        for (int s = crt ? it.g : 0; s <= it.g && ok; ++s) {
           for (int kb = kb0; kb < kb1; ++kb) {
             if (!wait_bar(&full[stage], phase, abort_flag)) {
               fail(4);
@@ -382,6 +384,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
   const bool leader = rank == 0;
   const int pair_id = blockIdx.x >> 1, npairs = gridDim.x >> 1;
   const int S = plan->S, G = S - 1;
+  const bool crt = plan->crt != 0;  // CRT form: item g is the single product A_g B_g
   const int tn_cols = BN * nsub;
   const int ntm = M_pad / BM_PAIR, ntn = N_pad / tn_cols, ntiles = ntm * ntn;
   const int nacc = 2 / nsub;             // accumulators
@@ -434,8 +437,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
         const int arow = it.tm * BM_PAIR + (int)rank * 128;
         const int brow = it.tn * tn_cols + (int)rank * 128;
-        for (int s = 0; s <= it.g && ok; ++s) {
-          int t = it.g - s;
+        for (int s = crt ? it.g : 0; s <= it.g && ok; ++s) {
+          int t = crt ? s : it.g - s;
           for (int kb = kb0; kb < kb1; ++kb) {
             if (!wait_bar(&empty[stage], phase ^ 1, abort_flag)) {
               fail(1);
@@ -489,7 +492,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
         mftc::tc_fence_after();
         const uint32_t d_tmem = tmem_base + (uint32_t)(acc * acc_cols);
         uint32_t accumulate = 0;
-        for (int s = 0; s <= it.g && ok; ++s) {
+        for (int s = crt ? it.g : 0; s <= it.g && ok; ++s) {
           for (int kb = kb0; kb < kb1; ++kb) {
             if (!wait_bar(&full[stage], phase, abort_flag)) {
               fail(4);
@@ -585,6 +588,54 @@ __global__ void __launch_bounds__(128) combine_kernel(const int32_t *__restrict_
 constexpr int COMBINE_THREADS = 128;
 
 // ---------------------------------------------------------------------------
+// CRT form (crt_device.cuh): plan, residue slicing, reconstruction
+// ---------------------------------------------------------------------------
+__global__ void crt_plan_kernel(StatSet st, int bits, double target, int64_t k, Plan *plan, CrtConst *cc) {
+  crt_plan_body(st, bits, target, k, plan, cc);
+}
+__global__ void __launch_bounds__(256) crt_slice_a_kernel(const double *__restrict__ A, int64_t M, int64_t K,
+                                                          int64_t stride, int64_t M_pad, int64_t K_pad,
+                                                          const int *sig, const int *flag, const Plan *plan,
+                                                          int8_t *__restrict__ As) {
+  extern __shared__ __align__(16) uint8_t crt_tile[];
+  crt_slice_a_body(A, M, K, stride, M_pad, K_pad, sig, flag, plan, As, crt_tile, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restrict__ B, int64_t K, int64_t N,
+                                                          int64_t stride, int64_t N_pad, int64_t K_pad,
+                                                          const int *sig, const int *flag, const Plan *plan,
+                                                          int8_t *__restrict__ Bs) {
+  const int64_t p8 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 8;
+  if (p8 >= K_pad) return;
+  crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, blockIdx.y, p8);
+}
+// Thread per row i of column j = blockIdx.y; `mode` as combine_kernel.
+__global__ void __launch_bounds__(128) crt_combine_kernel(const int32_t *__restrict__ D, const Plan *plan,
+                                                          const CrtConst *cc, const int *sigA, const int *flagA,
+                                                          const int *sigB, const int *flagB, int64_t M,
+                                                          int64_t N, int64_t M_pad, int64_t N_pad, int nkc,
+                                                          double *__restrict__ C, int64_t cstride, int mode) {
+  __shared__ CrtShared cs;
+  const int n = plan->S, nl = plan->nl, W = plan->W;
+  crt_load_shared(cc, n, cs);
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= M || j >= N) return;
+  const int64_t kstride = N_pad * M_pad, gstride = (int64_t)nkc * kstride;
+  double2 out;
+  if (flagA[i] | flagB[j])
+    out = make_double2(CUDART_NAN, 0.0);
+  else
+    out = crt_output(D + j * M_pad + i, gstride, kstride, nkc, n, nl, cs, sigA[i] + sigB[j] - 2 * W);
+  double2 *dst = reinterpret_cast<double2 *>(C) + (j * M + i) * cstride;
+  if (mode != 0) {
+    const double2 prev = *dst;
+    const mfdev::dd p = mfdev::make(out.x, out.y), q = mfdev::make(prev.x, prev.y);
+    const mfdev::dd r = mode == 1 ? mfdev::dd_sub(q, p) : mfdev::dd_add(q, p);
+    out = make_double2(r.hi, r.lo);
+  }
+  __stcs(dst, out);
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 // Workspace of one call with nA A-side operands (m x k) and nB B-side
@@ -593,9 +644,10 @@ constexpr int COMBINE_THREADS = 128;
 struct Layout {
   int64_t M_pad, N_pad, K_pad, kblocks, nkc;
   int nA, nB;
+  int nsl;    // slices per operand allocated (digit slices, or CRT moduli)
   bool pair;  // 256 x (256 nsub) tiles on CTA pairs (m > 128), else 128 x 256 tiles
   int nsub;   // 256-column halves per pair tile: 2 when n > 256
-  size_t off_plan, off_stats[4], off_slices[4], off_D, total;
+  size_t off_plan, off_crt, off_stats[4], off_slices[4], off_D, total;
 };
 
 static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
@@ -620,8 +672,18 @@ static int pair_nsub() {
   return v;
 }
 
-static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB) {
+// Most moduli the CRT form can need for inner dimension k (W <= bits, or
+// W <= CRT_WMAX when bits is 0).
+static int crt_slices_max(int64_t k, int bits) {
+  const int need = 2 * (bits > 0 ? bits : CRT_WMAX) + ceil_log2(k < 1 ? 1 : k) + 3;
+  int n = 1;
+  while (n < CRT_NMAX && crt_lg_host[n] < need) ++n;
+  return n;
+}
+
+static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB, int nsl = SMAX) {
   Layout L;
+  L.nsl = nsl;
   L.pair = use_pair(m);
   L.nsub = L.pair && n > BN ? pair_nsub() : 1;
   L.M_pad = round_up(m < 1 ? 1 : m, L.pair ? BM_PAIR : BM);
@@ -638,12 +700,13 @@ static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB) {
     return o;
   };
   L.off_plan = take(sizeof(Plan));
+  L.off_crt = take(sizeof(CrtConst));
   for (int o = 0; o < nA + nB; ++o) {
     int64_t rows = o < nA ? L.M_pad : L.N_pad;
     L.off_stats[o] = take(3 * sizeof(int) * rows);
-    L.off_slices[o] = take((size_t)SMAX * rows * L.K_pad);
+    L.off_slices[o] = take((size_t)nsl * rows * L.K_pad);
   }
-  L.off_D = take((size_t)SMAX * L.nkc * L.N_pad * L.M_pad * sizeof(int32_t));
+  L.off_D = take((size_t)nsl * L.nkc * L.N_pad * L.M_pad * sizeof(int32_t));
   L.total = off + 256 /* status word */;
   return L;
 }
@@ -660,10 +723,10 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, uint32_t box_rows) {
+static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, uint32_t box_rows, int nsl) {
   auto fn = encode_fn();
   if (!fn) return false;
-  cuuint64_t dims[3] = {(cuuint64_t)K_pad, (cuuint64_t)rows, (cuuint64_t)SMAX};
+  cuuint64_t dims[3] = {(cuuint64_t)K_pad, (cuuint64_t)rows, (cuuint64_t)nsl};
   cuuint64_t strides[2] = {(cuuint64_t)K_pad, (cuuint64_t)(rows * K_pad)};
   cuuint32_t box[3] = {(cuuint32_t)BK, box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
@@ -724,6 +787,10 @@ size_t workspace_size(int64_t m, int64_t k, int64_t n, bool complex_operands) {
   int no = complex_operands ? 2 : 1;
   return layout(m, k, n, no, no).total;
 }
+size_t crt_workspace_size(int64_t m, int64_t k, int64_t n, int bits, bool complex_operands) {
+  int no = complex_operands ? 2 : 1;
+  return layout(m, k, n, no, no, crt_slices_max(k, bits)).total;
+}
 
 static std::once_flag g_attr_once;
 
@@ -756,11 +823,13 @@ struct Product {
 // Runs the whole split pipeline for `nprod` products of the operands
 // A-side views (aview[o], stride astride[o]) and B-side views.  info (may be
 // NULL) receives {S, rho_A, rho_B}; a non-NULL info waits for completion.
+// crt = 1 runs the CRT form with `slices` read as the operand bits W (0 = from
+// the target); info then receives {moduli, rho_A, rho_B, W}.
 static int run_products(const double *const *aview, const int64_t *astride, int nA,
                         const double *const *bview, const int64_t *bstride, int nB,
                         const Product *prods, int nprod, int64_t m, int64_t k, int64_t n, int slices,
-                        double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info) {
-  Layout L = layout(m, k, n, nA, nB);
+                        double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info, int crt = 0) {
+  Layout L = layout(m, k, n, nA, nB, crt ? crt_slices_max(k, slices) : SMAX);
   if (L.M_pad > INT32_MAX / 2 || L.N_pad > INT32_MAX / 2 || L.kblocks > INT32_MAX / 2 ||
       L.N_pad > 65535 || L.K_pad / 64 > 65535)
     return MFCUDA_ERR_UNSUPPORTED;
@@ -773,6 +842,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
   }
   uint8_t *base = static_cast<uint8_t *>(ws);
   Plan *plan = reinterpret_cast<Plan *>(base + L.off_plan);
+  CrtConst *cc = reinterpret_cast<CrtConst *>(base + L.off_crt);
   int32_t *D = reinterpret_cast<int32_t *>(base + L.off_D);
   int *status = reinterpret_cast<int *>(base + L.total - 256);
   const int nops = nA + nB;
@@ -790,6 +860,8 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     std::call_once(g_attr_once, [] {
       cudaFuncSetAttribute(split_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
       cudaFuncSetAttribute(split_mma_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM);
+      cudaFuncSetAttribute(crt_slice_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           CRT_NMAX * SA_ROWS * SA_STRIDE);
     });
     prof_call_begin();
     mark(0, s);
@@ -812,22 +884,33 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
       st.count[o] = aside ? m : n;
       st.side[o] = aside ? 0 : 1;
     }
-    plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, plan);
+    if (crt)
+      crt_plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, k, plan, cc);
+    else
+      plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, plan);
     mark(1, s);
+    const dim3 ga((unsigned)(L.M_pad / 32), (unsigned)(L.K_pad / 64));
+    const dim3 gb((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad);
     for (int o = 0; o < nops; ++o) {
-      if (o < nA)
-        slice_a_kernel<<<dim3((unsigned)(L.M_pad / 32), (unsigned)(L.K_pad / 64)), 256, 0, s>>>(
-            aview[o], m, k, astride[o], L.M_pad, L.K_pad, sig[o], flag[o], plan, sl[o]);
+      if (o < nA && crt)
+        crt_slice_a_kernel<<<ga, 256, L.nsl * SA_ROWS * SA_STRIDE, s>>>(aview[o], m, k, astride[o], L.M_pad,
+                                                                       L.K_pad, sig[o], flag[o], plan, sl[o]);
+      else if (o < nA)
+        slice_a_kernel<<<ga, 256, 0, s>>>(aview[o], m, k, astride[o], L.M_pad, L.K_pad, sig[o], flag[o], plan,
+                                          sl[o]);
+      else if (crt)
+        crt_slice_b_kernel<<<gb, 256, 0, s>>>(bview[o - nA], k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o],
+                                              flag[o], plan, sl[o]);
       else
-        slice_b_kernel<<<dim3((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad), 256, 0, s>>>(
-            bview[o - nA], k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o], flag[o], plan, sl[o]);
+        slice_b_kernel<<<gb, 256, 0, s>>>(bview[o - nA], k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o],
+                                          flag[o], plan, sl[o]);
     }
     const int tile_m = L.pair ? BM_PAIR : BM;
-    int items_max = SMAX * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
+    int items_max = L.nsl * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
     int grid = sm_count();
     if (L.pair) {
-      // super-items (pairs of diagonals) of the largest plan, SMAX slices
-      const int supers_max = ((SMAX + 1) / 2) * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
+      // super-items (pairs of diagonals, or pairs of moduli) of the largest plan
+      const int supers_max = ((L.nsl + 1) / 2) * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
       grid = pair_grid();
       if (grid > 2 * supers_max) grid = 2 * supers_max;
     } else if (grid > items_max) {
@@ -838,8 +921,8 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     for (int q = 0; q < nprod && rc == MFCUDA_OK; ++q) {
       const int ia = prods[q].a, ib = nA + prods[q].b;
       CUtensorMap tmA, tmB;
-      if (!make_map(&tmA, sl[ia], L.M_pad, L.K_pad, BM) ||
-          !make_map(&tmB, sl[ib], L.N_pad, L.K_pad, L.pair ? 128 : BN)) {
+      if (!make_map(&tmA, sl[ia], L.M_pad, L.K_pad, BM, L.nsl) ||
+          !make_map(&tmB, sl[ib], L.N_pad, L.K_pad, L.pair ? 128 : BN, L.nsl)) {
         rc = MFCUDA_ERR_CUDA;
         break;
       }
@@ -852,9 +935,14 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                                                              (int)L.N_pad, (int)L.nkc, (int)L.kblocks,
                                                              status);
       if (q == nprod - 1) mark(3, s);
-      combine_kernel<<<dim3(cgx, (unsigned)n), COMBINE_THREADS, 0, s>>>(D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n,
-                                                  L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,
-                                                  prods[q].ostride, prods[q].mode);
+      if (crt)
+        crt_combine_kernel<<<dim3((unsigned)((m + 127) / 128), (unsigned)n), 128, 0, s>>>(
+            D, plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, n, L.M_pad, L.N_pad, (int)L.nkc,
+            prods[q].out, prods[q].ostride, prods[q].mode);
+      else
+        combine_kernel<<<dim3(cgx, (unsigned)n), COMBINE_THREADS, 0, s>>>(D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n,
+                                                    L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,
+                                                    prods[q].ostride, prods[q].mode);
     }
     mark(4, s);
     if (rc == MFCUDA_OK && cudaGetLastError() != cudaSuccess) rc = MFCUDA_ERR_CUDA;
@@ -870,6 +958,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
         info[0] = hp.S;
         info[1] = hp.rho_a;
         info[2] = hp.rho_b;
+        if (crt) info[3] = hp.W;
       }
     }
   } while (0);
@@ -906,6 +995,26 @@ int run(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t
   int64_t one[1] = {1};
   Product p = {0, 0, reinterpret_cast<double *>(c), 1, 0};
   return run_products(av, one, 1, bv, one, 1, &p, 1, m, k, n, slices, target, ws, ws_bytes, s, info);
+}
+
+// CRT form of run(): bits = W (0: from the target); info = {moduli, rho_A, rho_B, W}.
+int run_crt(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k, int64_t n,
+            int bits, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info) {
+  int rc = check_args(a, b, c, m, k, n, 0, target);
+  if (bits < 0 || (bits > 0 && bits < 8) || bits > CRT_WMAX) return MFCUDA_ERR_INVALID_ARG;
+  if (rc == -1) return MFCUDA_OK;
+  MF_TRY(rc);
+  MF_TRY(require_device());
+  if (k == 0) {
+    MF_TRY_CUDA(cudaMemsetAsync(c, 0, (size_t)(m * n) * sizeof(float64x2), s));
+    if (info) info[0] = info[1] = info[2] = info[3] = 0;
+    return MFCUDA_OK;
+  }
+  const double *av[1] = {reinterpret_cast<const double *>(a)};
+  const double *bv[1] = {reinterpret_cast<const double *>(b)};
+  int64_t one[1] = {1};
+  Product p = {0, 0, reinterpret_cast<double *>(c), 1, 0};
+  return run_products(av, one, 1, bv, one, 1, &p, 1, m, k, n, bits, target, ws, ws_bytes, s, info, 1);
 }
 
 // Complex: re = Ar Br - Ai Bi, im = Ar Bi + Ai Br (the Fortran cdd_matmul_mm
@@ -972,9 +1081,54 @@ static int split_host(const void *a, const void *b, void *c, int64_t m, int64_t 
   return MFCUDA_OK;
 }
 
+static int crt_host(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k, int64_t n,
+                    int bits, double *bound_out) {
+  const size_t elem = sizeof(float64x2);
+  if (m < 0 || k < 0 || n < 0 || !mul_ok(m, k) || !mul_ok(k, n) || !mul_ok(m, n))
+    return MFCUDA_ERR_INVALID_ARG;
+  if (bits < 0 || (bits > 0 && bits < 8) || bits > split::CRT_WMAX) return MFCUDA_ERR_INVALID_ARG;
+  if (m == 0 || n == 0) return MFCUDA_OK;
+  if (!c || (k > 0 && (!a || !b))) return MFCUDA_ERR_INVALID_ARG;
+  MF_TRY(require_device());
+  size_t ba = (size_t)(m * k) * elem, bb = (size_t)(k * n) * elem, bc = (size_t)(m * n) * elem;
+  size_t wsb = split::crt_workspace_size(m, k, n, bits, false);
+  size_t sz[4] = {ba, bb, bc, wsb};
+  Staging st;
+  MF_TRY(staging_acquire(st, sz));
+  if (ba) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[0], a, ba, cudaMemcpyHostToDevice, st.stream));
+  if (bb) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[1], b, bb, cudaMemcpyHostToDevice, st.stream));
+  int info[4] = {0, 0, 0, 0};
+  MF_TRY(split::run_crt(static_cast<float64x2 *>(st.buf[0]), static_cast<float64x2 *>(st.buf[1]),
+                        static_cast<float64x2 *>(st.buf[2]), m, k, n, bits, 8.0, st.buf[3], wsb, st.stream, info));
+  MF_TRY_CUDA(cudaMemcpyAsync(c, st.buf[2], bc, cudaMemcpyDeviceToHost, st.stream));
+  MF_TRY_CUDA(cudaStreamSynchronize(st.stream));
+  if (bound_out) *bound_out = info[0] > 0 ? split::crt_bound(info[3], info[1], info[2], k) : 0.0;
+  return MFCUDA_OK;
+}
+
 }  // namespace mfcuda
 
 extern "C" {
+
+MULTIFLOATS_CUDA_API size_t mfcuda_crt_workspace_size(int64_t m, int64_t k, int64_t n, int bits) {
+  if (m < 0 || k < 0 || n < 0 || bits < 0 || bits > mfcuda::split::CRT_WMAX) return 0;
+  return mfcuda::split::crt_workspace_size(m, k, n, bits, false);
+}
+MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_crt(const float64x2 *a, const float64x2 *b, float64x2 *c,
+                                                int64_t m, int64_t k, int64_t n, int bits, double target,
+                                                void *workspace, size_t workspace_bytes, int *info_out,
+                                                void *stream) {
+  return mfcuda::split::run_crt(a, b, c, m, k, n, bits, target, workspace, workspace_bytes,
+                                mfcuda::as_stream(stream), info_out);
+}
+MULTIFLOATS_CUDA_API void matmuldd_mm_crt(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m,
+                                          int64_t k, int64_t n, int bits, double *max_err_bound_out) {
+  mfcuda::set_last_error(mfcuda::crt_host(a, b, c, m, k, n, bits, max_err_bound_out));
+}
+MULTIFLOATS_CUDA_API double mfcuda_crt_bound(int bits, int rho_a, int rho_b, int64_t k) {
+  if (bits < 8 || bits > mfcuda::split::CRT_WMAX || k < 1) return -1.0;
+  return mfcuda::split::crt_bound(bits, rho_a, rho_b, k);
+}
 
 MULTIFLOATS_CUDA_API void mfcuda_phase_profile_begin(void) { mfcuda::split::profile_begin(); }
 MULTIFLOATS_CUDA_API int mfcuda_phase_profile_end(double *phase_ms_sum, int64_t *calls) {

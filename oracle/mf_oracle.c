@@ -1338,3 +1338,215 @@ int orc_wtrsm(char side, char uplo, char transa, char diag, int64_t m, int64_t n
 }
 #undef ODD
 #undef OSET
+
+/* ---- CRT (modular) split form, restated on the CPU -------------------------
+ * The device (split_gemm.cu, crt_device.cuh) recovers the exact integer
+ * product C' = X Y^T of the rounded operands from its residues modulo N
+ * moduli by the Chinese remainder theorem.  This restatement computes C'
+ * directly with a 256-bit accumulator -- no moduli -- so it checks the modular
+ * reconstruction too.  Same scan and exponent spreads as the digit-sliced
+ * form, same plan (the smallest W whose a-priori bound meets the target), same
+ * rounding X = round(a 2^(W - sigma)), same conversion to DD (C'' = |C'|
+ * truncated to its 160 leading bits, hi = RN(C''), lo = RN(C'' - hi)) and the
+ * same exact scaling by 2^(sigma_i + tau_j - 2W). */
+#include "../multifloats_b200/csrc/crt_tables.h"
+#define CRT_WMAX 110
+static int crt_ceil_log2(int64_t k) {
+  int b = 0;
+  while (b < 63 && ((int64_t)1 << b) < k) ++b;
+  return b;
+}
+double orc_crt_bound(int W, int ra, int rb, int64_t k) {
+  return (ldexp(1.0, 104 + ra - W) + ldexp(1.0, 104 + rb - W) + ldexp(1.0, 104 + ra + rb - 2 * W) + 0.5) /
+         (double)k;
+}
+int orc_crt_plan(int bits, double target, int ra, int rb, int64_t k, int *nmod) {
+  int W = bits;
+  if (W <= 0) {
+    W = CRT_WMAX;
+    for (int w = 8; w <= CRT_WMAX; ++w)
+      if (orc_crt_bound(w, ra, rb, k) <= target) {
+        W = w;
+        break;
+      }
+  }
+  const int need = 2 * W + crt_ceil_log2(k) + 3;
+  int n = 1;
+  while (n < CRT_NMAX && crt_lg[n] < need) ++n;
+  if (nmod) *nmod = n;
+  return W;
+}
+/* the split form's rounding to the W-bit grid */
+static __int128 crt_round(double hi, double lo, int sigma, int W) {
+  int t = W - sigma;
+  __int128 xf = split_scaled_fixed(hi, t) + split_scaled_fixed(lo, t);
+  __int128 X = (xf + ((__int128)1 << (SPLIT_FRAC - 1))) >> SPLIT_FRAC;
+  __int128 lim = ((__int128)1 << W) - 1;
+  if (X > lim) X = lim;
+  if (X < -lim) X = -lim;
+  return X;
+}
+/* acc (256-bit two's complement, 4 little-endian words) += x * y */
+static void acc_add_prod(uint64_t acc[4], __int128 x, __int128 y) {
+  int neg = (x < 0) != (y < 0);
+  unsigned __int128 ux = x < 0 ? (unsigned __int128)(-x) : (unsigned __int128)x;
+  unsigned __int128 uy = y < 0 ? (unsigned __int128)(-y) : (unsigned __int128)y;
+  uint64_t x0 = (uint64_t)ux, x1 = (uint64_t)(ux >> 64), y0 = (uint64_t)uy, y1 = (uint64_t)(uy >> 64);
+  unsigned __int128 p00 = (unsigned __int128)x0 * y0, p01 = (unsigned __int128)x0 * y1;
+  unsigned __int128 p10 = (unsigned __int128)x1 * y0, p11 = (unsigned __int128)x1 * y1;
+  uint64_t p[4] = {0, 0, 0, 0};
+  unsigned __int128 t = (unsigned __int128)(uint64_t)p00;
+  p[0] = (uint64_t)t;
+  t = (p00 >> 64) + (uint64_t)p01 + (uint64_t)p10;
+  p[1] = (uint64_t)t;
+  t = (t >> 64) + (p01 >> 64) + (p10 >> 64) + (uint64_t)p11;
+  p[2] = (uint64_t)t;
+  t = (t >> 64) + (p11 >> 64);
+  p[3] = (uint64_t)t;
+  if (neg) { /* two's complement of p */
+    unsigned __int128 c = 1;
+    for (int w = 0; w < 4; ++w) {
+      c += (uint64_t)~p[w];
+      p[w] = (uint64_t)c;
+      c >>= 64;
+    }
+  }
+  unsigned __int128 c = 0;
+  for (int w = 0; w < 4; ++w) {
+    c += (unsigned __int128)acc[w] + p[w];
+    acc[w] = (uint64_t)c;
+    c >>= 64;
+  }
+}
+/* RN to 53 bits of u: value = mant 2^sh */
+static void crt_rn53(unsigned __int128 u, uint64_t *mant, int *sh) {
+  int lead = -1;
+  for (int b = 127; b >= 0; --b)
+    if ((u >> b) & 1) {
+      lead = b;
+      break;
+    }
+  if (lead <= 52) {
+    *mant = (uint64_t)u;
+    *sh = 0;
+    return;
+  }
+  int s = lead - 52;
+  unsigned __int128 keep = u >> s, rem = u - (keep << s), half = (unsigned __int128)1 << (s - 1);
+  uint64_t kk = (uint64_t)keep;
+  if (rem > half || (rem == half && (kk & 1))) ++kk;
+  *mant = kk;
+  *sh = s;
+}
+/* C' (256-bit two's complement) -> (hi 2^eh, lo 2^el) */
+static void crt_to_dd_c(const uint64_t acc[4], double *hi, int *eh, double *lo, int *el) {
+  int neg = (int)(acc[3] >> 63);
+  uint64_t mag[4];
+  unsigned __int128 c = neg ? 1 : 0;
+  for (int w = 0; w < 4; ++w) {
+    uint64_t x = neg ? ~acc[w] : acc[w];
+    c += x;
+    mag[w] = (uint64_t)c;
+    c >>= 64;
+  }
+  int lead = -1; /* bit index of the leading one in mag */
+  for (int b = 255; b >= 0; --b)
+    if ((mag[b / 64] >> (b % 64)) & 1) {
+      lead = b;
+      break;
+    }
+  if (lead < 0) {
+    *hi = *lo = 0.0;
+    *eh = *el = 0;
+    return;
+  }
+  /* the 160-bit window: bits lead .. lead-159 (zeros below bit 0) */
+  int E = lead - 159;
+  uint32_t nw[5];
+  for (int q = 0; q < 5; ++q) { /* nw[q] = window bits 32q .. 32q+31 */
+    uint32_t v = 0;
+    for (int b = 0; b < 32; ++b) {
+      int src = E + 32 * q + b;
+      if (src >= 0 && ((mag[src / 64] >> (src % 64)) & 1)) v |= 1u << b;
+    }
+    nw[q] = v;
+  }
+  uint64_t T64 = ((uint64_t)nw[4] << 32) | nw[3];
+  uint64_t keep = T64 >> 11;
+  uint32_t r11 = (uint32_t)(T64 & 0x7FF);
+  int lowz = (nw[2] | nw[1] | nw[0]) == 0;
+  int up = r11 > 0x400 || (r11 == 0x400 && (!lowz || (keep & 1)));
+  keep += (uint64_t)up;
+  *hi = (double)keep;
+  *eh = E + 107;
+  __int128 R = ((__int128)((int64_t)r11 - (up ? 2048 : 0)) << 96) + ((__int128)nw[2] << 64) +
+               ((__int128)nw[1] << 32) + (__int128)nw[0];
+  unsigned __int128 u = R < 0 ? (unsigned __int128)(-R) : (unsigned __int128)R;
+  uint64_t mant;
+  int sh;
+  crt_rn53(u, &mant, &sh);
+  *lo = R < 0 ? -(double)mant : (double)mant;
+  *el = E + sh;
+  if (neg) {
+    *hi = -*hi;
+    *lo = -*lo;
+  }
+}
+/* info[0..3] = {N moduli, rho_a, rho_b, W}; rows i0 .. i1-1 of the product
+ * only (c holds (i1 - i0) x n outputs, leading dimension i1 - i0). */
+void orc_crt_gemm_rows(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n,
+                       int bits, double target, int *info, int64_t i0, int64_t i1) {
+  int *sa = malloc(sizeof(int) * m), *ma = malloc(sizeof(int) * m), *fa = malloc(sizeof(int) * m);
+  int *sb = malloc(sizeof(int) * n), *mb = malloc(sizeof(int) * n), *fb = malloc(sizeof(int) * n);
+  int ra = 0, rb = 0;
+  for (int64_t i = 0; i < m; ++i) {
+    split_stats(a + 2 * i, k, m, &sa[i], &ma[i], &fa[i]);
+    if (sa[i] != -100000 && sa[i] - ma[i] > ra) ra = sa[i] - ma[i];
+  }
+  for (int64_t j = 0; j < n; ++j) {
+    split_stats(b + 2 * j * k, k, 1, &sb[j], &mb[j], &fb[j]);
+    if (sb[j] != -100000 && sb[j] - mb[j] > rb) rb = sb[j] - mb[j];
+  }
+  for (int64_t i = 0; i < m; ++i)
+    if (sa[i] == -100000) sa[i] = 0;
+  for (int64_t j = 0; j < n; ++j)
+    if (sb[j] == -100000) sb[j] = 0;
+  int nmod = 0;
+  int W = orc_crt_plan(bits, target, ra, rb, k, &nmod);
+  if (info) {
+    info[0] = nmod;
+    info[1] = ra;
+    info[2] = rb;
+    info[3] = W;
+  }
+  int64_t mr = i1 - i0;
+  __int128 *X = malloc(sizeof(__int128) * (size_t)(mr * k + 1)), *Y = malloc(sizeof(__int128) * (size_t)(n * k + 1));
+  for (int64_t i = i0; i < i1; ++i)
+    for (int64_t p = 0; p < k; ++p)
+      X[(i - i0) * k + p] = fa[i] ? 0 : crt_round(a[2 * (p * m + i)], a[2 * (p * m + i) + 1], sa[i], W);
+  for (int64_t j = 0; j < n; ++j)
+    for (int64_t p = 0; p < k; ++p)
+      Y[j * k + p] = fb[j] ? 0 : crt_round(b[2 * (j * k + p)], b[2 * (j * k + p) + 1], sb[j], W);
+  for (int64_t j = 0; j < n; ++j)
+    for (int64_t i = i0; i < i1; ++i) {
+      uint64_t acc[4] = {0, 0, 0, 0};
+      for (int64_t p = 0; p < k; ++p) acc_add_prod(acc, X[(i - i0) * k + p], Y[j * k + p]);
+      double *o = c + 2 * (j * mr + (i - i0));
+      if (fa[i] | fb[j]) {
+        o[0] = NAN;
+        o[1] = 0.0;
+      } else {
+        double hi, lo;
+        int eh, el;
+        crt_to_dd_c(acc, &hi, &eh, &lo, &el);
+        int ex = sa[i] + sb[j] - 2 * W;
+        o[0] = ldexp(hi, eh + ex);
+        o[1] = ldexp(lo, el + ex);
+      }
+    }
+  free(sa); free(ma); free(fa); free(sb); free(mb); free(fb); free(X); free(Y);
+}
+void orc_crt_gemm(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n, int bits,
+                  double target, int *info) {
+  orc_crt_gemm_rows(a, b, c, m, k, n, bits, target, info, 0, m);
+}

@@ -69,6 +69,11 @@ def orc():
         L.orc_split_cgemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
         L.orc_split_gemm_kc.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64]
         L.orc_split_cgemm_kc.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64]
+        L.orc_crt_gemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
+        L.orc_crt_gemm_rows.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64, I64]
+        L.orc_crt_bound.argtypes = [C.c_int, C.c_int, C.c_int, I64]
+        L.orc_crt_bound.restype = C.c_double
+        L.orc_crt_plan.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, I64, C.POINTER(C.c_int)]
         L.orc_wgemm.argtypes = [C.c_char, C.c_char, I64, I64, I64, P, P, I64, P, I64, P, P, I64]
         L.orc_wgemm_info.argtypes = [C.c_char, C.c_char, I64, I64, I64, I64, I64, I64]
         L.orc_wtrsm.argtypes = [C.c_char, C.c_char, C.c_char, C.c_char, I64, I64, P, P, I64, P, I64]
@@ -282,6 +287,29 @@ def split_cgemm(a, b, m, k, n, slices=0, target=8.0, kc=73 * 128):
     info = np.zeros(3, dtype=np.int32)
     orc().orc_split_cgemm_kc(_p(a), _p(b), _p(c), m, k, n, slices, target, info.ctypes.data, kc)
     return c, tuple(int(v) for v in info)
+
+
+def crt_gemm(a, b, m, k, n, bits=0, target=8.0, rows=None):
+    """CRT split form restated (orc_crt_gemm): returns (C, info) with info =
+    [moduli, rho_a, rho_b, W]; rows=(i0, i1) restricts the output to those rows
+    (C is then (i1 - i0) x n, column-major)."""
+    a, b = _c(a), _c(b)
+    info = np.zeros(4, dtype=np.int32)
+    i0, i1 = rows if rows is not None else (0, m)
+    c = np.empty(2 * (i1 - i0) * n)
+    orc().orc_crt_gemm_rows(_p(a), _p(b), _p(c), m, k, n, bits, target, info.ctypes.data, i0, i1)
+    return c, info.tolist()
+
+
+def crt_plan(bits, target, rho_a, rho_b, k):
+    """(W, moduli) the CRT plan picks."""
+    nm = C.c_int(0)
+    w = orc().orc_crt_plan(bits, target, rho_a, rho_b, k, C.byref(nm))
+    return w, nm.value
+
+
+def crt_bound(W, rho_a, rho_b, k) -> float:
+    return orc().orc_crt_bound(W, rho_a, rho_b, k)
 
 
 def reduce_geometry(n: int) -> tuple[int, int]:

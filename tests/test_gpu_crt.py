@@ -1,0 +1,152 @@
+"""GPU parity of the CRT (modular) split-INT8 DD GEMM.
+
+The device recovers the exact integer product of the rounded operands from
+its residues modulo N moduli (one INT8 tensor-core product per modulus) and
+rounds it to DD; the oracle computes the same exact integer directly with a
+256-bit accumulator and applies the same rounding, so the results must match
+bit for bit -- which also checks the modular reconstruction.  Against the
+exact product the error stays within the stated bound err_ij <= 8 k 2^-104
+(|A||B|)_ij."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import to_dev, to_host
+from multifloats_b200 import _lib
+from multifloats_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+ULP = 2.0 ** -104
+
+
+def dev_crt(L, dev, A, B, m, k, n, bits=0, target=8.0, a=None, b=None):
+    import torch
+
+    a = to_dev(A, dev) if a is None else a
+    b = to_dev(B, dev) if b is None else b
+    c = torch.empty(2 * m * n, dtype=torch.float64, device=dev)
+    info = (C.c_int * 4)()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = L.mfcuda_matmuldd_mm_crt(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, k, n, bits, target,
+                                  None, 0, info, stream)
+    assert rc == 0, _lib.lib().mfcuda_error_string(rc)
+    return to_host(c), list(info)
+
+
+@pytest.mark.parametrize("shape", [(128, 128, 128), (256, 256, 256), (130, 300, 257), (1, 1, 1), (7, 129, 9),
+                                   (300, 64, 520), (64, 1000, 16), (40, 9500, 24)])
+@pytest.mark.parametrize("R", [0, 16, 64])
+def test_bit_exact_vs_restatement(cuda_lib, dev, shape, R):
+    m, k, n = shape
+    A = W.dd_rowcol_scaled(m, k, R, "row", seed=m + R + 3)
+    B = W.dd_rowcol_scaled(k, n, R, "col", seed=n + R + 4)
+    got, info = dev_crt(cuda_lib, dev, A, B, m, k, n)
+    want, winfo = O.crt_gemm(A, B, m, k, n)
+    assert info == winfo
+    ok = O.same_bits(got, want)
+    assert ok.all(), (np.count_nonzero(~ok), np.flatnonzero(~ok)[:5])
+
+
+@pytest.mark.parametrize("bits", [8, 40, 77, 110])
+def test_fixed_bits(cuda_lib, dev, bits):
+    m, k, n = 96, 200, 300
+    A, B = W.dd_uniform(m * k, seed=bits), W.dd_uniform(k * n, seed=bits + 50)
+    got, info = dev_crt(cuda_lib, dev, A, B, m, k, n, bits=bits)
+    want, winfo = O.crt_gemm(A, B, m, k, n, bits=bits)
+    assert info == winfo and info[3] == bits
+    assert O.same_bits(got, want).all()
+
+
+def test_nonfinite_zero_rows_and_wide_spread(cuda_lib, dev):
+    """Inf/NaN in a row of A or column of B -> NaN outputs there; zero rows
+    and columns -> exact zeros; entries spanning 2^+-300 within a row (the
+    plan raises W, and at W = 110 reports a bound above the target)."""
+    m, k, n = 150, 90, 270
+    A = W.dd_uniform(m * k, seed=5).reshape(k, m, 2)
+    B = W.dd_uniform(k * n, seed=6).reshape(n, k, 2)
+    A[3, 7] = (np.inf, 0.0)
+    A[:, 11] = 0.0
+    A[10, 20] = (np.nan, 0.0)
+    B[5, 40] = (-np.inf, 0.0)
+    B[33] = 0.0
+    A[:, 50] *= np.exp2(np.linspace(-300, 300, k))[:, None]
+    A, B = A.reshape(-1), B.reshape(-1)
+    got, info = dev_crt(cuda_lib, dev, A, B, m, k, n)
+    want, winfo = O.crt_gemm(A, B, m, k, n)
+    assert info == winfo
+    assert O.same_bits(got, want).all()
+    g = got.reshape(n, m, 2)
+    assert np.isnan(g[:, 7, 0]).all() and np.isnan(g[:, 20, 0]).all() and np.isnan(g[5, :, 0]).all()
+    assert (g[33, [0, 1, 2], :] == 0).all() and (g[[0, 1], 11, :] == 0).all()
+
+
+def test_k_zero_and_empty(cuda_lib, dev):
+    import torch
+
+    m, n = 5, 7
+    c = torch.full((2 * m * n,), 3.0, dtype=torch.float64, device=dev)
+    assert cuda_lib.mfcuda_matmuldd_mm_crt(None, None, c.data_ptr(), m, 0, n, 0, 8.0, None, 0, None, None) == 0
+    assert (to_host(c) == 0).all()
+    assert cuda_lib.mfcuda_matmuldd_mm_crt(None, None, None, 0, 5, 5, 0, 8.0, None, 0, None, None) == 0
+    # invalid: negative size, bits out of range, non-positive target
+    assert cuda_lib.mfcuda_matmuldd_mm_crt(None, None, None, -1, 2, 2, 0, 8.0, None, 0, None, None) == 1
+    assert cuda_lib.mfcuda_matmuldd_mm_crt(None, None, None, 2, 2, 2, 111, 8.0, None, 0, None, None) == 1
+    assert cuda_lib.mfcuda_matmuldd_mm_crt(None, None, None, 2, 2, 2, 0, 0.0, None, 0, None, None) == 1
+
+
+def test_unaligned_is_rejected_and_workspace(cuda_lib, dev):
+    import torch
+
+    m = k = n = 16
+    a = torch.zeros(2 * m * k + 1, dtype=torch.float64, device=dev)[1:]
+    b = torch.zeros(2 * k * n, dtype=torch.float64, device=dev)
+    c = torch.zeros(2 * m * n, dtype=torch.float64, device=dev)
+    assert cuda_lib.mfcuda_matmuldd_mm_crt(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, k, n, 0, 8.0,
+                                           None, 0, None, None) == 7  # MFCUDA_ERR_UNSUPPORTED
+    A, B = W.dd_uniform(m * k, seed=1), W.dd_uniform(k * n, seed=2)
+    ws_bytes = cuda_lib.mfcuda_crt_workspace_size(m, k, n, 0)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    da, db = to_dev(A, dev), to_dev(B, dev)
+    rc = cuda_lib.mfcuda_matmuldd_mm_crt(da.data_ptr(), db.data_ptr(), c.data_ptr(), m, k, n, 0, 8.0,
+                                         ws.data_ptr(), ws_bytes - 1, None, None)
+    assert rc == 6  # MFCUDA_ERR_WORKSPACE
+    rc = cuda_lib.mfcuda_matmuldd_mm_crt(da.data_ptr(), db.data_ptr(), c.data_ptr(), m, k, n, 0, 8.0,
+                                         ws.data_ptr(), ws_bytes, None, None)
+    assert rc == 0
+    want, _ = O.crt_gemm(A, B, m, k, n)
+    assert O.same_bits(to_host(c), want).all()
+
+
+def test_host_dropin(cuda_lib):
+    m, k, n = 70, 130, 90
+    A, B = W.dd_rowcol_scaled(m, k, 16, "row", 8), W.dd_rowcol_scaled(k, n, 16, "col", 9)
+    c = np.empty(2 * m * n)
+    bound = C.c_double()
+    cuda_lib.matmuldd_mm_crt(A.ctypes.data, B.ctypes.data, c.ctypes.data, m, k, n, 0, C.byref(bound))
+    assert cuda_lib.mfcuda_last_error() == 0
+    want, info = O.crt_gemm(A, B, m, k, n)
+    assert O.same_bits(c, want).all()
+    assert bound.value == pytest.approx(O.crt_bound(info[3], info[1], info[2], k)) and bound.value <= 8.0
+
+
+@pytest.mark.parametrize("R", [0, 16, 64])
+def test_4096_error_bound_and_sampled_rows(cuda_lib, dev, R):
+    """The benchmark shape: every sampled output within the a-priori bound of
+    the exact product, and four full rows bit-identical to the restatement."""
+    m = k = n = 4096
+    A = W.dd_rowcol_scaled(m, k, R, "row", seed=101)
+    B = W.dd_rowcol_scaled(k, n, R, "col", seed=102)
+    got, info = dev_crt(cuda_lib, dev, A, B, m, k, n)
+    assert (info[0], info[3]) == (27, 92)  # one binade per row / column: rho = 1
+    bound = O.crt_bound(info[3], info[1], info[2], k)
+    assert bound <= 8.0
+    rng = np.random.default_rng(R)
+    ii, jj = rng.integers(0, m, 256), rng.integers(0, n, 256)
+    err, absv = O.gemm_errors(A, B, got, m, k, n, ii, jj)
+    assert (np.abs(err) <= bound * k * ULP * absv).all()
+    rows = (1000, 1004)
+    want, _ = O.crt_gemm(A, B, m, k, n, rows=rows)
+    sub = np.ascontiguousarray(got.reshape(n, m, 2)[:, rows[0]:rows[1], :]).reshape(-1)
+    assert O.same_bits(sub, want).all()
