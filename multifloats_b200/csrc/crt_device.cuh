@@ -9,9 +9,9 @@
 //   C' = sum_t r_t e_t - q M,   e_t = (M / m_t) ((M / m_t)^-1 mod m_t),
 //   r_t = (X Y^T mod m_t) in [0, m_t),  q = round(sum_t r_t e_t / M),
 // which is exact because the moduli are chosen with M > 8 k 2^(2W) > 8 |C'|.
-// C' is then rounded to a double-double (hi = RN(C''), lo = RN(C'' - hi), C''
-// being C' truncated to its 160 leading bits) and scaled by 2^(sigma_i + tau_j
-// - 2W).  Compared with the digit-sliced form (S(S+1)/2 slice products for S
+// C' is then converted to a double-double (crt_to_dd: hi = C' rounded to 53
+// bits, lo the rest summed in doubles, renormalised) and scaled by
+// 2^(sigma_i + tau_j - 2W).  Compared with the digit-sliced form (S(S+1)/2 slice products for S
 // slices) the tensor work is N products: 27 instead of 105 at 4096^3.
 //
 // Error (a priori, per output; delta = rounding of an operand to its grid,
@@ -32,13 +32,14 @@ namespace mfcuda {
 namespace split {
 
 constexpr int CRT_NL = 8;  // most 32-bit limbs of a reconstruction (256 bits)
+constexpr int CRT_BATCH = 9;  // moduli whose residues a reconstruction thread loads at once
 constexpr int CRT_WMAX = 110;
 
 // Reconstruction constants of the plan's N moduli, computed on the device.
 struct CrtConst {
   uint32_t e[CRT_NMAX][CRT_NL];  // e_t mod 2^256
   uint32_t M[CRT_NL];            // M mod 2^256
-  double c[CRT_NMAX];            // ((M / m_t)^-1 mod m_t) / m_t, rounded
+  uint32_t cq[CRT_NMAX];         // round(2^32 ((M / m_t)^-1 mod m_t) / m_t): q = round(sum_t r_t cq_t 2^-32)
 };
 
 // ceil(log2 k) for k >= 1.
@@ -150,7 +151,7 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
       cc->e[t][l] = (uint32_t)v;
       carry = v >> 32;
     }
-    cc->c[t] = (double)inv / (double)mt;
+    cc->cq[t] = (uint32_t)((((uint64_t)inv << 32) + mt / 2) / mt);
     if (t == 0) {  // M = (M / m_0) m_0
       uint64_t cy = 0;
       for (int l = 0; l < CRT_NL; ++l) {
@@ -167,22 +168,27 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
 }
 
 // ---- residue slicing ----------------------------------------------------------
+// Non-negative residue of u < 2^30 modulo m_t (Barrett: the estimate is exact
+// or one too large).
+__device__ __forceinline__ uint32_t crt_mod_small(uint32_t u, int t) {
+  const uint32_t m = crt_mod[t];
+  const uint32_t q = __umulhi(u, crt_mu[t]);
+  const int r = (int)(u - q * m);
+  return (uint32_t)(r < 0 ? r + (int)m : r);
+}
 // The signed residue of X = sum_q d_q 256^q (balanced digits, read from the
 // biased words y of biased_bytes: digit q = byte q of y xor 0x80) modulo m_t,
-// in [crt_rlo, crt_rhi]: four dp4a against the digit weights give
-// rr = sum_q d_q c_q with |rr| < 14 * 128 * 128 < 2^18, then one rounded
-// float quotient and two range corrections.
+// in [crt_rlo, crt_rhi]: dp4a against the digit weights give
+// rr = sum_q d_q c_q with |rr| < 14 * 128 * 128 < 2^18, reduced exactly.
+// NW = digit words in use: 3 when W <= 94 (digits 12 and 13 are zero).
+template <int NW>
 __device__ __forceinline__ int crt_residue(const uint32_t (&dw)[4], int t) {
-  int rr = __dp4a((int)dw[3], (int)crt_digw[t][3], 0);
+  int rr = NW == 4 ? __dp4a((int)dw[3], (int)crt_digw[t][3], 0) : 0;
   rr = __dp4a((int)dw[2], (int)crt_digw[t][2], rr);
   rr = __dp4a((int)dw[1], (int)crt_digw[t][1], rr);
   rr = __dp4a((int)dw[0], (int)crt_digw[t][0], rr);
-  const int m = (int)crt_mod[t];
-  const int q = __float2int_rn(__int2float_rn(rr) * __uint_as_float(crt_inv_bits[t]));
-  int r = rr - q * m;
-  r = r > crt_rhi[t] ? r - m : r;
-  r = r < crt_rlo[t] ? r + m : r;
-  return r;
+  const int r = (int)crt_mod_small((uint32_t)(rr + (int)crt_off18[t]), t);
+  return r > crt_rhi[t] ? r - (int)crt_mod[t] : r;
 }
 // Signed digit words of the biased words of one entry.
 __device__ __forceinline__ void digit_words(const uint32_t (&y)[4], uint32_t (&dw)[4]) {
@@ -191,19 +197,27 @@ __device__ __forceinline__ void digit_words(const uint32_t (&y)[4], uint32_t (&d
 }
 // Calls f(t, word) with the residues modulo m_t of 8 entries packed in entry
 // order (byte e = entry e), for t < n.
+template <int NW, class F>
+__device__ __forceinline__ void residue_words_nw(const uint32_t (&dw)[8][4], int n, F f) {
+  for (int t = 0; t < n; ++t) {
+    uint32_t r[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) r[e] = (uint32_t)crt_residue<NW>(dw[e], t);
+    // low bytes of r[0..3] and r[4..7] packed in order (byte permutes)
+    const uint32_t lo = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+    const uint32_t hi = __byte_perm(__byte_perm(r[4], r[5], 0x0040), __byte_perm(r[6], r[7], 0x0040), 0x5410);
+    f(t, (uint64_t)lo | ((uint64_t)hi << 32));
+  }
+}
 template <class F>
-__device__ __forceinline__ void for_each_residue_word(const uint32_t (&y)[8][4], int n, F f) {
+__device__ __forceinline__ void for_each_residue_word(const uint32_t (&y)[8][4], int n, int W, F f) {
   uint32_t dw[8][4];
 #pragma unroll
   for (int e = 0; e < 8; ++e) digit_words(y[e], dw[e]);
-  for (int t = 0; t < n; ++t) {
-    uint32_t lo = 0, hi = 0;
-#pragma unroll
-    for (int e = 0; e < 4; ++e) lo |= ((uint32_t)crt_residue(dw[e], t) & 0xFFu) << (8 * e);
-#pragma unroll
-    for (int e = 0; e < 4; ++e) hi |= ((uint32_t)crt_residue(dw[e + 4], t) & 0xFFu) << (8 * e);
-    f(t, (uint64_t)lo | ((uint64_t)hi << 32));
-  }
+  if (W <= 94)
+    residue_words_nw<3>(dw, n, f);
+  else
+    residue_words_nw<4>(dw, n, f);
 }
 
 // A (m x k column-major view) -> As[t][i][p], as slice_a_body with residues
@@ -232,7 +246,7 @@ __device__ __forceinline__ void crt_slice_a_body(const double *__restrict__ A, i
       for (int w = 0; w < 4; ++w) y[e][w] = bias_word(w);  // X = 0: every residue zero
     }
   }
-  for_each_residue_word(y, n, [&](int sl, uint64_t word) {
+  for_each_residue_word(y, n, W, [&](int sl, uint64_t word) {
     *reinterpret_cast<uint64_t *>(&tile[(sl * SA_ROWS + ii) * SA_STRIDE + grp * 8]) = word;
   });
   __syncthreads();
@@ -263,148 +277,199 @@ __device__ __forceinline__ void crt_slice_b_one(const double *__restrict__ B, in
       for (int w = 0; w < 4; ++w) y[e][w] = bias_word(w);
     }
   }
-  for_each_residue_word(y, n, [&](int sl, uint64_t word) {
+  for_each_residue_word(y, n, W, [&](int sl, uint64_t word) {
     *reinterpret_cast<uint64_t *>(Bs + (((int64_t)sl * N_pad + j) * K_pad + p8)) = word;
   });
 }
 
 // ---- reconstruction ---------------------------------------------------------------
-// RN to 53 bits of the unsigned integer u < 2^127, as (integer mantissa, shift):
-// value = mant 2^sh, mant <= 2^53.
-__device__ __forceinline__ void rn53(unsigned __int128 u, uint64_t &mant, int &sh) {
-  const uint64_t hi = (uint64_t)(u >> 64), lo = (uint64_t)u;
-  const int lead = hi ? 127 - __clzll((long long)hi) : (lo ? 63 - __clzll((long long)lo) : -1);
-  if (lead <= 52) {
-    mant = lo;
-    sh = 0;
-    return;
-  }
-  sh = lead - 52;
-  const unsigned __int128 keep = u >> sh;
-  const unsigned __int128 rem = u - (keep << sh), half = (unsigned __int128)1 << (sh - 1);
-  uint64_t k = (uint64_t)keep;
-  if (rem > half || (rem == half && (k & 1))) ++k;
-  mant = k;
-}
-
-// The signed integer held in nl little-endian 32-bit limbs (two's complement)
-// as a double-double (hi, lo) with exponents: value ~ hi 2^eh + lo 2^el, hi
-// and lo integers of at most 53 bits (exact as doubles).  C'' = |C'| truncated
-// to its 160 leading bits; hi = RN(C''), lo = RN(C'' - hi).
-__device__ __forceinline__ void crt_to_dd(const uint32_t *limb, int nl, double &hi, int &eh, double &lo,
-                                          int &el) {
-  uint32_t v[CRT_NL + 5];
+// The signed integer held in nl little-endian 32-bit limbs (two's complement,
+// nl <= 8) as a double-double scaled by 2^e:
+//   the magnitude is normalised (whole-limb shifts, then a funnel shift) so
+//   that its leading one is bit 159 of a 160-bit window n4..n0 (bit 0 of
+//   weight 2^E; bits below the window dropped);
+//   hi = the window rounded to 53 bits (nearest, ties to even, the bits below
+//   bit 107 of the window deciding), exact as a double: keep 2^(E + 107);
+//   lo = the rest D 2^96 + n2 2^64 + n1 2^32 + n0 (D = the low 11 bits of the
+//   top 64 minus 2048 when rounded up) summed in doubles in that order,
+//   times 2^E; then fast_two_sum(hi, lo) in units of 2^(E + 107).
+// Returns (h, l) with value (h + l) 2^e, e = E + 107.
+__device__ __forceinline__ void crt_to_dd(const uint32_t *limb, int nl, double &h, double &l, int &e) {
   const bool neg = (limb[nl - 1] >> 31) != 0;
+  uint32_t m[CRT_NL];
   uint32_t carry = 1;
 #pragma unroll
-  for (int l = 0; l < CRT_NL; ++l) {
-    uint32_t x = l < nl ? limb[l] : (neg ? 0xFFFFFFFFu : 0u);
+  for (int q = 0; q < CRT_NL; ++q) {
+    uint32_t x = q < nl ? limb[q] : (neg ? 0xFFFFFFFFu : 0u);
     if (neg) {  // magnitude: two's complement negation
       x = ~x;
-      const uint32_t s = x + carry;
-      carry = (s < x) ? 1u : 0u;
-      x = s;
+      const uint32_t sm = x + carry;
+      carry = sm < x ? 1u : 0u;
+      x = sm;
     }
-    v[l + 5] = x;
+    m[q] = x;
   }
+  // whole-limb normalisation: the leading nonzero limb into m[7]
+  int E = 32 * (CRT_NL - 5);  // weight of window bit 0 before any shift
 #pragma unroll
-  for (int l = 0; l < 5; ++l) v[l] = 0;
-  // top nonzero limb (index into v)
-  int tl = -1;
+  for (int step = 4; step >= 1; step >>= 1) {
+    bool zero = true;
 #pragma unroll
-  for (int l = CRT_NL + 4; l >= 5; --l)
-    if (tl < 0 && v[l] != 0) tl = l;
-  if (tl < 0) {
-    hi = lo = 0.0;
-    eh = el = 0;
+    for (int q = CRT_NL - step; q < CRT_NL; ++q) zero = zero && m[q] == 0;
+    if (zero) {
+#pragma unroll
+      for (int q = CRT_NL - 1; q >= 0; --q) m[q] = q >= step ? m[q - step] : 0u;
+      E -= 32 * step;
+    }
+  }
+  if (m[CRT_NL - 1] == 0) {  // the value is zero
+    h = l = 0.0;
+    e = 0;
     return;
   }
-  const int s = __clz((int)v[tl]);
-  // 160-bit window n4..n0, leading one at bit 159; bit 0 has weight 2^E
+  const int s = __clz((int)m[CRT_NL - 1]);
   uint32_t n[5];
 #pragma unroll
-  for (int w = 0; w < 5; ++w) {
-    const uint32_t a = v[tl - w], b = v[tl - w - 1];
-    n[4 - w] = s ? (a << s) | (b >> (32 - s)) : a;
-  }
-  const int E = 32 * (tl - 5 - 4) - s;
+  for (int w = 0; w < 5; ++w) n[w] = __funnelshift_l(m[CRT_NL - 6 + w], m[CRT_NL - 5 + w], s);
+  E -= s;
   const uint64_t T64 = ((uint64_t)n[4] << 32) | n[3];
   uint64_t keep = T64 >> 11;
   const uint32_t r11 = (uint32_t)(T64 & 0x7FF);
   const bool lowz = (n[2] | n[1] | n[0]) == 0;
   const bool up = r11 > 0x400 || (r11 == 0x400 && (!lowz || (keep & 1)));
   keep += up;
-  hi = (double)keep;
-  eh = E + 107;
-  const __int128 R = ((__int128)((int64_t)r11 - (up ? 2048 : 0)) << 96) + ((__int128)n[2] << 64) +
-                     ((__int128)n[1] << 32) + (__int128)n[0];
-  const unsigned __int128 u = R < 0 ? (unsigned __int128)(-R) : (unsigned __int128)R;
-  uint64_t mant;
-  int sh;
-  rn53(u, mant, sh);
-  lo = R < 0 ? -(double)mant : (double)mant;
-  el = E + sh;
+  const int D = (int)r11 - (up ? 2048 : 0);
+  double lo = mfdev::mul((double)D, pow2(96));
+  lo = mfdev::add(lo, mfdev::mul((double)n[2], pow2(64)));
+  lo = mfdev::add(lo, mfdev::mul((double)n[1], pow2(32)));
+  lo = mfdev::add(lo, (double)n[0]);
+  double hi = (double)keep;
+  lo = mfdev::mul(lo, pow2(-107));  // into units of 2^(E + 107): exact
+  mfdev::fast_two_sum(hi, lo, h, l);
   if (neg) {
-    hi = -hi;
-    lo = -lo;
+    h = -h;
+    l = -l;
   }
+  e = E + 107;
 }
 
-// One output: residues of its N products (summed over the K chunks) -> C' ->
-// DD, scaled by 2^ex.  Constants from shared memory.
+// Reconstruction constants in shared memory.
 struct CrtShared {
   uint32_t e[CRT_NMAX][CRT_NL];
   uint32_t M[CRT_NL];
-  double c[CRT_NMAX];
-  double minv[CRT_NMAX];  // 1 / m_t rounded (quotient estimate, corrected below)
+  uint32_t cq[CRT_NMAX];
 };
 // Block prologue: the plan's constants into shared memory.
 __device__ __forceinline__ void crt_load_shared(const CrtConst *cc, int n, CrtShared &cs) {
   for (int x = threadIdx.x; x < n * CRT_NL; x += blockDim.x) cs.e[x / CRT_NL][x % CRT_NL] = cc->e[x / CRT_NL][x % CRT_NL];
   for (int x = threadIdx.x; x < CRT_NL; x += blockDim.x) cs.M[x] = cc->M[x];
-  for (int x = threadIdx.x; x < n; x += blockDim.x) {
-    cs.c[x] = cc->c[x];
-    cs.minv[x] = 1.0 / (double)crt_mod[x];
-  }
+  for (int x = threadIdx.x; x < n; x += blockDim.x) cs.cq[x] = cc->cq[x];
   __syncthreads();
 }
-__device__ __forceinline__ double2 crt_output(const int32_t *__restrict__ D, int64_t gstride, int64_t kstride,
-                                              int nkc, int n, int nl, const CrtShared &cs, int ex) {
-  uint32_t r[CRT_NMAX];
-  double f = 0.0;
-  for (int t = 0; t < n; ++t) {
-    int64_t v = 0;
-    for (int kc = 0; kc < nkc; ++kc) v += __ldcs(D + t * gstride + kc * kstride);
-    // v mod m_t in [0, m_t): |v| < 2^53, quotient from the rounded reciprocal,
-    // off by at most one, then corrected
-    const int64_t m = crt_mod[t];
-    const int64_t qq = (int64_t)floor((double)v * cs.minv[t]);
-    int64_t rt = v - qq * m;
-    rt = rt < 0 ? rt + m : (rt >= m ? rt - m : rt);
-    r[t] = (uint32_t)rt;
-    f = __fma_rn((double)rt, cs.c[t], f);
-  }
-  const int64_t q = (int64_t)rint(f);
-  int64_t acc[CRT_NL];
+
+// The residue of one product reduced in the tensor-core kernel's epilogue:
+// v = the INT32 sum of one K chunk (|v| < 2^28), stored as v mod m_t in [0, m_t).
+__device__ __forceinline__ uint8_t crt_residue_of_sum(int32_t v, int t) {
+  return (uint8_t)crt_mod_small((uint32_t)(v + (int32_t)crt_off28[t]), t);
+}
+
+// Rows i0 .. i0+3 of column j: the residues r_t (one 4-byte load per modulus
+// and K chunk of the byte residues D8[t][kc][N_pad][M_pad]), then
+//   q = round(sum_t r_t cq_t 2^-32),  C' = sum_t r_t e_t - q M  (mod 2^(32 nl)),
+// the DD rounding and the exact scaling; `mode` as the digit-sliced combine.
+__device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8, const Plan *plan,
+                                                  const CrtShared &cs, const int *sigA, const int *flagA,
+                                                  const int *sigB, const int *flagB, int64_t M, int64_t N,
+                                                  int64_t M_pad, int64_t N_pad, int nkc, double *__restrict__ C,
+                                                  int64_t cstride, int mode, int64_t quad, int64_t j) {
+  const int n = plan->S, nl = plan->nl, W = plan->W;
+  const int64_t i0 = quad * 4;
+  if (i0 >= M || j >= N) return;
+  const int64_t kstride = N_pad * M_pad, gstride = (int64_t)nkc * kstride;
+  const uint8_t *src = D8 + j * M_pad + i0;
+  uint64_t acc[4][CRT_NL], sq[4];
 #pragma unroll
-  for (int l = 0; l < CRT_NL; ++l) acc[l] = -(int64_t)q * (int64_t)cs.M[l];
-  for (int t = 0; t < n; ++t) {
-    const uint64_t rt = r[t];
+  for (int r = 0; r < 4; ++r) {
+    sq[r] = 0;
 #pragma unroll
-    for (int l = 0; l < CRT_NL; ++l) acc[l] += (int64_t)(rt * cs.e[t][l]);
+    for (int l = 0; l < CRT_NL; ++l) acc[r][l] = 0;
   }
-  uint32_t limb[CRT_NL];
-  int64_t carry = 0;
+  // moduli in batches of CRT_BATCH: the batch's loads are all in flight before
+  // its arithmetic
+  for (int t0 = 0; t0 < n; t0 += CRT_BATCH) {
+    uint32_t wv[CRT_BATCH];
 #pragma unroll
-  for (int l = 0; l < CRT_NL; ++l) {
-    const int64_t x = acc[l] + carry;
-    limb[l] = (uint32_t)x;
-    carry = x >> 32;  // arithmetic shift
+    for (int u = 0; u < CRT_BATCH; ++u) {
+      const int t = t0 + u;
+      if (t >= n) {
+        wv[u] = 0;
+      } else if (nkc == 1) {
+        wv[u] = __ldcs(reinterpret_cast<const uint32_t *>(src + t * gstride));
+      } else {  // per-row sums of the chunks' residues, reduced again
+        uint32_t sum[4] = {0, 0, 0, 0};
+        for (int kc = 0; kc < nkc; ++kc) {
+          const uint32_t w = __ldcs(reinterpret_cast<const uint32_t *>(src + t * gstride + kc * kstride));
+#pragma unroll
+          for (int r = 0; r < 4; ++r) sum[r] += (w >> (8 * r)) & 0xFFu;
+        }
+        uint32_t packed = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) packed |= crt_mod_small(sum[r], t) << (8 * r);
+        wv[u] = packed;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < CRT_BATCH; ++u) {
+      const int t = t0 + u;
+      if (t < n) {
+        const uint32_t cqt = cs.cq[t];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const uint32_t rv = (wv[u] >> (8 * r)) & 0xFFu;
+          sq[r] += (uint64_t)rv * cqt;
+#pragma unroll
+          for (int l = 0; l < CRT_NL; ++l)
+            if (l < nl) acc[r][l] += (uint64_t)rv * cs.e[t][l];
+        }
+      }
+    }
   }
-  double hi, lo;
-  int eh, el;
-  crt_to_dd(limb, nl, hi, eh, lo, el);
-  return make_double2(scale2(hi, eh + ex), scale2(lo, el + ex));
+  const int4 sa = *reinterpret_cast<const int4 *>(sigA + i0);
+  const int4 fa = *reinterpret_cast<const int4 *>(flagA + i0);
+  const int sav[4] = {sa.x, sa.y, sa.z, sa.w}, fav[4] = {fa.x, fa.y, fa.z, fa.w};
+  const int sb = sigB[j], fb = flagB[j];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int64_t i = i0 + r;
+    if (i >= M) break;
+    const uint64_t q = (sq[r] + (1ull << 31)) >> 32;
+    uint32_t limb[CRT_NL];
+    int64_t carry = 0;
+#pragma unroll
+    for (int l = 0; l < CRT_NL; ++l) {
+      const int64_t x = (int64_t)(acc[r][l] - q * (uint64_t)cs.M[l]) + carry;  // |true value| < 2^47
+      limb[l] = (uint32_t)x;
+      carry = x >> 32;  // arithmetic shift
+    }
+    double2 out;
+    if (fav[r] | fb) {
+      out = make_double2(CUDART_NAN, 0.0);
+    } else {
+      double hi, lo;
+      int e;
+      crt_to_dd(limb, nl, hi, lo, e);
+      const int ex = e + sav[r] + sb - 2 * W;
+      out = make_double2(scale2(hi, ex), scale2(lo, ex));
+    }
+    double2 *dst = reinterpret_cast<double2 *>(C) + (j * M + i) * cstride;
+    if (mode != 0) {
+      const double2 prev = *dst;
+      const mfdev::dd p = mfdev::make(out.x, out.y), pv = mfdev::make(prev.x, prev.y);
+      const mfdev::dd res = mode == 1 ? mfdev::dd_sub(pv, p) : mfdev::dd_add(pv, p);
+      out = make_double2(res.hi, res.lo);
+    }
+    __stcs(dst, out);
+  }
 }
 
 }  // namespace split

@@ -18,8 +18,11 @@ holds:
                        representation X = sum_q d_q 256^q (signed byte digits)
                        the dot product sum_q d_q c_q (four dp4a) is congruent
                        to X modulo m_t
-* ``crt_inv[t]``       1/m_t rounded to float (quotient estimate of the final
-                       reduction; the two range corrections make it exact)
+* ``crt_mu[t]``        ceil(2^32 / m_t): Barrett reduction of a non-negative
+                       u < 2^30 (the quotient umulhi(u, mu) is exact or one
+                       too large; one correction)
+* ``crt_off28[t]``, ``crt_off18[t]``  multiples of m_t of at least 2^28 / 2^18,
+                       added to signed values below those bounds first
 * ``crt_rlo[t]``, ``crt_rhi[t]``  the symmetric residue range
 
 Usage::
@@ -29,7 +32,6 @@ Usage::
 from __future__ import annotations
 
 import os
-import struct
 import sys
 from math import gcd
 
@@ -86,11 +88,14 @@ def main() -> int:
             w.append(f"0x{v:08x}u")
         words.append("{" + ", ".join(w) + "}")
     lines.append(f"MF_TABLE uint32_t crt_digw[{NMAX}][4] = {{" + ",\n    ".join(words) + "};")
-    inv = []
-    for m in ms:
-        b = struct.unpack("<I", struct.pack("<f", 1.0 / m))[0]
-        inv.append(f"0x{b:08x}u")
-    lines.append(f"MF_TABLE uint32_t crt_inv_bits[{NMAX}] = {{" + ", ".join(inv) + "};  // float(1/m) bit patterns")
+    # Barrett reduction of u < 2^30: q = umulhi(u, mu) is floor(u / m) or one more
+    lines.append(f"MF_TABLE uint32_t crt_mu[{NMAX}] = {{" + ", ".join(f"{-(-(1 << 32) // m)}u" for m in ms) +
+                 "};  // ceil(2^32 / m)")
+    # offsets making a signed value non-negative before the reduction
+    lines.append(f"MF_TABLE uint32_t crt_off28[{NMAX}] = {{" + ", ".join(f"{m * -(-(1 << 28) // m)}u" for m in ms) +
+                 "};  // m ceil(2^28 / m): |v| < 2^28")
+    lines.append(f"MF_TABLE uint32_t crt_off18[{NMAX}] = {{" + ", ".join(f"{m * -(-(1 << 18) // m)}u" for m in ms) +
+                 "};  // m ceil(2^18 / m): |v| < 2^18")
     lines.append(f"MF_TABLE int crt_rlo[{NMAX}] = {{" + ", ".join(str(-(m // 2)) for m in ms) + "};")
     lines.append(f"MF_TABLE int crt_rhi[{NMAX}] = {{" + ", ".join(str((m + 1) // 2 - 1) for m in ms) + "};")
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "crt_tables.h")

@@ -264,16 +264,35 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         break;
       }
       mftc::tc_fence_after();
-      int32_t *dst_base = D + (((int64_t)(it.g * nkc + it.kc) * N_pad + (int64_t)it.tn * BN) * M_pad +
-                               (int64_t)it.tm * BM + row);
+      const int64_t off = ((int64_t)(it.g * nkc + it.kc) * N_pad + (int64_t)it.tn * BN) * M_pad +
+                          (int64_t)it.tm * BM + row;
+      const uint32_t tm_addr = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * BN);
+      if (crt) {  // the residue modulo m_g, one byte per output (crt_device.cuh)
+        uint8_t *dst = reinterpret_cast<uint8_t *>(D) + off;
 #pragma unroll 1
-      for (int chunk = 0; chunk < BN / 32; ++chunk) {
-        uint32_t r[32];
-        mftc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * BN + chunk * 32), r);
-        mftc::tmem_wait_ld();
-        int32_t *dst = dst_base + (int64_t)chunk * 32 * M_pad;
+        for (int chunk = 0; chunk < BN / 32; ++chunk) {
+          uint32_t r[32];
+          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), r);
+          mftc::tmem_wait_ld();
 #pragma unroll
-        for (int q = 0; q < 32; ++q) __stcs(dst + (int64_t)q * M_pad, (int32_t)r[q]);  // evict-first: keep L2 for the slices
+          for (int q = 0; q < 32; ++q) {
+            __stcs(dst, crt_residue_of_sum((int32_t)r[q], it.g));
+            dst += M_pad;
+          }
+        }
+      } else {
+        int32_t *dst = D + off;
+#pragma unroll 1
+        for (int chunk = 0; chunk < BN / 32; ++chunk) {
+          uint32_t r[32];
+          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), r);
+          mftc::tmem_wait_ld();
+#pragma unroll
+          for (int q = 0; q < 32; ++q) {
+            __stcs(dst, (int32_t)r[q]);  // evict-first: keep L2 for the slices
+            dst += M_pad;
+          }
+        }
       }
       mftc::tc_fence_before();
       __syncwarp();
@@ -546,16 +565,35 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
         break;
       }
       mftc::tc_fence_after();
-      int32_t *dst_base = D + (((int64_t)(it.g * nkc + it.kc) * N_pad + (int64_t)it.tn * tn_cols) * M_pad +
-                               (int64_t)it.tm * BM_PAIR + (int64_t)rank * 128 + row);
+      const int64_t off = ((int64_t)(it.g * nkc + it.kc) * N_pad + (int64_t)it.tn * tn_cols) * M_pad +
+                          (int64_t)it.tm * BM_PAIR + (int64_t)rank * 128 + row;
+      const uint32_t tm_addr = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * acc_cols);
+      if (crt) {  // the residue modulo m_g, one byte per output (crt_device.cuh)
+        uint8_t *dst = reinterpret_cast<uint8_t *>(D) + off;
 #pragma unroll 1
-      for (int chunk = 0; chunk < acc_cols / 32; ++chunk) {
-        uint32_t v[32];
-        mftc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * acc_cols + chunk * 32), v);
-        mftc::tmem_wait_ld();
-        int32_t *dst = dst_base + (int64_t)chunk * 32 * M_pad;
+        for (int chunk = 0; chunk < acc_cols / 32; ++chunk) {
+          uint32_t v[32];
+          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
+          mftc::tmem_wait_ld();
 #pragma unroll
-        for (int q = 0; q < 32; ++q) __stcs(dst + (int64_t)q * M_pad, (int32_t)v[q]);  // evict-first: keep L2 for the slices
+          for (int q = 0; q < 32; ++q) {
+            __stcs(dst, crt_residue_of_sum((int32_t)v[q], it.g));
+            dst += M_pad;
+          }
+        }
+      } else {
+        int32_t *dst = D + off;
+#pragma unroll 1
+        for (int chunk = 0; chunk < acc_cols / 32; ++chunk) {
+          uint32_t v[32];
+          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
+          mftc::tmem_wait_ld();
+#pragma unroll
+          for (int q = 0; q < 32; ++q) {
+            __stcs(dst, (int32_t)v[q]);  // evict-first: keep L2 for the slices
+            dst += M_pad;
+          }
+        }
       }
       mftc::tc_fence_before();
       __syncwarp();
@@ -608,31 +646,17 @@ __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restri
   if (p8 >= K_pad) return;
   crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, blockIdx.y, p8);
 }
-// Thread per row i of column j = blockIdx.y; `mode` as combine_kernel.
-__global__ void __launch_bounds__(128) crt_combine_kernel(const int32_t *__restrict__ D, const Plan *plan,
+// Thread per 4 consecutive rows of column j = blockIdx.y (byte residues from
+// the tensor-core kernel's epilogue); `mode` as combine_kernel.
+__global__ void __launch_bounds__(128) crt_combine_kernel(const uint8_t *__restrict__ D8, const Plan *plan,
                                                           const CrtConst *cc, const int *sigA, const int *flagA,
                                                           const int *sigB, const int *flagB, int64_t M,
                                                           int64_t N, int64_t M_pad, int64_t N_pad, int nkc,
                                                           double *__restrict__ C, int64_t cstride, int mode) {
   __shared__ CrtShared cs;
-  const int n = plan->S, nl = plan->nl, W = plan->W;
-  crt_load_shared(cc, n, cs);
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
-  if (i >= M || j >= N) return;
-  const int64_t kstride = N_pad * M_pad, gstride = (int64_t)nkc * kstride;
-  double2 out;
-  if (flagA[i] | flagB[j])
-    out = make_double2(CUDART_NAN, 0.0);
-  else
-    out = crt_output(D + j * M_pad + i, gstride, kstride, nkc, n, nl, cs, sigA[i] + sigB[j] - 2 * W);
-  double2 *dst = reinterpret_cast<double2 *>(C) + (j * M + i) * cstride;
-  if (mode != 0) {
-    const double2 prev = *dst;
-    const mfdev::dd p = mfdev::make(out.x, out.y), q = mfdev::make(prev.x, prev.y);
-    const mfdev::dd r = mode == 1 ? mfdev::dd_sub(q, p) : mfdev::dd_add(q, p);
-    out = make_double2(r.hi, r.lo);
-  }
-  __stcs(dst, out);
+  crt_load_shared(cc, plan->S, cs);
+  crt_combine4_body(D8, plan, cs, sigA, flagA, sigB, flagB, M, N, M_pad, N_pad, nkc, C, cstride, mode,
+                    (int64_t)blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -936,9 +960,9 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                                                              status);
       if (q == nprod - 1) mark(3, s);
       if (crt)
-        crt_combine_kernel<<<dim3((unsigned)((m + 127) / 128), (unsigned)n), 128, 0, s>>>(
-            D, plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, n, L.M_pad, L.N_pad, (int)L.nkc,
-            prods[q].out, prods[q].ostride, prods[q].mode);
+        crt_combine_kernel<<<dim3(cgx, (unsigned)n), 128, 0, s>>>(
+            reinterpret_cast<const uint8_t *>(D), plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, n, L.M_pad,
+            L.N_pad, (int)L.nkc, prods[q].out, prods[q].ostride, prods[q].mode);
       else
         combine_kernel<<<dim3(cgx, (unsigned)n), COMBINE_THREADS, 0, s>>>(D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n,
                                                     L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,

@@ -1346,9 +1346,8 @@ int orc_wtrsm(char side, char uplo, char transa, char diag, int64_t m, int64_t n
  * directly with a 256-bit accumulator -- no moduli -- so it checks the modular
  * reconstruction too.  Same scan and exponent spreads as the digit-sliced
  * form, same plan (the smallest W whose a-priori bound meets the target), same
- * rounding X = round(a 2^(W - sigma)), same conversion to DD (C'' = |C'|
- * truncated to its 160 leading bits, hi = RN(C''), lo = RN(C'' - hi)) and the
- * same exact scaling by 2^(sigma_i + tau_j - 2W). */
+ * rounding X = round(a 2^(W - sigma)), same conversion to DD (crt_to_dd_c) and
+ * the same exact scaling by 2^(sigma_i + tau_j - 2W). */
 #include "../multifloats_b200/csrc/crt_tables.h"
 #define CRT_WMAX 110
 static int crt_ceil_log2(int64_t k) {
@@ -1418,28 +1417,12 @@ static void acc_add_prod(uint64_t acc[4], __int128 x, __int128 y) {
     c >>= 64;
   }
 }
-/* RN to 53 bits of u: value = mant 2^sh */
-static void crt_rn53(unsigned __int128 u, uint64_t *mant, int *sh) {
-  int lead = -1;
-  for (int b = 127; b >= 0; --b)
-    if ((u >> b) & 1) {
-      lead = b;
-      break;
-    }
-  if (lead <= 52) {
-    *mant = (uint64_t)u;
-    *sh = 0;
-    return;
-  }
-  int s = lead - 52;
-  unsigned __int128 keep = u >> s, rem = u - (keep << s), half = (unsigned __int128)1 << (s - 1);
-  uint64_t kk = (uint64_t)keep;
-  if (rem > half || (rem == half && (kk & 1))) ++kk;
-  *mant = kk;
-  *sh = s;
-}
-/* C' (256-bit two's complement) -> (hi 2^eh, lo 2^el) */
-static void crt_to_dd_c(const uint64_t acc[4], double *hi, int *eh, double *lo, int *el) {
+/* C' (256-bit two's complement) -> (h + l) 2^e: the magnitude's leading one
+ * at bit 159 of a 160-bit window (bits below it dropped), hi = the window
+ * rounded to 53 bits (nearest, ties to even), lo = the remainder
+ * D 2^96 + n2 2^64 + n1 2^32 + n0 summed in doubles in that order, then
+ * fast_two_sum(hi, lo 2^-107); e = weight of window bit 107. */
+static void crt_to_dd_c(const uint64_t acc[4], double *h, double *l, int *e) {
   int neg = (int)(acc[3] >> 63);
   uint64_t mag[4];
   unsigned __int128 c = neg ? 1 : 0;
@@ -1449,21 +1432,20 @@ static void crt_to_dd_c(const uint64_t acc[4], double *hi, int *eh, double *lo, 
     mag[w] = (uint64_t)c;
     c >>= 64;
   }
-  int lead = -1; /* bit index of the leading one in mag */
+  int lead = -1;
   for (int b = 255; b >= 0; --b)
     if ((mag[b / 64] >> (b % 64)) & 1) {
       lead = b;
       break;
     }
   if (lead < 0) {
-    *hi = *lo = 0.0;
-    *eh = *el = 0;
+    *h = *l = 0.0;
+    *e = 0;
     return;
   }
-  /* the 160-bit window: bits lead .. lead-159 (zeros below bit 0) */
   int E = lead - 159;
   uint32_t nw[5];
-  for (int q = 0; q < 5; ++q) { /* nw[q] = window bits 32q .. 32q+31 */
+  for (int q = 0; q < 5; ++q) {
     uint32_t v = 0;
     for (int b = 0; b < 32; ++b) {
       int src = E + 32 * q + b;
@@ -1477,20 +1459,22 @@ static void crt_to_dd_c(const uint64_t acc[4], double *hi, int *eh, double *lo, 
   int lowz = (nw[2] | nw[1] | nw[0]) == 0;
   int up = r11 > 0x400 || (r11 == 0x400 && (!lowz || (keep & 1)));
   keep += (uint64_t)up;
-  *hi = (double)keep;
-  *eh = E + 107;
-  __int128 R = ((__int128)((int64_t)r11 - (up ? 2048 : 0)) << 96) + ((__int128)nw[2] << 64) +
-               ((__int128)nw[1] << 32) + (__int128)nw[0];
-  unsigned __int128 u = R < 0 ? (unsigned __int128)(-R) : (unsigned __int128)R;
-  uint64_t mant;
-  int sh;
-  crt_rn53(u, &mant, &sh);
-  *lo = R < 0 ? -(double)mant : (double)mant;
-  *el = E + sh;
+  int D = (int)r11 - (up ? 2048 : 0);
+  double lo = (double)D * 0x1p96;
+  lo = lo + (double)nw[2] * 0x1p64;
+  lo = lo + (double)nw[1] * 0x1p32;
+  lo = lo + (double)nw[0];
+  double hi = (double)keep;
+  lo = lo * 0x1p-107;
+  double hs, ls;
+  fast_two_sum(hi, lo, &hs, &ls);
   if (neg) {
-    *hi = -*hi;
-    *lo = -*lo;
+    hs = -hs;
+    ls = -ls;
   }
+  *h = hs;
+  *l = ls;
+  *e = E + 107;
 }
 /* info[0..3] = {N moduli, rho_a, rho_b, W}; rows i0 .. i1-1 of the product
  * only (c holds (i1 - i0) x n outputs, leading dimension i1 - i0). */
@@ -1537,11 +1521,11 @@ void orc_crt_gemm_rows(const double *a, const double *b, double *c, int64_t m, i
         o[1] = 0.0;
       } else {
         double hi, lo;
-        int eh, el;
-        crt_to_dd_c(acc, &hi, &eh, &lo, &el);
-        int ex = sa[i] + sb[j] - 2 * W;
-        o[0] = ldexp(hi, eh + ex);
-        o[1] = ldexp(lo, el + ex);
+        int e;
+        crt_to_dd_c(acc, &hi, &lo, &e);
+        int ex = e + sa[i] + sb[j] - 2 * W;
+        o[0] = ldexp(hi, ex);
+        o[1] = ldexp(lo, ex);
       }
     }
   free(sa); free(ma); free(fa); free(sb); free(mb); free(fb); free(X); free(Y);
