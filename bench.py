@@ -272,15 +272,24 @@ def run_ours(args, ws, rank, local):
     dB = torch.from_numpy(B).to(dev)
     dC = torch.empty(2 * M * N, dtype=torch.float64, device=dev)
     wsb = L.mfcuda_split_workspace_size(M, K, N)
-    dWS = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    wcb = L.mfcuda_crt_workspace_size(M, K, N, 0)
+    dWS = torch.empty(max(wsb, wcb), dtype=torch.uint8, device=dev)
     info = (C.c_int * 3)()
     _lib.check(L.mfcuda_matmuldd_mm_split(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, 0, 8.0,
                                           dWS.data_ptr(), wsb, info, sp), "split (info)")
     S, rho_a, rho_b = tuple(info)
+    cinfo = (C.c_int * 4)()
+    _lib.check(L.mfcuda_matmuldd_mm_crt(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, 0, 8.0,
+                                        dWS.data_ptr(), wcb, cinfo, sp), "crt (info)")
+    NMOD, _, _, WBITS = tuple(cinfo)
 
     def split_step():
         _lib.check(L.mfcuda_matmuldd_mm_split(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, 0, 8.0,
                                               dWS.data_ptr(), wsb, None, sp), "split")
+
+    def crt_step():
+        _lib.check(L.mfcuda_matmuldd_mm_crt(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, 0, 8.0,
+                                            dWS.data_ptr(), wcb, None, sp), "crt")
 
     def plain_step():
         _lib.check(L.mfcuda_matmuldd_mm(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, RI, sp),
@@ -294,33 +303,43 @@ def run_ours(args, ws, rank, local):
     int8_burst, int8_sustained, int8_clk = int8_peaks(pk, sp)
     int8_peak = int8_sustained
 
-    # ---- timed region: K split steps, every launch's phases recorded ----
-    for _ in range(args.warmup):
-        split_step()
-    torch.cuda.synchronize()
-    barrier(ws)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with NvmlClocks(gpu_uuid()) as clk:
+    def timed(step, nclk):
+        """K steps after W warm-up steps, barrier + synchronize on both sides;
+        per-phase times from the library's own events."""
+        for _ in range(args.warmup):
+            step()
         torch.cuda.synchronize()
         barrier(ws)
-        L.mfcuda_phase_profile_begin()
-        e0.record(stream)
-        for _ in range(args.steps):
-            split_step()
-        e1.record(stream)
-        e1.synchronize()
-    sums = (C.c_double * 4)()
-    ncalls = C.c_int64()
-    _lib.check(L.mfcuda_phase_profile_end(sums, C.byref(ncalls)), "phase profile")
-    torch.cuda.synchronize()
-    ms = max_over_ranks(ws, e0.elapsed_time(e1))
-    per_step = ms / args.steps
-    phase = {nm: sums[q] / max(1, ncalls.value) for q, nm in enumerate(["scan", "slice", "mma", "combine"])}
-    flops = 2.0 * M * N * K
-    value = ws * flops / (per_step * 1e-3) / 1e9
-    launches = 9 * args.steps
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with NvmlClocks(gpu_uuid()) as clk:
+            torch.cuda.synchronize()
+            barrier(ws)
+            L.mfcuda_phase_profile_begin()
+            e0.record(stream)
+            for _ in range(args.steps):
+                step()
+            e1.record(stream)
+            e1.synchronize()
+        sums = (C.c_double * 4)()
+        ncalls = C.c_int64()
+        _lib.check(L.mfcuda_phase_profile_end(sums, C.byref(ncalls)), "phase profile")
+        torch.cuda.synchronize()
+        ms = max_over_ranks(ws, e0.elapsed_time(e1))
+        phase = {nm: sums[q] / max(1, ncalls.value) for q, nm in enumerate(["scan", "slice", "mma", "combine"])}
+        nclk.append(clk.summary())
+        return ms / args.steps, phase
 
-    # accuracy of the result just computed, against the exact product (sampled outputs)
+    flops = 2.0 * M * N * K
+    clks = []
+    # the digit-sliced form first, then the CRT form (the headline: same operands,
+    # same error target, fewer tensor-core products)
+    split_ms, split_phase = timed(split_step, clks)
+    per_step, phase = timed(crt_step, clks)
+    value = ws * flops / (per_step * 1e-3) / 1e9
+    split_val = ws * flops / (split_ms * 1e-3) / 1e9
+    launches = 9 * args.steps  # init x2, scan x2, plan, slice x2, tcgen05 MMA, reconstruction
+
+    # accuracy of the CRT result just computed, against the exact product (sampled outputs)
     acc = None
     if rank == 0:
         from oracle import oracle as O
@@ -331,7 +350,8 @@ def run_ours(args, ws, rank, local):
         err, ab = O.gemm_errors(A, B, Ch, M, K, N, ii, jj)
         acc = {"max_err_over_k_ulp_absab": float(np.max(np.abs(err) / (K * 2.0 ** -104 * ab))),
                "max_err_over_ulp_absab": float(np.max(np.abs(err) / (2.0 ** -104 * ab))),
-               "apriori_bound_k_ulp": (S + 1) * 2.0 ** (106 - 8 * S + rho_a + rho_b),
+               "apriori_bound_k_ulp": L.mfcuda_crt_bound(WBITS, rho_a, rho_b, K),
+               "digit_sliced_apriori_bound_k_ulp": (S + 1) * 2.0 ** (106 - 8 * S + rho_a + rho_b),
                "samples": 256, "oracle": "exact superaccumulator (oracle/mf_oracle.c)",
                "ulp": "1 DD ulp = 2^-104"}
 
@@ -355,29 +375,32 @@ def run_ours(args, ws, rank, local):
     hB = torch.from_numpy(B).pin_memory()
     hC = torch.empty(2 * M * N, dtype=torch.float64).pin_memory()
     bound = C.c_double()
-    L.matmuldd_mm_split(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, 0, C.byref(bound))
-    _lib.check_last("matmuldd_mm_split")
+    L.matmuldd_mm_crt(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, 0, C.byref(bound))
+    _lib.check_last("matmuldd_mm_crt")
     e2e_steps = max(1, min(args.steps, 5))
     barrier(ws)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        L.matmuldd_mm_split(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, 0, C.byref(bound))
+        L.matmuldd_mm_crt(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, 0, C.byref(bound))
     t_e2e = max_over_ranks(ws, (time.perf_counter() - t0) / e2e_steps)
-    _lib.check_last("matmuldd_mm_split")
+    _lib.check_last("matmuldd_mm_crt")
 
-    # roofline of the dominant kernel: split_mma_pair_kernel on the INT8 tensor pipe
-    int8_ops = (S * (S + 1) // 2) * 2.0 * M * N * K  # algorithmic INT8 ops per launch
+    # roofline of the dominant kernel: split_mma_pair_kernel (CRT items: one
+    # residue product per modulus) on the INT8 tensor pipe
+    int8_ops = NMOD * 2.0 * M * N * K  # algorithmic INT8 ops per launch
     achieved = int8_ops / (phase["mma"] * 1e-3)
+    split_achieved = (S * (S + 1) // 2) * 2.0 * M * N * K / (split_phase["mma"] * 1e-3)
     roof = {"bound": "tensor", "achieved": achieved / 1e12,
             "peak": int8_peak / 1e12 if int8_peak else None, "unit": "TFLOP/s",
             "frac": achieved / int8_peak if int8_peak else None,
-            "traffic": profile_traffic("split_mma_pair_kernel", "dd_gemm_4096"),
-            "kernel": "split_mma_pair_kernel", "op_kind": "INT8 tensor ops (multiply + add), S(S+1)/2 slice products",
+            "traffic": profile_traffic("split_mma_pair_kernel", "dd_gemm_4096_crt"),
+            "kernel": "split_mma_pair_kernel (CRT items)",
+            "op_kind": "INT8 tensor ops (multiply + add), one residue product per modulus",
             "peak_source": "own tcgen05 kind::i8 probe (multifloats_b200/csrc/peaks.cu), same process, "
                            "sustained: back-to-back launches for 1.5 s (the kernel is timed inside a "
                            "long step loop); of measured",
             "peak_burst": int8_burst / 1e12 if int8_burst else None, "peak_sustained_clocks": int8_clk,
-            "algorithmic_bytes": {"slices_read": 2 * 14 * M * K, "diagonals_written": 14 * M * N * 4}}
+            "algorithmic_bytes": {"residues_read": 2 * NMOD * M * K, "residue_bytes_written": NMOD * M * N}}
 
     if rank == 0:
         line = {
@@ -386,22 +409,29 @@ def run_ours(args, ws, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8+f64",
             "data": "synthetic (seeded; hi = +-u 2^e, u~U[1,2), e~U{-16..16} per row of A / column of B)",
             "config": {"workload": "dd_gemm_4096_split_int8", "M": M, "N": N, "K": K, "R": R,
-                       "slices": S, "rho_a": rho_a, "rho_b": rho_b, "target": "err <= 8 k 2^-104 (|A||B|)_ij",
+                       "form": "crt (modular split-INT8)", "moduli": NMOD, "bits": WBITS,
+                       "rho_a": rho_a, "rho_b": rho_b, "target": "err <= 8 k 2^-104 (|A||B|)_ij",
                        "l2": "operands 256 MiB each > 126 MB L2, no flush needed",
                        "parallelism": f"independent problem per GPU x{ws}"},
+            "digit_sliced": {"value": split_val, "unit": "DD-GFLOP/s", "ms_per_step": split_ms, "slices": S,
+                             "phases_ms": split_phase,
+                             "mma_int8_tops": split_achieved / 1e12,
+                             "mma_frac": split_achieved / int8_peak if int8_peak else None},
             "plain": {"value": plain_val, "unit": "DD-GFLOP/s", "ms_per_step": plain_ms, "steps": plain_steps,
                       "renorm_interval": RI, "fp64_instr_per_s": plain_fp64, "fp64_peak": fp64_peak,
                       "frac": plain_fp64 / fp64_peak},
             "speedup_split_vs_plain": value / plain_val,
+            "speedup_crt_vs_digit_sliced": value / split_val,
             "accuracy": acc,
             "phases_ms": phase,
             "e2e": {"value": ws * flops / t_e2e / 1e9, "unit": "DD-GFLOP/s",
                     "h2d_bytes_per_step": int(A.nbytes + B.nbytes), "d2h_bytes_per_step": int(hC.numel() * 8),
-                    "call": "matmuldd_mm_split (host pointers, pinned)"},
+                    "call": "matmuldd_mm_crt (host pointers, pinned)"},
             "gpu_launches": launches,
             "roofline": roof,
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
+            "clocks": clks[-1],
+            "clocks_digit_sliced": clks[0],
         }
         print(json.dumps(line), flush=True)
 
