@@ -4,8 +4,10 @@
 // (B) exactly as in the digit-sliced form -- X = round(a 2^(W - sigma_i)),
 // |X| < 2^W -- and the exact integer product C' = X Y^T is recovered from its
 // residues modulo N pairwise-coprime moduli m_t <= 256 (crt_tables.h): each
-// residue product (X mod m_t)(Y mod m_t)^T is one INT8 GEMM on the tensor
-// cores, and C' follows from the Chinese remainder theorem,
+// residue product (X mod m_t)(Y mod m_t)^T (residues in [0, m_t), unsigned
+// bytes) is one u8 x u8 -> s32 GEMM on the tensor cores, exact for K chunks of
+// up to 73 * 128 (73 * 128 * 255^2 < 2^30), and C' follows from the Chinese
+// remainder theorem,
 //   C' = sum_t r_t e_t - q M,   e_t = (M / m_t) ((M / m_t)^-1 mod m_t),
 //   r_t = (X Y^T mod m_t) in [0, m_t),  q = round(sum_t r_t e_t / M),
 // which is exact because the moduli are chosen with M > 8 k 2^(2W) > 8 |C'|.
@@ -176,19 +178,36 @@ __device__ __forceinline__ uint32_t crt_mod_small(uint32_t u, int t) {
   const int r = (int)(u - q * m);
   return (uint32_t)(r < 0 ? r + (int)m : r);
 }
-// The signed residue of X = sum_q d_q 256^q (balanced digits, read from the
-// biased words y of biased_bytes: digit q = byte q of y xor 0x80) modulo m_t,
-// in [crt_rlo, crt_rhi]: dp4a against the digit weights give
-// rr = sum_q d_q c_q with |rr| < 14 * 128 * 128 < 2^18, reduced exactly.
-// NW = digit words in use: 3 when W <= 94 (digits 12 and 13 are zero).
+// The residue in [0, m_t) of X = sum_q d_q 256^q (balanced digits, read from
+// the biased words y of biased_bytes: digit q = byte q of y xor 0x80): dp4a
+// against the digit weights give rr = sum_q d_q c_q with |rr| < 14 * 128 * 128
+// < 2^18, made non-negative and reduced exactly.  The per-modulus constants
+// are passed in (hoisted by the caller).  NW = digit words in use: 3 when
+// W <= 94 (digits 12 and 13 are zero).
+struct ModConst {
+  int c0, c1, c2, c3;  // digit weights, signed bytes packed
+  uint32_t m, mu, off;
+};
+__device__ __forceinline__ ModConst mod_const(int t) {
+  ModConst k;
+  k.c0 = (int)crt_digw[t][0];
+  k.c1 = (int)crt_digw[t][1];
+  k.c2 = (int)crt_digw[t][2];
+  k.c3 = (int)crt_digw[t][3];
+  k.m = crt_mod[t];
+  k.mu = crt_mu[t];
+  k.off = crt_off18[t];
+  return k;
+}
 template <int NW>
-__device__ __forceinline__ int crt_residue(const uint32_t (&dw)[4], int t) {
-  int rr = NW == 4 ? __dp4a((int)dw[3], (int)crt_digw[t][3], 0) : 0;
-  rr = __dp4a((int)dw[2], (int)crt_digw[t][2], rr);
-  rr = __dp4a((int)dw[1], (int)crt_digw[t][1], rr);
-  rr = __dp4a((int)dw[0], (int)crt_digw[t][0], rr);
-  const int r = (int)crt_mod_small((uint32_t)(rr + (int)crt_off18[t]), t);
-  return r > crt_rhi[t] ? r - (int)crt_mod[t] : r;
+__device__ __forceinline__ uint32_t crt_residue(const uint32_t (&dw)[4], const ModConst &k) {
+  int rr = NW == 4 ? __dp4a((int)dw[3], k.c3, 0) : 0;
+  rr = __dp4a((int)dw[2], k.c2, rr);
+  rr = __dp4a((int)dw[1], k.c1, rr);
+  rr = __dp4a((int)dw[0], k.c0, rr);
+  const uint32_t u = (uint32_t)rr + k.off;  // in [0, 2^19 + 256)
+  const int r = (int)(u - __umulhi(u, k.mu) * k.m);
+  return (uint32_t)(r < 0 ? r + (int)k.m : r);
 }
 // Signed digit words of the biased words of one entry.
 __device__ __forceinline__ void digit_words(const uint32_t (&y)[4], uint32_t (&dw)[4]) {
@@ -200,9 +219,10 @@ __device__ __forceinline__ void digit_words(const uint32_t (&y)[4], uint32_t (&d
 template <int NW, class F>
 __device__ __forceinline__ void residue_words_nw(const uint32_t (&dw)[8][4], int n, F f) {
   for (int t = 0; t < n; ++t) {
+    const ModConst k = mod_const(t);
     uint32_t r[8];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) r[e] = (uint32_t)crt_residue<NW>(dw[e], t);
+    for (int e = 0; e < 8; ++e) r[e] = crt_residue<NW>(dw[e], k);
     // low bytes of r[0..3] and r[4..7] packed in order (byte permutes)
     const uint32_t lo = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
     const uint32_t hi = __byte_perm(__byte_perm(r[4], r[5], 0x0040), __byte_perm(r[6], r[7], 0x0040), 0x5410);
@@ -368,9 +388,10 @@ __device__ __forceinline__ void crt_load_shared(const CrtConst *cc, int n, CrtSh
 }
 
 // The residue of one product reduced in the tensor-core kernel's epilogue:
-// v = the INT32 sum of one K chunk (|v| < 2^28), stored as v mod m_t in [0, m_t).
+// v = the INT32 sum of one K chunk of unsigned residue products
+// (0 <= v < 73 * 128 * 255^2 < 2^30), stored as v mod m_t in [0, m_t).
 __device__ __forceinline__ uint8_t crt_residue_of_sum(int32_t v, int t) {
-  return (uint8_t)crt_mod_small((uint32_t)(v + (int32_t)crt_off28[t]), t);
+  return (uint8_t)crt_mod_small((uint32_t)v, t);
 }
 
 // Rows i0 .. i0+3 of column j: the residues r_t (one 4-byte load per modulus

@@ -3,8 +3,8 @@
 
 The moduli are the pairwise-coprime integers m <= 256 taken greedily from 256
 down (256, 255, 253, 251, 247, 241, ...): every residue fits a signed byte in
-the symmetric range [-floor(m/2), ceil(m/2) - 1], so each modulus costs one
-INT8 x INT8 -> INT32 product on the tensor cores.  Per modulus the header
+[0, m) as an unsigned byte, so each modulus costs one u8 x u8 -> s32 product
+on the tensor cores.  Per modulus the header
 holds:
 
 * ``crt_mod[t]``       m_t
@@ -21,9 +21,8 @@ holds:
 * ``crt_mu[t]``        ceil(2^32 / m_t): Barrett reduction of a non-negative
                        u < 2^30 (the quotient umulhi(u, mu) is exact or one
                        too large; one correction)
-* ``crt_off28[t]``, ``crt_off18[t]``  multiples of m_t of at least 2^28 / 2^18,
-                       added to signed values below those bounds first
-* ``crt_rlo[t]``, ``crt_rhi[t]``  the symmetric residue range
+* ``crt_off18[t]``     a multiple of m_t of at least 2^18, added to a signed
+                       value below that bound first
 
 Usage::
 
@@ -92,12 +91,8 @@ def main() -> int:
     lines.append(f"MF_TABLE uint32_t crt_mu[{NMAX}] = {{" + ", ".join(f"{-(-(1 << 32) // m)}u" for m in ms) +
                  "};  // ceil(2^32 / m)")
     # offsets making a signed value non-negative before the reduction
-    lines.append(f"MF_TABLE uint32_t crt_off28[{NMAX}] = {{" + ", ".join(f"{m * -(-(1 << 28) // m)}u" for m in ms) +
-                 "};  // m ceil(2^28 / m): |v| < 2^28")
     lines.append(f"MF_TABLE uint32_t crt_off18[{NMAX}] = {{" + ", ".join(f"{m * -(-(1 << 18) // m)}u" for m in ms) +
                  "};  // m ceil(2^18 / m): |v| < 2^18")
-    lines.append(f"MF_TABLE int crt_rlo[{NMAX}] = {{" + ", ".join(str(-(m // 2)) for m in ms) + "};")
-    lines.append(f"MF_TABLE int crt_rhi[{NMAX}] = {{" + ", ".join(str((m + 1) // 2 - 1) for m in ms) + "};")
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "crt_tables.h")
     with open(out, "w") as f:
         f.write("\n".join(lines) + "\n")

@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       // ---- MMA issuer ----
-      const uint32_t idesc = mftc::idesc_i8(BM, BN);
+      const uint32_t idesc = crt ? mftc::idesc_u8(BM, BN) : mftc::idesc_i8(BM, BN);  // CRT residues are unsigned
       int stage = 0;
       uint32_t phase = 0;
       int acc = 0;
@@ -494,7 +494,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
   } else if (warp == 1) {
     if (lane == 0 && leader) {
       // ---- MMA issuer (even CTA) ----
-      const uint32_t idesc = mftc::idesc_i8(BM_PAIR, BN);
+      const uint32_t idesc = crt ? mftc::idesc_u8(BM_PAIR, BN) : mftc::idesc_i8(BM_PAIR, BN);  // CRT residues are unsigned
       int stage = 0;
       uint32_t phase = 0;
       int acc = 0;
