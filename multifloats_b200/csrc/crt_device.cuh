@@ -38,10 +38,15 @@ constexpr int CRT_BATCH = 9;  // moduli whose residues a reconstruction thread l
 constexpr int CRT_WMAX = 110;
 
 // Reconstruction constants of the plan's N moduli, computed on the device.
+// The reconstruction sums r_t e_t in 39-bit limbs held in doubles: a residue
+// (< 2^8) times a limb (< 2^39) is exact, and so are sums of up to 36 such
+// products (< 2^53), so the FP64 pipe does the multiply-adds exactly.
+constexpr int CRT_LB = 39;   // bits per reconstruction limb
+constexpr int CRT_NL39 = 7;  // limbs: 273 bits >= 2W + log2(k) + 1 for W <= 110, k < 2^31
 struct CrtConst {
-  uint32_t e[CRT_NMAX][CRT_NL];  // e_t mod 2^256
-  uint32_t M[CRT_NL];            // M mod 2^256
-  uint32_t cq[CRT_NMAX];         // round(2^32 ((M / m_t)^-1 mod m_t) / m_t): q = round(sum_t r_t cq_t 2^-32)
+  double e[CRT_NMAX][CRT_NL39];  // e_t mod 2^273, 39-bit limbs
+  double M[CRT_NL39];            // M mod 2^273, 39-bit limbs
+  double c[CRT_NMAX];            // ((M / m_t)^-1 mod m_t) / m_t, rounded: q = round(sum_t r_t c_t)
 };
 
 // ceil(log2 k) for k >= 1.
@@ -63,8 +68,18 @@ __host__ __device__ inline int crt_moduli(int W, int64_t k, const int *lg) {
   while (n < CRT_NMAX && lg[n] < need) ++n;
   return n;
 }
-// 32-bit limbs holding |C'| < k 2^(2W) with its sign (two's complement).
-__host__ __device__ inline int crt_limbs(int W, int64_t k) { return (2 * W + ceil_log2(k) + 1 + 31) / 32; }
+// 39-bit limbs holding |C'| < k 2^(2W) with its sign (two's complement).
+__host__ __device__ inline int crt_limbs(int W, int64_t k) {
+  return (2 * W + ceil_log2(k) + 1 + CRT_LB - 1) / CRT_LB;
+}
+// Bits [39 l, 39 l + 39) of the little-endian 32-bit limbs v (>= 11 limbs), as a double.
+__device__ __forceinline__ double limb39(const uint32_t *v, int l) {
+  const int b = CRT_LB * l, w = b / 32, o = b % 32;
+  uint64_t x = ((uint64_t)v[w + 1] << 32) | v[w];
+  x >>= o;
+  if (o + CRT_LB > 64) x |= (uint64_t)v[w + 2] << (64 - o);
+  return (double)(x & ((1ull << CRT_LB) - 1));
+}
 
 // Inverse of a modulo m (gcd(a, m) = 1, m <= 256), extended Euclid.
 __device__ __forceinline__ uint32_t inv_mod_small(uint32_t a, uint32_t m) {
@@ -147,20 +162,26 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
       rem = (rem * (ms % mt)) % mt;
     }
     const uint32_t inv = inv_mod_small(rem, mt);
+    uint32_t ev[CRT_NL + 3];  // e_t mod 2^288 (9 limbs) and two zero limbs for limb39
     uint64_t carry = 0;
-    for (int l = 0; l < CRT_NL; ++l) {
+    for (int l = 0; l <= CRT_NL; ++l) {
       const uint64_t v = (uint64_t)q[l] * inv + carry;
-      cc->e[t][l] = (uint32_t)v;
+      ev[l] = (uint32_t)v;
       carry = v >> 32;
     }
-    cc->cq[t] = (uint32_t)((((uint64_t)inv << 32) + mt / 2) / mt);
+    ev[CRT_NL + 1] = ev[CRT_NL + 2] = 0;
+    for (int l = 0; l < CRT_NL39; ++l) cc->e[t][l] = limb39(ev, l);
+    cc->c[t] = (double)inv / (double)mt;
     if (t == 0) {  // M = (M / m_0) m_0
+      uint32_t mv[CRT_NL + 3];
       uint64_t cy = 0;
-      for (int l = 0; l < CRT_NL; ++l) {
+      for (int l = 0; l <= CRT_NL; ++l) {
         const uint64_t v = (uint64_t)q[l] * mt + cy;
-        cc->M[l] = (uint32_t)v;
+        mv[l] = (uint32_t)v;
         cy = v >> 32;
       }
+      mv[CRT_NL + 1] = mv[CRT_NL + 2] = 0;
+      for (int l = 0; l < CRT_NL39; ++l) cc->M[l] = limb39(mv, l);
     }
   }
   __syncthreads();
@@ -375,15 +396,16 @@ __device__ __forceinline__ void crt_to_dd(const uint32_t *limb, int nl, double &
 
 // Reconstruction constants in shared memory.
 struct CrtShared {
-  uint32_t e[CRT_NMAX][CRT_NL];
-  uint32_t M[CRT_NL];
-  uint32_t cq[CRT_NMAX];
+  double e[CRT_NMAX][CRT_NL39];
+  double M[CRT_NL39];
+  double c[CRT_NMAX];
 };
 // Block prologue: the plan's constants into shared memory.
 __device__ __forceinline__ void crt_load_shared(const CrtConst *cc, int n, CrtShared &cs) {
-  for (int x = threadIdx.x; x < n * CRT_NL; x += blockDim.x) cs.e[x / CRT_NL][x % CRT_NL] = cc->e[x / CRT_NL][x % CRT_NL];
-  for (int x = threadIdx.x; x < CRT_NL; x += blockDim.x) cs.M[x] = cc->M[x];
-  for (int x = threadIdx.x; x < n; x += blockDim.x) cs.cq[x] = cc->cq[x];
+  for (int x = threadIdx.x; x < n * CRT_NL39; x += blockDim.x)
+    cs.e[x / CRT_NL39][x % CRT_NL39] = cc->e[x / CRT_NL39][x % CRT_NL39];
+  for (int x = threadIdx.x; x < CRT_NL39; x += blockDim.x) cs.M[x] = cc->M[x];
+  for (int x = threadIdx.x; x < n; x += blockDim.x) cs.c[x] = cc->c[x];
   __syncthreads();
 }
 
@@ -396,8 +418,10 @@ __device__ __forceinline__ uint8_t crt_residue_of_sum(int32_t v, int t) {
 
 // Rows i0 .. i0+3 of column j: the residues r_t (one 4-byte load per modulus
 // and K chunk of the byte residues D8[t][kc][N_pad][M_pad]), then
-//   q = round(sum_t r_t cq_t 2^-32),  C' = sum_t r_t e_t - q M  (mod 2^(32 nl)),
-// the DD rounding and the exact scaling; `mode` as the digit-sliced combine.
+//   q = round(sum_t r_t c_t),  C' = sum_t r_t e_t - q M  in 39-bit limbs,
+// every limb an exact FP64 multiply-add (see CRT_LB), carried in int64 and
+// repacked into 32-bit limbs; the DD conversion and exact scaling; `mode` as
+// the digit-sliced combine.
 __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8, const Plan *plan,
                                                   const CrtShared &cs, const int *sigA, const int *flagA,
                                                   const int *sigB, const int *flagB, int64_t M, int64_t N,
@@ -408,12 +432,12 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
   if (i0 >= M || j >= N) return;
   const int64_t kstride = N_pad * M_pad, gstride = (int64_t)nkc * kstride;
   const uint8_t *src = D8 + j * M_pad + i0;
-  uint64_t acc[4][CRT_NL], sq[4];
+  double acc[4][CRT_NL39], f[4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    sq[r] = 0;
+    f[r] = 0.0;
 #pragma unroll
-    for (int l = 0; l < CRT_NL; ++l) acc[r][l] = 0;
+    for (int l = 0; l < CRT_NL39; ++l) acc[r][l] = 0.0;
   }
   // moduli in batches of CRT_BATCH: the batch's loads are all in flight before
   // its arithmetic
@@ -443,14 +467,15 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
     for (int u = 0; u < CRT_BATCH; ++u) {
       const int t = t0 + u;
       if (t < n) {
-        const uint32_t cqt = cs.cq[t];
+        const double ct = cs.c[t];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-          const uint32_t rv = (wv[u] >> (8 * r)) & 0xFFu;
-          sq[r] += (uint64_t)rv * cqt;
+          // the residue byte as a double: 2^52 + r_t exactly, minus 2^52
+          const double rd = mfdev::sub(__hiloint2double(0x43300000, (int)((wv[u] >> (8 * r)) & 0xFFu)), 0x1p52);
+          f[r] = mfdev::fma_(rd, ct, f[r]);
 #pragma unroll
-          for (int l = 0; l < CRT_NL; ++l)
-            if (l < nl) acc[r][l] += (uint64_t)rv * cs.e[t][l];
+          for (int l = 0; l < CRT_NL39; ++l)
+            if (l < nl) acc[r][l] = mfdev::fma_(rd, cs.e[t][l], acc[r][l]);
         }
       }
     }
@@ -463,14 +488,35 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
   for (int r = 0; r < 4; ++r) {
     const int64_t i = i0 + r;
     if (i >= M) break;
-    const uint64_t q = (sq[r] + (1ull << 31)) >> 32;
-    uint32_t limb[CRT_NL];
+    // |sum_t r_t e_t / M - C'/M - q| < 1/8 + rounding, so rint gives q exactly
+    const double q = rint(f[r]);
+    uint64_t L[CRT_NL39];
     int64_t carry = 0;
 #pragma unroll
-    for (int l = 0; l < CRT_NL; ++l) {
-      const int64_t x = (int64_t)(acc[r][l] - q * (uint64_t)cs.M[l]) + carry;  // |true value| < 2^47
-      limb[l] = (uint32_t)x;
-      carry = x >> 32;  // arithmetic shift
+    for (int l = 0; l < CRT_NL39; ++l) {
+      // acc - q M: both exact integers below 2^53, so the FMA is exact
+      const int64_t x = (l < nl ? __double2ll_rn(mfdev::fma_(-q, cs.M[l], acc[r][l])) : 0) + carry;
+      L[l] = (uint64_t)x & ((1ull << CRT_LB) - 1);
+      carry = x >> CRT_LB;  // arithmetic shift
+    }
+    (void)carry;
+    // C' mod 2^(39 nl) is exact (e and M are truncated there, so the carry out
+    // of the top limb is not the sign); |C'| < 2^(39 nl - 1), so the top bit of
+    // limb nl - 1 is the sign, copied into the limbs above
+    uint64_t top = 0;
+#pragma unroll
+    for (int l = 0; l < CRT_NL39; ++l) top = l == nl - 1 ? L[l] : top;
+    const uint64_t fill = (top >> (CRT_LB - 1)) & 1 ? (1ull << CRT_LB) - 1 : 0;
+#pragma unroll
+    for (int l = 0; l < CRT_NL39; ++l) L[l] = l < nl ? L[l] : fill;
+    // repack the two's complement value into 8 32-bit limbs
+    uint32_t limb[CRT_NL];
+#pragma unroll
+    for (int o = 0; o < CRT_NL; ++o) {
+      const int b = 32 * o, l1 = b / CRT_LB, off = b % CRT_LB;
+      uint64_t x = L[l1] >> off;
+      if (off + 32 > CRT_LB) x |= (l1 + 1 < CRT_NL39 ? L[l1 + 1] : fill) << (CRT_LB - off);
+      limb[o] = (uint32_t)x;
     }
     double2 out;
     if (fav[r] | fb) {
@@ -478,7 +524,7 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
     } else {
       double hi, lo;
       int e;
-      crt_to_dd(limb, nl, hi, lo, e);
+      crt_to_dd(limb, CRT_NL, hi, lo, e);
       const int ex = e + sav[r] + sb - 2 * W;
       out = make_double2(scale2(hi, ex), scale2(lo, ex));
     }
