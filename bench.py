@@ -697,8 +697,14 @@ def run_complex(args):
     ms_s = _events_time(lambda: _lib.check(L.mfcuda_cmatmuldd_mm_split(A.data_ptr(), B.data_ptr(), Cm.data_ptr(), m, m, m, 0, 8.0, ws.data_ptr(), wsb, None, sp), "cs"),
                         max(1, args.steps // 3), args.warmup, stream)
     ms_p = _events_time(lambda: _lib.check(L.mfcuda_cmatmuldd_mm(A.data_ptr(), B.data_ptr(), Cm.data_ptr(), m, m, m, RI, sp), "cp"), 1, 1, stream)
+    del ws
+    torch.cuda.empty_cache()
+    wcb = L.mfcuda_ccrt_workspace_size(m, m, m, 0)
+    wsc = torch.empty(wcb, dtype=torch.uint8, device=dev)
+    ms_c = _events_time(lambda: _lib.check(L.mfcuda_cmatmuldd_mm_crt(A.data_ptr(), B.data_ptr(), Cm.data_ptr(), m, m, m, 0, 8.0, wsc.data_ptr(), wcb, None, sp), "cc"),
+                        max(1, args.steps // 3), args.warmup, stream)
     flops = 8.0 * m ** 3  # four real products
-    del A, B, Cm, ws
+    del A, B, Cm, wsc
     torch.cuda.empty_cache()
     # complex dot / norm2 over 2^24 elements (device calls, preallocated workspace)
     nc = 1 << 24
@@ -736,10 +742,11 @@ def run_complex(args):
         _lib.check(L.mfcuda_batch_status(p), "status")
         batch[name] = {"ms": bms, "dd_gflops": bflops / bms / 1e6, "work_items": L.mfcuda_batch_work_items(p)}
         L.mfcuda_batch_destroy(p)
-    _line(args, "complex_dd_gemm_4096_split", "complex64x2 GEMM 4096^3 real DD-GFLOP/s (8mnk), split-INT8 vs plain",
-          flops / ms_s / 1e6, "DD-GFLOP/s",
-          {"dtype": "int8+f64", "split_ms": ms_s, "plain_ms": ms_p, "plain_dd_gflops": flops / ms_p / 1e6,
-           "speedup_split_vs_plain": ms_p / ms_s,
+    _line(args, "complex_dd_gemm_4096_split", "complex64x2 GEMM 4096^3 real DD-GFLOP/s (8mnk), split-INT8 (CRT form) vs plain",
+          flops / ms_c / 1e6, "DD-GFLOP/s",
+          {"dtype": "int8+f64", "crt_ms": ms_c, "split_ms": ms_s, "split_dd_gflops": flops / ms_s / 1e6,
+           "plain_ms": ms_p, "plain_dd_gflops": flops / ms_p / 1e6,
+           "speedup_split_vs_plain": ms_p / ms_c, "speedup_crt_vs_digit_sliced": ms_s / ms_c,
            "cdot_2^24": {"ms": ms_dot, "gbs": 64 * nc / ms_dot / 1e6, "frac_hbm": 64 * nc / ms_dot / 1e6 / HBM_GBS},
            "cnorm2_2^24": {"ms": ms_n2, "gbs": 32 * nc / ms_n2 / 1e6, "frac_hbm": 32 * nc / ms_n2 / 1e6 / HBM_GBS},
            "batch_512_complex_32_512": {**batch, "speedup_split_vs_plain": batch["plain"]["ms"] / batch["split"]["ms"],

@@ -176,7 +176,7 @@ MULTIFLOATS_CUDA_API void cmatmuldd_mm_split(const complex64x2 *a, const complex
  * <= 256 (one INT8 GEMM per modulus on the tcgen05 tensor cores, exact INT32
  * accumulation) by the Chinese remainder theorem, then rounded to DD and
  * scaled.  bits = 0 picks the smallest W whose a-priori bound meets
- * err_ij <= 8 k 2^-104 (|A||B|)_ij (W = 92, N = 27 at k = 4096 for operands
+ * err_ij <= 8 k 2^-104 (|A||B|)_ij (W = 92, N = 26 at k = 4096 for operands
  * spanning one binade per row / column); 8..110 = fixed W.  *max_err_bound_out
  * (may be NULL) receives the bound in units of k 2^-104 (|A||B|)_ij.  Inf/NaN
  * in a row of A or column of B yields NaN in the affected outputs.  Host
@@ -184,6 +184,13 @@ MULTIFLOATS_CUDA_API void cmatmuldd_mm_split(const complex64x2 *a, const complex
 MULTIFLOATS_CUDA_API void matmuldd_mm_crt(const float64x2 *a, const float64x2 *b, float64x2 *c,
                                           int64_t m, int64_t k, int64_t n, int bits,
                                           double *max_err_bound_out);
+/* Complex CRT form: re = Ar Br - Ai Bi, im = Ar Bi + Ai Br (the Fortran
+ * cdd_matmul_mm composition) with one W and moduli set for all four real
+ * products (planned from all four parts, each part reduced once); the bound
+ * applies to each real product. */
+MULTIFLOATS_CUDA_API void cmatmuldd_mm_crt(const complex64x2 *a, const complex64x2 *b, complex64x2 *c,
+                                           int64_t m, int64_t k, int64_t n, int bits,
+                                           double *max_err_bound_out);
 
 /* ==========================================================================
  * 2. Device-pointer API (asynchronous on `stream`, a cudaStream_t; NULL = legacy
@@ -222,6 +229,11 @@ MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_crt(const float64x2 *a, const float6
                                                 void *workspace, size_t workspace_bytes, int *info_out,
                                                 void *stream);
 MULTIFLOATS_CUDA_API double mfcuda_crt_bound(int bits, int rho_a, int rho_b, int64_t k);
+MULTIFLOATS_CUDA_API size_t mfcuda_ccrt_workspace_size(int64_t m, int64_t k, int64_t n, int bits);
+MULTIFLOATS_CUDA_API int mfcuda_cmatmuldd_mm_crt(const complex64x2 *a, const complex64x2 *b, complex64x2 *c,
+                                                 int64_t m, int64_t k, int64_t n, int bits, double target,
+                                                 void *workspace, size_t workspace_bytes, int *info_out,
+                                                 void *stream);
 MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_split(const float64x2 *a, const float64x2 *b,
                                                   float64x2 *c, int64_t m, int64_t k, int64_t n,
                                                   int slices, double target, void *workspace,

@@ -70,6 +70,9 @@ SIGNATURES = {
     "mfcuda_matmuldd_mm_crt": (C.c_int, [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, C.c_size_t, P, P]),
     "matmuldd_mm_crt": (None, [P, P, P, I64, I64, I64, C.c_int, C.POINTER(C.c_double)]),
     "mfcuda_crt_bound": (C.c_double, [C.c_int, C.c_int, C.c_int, I64]),
+    "mfcuda_ccrt_workspace_size": (C.c_size_t, [I64, I64, I64, C.c_int]),
+    "mfcuda_cmatmuldd_mm_crt": (C.c_int, [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, C.c_size_t, P, P]),
+    "cmatmuldd_mm_crt": (None, [P, P, P, I64, I64, I64, C.c_int, C.POINTER(C.c_double)]),
     "mfcuda_csplit_workspace_size": (C.c_size_t, [I64, I64, I64]),
     "mfcuda_cmatmuldd_mm_split": (C.c_int, [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, C.c_size_t,
                                             P, P]),

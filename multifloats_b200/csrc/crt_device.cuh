@@ -10,11 +10,11 @@
 // remainder theorem,
 //   C' = sum_t r_t e_t - q M,   e_t = (M / m_t) ((M / m_t)^-1 mod m_t),
 //   r_t = (X Y^T mod m_t) in [0, m_t),  q = round(sum_t r_t e_t / M),
-// which is exact because the moduli are chosen with M > 8 k 2^(2W) > 8 |C'|.
+// which is exact because the moduli are chosen with M >= 4 k 2^(2W) > 4 |C'|.
 // C' is then converted to a double-double (crt_to_dd: hi = C' rounded to 53
 // bits, lo the rest summed in doubles, renormalised) and scaled by
 // 2^(sigma_i + tau_j - 2W).  Compared with the digit-sliced form (S(S+1)/2 slice products for S
-// slices) the tensor work is N products: 27 instead of 105 at 4096^3.
+// slices) the tensor work is N products: 26 instead of 105 at 4096^3.
 //
 // Error (a priori, per output; delta = rounding of an operand to its grid,
 // |delta a_ip| <= 2^(sigma_i - W), zero for zero entries):
@@ -61,9 +61,10 @@ __host__ __device__ inline double crt_bound(int W, int ra, int rb, int64_t k) {
   return (ldexp(1.0, 104 + ra - W) + ldexp(1.0, 104 + rb - W) + ldexp(1.0, 104 + ra + rb - 2 * W) + 0.5) /
          (double)k;
 }
-// Moduli needed for W-bit operands and inner dimension k: M > 8 k 2^(2W).
+// Moduli needed for W-bit operands and inner dimension k: M >= 4 k 2^(2W) > 4 |C'|,
+// so |C'| / M < 1/4 and the rounded quotient estimate has a margin of 1/4.
 __host__ __device__ inline int crt_moduli(int W, int64_t k, const int *lg) {
-  const int need = 2 * W + ceil_log2(k) + 3;
+  const int need = 2 * W + ceil_log2(k) + 2;
   int n = 1;
   while (n < CRT_NMAX && lg[n] < need) ++n;
   return n;
@@ -468,15 +469,21 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
       const int t = t0 + u;
       if (t < n) {
         const double ct = cs.c[t];
+        double rd[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
           // the residue byte as a double: 2^52 + r_t exactly, minus 2^52
-          const double rd = mfdev::sub(__hiloint2double(0x43300000, (int)((wv[u] >> (8 * r)) & 0xFFu)), 0x1p52);
-          f[r] = mfdev::fma_(rd, ct, f[r]);
-#pragma unroll
-          for (int l = 0; l < CRT_NL39; ++l)
-            if (l < nl) acc[r][l] = mfdev::fma_(rd, cs.e[t][l], acc[r][l]);
+          rd[r] = mfdev::sub(__hiloint2double(0x43300000, (int)((wv[u] >> (8 * r)) & 0xFFu)), 0x1p52);
+          f[r] = mfdev::fma_(rd[r], ct, f[r]);
         }
+        // each limb constant loaded once for the thread's four rows
+#pragma unroll
+        for (int l = 0; l < CRT_NL39; ++l)
+          if (l < nl) {
+            const double el = cs.e[t][l];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[r][l] = mfdev::fma_(rd[r], el, acc[r][l]);
+          }
       }
     }
   }
@@ -488,7 +495,7 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
   for (int r = 0; r < 4; ++r) {
     const int64_t i = i0 + r;
     if (i >= M) break;
-    // |sum_t r_t e_t / M - C'/M - q| < 1/8 + rounding, so rint gives q exactly
+    // |sum_t r_t e_t / M - C'/M - q| < 1/4 + rounding, so rint gives q exactly
     const double q = rint(f[r]);
     uint64_t L[CRT_NL39];
     int64_t carry = 0;

@@ -699,7 +699,7 @@ static int pair_nsub() {
 // Most moduli the CRT form can need for inner dimension k (W <= bits, or
 // W <= CRT_WMAX when bits is 0).
 static int crt_slices_max(int64_t k, int bits) {
-  const int need = 2 * (bits > 0 ? bits : CRT_WMAX) + ceil_log2(k < 1 ? 1 : k) + 3;
+  const int need = 2 * (bits > 0 ? bits : CRT_WMAX) + ceil_log2(k < 1 ? 1 : k) + 2;
   int n = 1;
   while (n < CRT_NMAX && crt_lg_host[n] < need) ++n;
   return n;
@@ -1069,6 +1069,34 @@ int run_complex(const complex64x2 *a, const complex64x2 *b, complex64x2 *c, int6
   return run_products(av, two, 2, bv, two, 2, p, 4, m, k, n, slices, target, ws, ws_bytes, s, info);
 }
 
+// Complex CRT form: the four real products of run_complex with one W and one
+// moduli set for all four (planned from all four operands), the four parts
+// reduced to residues once.
+int run_complex_crt(const complex64x2 *a, const complex64x2 *b, complex64x2 *c, int64_t m, int64_t k,
+                    int64_t n, int bits, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info) {
+  int rc = check_args(a, b, c, m, k, n, 0, target);
+  if (bits < 0 || (bits > 0 && bits < 8) || bits > CRT_WMAX) return MFCUDA_ERR_INVALID_ARG;
+  if (rc == -1) return MFCUDA_OK;
+  MF_TRY(rc);
+  MF_TRY(require_device());
+  if (k == 0) {
+    MF_TRY_CUDA(cudaMemsetAsync(c, 0, (size_t)(m * n) * sizeof(complex64x2), s));
+    if (info) info[0] = info[1] = info[2] = info[3] = 0;
+    return MFCUDA_OK;
+  }
+  const double *A = reinterpret_cast<const double *>(a);
+  const double *B = reinterpret_cast<const double *>(b);
+  double *Cd = reinterpret_cast<double *>(c);
+  const double *av[2] = {A, A + 2};
+  const double *bv[2] = {B, B + 2};
+  int64_t two[2] = {2, 2};
+  Product p[4] = {{0, 0, Cd, 2, 0},       // re  = Ar Br
+                  {1, 1, Cd, 2, 1},       // re -= Ai Bi
+                  {0, 1, Cd + 2, 2, 0},   // im  = Ar Bi
+                  {1, 0, Cd + 2, 2, 2}};  // im += Ai Br
+  return run_products(av, two, 2, bv, two, 2, p, 4, m, k, n, bits, target, ws, ws_bytes, s, info, 1);
+}
+
 }  // namespace split
 
 template <bool CPLX>
@@ -1105,9 +1133,10 @@ static int split_host(const void *a, const void *b, void *c, int64_t m, int64_t 
   return MFCUDA_OK;
 }
 
-static int crt_host(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k, int64_t n,
-                    int bits, double *bound_out) {
-  const size_t elem = sizeof(float64x2);
+template <bool CPLX>
+static int crt_host(const void *a, const void *b, void *c, int64_t m, int64_t k, int64_t n, int bits,
+                    double *bound_out) {
+  const size_t elem = CPLX ? sizeof(complex64x2) : sizeof(float64x2);
   if (m < 0 || k < 0 || n < 0 || !mul_ok(m, k) || !mul_ok(k, n) || !mul_ok(m, n))
     return MFCUDA_ERR_INVALID_ARG;
   if (bits < 0 || (bits > 0 && bits < 8) || bits > split::CRT_WMAX) return MFCUDA_ERR_INVALID_ARG;
@@ -1115,15 +1144,21 @@ static int crt_host(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_
   if (!c || (k > 0 && (!a || !b))) return MFCUDA_ERR_INVALID_ARG;
   MF_TRY(require_device());
   size_t ba = (size_t)(m * k) * elem, bb = (size_t)(k * n) * elem, bc = (size_t)(m * n) * elem;
-  size_t wsb = split::crt_workspace_size(m, k, n, bits, false);
+  size_t wsb = split::crt_workspace_size(m, k, n, bits, CPLX);
   size_t sz[4] = {ba, bb, bc, wsb};
   Staging st;
   MF_TRY(staging_acquire(st, sz));
   if (ba) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[0], a, ba, cudaMemcpyHostToDevice, st.stream));
   if (bb) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[1], b, bb, cudaMemcpyHostToDevice, st.stream));
   int info[4] = {0, 0, 0, 0};
-  MF_TRY(split::run_crt(static_cast<float64x2 *>(st.buf[0]), static_cast<float64x2 *>(st.buf[1]),
-                        static_cast<float64x2 *>(st.buf[2]), m, k, n, bits, 8.0, st.buf[3], wsb, st.stream, info));
+  if (CPLX)
+    MF_TRY(split::run_complex_crt(static_cast<complex64x2 *>(st.buf[0]), static_cast<complex64x2 *>(st.buf[1]),
+                                  static_cast<complex64x2 *>(st.buf[2]), m, k, n, bits, 8.0, st.buf[3], wsb,
+                                  st.stream, info));
+  else
+    MF_TRY(split::run_crt(static_cast<float64x2 *>(st.buf[0]), static_cast<float64x2 *>(st.buf[1]),
+                          static_cast<float64x2 *>(st.buf[2]), m, k, n, bits, 8.0, st.buf[3], wsb, st.stream,
+                          info));
   MF_TRY_CUDA(cudaMemcpyAsync(c, st.buf[2], bc, cudaMemcpyDeviceToHost, st.stream));
   MF_TRY_CUDA(cudaStreamSynchronize(st.stream));
   if (bound_out) *bound_out = info[0] > 0 ? split::crt_bound(info[3], info[1], info[2], k) : 0.0;
@@ -1147,7 +1182,23 @@ MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_crt(const float64x2 *a, const float6
 }
 MULTIFLOATS_CUDA_API void matmuldd_mm_crt(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m,
                                           int64_t k, int64_t n, int bits, double *max_err_bound_out) {
-  mfcuda::set_last_error(mfcuda::crt_host(a, b, c, m, k, n, bits, max_err_bound_out));
+  mfcuda::set_last_error(mfcuda::crt_host<false>(a, b, c, m, k, n, bits, max_err_bound_out));
+}
+MULTIFLOATS_CUDA_API size_t mfcuda_ccrt_workspace_size(int64_t m, int64_t k, int64_t n, int bits) {
+  if (m < 0 || k < 0 || n < 0 || bits < 0 || bits > mfcuda::split::CRT_WMAX) return 0;
+  return mfcuda::split::crt_workspace_size(m, k, n, bits, true);
+}
+MULTIFLOATS_CUDA_API int mfcuda_cmatmuldd_mm_crt(const complex64x2 *a, const complex64x2 *b, complex64x2 *c,
+                                                 int64_t m, int64_t k, int64_t n, int bits, double target,
+                                                 void *workspace, size_t workspace_bytes, int *info_out,
+                                                 void *stream) {
+  return mfcuda::split::run_complex_crt(a, b, c, m, k, n, bits, target, workspace, workspace_bytes,
+                                        mfcuda::as_stream(stream), info_out);
+}
+MULTIFLOATS_CUDA_API void cmatmuldd_mm_crt(const complex64x2 *a, const complex64x2 *b, complex64x2 *c,
+                                           int64_t m, int64_t k, int64_t n, int bits,
+                                           double *max_err_bound_out) {
+  mfcuda::set_last_error(mfcuda::crt_host<true>(a, b, c, m, k, n, bits, max_err_bound_out));
 }
 MULTIFLOATS_CUDA_API double mfcuda_crt_bound(int bits, int rho_a, int rho_b, int64_t k) {
   if (bits < 8 || bits > mfcuda::split::CRT_WMAX || k < 1) return -1.0;

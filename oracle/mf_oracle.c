@@ -1369,7 +1369,7 @@ int orc_crt_plan(int bits, double target, int ra, int rb, int64_t k, int *nmod) 
         break;
       }
   }
-  const int need = 2 * W + crt_ceil_log2(k) + 3;
+  const int need = 2 * W + crt_ceil_log2(k) + 2;
   int n = 1;
   while (n < CRT_NMAX && crt_lg[n] < need) ++n;
   if (nmod) *nmod = n;
@@ -1533,4 +1533,56 @@ void orc_crt_gemm_rows(const double *a, const double *b, double *c, int64_t m, i
 void orc_crt_gemm(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n, int bits,
                   double target, int *info) {
   orc_crt_gemm_rows(a, b, c, m, k, n, bits, target, info, 0, m);
+}
+
+/* Complex CRT form: the four real products with one W (planned from the
+ * exponent spreads of all four parts: A side Ar, Ai rows; B side Br, Bi
+ * columns), re = Ar Br - Ai Bi, im = Ar Bi + Ai Br with the DD operators in
+ * the device's order (store, subtract, store, add).  info = {N, rho_a, rho_b, W}. */
+void orc_crt_cgemm(const double *a, const double *b, double *c, int64_t m, int64_t k, int64_t n, int bits,
+                   double target, int *info) {
+  double *ar = malloc(sizeof(double) * 2 * m * k), *ai = malloc(sizeof(double) * 2 * m * k);
+  double *br = malloc(sizeof(double) * 2 * k * n), *bi = malloc(sizeof(double) * 2 * k * n);
+  for (int64_t e = 0; e < m * k; ++e) {
+    ar[2 * e] = a[4 * e]; ar[2 * e + 1] = a[4 * e + 1];
+    ai[2 * e] = a[4 * e + 2]; ai[2 * e + 1] = a[4 * e + 3];
+  }
+  for (int64_t e = 0; e < k * n; ++e) {
+    br[2 * e] = b[4 * e]; br[2 * e + 1] = b[4 * e + 1];
+    bi[2 * e] = b[4 * e + 2]; bi[2 * e + 1] = b[4 * e + 3];
+  }
+  int ra = 0, rb = 0;
+  for (int part = 0; part < 2; ++part) {
+    const double *x = part ? ai : ar, *y = part ? bi : br;
+    for (int64_t i = 0; i < m; ++i) {
+      int sg, mu, bad;
+      split_stats(x + 2 * i, k, m, &sg, &mu, &bad);
+      if (sg != -100000 && sg - mu > ra) ra = sg - mu;
+    }
+    for (int64_t j = 0; j < n; ++j) {
+      int sg, mu, bad;
+      split_stats(y + 2 * j * k, k, 1, &sg, &mu, &bad);
+      if (sg != -100000 && sg - mu > rb) rb = sg - mu;
+    }
+  }
+  int nmod = 0;
+  int W = orc_crt_plan(bits, target, ra, rb, k, &nmod);
+  if (info) {
+    info[0] = nmod;
+    info[1] = ra;
+    info[2] = rb;
+    info[3] = W;
+  }
+  double *rr = malloc(sizeof(double) * 2 * m * n), *ii = malloc(sizeof(double) * 2 * m * n);
+  double *ri = malloc(sizeof(double) * 2 * m * n), *ir = malloc(sizeof(double) * 2 * m * n);
+  orc_crt_gemm(ar, br, rr, m, k, n, W, target, NULL);
+  orc_crt_gemm(ai, bi, ii, m, k, n, W, target, NULL);
+  orc_crt_gemm(ar, bi, ri, m, k, n, W, target, NULL);
+  orc_crt_gemm(ai, br, ir, m, k, n, W, target, NULL);
+  for (int64_t e = 0; e < m * n; ++e) {
+    dd re = dd_sub(mk(rr[2 * e], rr[2 * e + 1]), mk(ii[2 * e], ii[2 * e + 1]));
+    dd im = dd_add(mk(ri[2 * e], ri[2 * e + 1]), mk(ir[2 * e], ir[2 * e + 1]));
+    c[4 * e] = re.hi; c[4 * e + 1] = re.lo; c[4 * e + 2] = im.hi; c[4 * e + 3] = im.lo;
+  }
+  free(ar); free(ai); free(br); free(bi); free(rr); free(ii); free(ri); free(ir);
 }

@@ -70,6 +70,7 @@ def orc():
         L.orc_split_gemm_kc.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64]
         L.orc_split_cgemm_kc.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64]
         L.orc_crt_gemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
+        L.orc_crt_cgemm.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P]
         L.orc_crt_gemm_rows.argtypes = [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, I64, I64]
         L.orc_crt_bound.argtypes = [C.c_int, C.c_int, C.c_int, I64]
         L.orc_crt_bound.restype = C.c_double
@@ -298,6 +299,15 @@ def crt_gemm(a, b, m, k, n, bits=0, target=8.0, rows=None):
     i0, i1 = rows if rows is not None else (0, m)
     c = np.empty(2 * (i1 - i0) * n)
     orc().orc_crt_gemm_rows(_p(a), _p(b), _p(c), m, k, n, bits, target, info.ctypes.data, i0, i1)
+    return c, info.tolist()
+
+
+def crt_cgemm(a, b, m, k, n, bits=0, target=8.0):
+    """Complex CRT form restated (orc_crt_cgemm): (C, [moduli, rho_a, rho_b, W])."""
+    a, b = _c(a), _c(b)
+    info = np.zeros(4, dtype=np.int32)
+    c = np.empty(4 * m * n)
+    orc().orc_crt_cgemm(_p(a), _p(b), _p(c), m, k, n, bits, target, info.ctypes.data)
     return c, info.tolist()
 
 

@@ -139,7 +139,7 @@ def test_4096_error_bound_and_sampled_rows(cuda_lib, dev, R):
     A = W.dd_rowcol_scaled(m, k, R, "row", seed=101)
     B = W.dd_rowcol_scaled(k, n, R, "col", seed=102)
     got, info = dev_crt(cuda_lib, dev, A, B, m, k, n)
-    assert (info[0], info[3]) == (27, 92)  # one binade per row / column: rho = 1
+    assert (info[0], info[3]) == (26, 92)  # one binade per row / column: rho = 1
     bound = O.crt_bound(info[3], info[1], info[2], k)
     assert bound <= 8.0
     rng = np.random.default_rng(R)
@@ -150,3 +150,28 @@ def test_4096_error_bound_and_sampled_rows(cuda_lib, dev, R):
     want, _ = O.crt_gemm(A, B, m, k, n, rows=rows)
     sub = np.ascontiguousarray(got.reshape(n, m, 2)[:, rows[0]:rows[1], :]).reshape(-1)
     assert O.same_bits(sub, want).all()
+
+
+@pytest.mark.parametrize("shape", [(96, 130, 64), (300, 200, 520), (1, 3, 2)])
+def test_complex_bit_exact_and_host(cuda_lib, dev, shape):
+    """Complex CRT form: four real products with one plan (from all four
+    parts), combined re = ArBr - AiBi, im = ArBi + AiBr."""
+    import torch
+
+    m, k, n = shape
+    A = W.complex_from_parts(W.dd_rowcol_scaled(m, k, 16, "row", 31), W.dd_rowcol_scaled(m, k, 16, "row", 32))
+    B = W.complex_from_parts(W.dd_rowcol_scaled(k, n, 16, "col", 33), W.dd_rowcol_scaled(k, n, 16, "col", 34))
+    a, b = to_dev(A, dev), to_dev(B, dev)
+    c = torch.empty(4 * m * n, dtype=torch.float64, device=dev)
+    info = (C.c_int * 4)()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = cuda_lib.mfcuda_cmatmuldd_mm_crt(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, k, n, 0, 8.0, None, 0,
+                                          info, stream)
+    assert rc == 0
+    want, winfo = O.crt_cgemm(A, B, m, k, n)
+    assert list(info) == winfo
+    assert O.same_bits(to_host(c), want).all()
+    h = np.empty(4 * m * n)
+    bound = C.c_double()
+    cuda_lib.cmatmuldd_mm_crt(A.ctypes.data, B.ctypes.data, h.ctypes.data, m, k, n, 0, C.byref(bound))
+    assert cuda_lib.mfcuda_last_error() == 0 and O.same_bits(h, want).all()
