@@ -410,15 +410,32 @@ __device__ __forceinline__ void crt_load_shared(const CrtConst *cc, int n, CrtSh
   __syncthreads();
 }
 
+// Residue layout of one product (modulus t, K chunk kc): N_pad x M_pad bytes,
+// four consecutive columns interleaved per row -- byte (j, i) at
+// ((j / 4) M_pad + i) 4 + j % 4 -- so a thread holding one row writes one
+// 32-bit word per four columns.  Word index of the element at byte offset
+// off = (plane) + j M_pad + i with j % 4 == 0:
+__device__ __forceinline__ int64_t crt_word_index(int64_t off, int64_t M_pad) {
+  const int64_t plane = off / (4 * M_pad) * (4 * M_pad);  // (t, kc) plane plus whole column quads
+  const int64_t rest = off - plane;                        // j % 4 == 0 within the quad: rest = i
+  return plane / 4 + rest;
+}
+// The residues of four INT32 sums packed in column order.
+__device__ __forceinline__ uint32_t crt_pack4(uint32_t v0, uint32_t v1, uint32_t v2, uint32_t v3, int t);
+
 // The residue of one product reduced in the tensor-core kernel's epilogue:
 // v = the INT32 sum of one K chunk of unsigned residue products
 // (0 <= v < 73 * 128 * 255^2 < 2^30), stored as v mod m_t in [0, m_t).
 __device__ __forceinline__ uint8_t crt_residue_of_sum(int32_t v, int t) {
   return (uint8_t)crt_mod_small((uint32_t)v, t);
 }
+__device__ __forceinline__ uint32_t crt_pack4(uint32_t v0, uint32_t v1, uint32_t v2, uint32_t v3, int t) {
+  return __byte_perm(__byte_perm(crt_mod_small(v0, t), crt_mod_small(v1, t), 0x0040),
+                     __byte_perm(crt_mod_small(v2, t), crt_mod_small(v3, t), 0x0040), 0x5410);
+}
 
-// Rows i0 .. i0+3 of column j: the residues r_t (one 4-byte load per modulus
-// and K chunk of the byte residues D8[t][kc][N_pad][M_pad]), then
+// Row i of columns j0 .. j0+3 (j0 % 4 == 0): the residues r_t (one 32-bit load
+// per modulus and K chunk from the column-quad layout of crt_word_index), then
 //   q = round(sum_t r_t c_t),  C' = sum_t r_t e_t - q M  in 39-bit limbs,
 // every limb an exact FP64 multiply-add (see CRT_LB), carried in int64 and
 // repacked into 32-bit limbs; the DD conversion and exact scaling; `mode` as
@@ -427,12 +444,11 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
                                                   const CrtShared &cs, const int *sigA, const int *flagA,
                                                   const int *sigB, const int *flagB, int64_t M, int64_t N,
                                                   int64_t M_pad, int64_t N_pad, int nkc, double *__restrict__ C,
-                                                  int64_t cstride, int mode, int64_t quad, int64_t j) {
+                                                  int64_t cstride, int mode, int64_t i, int64_t j0) {
   const int n = plan->S, nl = plan->nl, W = plan->W;
-  const int64_t i0 = quad * 4;
-  if (i0 >= M || j >= N) return;
-  const int64_t kstride = N_pad * M_pad, gstride = (int64_t)nkc * kstride;
-  const uint8_t *src = D8 + j * M_pad + i0;
+  if (i >= M || j0 >= N) return;
+  const int64_t kstride = N_pad * M_pad / 4, gstride = (int64_t)nkc * kstride;  // in 32-bit words
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(D8) + (j0 / 4) * M_pad + i;
   double acc[4][CRT_NL39], f[4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
@@ -450,11 +466,11 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
       if (t >= n) {
         wv[u] = 0;
       } else if (nkc == 1) {
-        wv[u] = __ldcs(reinterpret_cast<const uint32_t *>(src + t * gstride));
+        wv[u] = __ldcs(src + t * gstride);
       } else {  // per-row sums of the chunks' residues, reduced again
         uint32_t sum[4] = {0, 0, 0, 0};
         for (int kc = 0; kc < nkc; ++kc) {
-          const uint32_t w = __ldcs(reinterpret_cast<const uint32_t *>(src + t * gstride + kc * kstride));
+          const uint32_t w = __ldcs(src + t * gstride + kc * kstride);
 #pragma unroll
           for (int r = 0; r < 4; ++r) sum[r] += (w >> (8 * r)) & 0xFFu;
         }
@@ -487,14 +503,14 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
       }
     }
   }
-  const int4 sa = *reinterpret_cast<const int4 *>(sigA + i0);
-  const int4 fa = *reinterpret_cast<const int4 *>(flagA + i0);
-  const int sav[4] = {sa.x, sa.y, sa.z, sa.w}, fav[4] = {fa.x, fa.y, fa.z, fa.w};
-  const int sb = sigB[j], fb = flagB[j];
+  const int4 sb4 = *reinterpret_cast<const int4 *>(sigB + j0);
+  const int4 fb4 = *reinterpret_cast<const int4 *>(flagB + j0);
+  const int sbv[4] = {sb4.x, sb4.y, sb4.z, sb4.w}, fbv[4] = {fb4.x, fb4.y, fb4.z, fb4.w};
+  const int sa = sigA[i], fa = flagA[i];
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int64_t i = i0 + r;
-    if (i >= M) break;
+  for (int r = 0; r < 4; ++r) {  // r: column j0 + r
+    const int64_t j = j0 + r;
+    if (j >= N) break;
     // |sum_t r_t e_t / M - C'/M - q| < 1/4 + rounding, so rint gives q exactly
     const double q = rint(f[r]);
     uint64_t L[CRT_NL39];
@@ -526,13 +542,13 @@ __device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8
       limb[o] = (uint32_t)x;
     }
     double2 out;
-    if (fav[r] | fb) {
+    if (fa | fbv[r]) {
       out = make_double2(CUDART_NAN, 0.0);
     } else {
       double hi, lo;
       int e;
       crt_to_dd(limb, CRT_NL, hi, lo, e);
-      const int ex = e + sav[r] + sb - 2 * W;
+      const int ex = e + sa + sbv[r] - 2 * W;
       out = make_double2(scale2(hi, ex), scale2(lo, ex));
     }
     double2 *dst = reinterpret_cast<double2 *>(C) + (j * M + i) * cstride;

@@ -267,16 +267,16 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
       const int64_t off = ((int64_t)(it.g * nkc + it.kc) * N_pad + (int64_t)it.tn * BN) * M_pad +
                           (int64_t)it.tm * BM + row;
       const uint32_t tm_addr = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * BN);
-      if (crt) {  // the residue modulo m_g, one byte per output (crt_device.cuh)
-        uint8_t *dst = reinterpret_cast<uint8_t *>(D) + off;
+      if (crt) {  // residues modulo m_g, four columns per 32-bit word (crt_device.cuh)
+        uint32_t *dst = reinterpret_cast<uint32_t *>(D) + crt_word_index(off, M_pad);
 #pragma unroll 1
         for (int chunk = 0; chunk < BN / 32; ++chunk) {
           uint32_t r[32];
           mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), r);
           mftc::tmem_wait_ld();
 #pragma unroll
-          for (int q = 0; q < 32; ++q) {
-            __stcs(dst, crt_residue_of_sum((int32_t)r[q], it.g));
+          for (int g = 0; g < 8; ++g) {
+            __stcs(dst, crt_pack4(r[4 * g], r[4 * g + 1], r[4 * g + 2], r[4 * g + 3], it.g));
             dst += M_pad;
           }
         }
@@ -568,16 +568,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
       const int64_t off = ((int64_t)(it.g * nkc + it.kc) * N_pad + (int64_t)it.tn * tn_cols) * M_pad +
                           (int64_t)it.tm * BM_PAIR + (int64_t)rank * 128 + row;
       const uint32_t tm_addr = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * acc_cols);
-      if (crt) {  // the residue modulo m_g, one byte per output (crt_device.cuh)
-        uint8_t *dst = reinterpret_cast<uint8_t *>(D) + off;
+      if (crt) {  // residues modulo m_g, four columns per 32-bit word (crt_device.cuh)
+        uint32_t *dst = reinterpret_cast<uint32_t *>(D) + crt_word_index(off, M_pad);
 #pragma unroll 1
         for (int chunk = 0; chunk < acc_cols / 32; ++chunk) {
           uint32_t v[32];
           mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
           mftc::tmem_wait_ld();
 #pragma unroll
-          for (int q = 0; q < 32; ++q) {
-            __stcs(dst, crt_residue_of_sum((int32_t)v[q], it.g));
+          for (int g = 0; g < 8; ++g) {
+            __stcs(dst, crt_pack4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3], it.g));
             dst += M_pad;
           }
         }
@@ -646,7 +646,7 @@ __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restri
   if (p8 >= K_pad) return;
   crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, blockIdx.y, p8);
 }
-// Thread per 4 consecutive rows of column j = blockIdx.y (byte residues from
+// Thread per row i and 4 consecutive columns j0 = 4 blockIdx.y (residues from
 // the tensor-core kernel's epilogue); `mode` as combine_kernel.
 __global__ void __launch_bounds__(128) crt_combine_kernel(const uint8_t *__restrict__ D8, const Plan *plan,
                                                           const CrtConst *cc, const int *sigA, const int *flagA,
@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(128) crt_combine_kernel(const uint8_t *__restr
   __shared__ CrtShared cs;
   crt_load_shared(cc, plan->S, cs);
   crt_combine4_body(D8, plan, cs, sigA, flagA, sigB, flagB, M, N, M_pad, N_pad, nkc, C, cstride, mode,
-                    (int64_t)blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
+                    (int64_t)blockIdx.x * blockDim.x + threadIdx.x, 4 * (int64_t)blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -960,7 +960,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                                                              status);
       if (q == nprod - 1) mark(3, s);
       if (crt)
-        crt_combine_kernel<<<dim3(cgx, (unsigned)n), 128, 0, s>>>(
+        crt_combine_kernel<<<dim3((unsigned)((m + 127) / 128), (unsigned)((n + 3) / 4)), 128, 0, s>>>(
             reinterpret_cast<const uint8_t *>(D), plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, n, L.M_pad,
             L.N_pad, (int)L.nkc, prods[q].out, prods[q].ostride, prods[q].mode);
       else
