@@ -928,11 +928,28 @@ def run_gemm8192(args):
             res[f"{n}_R{R}"] = {"ms": ms, "dd_gflops": 2.0 * n ** 3 / ms / 1e6, "slices": info[0],
                                 "max_err_over_k_ulp_absab": float(np.max(np.abs(err) / (n * 2.0 ** -104 * ab))),
                                 "max_err_over_ulp_absab": float(np.max(np.abs(err) / (2.0 ** -104 * ab)))}
-            log(n, R, res[f"{n}_R{R}"])
-            del dA, dB, dC, ws
+            del ws
             torch.cuda.empty_cache()
-    _line(args, "dd_gemm_split_4096_8192_R", "split-INT8 DD-GEMM DD-GFLOP/s 8192^3 (R=16)", res["8192_R16"]["dd_gflops"],
-          "DD-GFLOP/s", {"dtype": "int8+f64", "per_config": res, "ulp": "1 DD ulp = 2^-104"})
+            # the CRT form on the same operands
+            wcb = L.mfcuda_crt_workspace_size(n, n, n, 0)
+            wsc = torch.empty(wcb, dtype=torch.uint8, device=dev)
+            cinfo = (C.c_int * 4)()
+            _lib.check(L.mfcuda_matmuldd_mm_crt(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), n, n, n, 0, 8.0, wsc.data_ptr(), wcb, cinfo, sp), "c")
+            ms_c = _events_time(lambda: _lib.check(L.mfcuda_matmuldd_mm_crt(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), n, n, n, 0, 8.0, wsc.data_ptr(), wcb, None, sp), "c"),
+                                max(1, args.steps // 5), args.warmup, stream)
+            err_c, ab_c = O.gemm_errors(A, B, dC.cpu().numpy(), n, n, n, ii, jj)
+            res[f"{n}_R{R}"]["crt"] = {"ms": ms_c, "dd_gflops": 2.0 * n ** 3 / ms_c / 1e6, "moduli": cinfo[0],
+                                       "bits": cinfo[3],
+                                       "apriori_bound_k_ulp": L.mfcuda_crt_bound(cinfo[3], cinfo[1], cinfo[2], n),
+                                       "max_err_over_k_ulp_absab": float(np.max(np.abs(err_c) / (n * 2.0 ** -104 * ab_c))),
+                                       "max_err_over_ulp_absab": float(np.max(np.abs(err_c) / (2.0 ** -104 * ab_c)))}
+            log(n, R, res[f"{n}_R{R}"])
+            del dA, dB, dC, wsc
+            torch.cuda.empty_cache()
+    _line(args, "dd_gemm_split_4096_8192_R", "split-INT8 DD-GEMM DD-GFLOP/s 8192^3 (R=16), CRT form",
+          res["8192_R16"]["crt"]["dd_gflops"],
+          "DD-GFLOP/s", {"dtype": "int8+f64", "per_config": res, "ulp": "1 DD ulp = 2^-104",
+                         "digit_sliced_8192_R16": res["8192_R16"]["dd_gflops"]})
 
 
 def run_reference(args, ws, rank):

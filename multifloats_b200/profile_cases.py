@@ -1,6 +1,6 @@
 """Small, self-ending workloads for profiling each hot kernel once under ncu.
 
-    python -m multifloats_b200.profile_cases {split,plain,elementwise,reduce,all} [--n N]
+    python -m multifloats_b200.profile_cases {split,crt,plain,elementwise,reduce,batched,gemv,blas,all} [--n N]
 
 Inputs exceed the 126 MB L2 where DRAM figures matter, while the whole case
 stays within a few GB of device memory and a few kernel launches.
@@ -24,7 +24,8 @@ def main() -> int:
     from multifloats_b200 import workloads as W
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["split", "plain", "elementwise", "reduce", "batched", "gemv", "blas", "all"])
+    ap.add_argument("case", choices=["split", "crt", "plain", "elementwise", "reduce", "batched", "gemv", "blas",
+                                     "all"])
     ap.add_argument("--n", type=int, default=2048, help="matrix size for split / plain")
     args = ap.parse_args()
     dev = torch.device("cuda:0")
@@ -41,6 +42,13 @@ def main() -> int:
         c = torch.empty_like(a)
         _lib.check(L.mfcuda_matmuldd_mm_split(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, m, m, 0, 8.0,
                                               None, 0, None, sp), "split")
+    if args.case in ("crt", "all"):
+        m = args.n
+        a = d(W.dd_rowcol_scaled(m, m, 16, "row", 1))
+        b = d(W.dd_rowcol_scaled(m, m, 16, "col", 2))
+        c = torch.empty_like(a)
+        _lib.check(L.mfcuda_matmuldd_mm_crt(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, m, m, 0, 8.0,
+                                            None, 0, None, sp), "crt")
     if args.case in ("plain", "all"):
         m = args.n
         a, b = d(W.dd_uniform(m * m, 1)), d(W.dd_uniform(m * m, 2))
