@@ -339,6 +339,11 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
 // super-items together and, at any moment, multiply the same slice pair (s,
 // t) of different tiles: the slices they read are shared through L2 instead
 // of being fetched from DRAM once per pair.
+// Threads of the pair kernel: warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two
+// warps per TMEM lane quadrant, each draining half of the accumulator's
+// columns, so the drain the next item's MMAs wait for takes half as long).
+constexpr int PAIR_THREADS = 320;
+constexpr int PAIR_EPI_WARPS = 8;
 constexpr int P_STAGE_A = 128 * BK;  // 16 KiB: this CTA's 128 rows of A
 constexpr int P_HALF_B = 128 * BK;   // 16 KiB: this CTA's 128 rows of one B half
 constexpr int BM_PAIR = 256;
@@ -379,7 +384,7 @@ struct PairSched {
   }
 };
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     split_mma_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                           const Plan *plan, int32_t *__restrict__ D, int M_pad, int N_pad, int nkc,
                           int kblocks, int nsub, int *status) {
@@ -416,7 +421,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mftc::mbar_init(&tfull[a], 1);
-      mftc::mbar_init(&tempty[a], 8);
+      mftc::mbar_init(&tempty[a], 2 * PAIR_EPI_WARPS);  // every epilogue warp of both CTAs
     }
     mftc::mbar_init(drain, 1);
     *abort_flag = 0;
@@ -551,9 +556,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
       }
     }
   } else {
-    // ---- epilogue: warps 2..5 of both CTAs, TMEM lane quadrant = warp % 4 ----
+    // ---- epilogue: warps 2..9 of both CTAs, TMEM lane quadrant = warp % 4,
+    // warps 2-5 drain the first half of the accumulator's columns, 6-9 the second ----
     const int quad = warp & 3;
     const int row = quad * 32 + lane;
+    const int nch = acc_cols / 32 / 2, ch0 = ((warp - 2) / 4) * nch;  // this warp's 32-column chunks
     int acc = 0;
     uint32_t acc_phase = 0;
     PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles);
@@ -569,9 +576,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
                           (int64_t)it.tm * BM_PAIR + (int64_t)rank * 128 + row;
       const uint32_t tm_addr = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * acc_cols);
       if (crt) {  // residues modulo m_g, four columns per 32-bit word (crt_device.cuh)
-        uint32_t *dst = reinterpret_cast<uint32_t *>(D) + crt_word_index(off, M_pad);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(D) + crt_word_index(off, M_pad) + (int64_t)ch0 * 8 * M_pad;
 #pragma unroll 1
-        for (int chunk = 0; chunk < acc_cols / 32; ++chunk) {
+        for (int chunk = ch0; chunk < ch0 + nch; ++chunk) {
           uint32_t v[32];
           mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
           mftc::tmem_wait_ld();
@@ -582,9 +589,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MMA_THREADS, 1)
           }
         }
       } else {
-        int32_t *dst = D + off;
+        int32_t *dst = D + off + (int64_t)ch0 * 32 * M_pad;
 #pragma unroll 1
-        for (int chunk = 0; chunk < acc_cols / 32; ++chunk) {
+        for (int chunk = ch0; chunk < ch0 + nch; ++chunk) {
           uint32_t v[32];
           mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
           mftc::tmem_wait_ld();
@@ -823,7 +830,7 @@ static int pair_grid() {
   static int grid = [] {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(2 * (unsigned)sm_count(), 1, 1);
-    cfg.blockDim = dim3(MMA_THREADS, 1, 1);
+    cfg.blockDim = dim3(PAIR_THREADS, 1, 1);
     cfg.dynamicSmemBytes = PAIR_SMEM;
     int clusters = 0;
     if (cudaOccupancyMaxActiveClusters(&clusters, split_mma_pair_kernel, &cfg) != cudaSuccess || clusters < 1) {
@@ -951,7 +958,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
         break;
       }
       if (L.pair)
-        split_mma_pair_kernel<<<grid, MMA_THREADS, PAIR_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad,
+        split_mma_pair_kernel<<<grid, PAIR_THREADS, PAIR_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad,
                                                                    (int)L.N_pad, (int)L.nkc,
                                                                    (int)L.kblocks, L.nsub, status);
       else
