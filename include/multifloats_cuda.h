@@ -357,6 +357,11 @@ MULTIFLOATS_CUDA_API int mfcuda_reduce_combine(int kind, const void *parts, int6
  *     item of every problem; per problem a tile width N of 256, 128 or 64 and a
  *     shared K chunk (split-K when the batch is too small to fill the GPU);
  *     slices/target as in mfcuda_matmuldd_mm_split.  Operands 16-byte aligned.
+ *   form MFCUDA_FORM_CRT: the CRT (modular) split pipeline of
+ *     mfcuda_matmuldd_mm_crt in the same grouped launches (one item per
+ *     modulus, K chunk and tile); `slices` is the operand bits W (0, or 8 ..
+ *     110) and target as there.  Bit-identical to the single call for every
+ *     K chunk (residues of chunk sums add modulo each modulus).
  * tune != 0 times the candidate tile shapes of every new shape bucket on
  * synthetic problems and caches the winners in MFCUDA_AUTOTUNE_CACHE (default
  * $HOME/.cache/multifloats_b200/autotune.txt); tune == 0 uses cached winners or
@@ -368,7 +373,7 @@ typedef struct mfcuda_gemm_desc {
   int64_t m, k, n;
 } mfcuda_gemm_desc;
 typedef struct mfcuda_batch mfcuda_batch;
-enum { MFCUDA_FORM_PLAIN = 0, MFCUDA_FORM_SPLIT = 1 };
+enum { MFCUDA_FORM_PLAIN = 0, MFCUDA_FORM_SPLIT = 1, MFCUDA_FORM_CRT = 2 };
 MULTIFLOATS_CUDA_API int mfcuda_batch_create_gemm(const mfcuda_gemm_desc *descs, int64_t count,
                                                   int form, int64_t renorm_interval, int slices,
                                                   double target, int tune, mfcuda_batch **plan);
@@ -379,7 +384,8 @@ MULTIFLOATS_CUDA_API int mfcuda_batch_create_gemm(const mfcuda_gemm_desc *descs,
  * mfcuda_cmatmuldd_mm_split (one slice count from all four operands, each
  * operand sliced once, re = ArBr - AiBi and im = ArBi + AiBr combined in that
  * order), bit-identical to it when the plan's K chunk (mfcuda_batch_kchunk)
- * is the single call's 73 x 128. */
+ * is the single call's 73 x 128; MFCUDA_FORM_CRT runs the four products of
+ * mfcuda_cmatmuldd_mm_crt the same way (bit-identical to it). */
 MULTIFLOATS_CUDA_API int mfcuda_batch_create_cgemm(const mfcuda_gemm_desc *descs, int64_t count,
                                                    int form, int64_t renorm_interval, int slices,
                                                    double target, int tune, mfcuda_batch **plan);

@@ -37,6 +37,7 @@
 #include "common.cuh"
 #include "dd_device.cuh"
 #include "gemm_tile.cuh"
+#include "crt_device.cuh"
 #include "split_device.cuh"
 #include "tcgen05.cuh"
 
@@ -183,6 +184,9 @@ struct SProb {
   int8_t *As, *Bs;
   int32_t *D;
   Plan *plan;
+  int crt;       // CRT form (crt_device.cuh): slices are residues, items single products
+  int nsl;       // slice slots per operand: SMAX digits, or the most moduli the CRT plan can use
+  CrtConst *cc;  // the plan's reconstruction constants (CRT form)
 };
 // phases with a per-problem block count (prefix sums in a table); the
 // recombination runs in two launches: stores first, then the - / + updates
@@ -230,7 +234,10 @@ __global__ void __launch_bounds__(256) g_plan(const SProb *probs, int slices, do
   if (P.sigA2) add(P.sigA2, P.muA2, P.m, 0);
   add(P.sigB, P.muB, P.n, 1);
   if (P.sigB2) add(P.sigB2, P.muB2, P.n, 1);
-  plan_body(st, slices, target, P.plan);
+  if (P.crt)
+    crt_plan_body(st, slices, target, P.k, P.plan, P.cc);  // slices: the operand bits W (0 = from target)
+  else
+    plan_body(st, slices, target, P.plan);
 }
 __global__ void __launch_bounds__(256) g_slice_a(const SProb *probs, const int64_t *prefix, int nprob) {
   const int p = find_prob(prefix, nprob, blockIdx.x);
@@ -238,6 +245,25 @@ __global__ void __launch_bounds__(256) g_slice_a(const SProb *probs, const int64
   const int64_t l = blockIdx.x - prefix[p];
   const int64_t nbx = P.M_pad / 32;
   slice_a_body(P.A, P.m, P.k, P.astride, P.M_pad, P.K_pad, P.sigA, P.flagA, P.plan, P.As, l % nbx, l / nbx);
+}
+// CRT form: residues instead of digits (the transposing tile in dynamic shared memory)
+__global__ void __launch_bounds__(256) g_crt_slice_a(const SProb *probs, const int64_t *prefix, int nprob) {
+  extern __shared__ __align__(16) uint8_t crt_tile[];
+  const int p = find_prob(prefix, nprob, blockIdx.x);
+  const SProb &P = probs[p];
+  const int64_t l = blockIdx.x - prefix[p];
+  const int64_t nbx = P.M_pad / 32;
+  crt_slice_a_body(P.A, P.m, P.k, P.astride, P.M_pad, P.K_pad, P.sigA, P.flagA, P.plan, P.As, crt_tile, l % nbx,
+                   l / nbx);
+}
+__global__ void __launch_bounds__(256) g_crt_slice_b(const SProb *probs, const int64_t *prefix, int nprob) {
+  const int p = find_prob(prefix, nprob, blockIdx.x);
+  const SProb &P = probs[p];
+  const int64_t t = (int64_t)(blockIdx.x - prefix[p]) * 256 + threadIdx.x;
+  const int64_t per_col = P.K_pad / 8;
+  const int64_t j = t / per_col;
+  if (j < P.N_pad)
+    crt_slice_b_one(P.B, P.k, P.n, P.bstride, P.N_pad, P.K_pad, P.sigB, P.flagB, P.plan, P.Bs, j, (t % per_col) * 8);
 }
 // flat: thread t of the problem takes column t / (K_pad / 8), entries 8 (t % (K_pad / 8)) .. + 7
 __global__ void __launch_bounds__(256) g_slice_b(const SProb *probs, const int64_t *prefix, int nprob) {
@@ -264,6 +290,21 @@ __global__ void __launch_bounds__(kCombineThreads) g_combine(const SProb *probs,
                 P.cstride, P.mode, t % q, t / q);
 }
 
+// CRT form: thread t of the problem owns row t % m of columns 4 (t / m) .. + 3
+// (crt_combine4_body); the block's problem provides the constants.
+static int64_t crt_combine_blocks(int64_t m, int64_t n) {
+  return (m * ((n + 3) / 4) + kCombineThreads - 1) / kCombineThreads;
+}
+__global__ void __launch_bounds__(kCombineThreads) g_crt_combine(const SProb *probs, const int64_t *prefix, int nprob) {
+  __shared__ CrtShared cs;
+  const int p = find_prob(prefix, nprob, blockIdx.x);
+  const SProb &P = probs[p];
+  crt_load_shared(P.cc, P.plan->S, cs);
+  const int64_t t = (int64_t)(blockIdx.x - prefix[p]) * kCombineThreads + threadIdx.x;
+  crt_combine4_body(reinterpret_cast<const uint8_t *>(P.D), P.plan, cs, P.sigA, P.flagA, P.sigB, P.flagB, P.m,
+                    P.n, P.M_pad, P.N_pad, P.nkc, P.C, P.cstride, P.mode, t % P.m, 4 * (t / P.m));
+}
+
 struct GItem {
   int g, kc, tm, tn;
 };
@@ -271,7 +312,7 @@ __device__ __forceinline__ GItem decode_item(const SProb &P, int64_t local) {
   GItem it;
   const int ntiles = P.ntm * P.ntn;
   const int64_t per_g = (int64_t)P.nkc * ntiles;
-  it.g = SMAX - 1 - (int)(local / per_g);
+  it.g = P.nsl - 1 - (int)(local / per_g);
   const int64_t r = local % per_g;
   it.kc = (int)(r / ntiles);
   const int tile = (int)(r % ntiles);
@@ -348,7 +389,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         const SProb &P = probs[p];
         const int kb0 = it.kc * P.kcb, kb1 = min(P.kblocks, kb0 + P.kcb);
         const uint32_t bytes = (uint32_t)(A_STAGE + P.bn * BK);
-        for (int s = 0; s <= it.g && ok; ++s) {
+        for (int s = P.crt ? it.g : 0; s <= it.g && ok; ++s) {  // CRT: the single product A_g B_g
           for (int kb = kb0; kb < kb1; ++kb) {
             if (!wait_bar(&empty[stage], phase ^ 1, abort_flag)) {
               fail(1);
@@ -358,7 +399,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
             mftc::mbar_arrive_expect_tx(&full[stage], bytes);
             mftc::tma_load_3d(sA + stage * A_STAGE, &maps[2 * p], &full[stage], kb * BK, it.tm * BM, s);
             mftc::tma_load_3d(sB + stage * B_STAGE, &maps[2 * p + 1], &full[stage], kb * BK, it.tn * P.bn,
-                              it.g - s);
+                              P.crt ? s : it.g - s);
             armed[stage] = true;
             armed_parity[stage] = phase;
             if (++stage == NSTAGE) {
@@ -390,7 +431,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         if (!lookup(w, p, it)) continue;
         const SProb &P = probs[p];
         const int kb0 = it.kc * P.kcb, kb1 = min(P.kblocks, kb0 + P.kcb);
-        const uint32_t idesc = mftc::idesc_i8(BM, P.bn);
+        const uint32_t idesc = P.crt ? mftc::idesc_u8(BM, P.bn) : mftc::idesc_i8(BM, P.bn);  // CRT residues unsigned
         if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag)) {
           fail(2);
           break;
@@ -398,7 +439,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         mftc::tc_fence_after();
         const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
         uint32_t accumulate = 0;
-        for (int s = 0; s <= it.g && ok; ++s) {
+        for (int s = P.crt ? it.g : 0; s <= it.g && ok; ++s) {
           for (int kb = kb0; kb < kb1; ++kb) {
             if (!wait_bar(&full[stage], phase, abort_flag)) {
               fail(4);
@@ -449,15 +490,30 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         break;
       }
       mftc::tc_fence_after();
-      int32_t *dst_base = P.D + (((int64_t)(it.g * P.nkc + it.kc) * P.N_pad + (int64_t)it.tn * P.bn) * P.M_pad +
-                                 (int64_t)it.tm * BM + row);
-      for (int chunk = 0; chunk < P.bn / 32; ++chunk) {
-        uint32_t r[32];
-        mftc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * BN + chunk * 32), r);
-        mftc::tmem_wait_ld();
-        int32_t *dst = dst_base + (int64_t)chunk * 32 * P.M_pad;
+      const int64_t off = ((int64_t)(it.g * P.nkc + it.kc) * P.N_pad + (int64_t)it.tn * P.bn) * P.M_pad +
+                          (int64_t)it.tm * BM + row;
+      if (P.crt) {  // residues modulo m_g, four columns per 32-bit word (crt_device.cuh)
+        uint32_t *dst = reinterpret_cast<uint32_t *>(P.D) + crt_word_index(off, P.M_pad);
+        for (int chunk = 0; chunk < P.bn / 32; ++chunk) {
+          uint32_t r[32];
+          mftc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * BN + chunk * 32), r);
+          mftc::tmem_wait_ld();
 #pragma unroll
-        for (int q = 0; q < 32; ++q) __stcs(dst + (int64_t)q * P.M_pad, (int32_t)r[q]);  // evict-first: keep L2 for the slices
+          for (int g = 0; g < 8; ++g) {
+            __stcs(dst, crt_pack4(r[4 * g], r[4 * g + 1], r[4 * g + 2], r[4 * g + 3], it.g));
+            dst += P.M_pad;
+          }
+        }
+      } else {
+        int32_t *dst_base = P.D + off;
+        for (int chunk = 0; chunk < P.bn / 32; ++chunk) {
+          uint32_t r[32];
+          mftc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * BN + chunk * 32), r);
+          mftc::tmem_wait_ld();
+          int32_t *dst = dst_base + (int64_t)chunk * 32 * P.M_pad;
+#pragma unroll
+          for (int q = 0; q < 32; ++q) __stcs(dst + (int64_t)q * P.M_pad, (int32_t)r[q]);  // evict-first: keep L2 for the slices
+        }
       }
       mftc::tc_fence_before();
       __syncwarp();
@@ -682,10 +738,10 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   }();
   return fn;
 }
-static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, uint32_t box_rows) {
+static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, uint32_t box_rows, int nsl) {
   auto fn = encode_fn();
   if (!fn) return false;
-  cuuint64_t dims[3] = {(cuuint64_t)K_pad, (cuuint64_t)rows, (cuuint64_t)SMAX};
+  cuuint64_t dims[3] = {(cuuint64_t)K_pad, (cuuint64_t)rows, (cuuint64_t)nsl};
   cuuint64_t strides[2] = {(cuuint64_t)K_pad, (cuuint64_t)(rows * K_pad)};
   cuuint32_t box[3] = {(cuuint32_t)BK, box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
@@ -708,9 +764,10 @@ struct Spec {
   int a_src, b_src, plan_src, plan_a2, plan_b2;
 };
 
-// kcb: K chunk in blocks of 128 (shared by all products).
+// kcb: K chunk in blocks of 128 (shared by all products).  crt: the CRT form,
+// `slices` then being the operand bits W (0: chosen for `target`).
 static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices, double target,
-                              const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out) {
+                              const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out, bool crt) {
   // longest K first (stable: the products of one complex problem stay together)
   const int np = (int)specs.size();
   std::vector<int> order(np), pos(np);
@@ -729,7 +786,7 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
   size_t o_prefix = ar.take(sizeof(int64_t) * PH_COUNT * std::max(np, 1));
   size_t o_maps = ar.take(sizeof(CUtensorMap) * 2 * std::max(np, 1), 128);
   size_t o_status = ar.take(sizeof(int));
-  std::vector<size_t> o_plan(np, 0), o_as(np, 0), o_bs(np, 0), o_d(np);
+  std::vector<size_t> o_plan(np, 0), o_cc(np, 0), o_as(np, 0), o_bs(np, 0), o_d(np);
   std::vector<int64_t> rowA(np, -1), rowB(np, -1);  // statistics rows of owned operands
   int64_t rows_total = 0;
   std::vector<int64_t> prefix(PH_COUNT * (size_t)std::max(np, 1), 0);
@@ -759,19 +816,26 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
     P.nkc = (P.kblocks + P.kcb - 1) / P.kcb;
     P.ntm = (int)(P.M_pad / BM);
     P.ntn = (int)(P.N_pad / P.bn);
-    if (P.own_plan) o_plan[q] = ar.take(sizeof(Plan));
+    P.crt = crt ? 1 : 0;
+    P.nsl = crt ? crt_slices_max(g.k < 1 ? 1 : g.k, slices) : SMAX;
+    P.cc = nullptr;
+    if (P.own_plan) {
+      o_plan[q] = ar.take(sizeof(Plan));
+      if (crt) o_cc[q] = ar.take(sizeof(CrtConst));
+    }
     if (P.own_a) {
       rowA[q] = rows_total;
       rows_total += P.M_pad;
-      o_as[q] = ar.take((size_t)SMAX * P.M_pad * P.K_pad, 1024);
+      o_as[q] = ar.take((size_t)P.nsl * P.M_pad * P.K_pad, 1024);
     }
     if (P.own_b) {
       rowB[q] = rows_total;
       rows_total += P.N_pad;
-      o_bs[q] = ar.take((size_t)SMAX * P.N_pad * P.K_pad, 1024);
+      o_bs[q] = ar.take((size_t)P.nsl * P.N_pad * P.K_pad, 1024);
     }
-    o_d[q] = ar.take((size_t)SMAX * P.nkc * P.N_pad * P.M_pad * sizeof(int32_t));
-    const int64_t comb = combine_blocks(P.m, P.n);
+    // INT32 diagonal sums, or (CRT) byte residues four columns to a word
+    o_d[q] = ar.take((size_t)P.nsl * P.nkc * P.N_pad * P.M_pad * (crt ? 1 : sizeof(int32_t)));
+    const int64_t comb = crt ? crt_combine_blocks(P.m, P.n) : combine_blocks(P.m, P.n);
     const int64_t blocks[PH_COUNT] = {
         P.own_a ? ((P.m + 255) / 256) * ((P.k + 63) / 64) : 0,
         P.own_b && P.k > 0 ? (P.n + 7) / 8 : 0,
@@ -779,7 +843,7 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
         P.own_b ? (P.N_pad * (P.K_pad / 8) + 255) / 256 : 0,
         P.mode == 0 ? comb : 0,
         P.mode != 0 ? comb : 0,
-        (int64_t)SMAX * P.nkc * P.ntm * P.ntn};
+        (int64_t)P.nsl * P.nkc * P.ntm * P.ntn};
     for (int ph = 0; ph < PH_COUNT; ++ph) {
       prefix[(size_t)ph * np + q] = total[ph];
       total[ph] += blocks[ph];
@@ -810,7 +874,10 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
   // owned storage first, then the borrowed pointers
   for (int q = 0; q < np; ++q) {
     SProb &P = probs[q];
-    if (P.own_plan) P.plan = reinterpret_cast<Plan *>(base + o_plan[q]);
+    if (P.own_plan) {
+      P.plan = reinterpret_cast<Plan *>(base + o_plan[q]);
+      if (crt) P.cc = reinterpret_cast<CrtConst *>(base + o_cc[q]);
+    }
     if (P.own_a) {
       P.sigA = sig0 + rowA[q];
       P.muA = mu0 + rowA[q];
@@ -829,7 +896,10 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
   for (int q = 0; q < np; ++q) {
     SProb &P = probs[q];
     const Spec &g = sp[q];
-    if (!P.own_plan) P.plan = probs[g.plan_src].plan;
+    if (!P.own_plan) {
+      P.plan = probs[g.plan_src].plan;
+      P.cc = probs[g.plan_src].cc;
+    }
     if (!P.own_a) {
       const SProb &S = probs[g.a_src];
       P.sigA = S.sigA;
@@ -848,8 +918,8 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
     P.muA2 = g.plan_a2 >= 0 ? probs[g.plan_a2].muA : nullptr;
     P.sigB2 = g.plan_b2 >= 0 ? probs[g.plan_b2].sigB : nullptr;
     P.muB2 = g.plan_b2 >= 0 ? probs[g.plan_b2].muB : nullptr;
-    if (!make_map(&maps[2 * q], P.As, P.M_pad, P.K_pad, BM) ||
-        !make_map(&maps[2 * q + 1], P.Bs, P.N_pad, P.K_pad, (uint32_t)P.bn)) {
+    if (!make_map(&maps[2 * q], P.As, P.M_pad, P.K_pad, BM, P.nsl) ||
+        !make_map(&maps[2 * q + 1], P.Bs, P.N_pad, P.K_pad, (uint32_t)P.bn, P.nsl)) {
       destroy(b);
       return MFCUDA_ERR_CUDA;
     }
@@ -868,7 +938,13 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
   }
   std::call_once(g_gmma_attr, [] {
     cudaFuncSetAttribute(g_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
+    cudaFuncSetAttribute(g_crt_slice_a, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         CRT_NMAX * SA_ROWS * SA_STRIDE);
   });
+  // the residue tile of g_crt_slice_a holds the most moduli of any product
+  int nsl_max = 1;
+  for (int q = 0; q < np; ++q) nsl_max = std::max(nsl_max, probs[q].nsl);
+  const size_t crt_tile = (size_t)nsl_max * SA_ROWS * SA_STRIDE;
   int mma_grid = sm_count();
   if (mma_grid > total[PH_ITEMS]) mma_grid = (int)std::max<int64_t>(total[PH_ITEMS], 1);
   int rc = capture(b, [&](cudaStream_t cs) {
@@ -881,16 +957,23 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
     if (total[PH_SCAN_A]) g_scan_a<<<(unsigned)total[PH_SCAN_A], 256, 0, cs>>>(dp, dprefix + PH_SCAN_A * np, np);
     if (total[PH_SCAN_B]) g_scan_b<<<(unsigned)total[PH_SCAN_B], 256, 0, cs>>>(dp, dprefix + PH_SCAN_B * np, np);
     g_plan<<<np, 256, 0, cs>>>(dp, slices, target);
-    if (total[PH_SLICE_A])
+    if (total[PH_SLICE_A] && crt)
+      g_crt_slice_a<<<(unsigned)total[PH_SLICE_A], 256, crt_tile, cs>>>(dp, dprefix + PH_SLICE_A * np, np);
+    else if (total[PH_SLICE_A])
       g_slice_a<<<(unsigned)total[PH_SLICE_A], 256, 0, cs>>>(dp, dprefix + PH_SLICE_A * np, np);
-    if (total[PH_SLICE_B])
+    if (total[PH_SLICE_B] && crt)
+      g_crt_slice_b<<<(unsigned)total[PH_SLICE_B], 256, 0, cs>>>(dp, dprefix + PH_SLICE_B * np, np);
+    else if (total[PH_SLICE_B])
       g_slice_b<<<(unsigned)total[PH_SLICE_B], 256, 0, cs>>>(dp, dprefix + PH_SLICE_B * np, np);
     g_mma<<<mma_grid, MMA_THREADS, MMA_SMEM, cs>>>(dp, dmaps, dprefix + PH_ITEMS * np, np, total[PH_ITEMS],
                                                    b->status);
-    if (total[PH_COMBINE])
-      g_combine<<<(unsigned)total[PH_COMBINE], kCombineThreads, 0, cs>>>(dp, dprefix + PH_COMBINE * np, np);
-    if (total[PH_COMBINE2])
-      g_combine<<<(unsigned)total[PH_COMBINE2], kCombineThreads, 0, cs>>>(dp, dprefix + PH_COMBINE2 * np, np);
+    for (int ph : {PH_COMBINE, PH_COMBINE2}) {
+      if (!total[ph]) continue;
+      if (crt)
+        g_crt_combine<<<(unsigned)total[ph], kCombineThreads, 0, cs>>>(dp, dprefix + ph * np, np);
+      else
+        g_combine<<<(unsigned)total[ph], kCombineThreads, 0, cs>>>(dp, dprefix + ph * np, np);
+    }
   });
   if (rc != MFCUDA_OK) {
     destroy(b);
@@ -906,7 +989,7 @@ static bool split_args_ok(const mfcuda_gemm_desc &g) {
 
 // Real problems: one product each.  cfg[p] = tile width N (256, 128 or 64).
 static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, double target,
-                        const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out) {
+                        const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out, bool crt) {
   std::vector<Spec> specs;
   for (int64_t p = 0; p < count; ++p) {
     if (!split_args_ok(d[p])) return MFCUDA_ERR_UNSUPPORTED;
@@ -915,7 +998,7 @@ static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, do
                      static_cast<double *>(d[p].c), 1, 1, 1, 0, d[p].m, d[p].k, d[p].n, cfg[p], -1, -1, -1, -1,
                      -1});
   }
-  return create_split_specs(std::move(specs), count, slices, target, cfg, kcb_all, out);
+  return create_split_specs(std::move(specs), count, slices, target, cfg, kcb_all, out, crt);
 }
 
 // Complex problems (complex64x2 operands): four real products each, in the
@@ -923,7 +1006,7 @@ static int create_split(const mfcuda_gemm_desc *d, int64_t count, int slices, do
 // re - AiBi; im = ArBi, then im + AiBr), one plan from all four operands, each
 // operand sliced once.
 static int create_csplit(const mfcuda_gemm_desc *d, int64_t count, int slices, double target,
-                         const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out) {
+                         const std::vector<int> &cfg, int kcb_all, mfcuda_batch **out, bool crt) {
   std::vector<Spec> specs;
   for (int64_t p = 0; p < count; ++p) {
     if (!split_args_ok(d[p])) return MFCUDA_ERR_UNSUPPORTED;
@@ -938,7 +1021,7 @@ static int create_csplit(const mfcuda_gemm_desc *d, int64_t count, int slices, d
     specs.push_back({A, B + 2, Cm + 2, 2, 2, 2, 0, m, k, n, cfg[p], q, q + 1, q, -1, -1});        // im  = Ar Bi
     specs.push_back({A + 2, B, Cm + 2, 2, 2, 2, 2, m, k, n, cfg[p], q + 1, q, q, -1, -1});        // im += Ai Br
   }
-  return create_split_specs(std::move(specs), count, slices, target, cfg, kcb_all, out);
+  return create_split_specs(std::move(specs), count, slices, target, cfg, kcb_all, out, crt);
 }
 
 // ---- ragged elementwise -------------------------------------------------------
@@ -1065,11 +1148,11 @@ static int tune_bucket(int form, const Bucket &bk, int64_t ri) {
   int best = cands[0];
   double best_ms = 1e30;
   for (int cand : cands) {
-    if (form == 1 && cand > 64 && cand >= 2 * n) continue;  // wider than twice the problem: pure padding
+    if (form != 0 && cand > 64 && cand >= 2 * n) continue;  // wider than twice the problem: pure padding
     mfcuda_batch *b = nullptr;
     std::vector<int> cfg(copies, cand);
     int rc = form == 0 ? create_plain(descs.data(), copies, ri, cfg, &b)
-                       : create_split(descs.data(), copies, 0, 8.0, cfg, KC_BLOCKS, &b);
+                       : create_split(descs.data(), copies, 0, 8.0, cfg, KC_BLOCKS, &b, form == 2);
     if (rc != MFCUDA_OK) continue;
     double ms = time_plan(b, 2);
     destroy(b);
@@ -1092,7 +1175,8 @@ static std::string bucket_key(int form, const Bucket &b) {
   for (char *c = dev; *c; ++c)
     if (*c == ' ') *c = '_';
   char key[512];
-  std::snprintf(key, sizeof key, "%s:%s:%d:%d:%d", dev, form == 0 ? "plain" : "split", b.bm, b.bn, b.bk);
+  std::snprintf(key, sizeof key, "%s:%s:%d:%d:%d", dev, form == 0 ? "plain" : form == 1 ? "split" : "crt", b.bm,
+                b.bn, b.bk);
   return key;
 }
 
@@ -1151,13 +1235,15 @@ static std::vector<int> choose(int form, const mfcuda_gemm_desc *d, int64_t coun
 // Split-K rule: K chunks of at most KC_BLOCKS blocks (the INT32 bound); when
 // the whole batch has fewer items than four per SM, shorter chunks raise the
 // item count (the chunks' INT32 partials are summed exactly in the combine).
-static int choose_kcb(const mfcuda_gemm_desc *d, int64_t count, const std::vector<int> &cfg, int prods = 1) {
+// nsl(k): slice slots (and so items per tile) of a product with inner size k.
+template <class SlotFn>
+static int choose_kcb(const mfcuda_gemm_desc *d, int64_t count, const std::vector<int> &cfg, int prods, SlotFn nsl) {
   int64_t items = 0, kmax = 1;
   for (int64_t p = 0; p < count; ++p) {
     if (d[p].m <= 0 || d[p].n <= 0) continue;
     int64_t kb = (ru(std::max<int64_t>(d[p].k, 1), BK)) / BK;
     kmax = std::max(kmax, kb);
-    items += (int64_t)prods * SMAX * ((kb + KC_BLOCKS - 1) / KC_BLOCKS) * (ru(d[p].m, BM) / BM) *
+    items += (int64_t)prods * nsl(d[p].k) * ((kb + KC_BLOCKS - 1) / KC_BLOCKS) * (ru(d[p].m, BM) / BM) *
              (ru(d[p].n, cfg[p]) / cfg[p]);
   }
   const int64_t want = (int64_t)sm_count() * 4;
@@ -1177,8 +1263,12 @@ static int batch_create(const mfcuda_gemm_desc *descs, int64_t count, int form, 
   using namespace mfcuda;
   if (!plan || count < 0 || (count > 0 && !descs)) return MFCUDA_ERR_INVALID_ARG;
   *plan = nullptr;
-  if (form != MFCUDA_FORM_PLAIN && form != MFCUDA_FORM_SPLIT) return MFCUDA_ERR_INVALID_ARG;
+  if (form != MFCUDA_FORM_PLAIN && form != MFCUDA_FORM_SPLIT && form != MFCUDA_FORM_CRT)
+    return MFCUDA_ERR_INVALID_ARG;
   if (form == MFCUDA_FORM_SPLIT && (slices < 0 || slices > split::SMAX || slices == 1 || !(target > 0.0)))
+    return MFCUDA_ERR_INVALID_ARG;
+  if (form == MFCUDA_FORM_CRT &&
+      (slices < 0 || (slices > 0 && slices < 8) || slices > split::CRT_WMAX || !(target > 0.0)))
     return MFCUDA_ERR_INVALID_ARG;
   for (int64_t p = 0; p < count; ++p) {
     const mfcuda_gemm_desc &g = descs[p];
@@ -1191,9 +1281,12 @@ static int batch_create(const mfcuda_gemm_desc *descs, int64_t count, int form, 
     return batch::create_plain(descs, count, renorm_interval, std::vector<int>(count, 1), plan, true);
   std::vector<int> cfg = batch::choose(form, descs, count, tune, renorm_interval);
   if (form == MFCUDA_FORM_PLAIN) return batch::create_plain(descs, count, renorm_interval, cfg, plan);
-  int kcb = batch::choose_kcb(descs, count, cfg, complex ? 4 : 1);
-  if (complex) return batch::create_csplit(descs, count, slices, target, cfg, kcb, plan);
-  return batch::create_split(descs, count, slices, target, cfg, kcb, plan);
+  const bool crt = form == MFCUDA_FORM_CRT;
+  int kcb = batch::choose_kcb(descs, count, cfg, complex ? 4 : 1, [&](int64_t k) {
+    return crt ? split::crt_slices_max(k < 1 ? 1 : k, slices) : split::SMAX;
+  });
+  if (complex) return batch::create_csplit(descs, count, slices, target, cfg, kcb, plan, crt);
+  return batch::create_split(descs, count, slices, target, cfg, kcb, plan, crt);
 }
 
 MULTIFLOATS_CUDA_API int mfcuda_batch_create_gemm(const mfcuda_gemm_desc *descs, int64_t count, int form,

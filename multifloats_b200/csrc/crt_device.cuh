@@ -69,6 +69,14 @@ __host__ __device__ inline int crt_moduli(int W, int64_t k, const int *lg) {
   while (n < CRT_NMAX && lg[n] < need) ++n;
   return n;
 }
+// Most moduli the CRT form can need for inner dimension k (W <= bits, or
+// W <= CRT_WMAX when bits is 0): workspace sizing on the host.
+inline int crt_slices_max(int64_t k, int bits) {
+  const int need = 2 * (bits > 0 ? bits : CRT_WMAX) + ceil_log2(k < 1 ? 1 : k) + 2;
+  int n = 1;
+  while (n < CRT_NMAX && crt_lg_host[n] < need) ++n;
+  return n;
+}
 // 39-bit limbs holding |C'| < k 2^(2W) with its sign (two's complement).
 __host__ __device__ inline int crt_limbs(int W, int64_t k) {
   return (2 * W + ceil_log2(k) + 1 + CRT_LB - 1) / CRT_LB;

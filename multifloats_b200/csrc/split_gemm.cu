@@ -703,15 +703,6 @@ static int pair_nsub() {
   return v;
 }
 
-// Most moduli the CRT form can need for inner dimension k (W <= bits, or
-// W <= CRT_WMAX when bits is 0).
-static int crt_slices_max(int64_t k, int bits) {
-  const int need = 2 * (bits > 0 ? bits : CRT_WMAX) + ceil_log2(k < 1 ? 1 : k) + 2;
-  int n = 1;
-  while (n < CRT_NMAX && crt_lg_host[n] < need) ++n;
-  return n;
-}
-
 static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB, int nsl = SMAX) {
   Layout L;
   L.nsl = nsl;

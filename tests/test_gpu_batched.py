@@ -185,6 +185,8 @@ def test_batch_invalid_arguments(cuda_lib):
     assert cuda_lib.mfcuda_batch_create_gemm(d, 1, 0, 8, 0, 8.0, 0, C.byref(p)) == 1
     d[0].m = 2
     assert cuda_lib.mfcuda_batch_create_gemm(d, 1, 7, 8, 0, 8.0, 0, C.byref(p)) == 1  # bad form
+    assert cuda_lib.mfcuda_batch_create_gemm(d, 1, 2, 8, 5, 8.0, 0, C.byref(p)) == 1  # CRT bits below 8
+    assert cuda_lib.mfcuda_batch_create_gemm(d, 1, 2, 8, 111, 8.0, 0, C.byref(p)) == 1  # CRT bits above 110
     assert cuda_lib.mfcuda_batch_create_gemm(d, 1, 0, 8, 0, 8.0, 0, C.byref(p)) == 1  # NULL pointers
     assert cuda_lib.mfcuda_batch_run(None, None) == 1
 
@@ -280,5 +282,89 @@ def test_complex_split_batch_matches_single_call(cuda_lib, dev):
                                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
         assert rc == 0
         assert O.same_bits(to_host(bt.C[0]), to_host(c)).all()
+    finally:
+        cuda_lib.mfcuda_batch_destroy(p)
+
+
+# ---- CRT (modular) split form in the grouped pipeline ----
+@pytest.mark.parametrize("tune", [0, 1])
+def test_crt_batch_bit_exact(cuda_lib, dev, tune):
+    """Every problem equals the CRT restatement bit for bit, whatever K chunk
+    the plan chose (residues of chunk sums add modulo each modulus)."""
+    rng = np.random.default_rng(40 + tune)
+    shapes = _shapes(rng, 20, 4, 300)
+    bt = Batch(cuda_lib, dev, shapes, 2100, W.dd_uniform)
+    p = bt.plan(2, tune=tune)
+    try:
+        assert {cuda_lib.mfcuda_batch_config(p, i) for i in range(len(shapes))} <= {64, 128, 256}
+        bt.run(p)
+        for i, (m, k, n) in enumerate(shapes):
+            if m * n == 0:
+                continue
+            want, _ = O.crt_gemm(bt.hA[i], bt.hB[i], m, k, n)
+            assert O.same_bits(bt.result(i), want).all(), (i, m, k, n)
+        if tune:
+            assert ":crt:" in open(os.environ["MFCUDA_AUTOTUNE_CACHE"]).read()
+    finally:
+        cuda_lib.mfcuda_batch_destroy(p)
+
+
+def test_crt_batch_fixed_bits_and_split_k(cuda_lib, dev):
+    """A forced operand width, and one tall-K product whose plan shortens the K
+    chunk: still the restatement's bits."""
+    shapes = [(64, 6000, 40), (130, 700, 33)]
+    bt = Batch(cuda_lib, dev, shapes, 2300, W.dd_uniform)
+    p = bt.plan(2, slices=64)
+    try:
+        assert cuda_lib.mfcuda_batch_kchunk(p) < 73 * 128
+        bt.run(p)
+        for i, (m, k, n) in enumerate(shapes):
+            want, info = O.crt_gemm(bt.hA[i], bt.hB[i], m, k, n, bits=64)
+            assert info[3] == 64
+            assert O.same_bits(bt.result(i), want).all(), (i, m, k, n)
+    finally:
+        cuda_lib.mfcuda_batch_destroy(p)
+
+
+def test_crt_batch_matches_single_call(cuda_lib, dev):
+    import torch
+
+    shapes = [(300, 500, 200), (129, 257, 65)]
+    bt = Batch(cuda_lib, dev, shapes, 2500, W.dd_uniform)
+    p = bt.plan(2)
+    try:
+        bt.run(p)
+        for i, (m, k, n) in enumerate(shapes):
+            c = torch.empty(2 * m * n, dtype=torch.float64, device=dev)
+            rc = cuda_lib.mfcuda_matmuldd_mm_crt(bt.A[i].data_ptr(), bt.B[i].data_ptr(), c.data_ptr(), m, k, n, 0,
+                                                 8.0, None, 0, None,
+                                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+            assert rc == 0
+            assert O.same_bits(bt.result(i), to_host(c)).all(), i
+    finally:
+        cuda_lib.mfcuda_batch_destroy(p)
+
+
+def test_complex_crt_batch_bit_exact(cuda_lib, dev):
+    import torch
+
+    rng = np.random.default_rng(44)
+    shapes = _shapes(rng, 12, 4, 240)
+    bt = CBatch(cuda_lib, dev, shapes, 2700, R=8)
+    p = bt.plan(2)
+    try:
+        bt.run(p)
+        for i, (m, k, n) in enumerate(shapes):
+            if m * n == 0:
+                continue
+            want, _ = O.crt_cgemm(bt.hA[i], bt.hB[i], m, k, n)
+            assert O.same_bits(to_host(bt.C[i]), want).all(), (i, m, k, n)
+        i = max(range(len(shapes)), key=lambda q: shapes[q][0] * shapes[q][1] * shapes[q][2])
+        m, k, n = shapes[i]
+        c = torch.empty(4 * m * n, dtype=torch.float64, device=dev)
+        rc = cuda_lib.mfcuda_cmatmuldd_mm_crt(bt.A[i].data_ptr(), bt.B[i].data_ptr(), c.data_ptr(), m, k, n, 0, 8.0,
+                                              None, 0, None, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == 0
+        assert O.same_bits(to_host(bt.C[i]), to_host(c)).all()
     finally:
         cuda_lib.mfcuda_batch_destroy(p)
