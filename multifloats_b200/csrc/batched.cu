@@ -290,19 +290,21 @@ __global__ void __launch_bounds__(kCombineThreads) g_combine(const SProb *probs,
                 P.cstride, P.mode, t % q, t / q);
 }
 
-// CRT form: thread t of the problem owns row t % m of columns 4 (t / m) .. + 3
-// (crt_combine4_body); the block's problem provides the constants.
+// CRT form: the tensor-core reconstruction (crt_combine_tc_body), a block
+// per 128 rows and CTC_QUADS column quads of a problem.
 static int64_t crt_combine_blocks(int64_t m, int64_t n) {
-  return (m * ((n + 3) / 4) + kCombineThreads - 1) / kCombineThreads;
+  return ((m + CTC_THREADS - 1) / CTC_THREADS) * (((n + 3) / 4 + CTC_QUADS - 1) / CTC_QUADS);
 }
-__global__ void __launch_bounds__(kCombineThreads) g_crt_combine(const SProb *probs, const int64_t *prefix, int nprob) {
-  __shared__ CrtShared cs;
+__global__ void __launch_bounds__(CTC_THREADS) g_crt_combine(const SProb *probs, const int64_t *prefix, int nprob,
+                                                             int *status) {
+  extern __shared__ uint8_t ctc_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(ctc_raw) + 1023) & ~uintptr_t(1023));
   const int p = find_prob(prefix, nprob, blockIdx.x);
   const SProb &P = probs[p];
-  crt_load_shared(P.cc, P.plan->S, cs);
-  const int64_t t = (int64_t)(blockIdx.x - prefix[p]) * kCombineThreads + threadIdx.x;
-  crt_combine4_body(reinterpret_cast<const uint8_t *>(P.D), P.plan, cs, P.sigA, P.flagA, P.sigB, P.flagB, P.m,
-                    P.n, P.M_pad, P.N_pad, P.nkc, P.C, P.cstride, P.mode, t % P.m, 4 * (t / P.m));
+  const int64_t l = blockIdx.x - prefix[p], nbx = (P.m + CTC_THREADS - 1) / CTC_THREADS;
+  crt_combine_tc_body(reinterpret_cast<const uint8_t *>(P.D), P.plan, P.cc, P.sigA, P.flagA, P.sigB, P.flagB, P.m,
+                      P.n, P.M_pad, P.N_pad, P.nkc, P.k, P.C, P.cstride, P.mode, (l % nbx) * CTC_THREADS,
+                      (l / nbx) * CTC_QUADS, smem, status);
 }
 
 struct GItem {
@@ -940,6 +942,8 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
     cudaFuncSetAttribute(g_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
     cudaFuncSetAttribute(g_crt_slice_a, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          CRT_NMAX * SA_ROWS * SA_STRIDE);
+    cudaFuncSetAttribute(g_crt_combine, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         crt_tc_smem((CRT_NMAX + 31) / 32));
   });
   // the residue tile of g_crt_slice_a holds the most moduli of any product
   int nsl_max = 1;
@@ -970,7 +974,8 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
     for (int ph : {PH_COMBINE, PH_COMBINE2}) {
       if (!total[ph]) continue;
       if (crt)
-        g_crt_combine<<<(unsigned)total[ph], kCombineThreads, 0, cs>>>(dp, dprefix + ph * np, np);
+        g_crt_combine<<<(unsigned)total[ph], CTC_THREADS, crt_tc_smem((nsl_max + 31) / 32), cs>>>(
+            dp, dprefix + ph * np, np, b->status);
       else
         g_combine<<<(unsigned)total[ph], kCombineThreads, 0, cs>>>(dp, dprefix + ph * np, np);
     }

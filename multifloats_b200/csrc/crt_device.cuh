@@ -11,6 +11,10 @@
 //   C' = sum_t r_t e_t - q M,   e_t = (M / m_t) ((M / m_t)^-1 mod m_t),
 //   r_t = (X Y^T mod m_t) in [0, m_t),  q = round(sum_t r_t e_t / M),
 // which is exact because the moduli are chosen with M >= 4 k 2^(2W) > 4 |C'|.
+// The sums over t are themselves a small u8 x u8 matrix product (residues
+// times the bytes of e_t and of c_t = e_t / M in fixed point), so the
+// reconstruction runs on the tensor cores too (crt_combine_tc_body), with the
+// carries, q M and the sign in 32-bit integer limbs.
 // C' is then converted to a double-double (crt_to_dd: hi = C' rounded to 53
 // bits, lo the rest summed in doubles, renormalised) and scaled by
 // 2^(sigma_i + tau_j - 2W).  Compared with the digit-sliced form (S(S+1)/2 slice products for S
@@ -29,24 +33,22 @@
 
 #include "split_device.cuh"  // first: dd_device.cuh defines MF_TABLE as device constant memory
 #include "crt_tables.h"
+#include "tcgen05.cuh"
 
 namespace mfcuda {
 namespace split {
 
 constexpr int CRT_NL = 8;  // most 32-bit limbs of a reconstruction (256 bits)
-constexpr int CRT_BATCH = 9;  // moduli whose residues a reconstruction thread loads at once
 constexpr int CRT_WMAX = 110;
 
-// Reconstruction constants of the plan's N moduli, computed on the device.
-// The reconstruction sums r_t e_t in 39-bit limbs held in doubles: a residue
-// (< 2^8) times a limb (< 2^39) is exact, and so are sums of up to 36 such
-// products (< 2^53), so the FP64 pipe does the multiply-adds exactly.
-constexpr int CRT_LB = 39;   // bits per reconstruction limb
-constexpr int CRT_NL39 = 7;  // limbs: 273 bits >= 2W + log2(k) + 1 for W <= 110, k < 2^31
+// Reconstruction constants of the plan's N moduli, computed on the device:
+// e_t = (M / m_t) ((M / m_t)^-1 mod m_t) and M = prod m_t modulo 2^256 in
+// 32-bit limbs, and c_t = e_t / M = ((M / m_t)^-1 mod m_t) / m_t as 24-bit
+// fixed point, round(c_t 2^24).
 struct CrtConst {
-  double e[CRT_NMAX][CRT_NL39];  // e_t mod 2^273, 39-bit limbs
-  double M[CRT_NL39];            // M mod 2^273, 39-bit limbs
-  double c[CRT_NMAX];            // ((M / m_t)^-1 mod m_t) / m_t, rounded: q = round(sum_t r_t c_t)
+  uint32_t ew[CRT_NMAX][CRT_NL];
+  uint32_t Mw[CRT_NL];
+  uint32_t cfix[CRT_NMAX];
 };
 
 // ceil(log2 k) for k >= 1.
@@ -77,17 +79,12 @@ inline int crt_slices_max(int64_t k, int bits) {
   while (n < CRT_NMAX && crt_lg_host[n] < need) ++n;
   return n;
 }
-// 39-bit limbs holding |C'| < k 2^(2W) with its sign (two's complement).
-__host__ __device__ inline int crt_limbs(int W, int64_t k) {
-  return (2 * W + ceil_log2(k) + 1 + CRT_LB - 1) / CRT_LB;
-}
-// Bits [39 l, 39 l + 39) of the little-endian 32-bit limbs v (>= 11 limbs), as a double.
-__device__ __forceinline__ double limb39(const uint32_t *v, int l) {
-  const int b = CRT_LB * l, w = b / 32, o = b % 32;
-  uint64_t x = ((uint64_t)v[w + 1] << 32) | v[w];
-  x >>= o;
-  if (o + CRT_LB > 64) x |= (uint64_t)v[w + 2] << (64 - o);
-  return (double)(x & ((1ull << CRT_LB) - 1));
+// Bytes of the reconstruction (a multiple of 4): C' is computed modulo
+// 2^(8 nbe) with nbe = 4 ceil(need / 32), need = 2W + ceil(log2 k) + 2 the
+// bound the moduli are chosen for, so |C'| < 2^(8 nbe - 2) and bit 8 nbe - 1
+// is the sign.
+__host__ __device__ inline int crt_tc_bytes(int W, int64_t k) {
+  return 4 * ((2 * W + ceil_log2(k) + 2 + 31) / 32);
 }
 
 // Inverse of a modulo m (gcd(a, m) = 1, m <= 256), extended Euclid.
@@ -146,7 +143,7 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
     plan->rho_a = ra;
     plan->rho_b = rb;
     plan->crt = 1;
-    plan->nl = crt_limbs(W, k);
+    plan->nl = crt_tc_bytes(W, k) / 4;
     sh_n = n;
   }
   __syncthreads();
@@ -171,26 +168,22 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
       rem = (rem * (ms % mt)) % mt;
     }
     const uint32_t inv = inv_mod_small(rem, mt);
-    uint32_t ev[CRT_NL + 3];  // e_t mod 2^288 (9 limbs) and two zero limbs for limb39
+    uint32_t ev[CRT_NL + 1];  // e_t mod 2^288
     uint64_t carry = 0;
     for (int l = 0; l <= CRT_NL; ++l) {
       const uint64_t v = (uint64_t)q[l] * inv + carry;
       ev[l] = (uint32_t)v;
       carry = v >> 32;
     }
-    ev[CRT_NL + 1] = ev[CRT_NL + 2] = 0;
-    for (int l = 0; l < CRT_NL39; ++l) cc->e[t][l] = limb39(ev, l);
-    cc->c[t] = (double)inv / (double)mt;
+    for (int l = 0; l < CRT_NL; ++l) cc->ew[t][l] = ev[l];
+    cc->cfix[t] = (uint32_t)((((uint64_t)inv << 24) + mt / 2) / mt);
     if (t == 0) {  // M = (M / m_0) m_0
-      uint32_t mv[CRT_NL + 3];
       uint64_t cy = 0;
-      for (int l = 0; l <= CRT_NL; ++l) {
+      for (int l = 0; l < CRT_NL; ++l) {
         const uint64_t v = (uint64_t)q[l] * mt + cy;
-        mv[l] = (uint32_t)v;
+        cc->Mw[l] = (uint32_t)v;
         cy = v >> 32;
       }
-      mv[CRT_NL + 1] = mv[CRT_NL + 2] = 0;
-      for (int l = 0; l < CRT_NL39; ++l) cc->M[l] = limb39(mv, l);
     }
   }
   __syncthreads();
@@ -403,19 +396,28 @@ __device__ __forceinline__ void crt_to_dd(const uint32_t *limb, int nl, double &
   e = E + 107;
 }
 
-// Reconstruction constants in shared memory.
-struct CrtShared {
-  double e[CRT_NMAX][CRT_NL39];
-  double M[CRT_NL39];
-  double c[CRT_NMAX];
-};
-// Block prologue: the plan's constants into shared memory.
-__device__ __forceinline__ void crt_load_shared(const CrtConst *cc, int n, CrtShared &cs) {
-  for (int x = threadIdx.x; x < n * CRT_NL39; x += blockDim.x)
-    cs.e[x / CRT_NL39][x % CRT_NL39] = cc->e[x / CRT_NL39][x % CRT_NL39];
-  for (int x = threadIdx.x; x < CRT_NL39; x += blockDim.x) cs.M[x] = cc->M[x];
-  for (int x = threadIdx.x; x < n; x += blockDim.x) cs.c[x] = cc->c[x];
-  __syncthreads();
+// Writes the two's complement integer C' held in CRT_NL limbs, times
+// 2^shift, as a DD to dst (NaN when `nan`); mode 0 stores it, 1 subtracts it
+// from the DD at dst, 2 adds it.
+__device__ __forceinline__ void crt_emit(const uint32_t (&limb)[CRT_NL], bool nan, int shift,
+                                         double *__restrict__ dst, int mode) {
+  double2 out;
+  if (nan) {
+    out = make_double2(CUDART_NAN, 0.0);
+  } else {
+    double hi, lo;
+    int e;
+    crt_to_dd(limb, CRT_NL, hi, lo, e);
+    out = make_double2(scale2(hi, e + shift), scale2(lo, e + shift));
+  }
+  double2 *d2 = reinterpret_cast<double2 *>(dst);
+  if (mode != 0) {
+    const double2 prev = *d2;
+    const mfdev::dd p = mfdev::make(out.x, out.y), pv = mfdev::make(prev.x, prev.y);
+    const mfdev::dd res = mode == 1 ? mfdev::dd_sub(pv, p) : mfdev::dd_add(pv, p);
+    out = make_double2(res.hi, res.lo);
+  }
+  __stcs(d2, out);
 }
 
 // Residue layout of one product (modulus t, K chunk kc): N_pad x M_pad bytes,
@@ -442,132 +444,224 @@ __device__ __forceinline__ uint32_t crt_pack4(uint32_t v0, uint32_t v1, uint32_t
                      __byte_perm(crt_mod_small(v2, t), crt_mod_small(v3, t), 0x0040), 0x5410);
 }
 
-// Row i of columns j0 .. j0+3 (j0 % 4 == 0): the residues r_t (one 32-bit load
-// per modulus and K chunk from the column-quad layout of crt_word_index), then
-//   q = round(sum_t r_t c_t),  C' = sum_t r_t e_t - q M  in 39-bit limbs,
-// every limb an exact FP64 multiply-add (see CRT_LB), carried in int64 and
-// repacked into 32-bit limbs; the DD conversion and exact scaling; `mode` as
-// the digit-sliced combine.
-__device__ __forceinline__ void crt_combine4_body(const uint8_t *__restrict__ D8, const Plan *plan,
-                                                  const CrtShared &cs, const int *sigA, const int *flagA,
-                                                  const int *sigB, const int *flagB, int64_t M, int64_t N,
-                                                  int64_t M_pad, int64_t N_pad, int nkc, double *__restrict__ C,
-                                                  int64_t cstride, int mode, int64_t i, int64_t j0) {
-  const int n = plan->S, nl = plan->nl, W = plan->W;
-  if (i >= M || j0 >= N) return;
-  const int64_t kstride = N_pad * M_pad / 4, gstride = (int64_t)nkc * kstride;  // in 32-bit words
-  const uint32_t *src = reinterpret_cast<const uint32_t *>(D8) + (j0 / 4) * M_pad + i;
-  double acc[4][CRT_NL39], f[4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    f[r] = 0.0;
-#pragma unroll
-    for (int l = 0; l < CRT_NL39; ++l) acc[r][l] = 0.0;
+// ---- reconstruction on the tensor cores ---------------------------------------
+// The sums over moduli are an integer matrix product: for an output with
+// residues r_t, the column sums
+//   S_b = sum_t r_t E[t][b]   (E[t][b] = byte b of e_t mod 2^(8 nbe) for b < nbe,
+//                              byte b - nbe of round(c_t 2^24) for the next 3)
+// are exact in INT32 (< 36 * 255^2), so
+//   V = sum_{b < nbe} S_b 2^(8b) = sum_t r_t e_t  (mod 2^(8 nbe)),
+//   q = round((S_nbe + S_nbe+1 2^8 + S_nbe+2 2^16) / 2^24)  (error < 36 * 255 * 2^-25 < 1/4),
+//   C' = V - q M  (mod 2^(8 nbe)),
+// and |C'| < 2^(8 nbe - 2) makes bit 8 nbe - 1 the sign.  One tcgen05 u8 x u8
+// MMA per output column of a 128-row tile gives the S_b of 128 outputs.
+// nbe = crt_tc_bytes(W, k).
+// MMA columns: nbe + 3 rounded up to 16 (32 or 48).
+__host__ __device__ inline int crt_tc_cols(int nbe) { return (nbe + 3 + 15) / 16 * 16; }
+constexpr int CTC_THREADS = 128;                   // one output row per thread and TMEM lane
+constexpr int CTC_QUADS = 8;                       // column quads per CTA
+constexpr int CTC_B_BYTES = 48 * 128;              // E tile: up to 48 rows of 128 bytes (swizzled)
+constexpr int CTC_A_OFF = 8192;                    // residue tiles (1024-aligned), 16 KiB per 32 moduli
+__host__ __device__ constexpr int crt_tc_smem(int ktmax) { return CTC_A_OFF + ktmax * 16384 + 1024; }
+
+// 16 bytes at logical chunk `chunk` (0..7) of row `row` of a K-major tile with
+// 128-byte rows and the 128-byte swizzle (8-row atoms of 1024 bytes).
+__device__ __forceinline__ void sw128_store16(uint8_t *tile, int row, int chunk, uint4 v) {
+  *reinterpret_cast<uint4 *>(tile + (row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4)) = v;
+}
+// Bytes c of the four words a, b, c, d (one residue word per modulus holds
+// four columns) regrouped per column: out[c] = {a_c, b_c, c_c, d_c}.
+__device__ __forceinline__ void crt_transpose4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t (&o)[4]) {
+  const uint32_t ab0 = __byte_perm(a, b, 0x5140), ab1 = __byte_perm(a, b, 0x7362);
+  const uint32_t cd0 = __byte_perm(c, d, 0x5140), cd1 = __byte_perm(c, d, 0x7362);
+  o[0] = __byte_perm(ab0, cd0, 0x5410);
+  o[1] = __byte_perm(ab0, cd0, 0x7632);
+  o[2] = __byte_perm(ab1, cd1, 0x5410);
+  o[3] = __byte_perm(ab1, cd1, 0x7632);
+}
+
+// CTA of CTC_THREADS threads: rows i0 .. i0+127 of column quads qd0 ..
+// qd0+CTC_QUADS-1 (thread T: row i0+T, columns 4 qd .. 4 qd + 3).  `smem`
+// is 1024-aligned, crt_tc_smem(ceil(n / 32)) bytes.  `status` receives
+// MFCUDA_ERR_TIMEOUT-style bit 2 if a bounded wait for the MMAs expires.
+__device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ D8, const Plan *plan,
+                                                    const CrtConst *cc, const int *sigA, const int *flagA,
+                                                    const int *sigB, const int *flagB, int64_t M, int64_t N,
+                                                    int64_t M_pad, int64_t N_pad, int nkc, int64_t k,
+                                                    double *__restrict__ C, int64_t cstride, int mode,
+                                                    int64_t i0, int64_t qd0, uint8_t *smem, int *status) {
+  const int T = threadIdx.x, warp = T >> 5;
+  const int n = plan->S, W = plan->W;
+  const int ktn = (n + 31) / 32;
+  const int nbe = crt_tc_bytes(W, k), nb = crt_tc_cols(nbe);
+  const uint32_t ncols = 4 * nb <= 128 ? 128u : 256u;
+  uint8_t *sB = smem;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + CTC_B_BYTES);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  uint8_t *sA = smem + CTC_A_OFF;
+  if (T == 0) {
+    mftc::mbar_init(bar, 1);
+    mftc::fence_mbar_init();
   }
-  // moduli in batches of CRT_BATCH: the batch's loads are all in flight before
-  // its arithmetic
-  for (int t0 = 0; t0 < n; t0 += CRT_BATCH) {
-    uint32_t wv[CRT_BATCH];
+  if (warp == 0) {
+    mftc::tmem_alloc(tslot, ncols);
+    mftc::tmem_relinquish();
+  }
+  // the E tile: row b = T holds E[t][b] at byte t (moduli 32 kt .. in bytes 32 kt ..)
+  if (T < 48) {
+    for (int kt = 0; kt < ktn; ++kt)
+      for (int h = 0; h < 2; ++h) {
+        uint32_t w4[4];
 #pragma unroll
-    for (int u = 0; u < CRT_BATCH; ++u) {
-      const int t = t0 + u;
-      if (t >= n) {
-        wv[u] = 0;
-      } else if (nkc == 1) {
-        wv[u] = __ldcs(src + t * gstride);
-      } else {  // per-row sums of the chunks' residues, reduced again
-        uint32_t sum[4] = {0, 0, 0, 0};
-        for (int kc = 0; kc < nkc; ++kc) {
-          const uint32_t w = __ldcs(src + t * gstride + kc * kstride);
+        for (int q = 0; q < 4; ++q) {
+          uint32_t word = 0;
 #pragma unroll
-          for (int r = 0; r < 4; ++r) sum[r] += (w >> (8 * r)) & 0xFFu;
-        }
-        uint32_t packed = 0;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) packed |= crt_mod_small(sum[r], t) << (8 * r);
-        wv[u] = packed;
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < CRT_BATCH; ++u) {
-      const int t = t0 + u;
-      if (t < n) {
-        const double ct = cs.c[t];
-        double rd[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          // the residue byte as a double: 2^52 + r_t exactly, minus 2^52
-          rd[r] = mfdev::sub(__hiloint2double(0x43300000, (int)((wv[u] >> (8 * r)) & 0xFFu)), 0x1p52);
-          f[r] = mfdev::fma_(rd[r], ct, f[r]);
-        }
-        // each limb constant loaded once for the thread's four rows
-#pragma unroll
-        for (int l = 0; l < CRT_NL39; ++l)
-          if (l < nl) {
-            const double el = cs.e[t][l];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) acc[r][l] = mfdev::fma_(rd[r], el, acc[r][l]);
+          for (int bb = 0; bb < 4; ++bb) {
+            const int t = 32 * kt + 16 * h + 4 * q + bb;
+            uint32_t v = 0;
+            if (t < n && T < nb) {
+              if (T < nbe)
+                v = (cc->ew[t][T >> 2] >> (8 * (T & 3))) & 0xFFu;
+              else if (T < nbe + 3)
+                v = (cc->cfix[t] >> (8 * (T - nbe))) & 0xFFu;
+            }
+            word |= v << (8 * bb);
           }
+          w4[q] = word;
+        }
+        sw128_store16(sB, T, 2 * kt + h, make_uint4(w4[0], w4[1], w4[2], w4[3]));
+      }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mftc::tc_fence_before();
+  __syncthreads();
+  mftc::tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = mftc::idesc_u8(128, nb);
+  const int64_t i = i0 + T;
+  const bool row_ok = i < M;
+  const int sa = row_ok ? sigA[i] : 0, fa = row_ok ? flagA[i] : 1;
+  const int64_t nq = (N + 3) / 4;
+  const int64_t kstride = N_pad * M_pad / 4, gstride = (int64_t)nkc * kstride;  // in 32-bit words
+  uint32_t Mw[CRT_NL];
+#pragma unroll
+  for (int w = 0; w < CRT_NL; ++w) Mw[w] = cc->Mw[w];
+  uint32_t phase = 0;
+  // the residue words of column quad qd (modulus t: four columns in a word)
+  auto load_words = [&](int64_t qd, uint32_t (&wv)[CRT_NMAX]) {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(D8) + qd * M_pad + (row_ok ? i : 0);
+#pragma unroll
+    for (int t = 0; t < CRT_NMAX; ++t) {
+      uint32_t w = 0;
+      if (row_ok && t < n) {
+        if (nkc == 1) {
+          w = __ldcs(src + t * gstride);
+        } else {  // per-column sums of the chunks' residues, reduced again
+          uint32_t sum[4] = {0, 0, 0, 0};
+          for (int kc = 0; kc < nkc; ++kc) {
+            const uint32_t v = __ldcs(src + t * gstride + kc * kstride);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) sum[r] += (v >> (8 * r)) & 0xFFu;
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) w |= crt_mod_small(sum[r], t) << (8 * r);
+        }
+      }
+      wv[t] = w;
+    }
+  };
+  uint32_t wv[CRT_NMAX];
+  const int64_t qend = min(qd0 + CTC_QUADS, nq);
+  if (qd0 < qend) load_words(qd0, wv);
+  for (int64_t qd = qd0; qd < qend; ++qd) {
+    // residues of the four outputs into the A tiles: row T, column c at bytes
+    // [32 c, 32 c + 32) of tile kt (moduli 32 kt ..)
+#pragma unroll
+    for (int kt = 0; kt < (CRT_NMAX + 31) / 32; ++kt) {
+      if (kt >= ktn) break;
+      uint32_t x[4][8];
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {
+        uint32_t o[4];
+        const int t = 32 * kt + 4 * g;
+        crt_transpose4(t < CRT_NMAX ? wv[t] : 0u, t + 1 < CRT_NMAX ? wv[t + 1] : 0u,
+                       t + 2 < CRT_NMAX ? wv[t + 2] : 0u, t + 3 < CRT_NMAX ? wv[t + 3] : 0u, o);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) x[c][g] = o[c];
+      }
+      uint8_t *tile = sA + kt * 16384;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        sw128_store16(tile, T, 2 * c, make_uint4(x[c][0], x[c][1], x[c][2], x[c][3]));
+        sw128_store16(tile, T, 2 * c + 1, make_uint4(x[c][4], x[c][5], x[c][6], x[c][7]));
       }
     }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mftc::tc_fence_before();
+    __syncthreads();
+    if (T == 0) {
+      mftc::tc_fence_after();
+      for (int c = 0; c < 4; ++c)
+        for (int kt = 0; kt < ktn; ++kt)
+          mftc::umma_i8(tmem + (uint32_t)(c * nb), mftc::smem_desc_k_sw128(mftc::smem_u32(sA + kt * 16384 + 32 * c)),
+                        mftc::smem_desc_k_sw128(mftc::smem_u32(sB + 32 * kt)), idesc, kt > 0 ? 1u : 0u);
+      mftc::umma_commit(bar);
+    }
+    if (qd + 1 < qend) load_words(qd + 1, wv);  // in flight during the MMAs and this quad's outputs
+    const bool ok = mftc::mbar_wait(bar, phase, 1u << 22);
+    phase ^= 1;
+    if (__syncthreads_or(!ok)) {  // uniform: every thread leaves together
+      if (T == 0) atomicOr(status, 2);  // a bounded wait expired
+      break;
+    }
+    mftc::tc_fence_after();
+    const int4 sb4 = *reinterpret_cast<const int4 *>(sigB + 4 * qd);
+    const int4 fb4 = *reinterpret_cast<const int4 *>(flagB + 4 * qd);
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+      uint32_t S[48];
+#pragma unroll
+      for (int b = 32; b < 48; ++b) S[b] = 0;
+      mftc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * nb), *reinterpret_cast<uint32_t(*)[32]>(S));
+      if (nb > 32)
+        mftc::tmem_ld_32x32b_x16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * nb + 32),
+                                 *reinterpret_cast<uint32_t(*)[16]>(S + 32));
+      mftc::tmem_wait_ld();
+      const int64_t j = 4 * qd + c;
+      if (!row_ok || j >= N) continue;
+      // q from the three fixed-point columns after the nbe limb bytes
+      uint64_t Q = 0;
+#pragma unroll
+      for (int L = 1; L <= CRT_NL; ++L)
+        if (4 * L == nbe)
+          Q = (uint64_t)S[4 * L] + ((uint64_t)S[4 * L + 1] << 8) + ((uint64_t)S[4 * L + 2] << 16);
+      const uint32_t q = (uint32_t)((Q + (1u << 23)) >> 24);
+      uint32_t limb[CRT_NL];
+      int64_t carry = 0;
+#pragma unroll
+      for (int w = 0; w < CRT_NL; ++w) {
+        const uint64_t lo = S[4 * w] + ((uint64_t)S[4 * w + 1] << 8);
+        const uint64_t hi = S[4 * w + 2] + ((uint64_t)S[4 * w + 3] << 8);
+        const int64_t v = (int64_t)(lo + (hi << 16)) - (int64_t)((uint64_t)q * Mw[w]) + carry;
+        limb[w] = (uint32_t)v;
+        carry = v >> 32;  // arithmetic shift
+      }
+      // C' mod 2^(8 nbe): the top bit of limb nbe / 4 - 1 is the sign, copied above
+      uint32_t top = 0;
+#pragma unroll
+      for (int w = 0; w < CRT_NL; ++w) top = 4 * (w + 1) == nbe ? limb[w] : top;
+      const uint32_t fill = (top >> 31) ? 0xFFFFFFFFu : 0u;
+#pragma unroll
+      for (int w = 0; w < CRT_NL; ++w) limb[w] = 4 * w < nbe ? limb[w] : fill;
+      const int sbc = c == 0 ? sb4.x : c == 1 ? sb4.y : c == 2 ? sb4.z : sb4.w;
+      const int fbc = c == 0 ? fb4.x : c == 1 ? fb4.y : c == 2 ? fb4.z : fb4.w;
+      crt_emit(limb, (fa | fbc) != 0, sa + sbc - 2 * W, C + 2 * (j * M + i) * cstride, mode);
+    }
+    mftc::tc_fence_before();  // this round's TMEM reads before the next round's MMAs
   }
-  const int4 sb4 = *reinterpret_cast<const int4 *>(sigB + j0);
-  const int4 fb4 = *reinterpret_cast<const int4 *>(flagB + j0);
-  const int sbv[4] = {sb4.x, sb4.y, sb4.z, sb4.w}, fbv[4] = {fb4.x, fb4.y, fb4.z, fb4.w};
-  const int sa = sigA[i], fa = flagA[i];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {  // r: column j0 + r
-    const int64_t j = j0 + r;
-    if (j >= N) break;
-    // |sum_t r_t e_t / M - C'/M - q| < 1/4 + rounding, so rint gives q exactly
-    const double q = rint(f[r]);
-    uint64_t L[CRT_NL39];
-    int64_t carry = 0;
-#pragma unroll
-    for (int l = 0; l < CRT_NL39; ++l) {
-      // acc - q M: both exact integers below 2^53, so the FMA is exact
-      const int64_t x = (l < nl ? __double2ll_rn(mfdev::fma_(-q, cs.M[l], acc[r][l])) : 0) + carry;
-      L[l] = (uint64_t)x & ((1ull << CRT_LB) - 1);
-      carry = x >> CRT_LB;  // arithmetic shift
-    }
-    (void)carry;
-    // C' mod 2^(39 nl) is exact (e and M are truncated there, so the carry out
-    // of the top limb is not the sign); |C'| < 2^(39 nl - 1), so the top bit of
-    // limb nl - 1 is the sign, copied into the limbs above
-    uint64_t top = 0;
-#pragma unroll
-    for (int l = 0; l < CRT_NL39; ++l) top = l == nl - 1 ? L[l] : top;
-    const uint64_t fill = (top >> (CRT_LB - 1)) & 1 ? (1ull << CRT_LB) - 1 : 0;
-#pragma unroll
-    for (int l = 0; l < CRT_NL39; ++l) L[l] = l < nl ? L[l] : fill;
-    // repack the two's complement value into 8 32-bit limbs
-    uint32_t limb[CRT_NL];
-#pragma unroll
-    for (int o = 0; o < CRT_NL; ++o) {
-      const int b = 32 * o, l1 = b / CRT_LB, off = b % CRT_LB;
-      uint64_t x = L[l1] >> off;
-      if (off + 32 > CRT_LB) x |= (l1 + 1 < CRT_NL39 ? L[l1 + 1] : fill) << (CRT_LB - off);
-      limb[o] = (uint32_t)x;
-    }
-    double2 out;
-    if (fa | fbv[r]) {
-      out = make_double2(CUDART_NAN, 0.0);
-    } else {
-      double hi, lo;
-      int e;
-      crt_to_dd(limb, CRT_NL, hi, lo, e);
-      const int ex = e + sa + sbv[r] - 2 * W;
-      out = make_double2(scale2(hi, ex), scale2(lo, ex));
-    }
-    double2 *dst = reinterpret_cast<double2 *>(C) + (j * M + i) * cstride;
-    if (mode != 0) {
-      const double2 prev = *dst;
-      const mfdev::dd p = mfdev::make(out.x, out.y), pv = mfdev::make(prev.x, prev.y);
-      const mfdev::dd res = mode == 1 ? mfdev::dd_sub(pv, p) : mfdev::dd_add(pv, p);
-      out = make_double2(res.hi, res.lo);
-    }
-    __stcs(dst, out);
-  }
+  __syncthreads();
+  mftc::tc_fence_after();
+  if (warp == 0) mftc::tmem_dealloc(tmem, ncols);
 }
 
 }  // namespace split

@@ -653,17 +653,17 @@ __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restri
   if (p8 >= K_pad) return;
   crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, blockIdx.y, p8);
 }
-// Thread per row i and 4 consecutive columns j0 = 4 blockIdx.y (residues from
-// the tensor-core kernel's epilogue); `mode` as combine_kernel.
-__global__ void __launch_bounds__(128) crt_combine_kernel(const uint8_t *__restrict__ D8, const Plan *plan,
-                                                          const CrtConst *cc, const int *sigA, const int *flagA,
-                                                          const int *sigB, const int *flagB, int64_t M,
-                                                          int64_t N, int64_t M_pad, int64_t N_pad, int nkc,
-                                                          double *__restrict__ C, int64_t cstride, int mode) {
-  __shared__ CrtShared cs;
-  crt_load_shared(cc, plan->S, cs);
-  crt_combine4_body(D8, plan, cs, sigA, flagA, sigB, flagB, M, N, M_pad, N_pad, nkc, C, cstride, mode,
-                    (int64_t)blockIdx.x * blockDim.x + threadIdx.x, 4 * (int64_t)blockIdx.y);
+// Tensor-core reconstruction (crt_combine_tc_body): block (x, y) takes rows
+// 128 x .. of column quads CTC_QUADS y ..; dynamic shared memory
+// crt_tc_smem(ceil(moduli / 32)).
+__global__ void __launch_bounds__(CTC_THREADS) crt_combine_tc_kernel(
+    const uint8_t *__restrict__ D8, const Plan *plan, const CrtConst *cc, const int *sigA, const int *flagA,
+    const int *sigB, const int *flagB, int64_t M, int64_t N, int64_t M_pad, int64_t N_pad, int nkc, int64_t k,
+    double *__restrict__ C, int64_t cstride, int mode, int *status) {
+  extern __shared__ uint8_t ctc_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(ctc_raw) + 1023) & ~uintptr_t(1023));
+  crt_combine_tc_body(D8, plan, cc, sigA, flagA, sigB, flagB, M, N, M_pad, N_pad, nkc, k, C, cstride, mode,
+                      (int64_t)blockIdx.x * CTC_THREADS, (int64_t)blockIdx.y * CTC_QUADS, smem, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -884,6 +884,8 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
       cudaFuncSetAttribute(split_mma_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM);
       cudaFuncSetAttribute(crt_slice_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            CRT_NMAX * SA_ROWS * SA_STRIDE);
+      cudaFuncSetAttribute(crt_combine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           crt_tc_smem((CRT_NMAX + 31) / 32));
     });
     prof_call_begin();
     mark(0, s);
@@ -958,9 +960,11 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                                                              status);
       if (q == nprod - 1) mark(3, s);
       if (crt)
-        crt_combine_kernel<<<dim3((unsigned)((m + 127) / 128), (unsigned)((n + 3) / 4)), 128, 0, s>>>(
+        crt_combine_tc_kernel<<<dim3((unsigned)((m + CTC_THREADS - 1) / CTC_THREADS),
+                                     (unsigned)(((n + 3) / 4 + CTC_QUADS - 1) / CTC_QUADS)),
+                                CTC_THREADS, crt_tc_smem((L.nsl + 31) / 32), s>>>(
             reinterpret_cast<const uint8_t *>(D), plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, n, L.M_pad,
-            L.N_pad, (int)L.nkc, prods[q].out, prods[q].ostride, prods[q].mode);
+            L.N_pad, (int)L.nkc, k, prods[q].out, prods[q].ostride, prods[q].mode, status);
       else
         combine_kernel<<<dim3(cgx, (unsigned)n), COMBINE_THREADS, 0, s>>>(D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n,
                                                     L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,
