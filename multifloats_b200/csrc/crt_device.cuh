@@ -204,9 +204,13 @@ __device__ __forceinline__ uint32_t crt_mod_small(uint32_t u, int t) {
 // The residue in [0, m_t) of X = sum_q d_q 256^q (balanced digits, read from
 // the biased words y of biased_bytes: digit q = byte q of y xor 0x80): dp4a
 // against the digit weights give rr = sum_q d_q c_q with |rr| < 14 * 128 * 128
-// < 2^18, made non-negative and reduced exactly.  The per-modulus constants
-// are passed in (hoisted by the caller).  NW = digit words in use: 3 when
-// W <= 94 (digits 12 and 13 are zero).
+// < 2^18, made non-negative by the offset (a multiple of m_t of at least
+// 2^18, the first dp4a's addend: u < 2^19 + 256) and reduced exactly.  For
+// u < 2^20 the Barrett quotient umulhi(u, ceil(2^32 / m)) is floor(u / m)
+// itself (its error u (mu m - 2^32) / (m 2^32) < u / 2^32 < 1 / m), so no
+// correction step follows.  The per-modulus constants are passed in (hoisted
+// by the caller).  NW = digit words in use: 3 when W <= 94 (digits 12 and 13
+// are zero).
 struct ModConst {
   int c0, c1, c2, c3;  // digit weights, signed bytes packed
   uint32_t m, mu, off;
@@ -224,13 +228,12 @@ __device__ __forceinline__ ModConst mod_const(int t) {
 }
 template <int NW>
 __device__ __forceinline__ uint32_t crt_residue(const uint32_t (&dw)[4], const ModConst &k) {
-  int rr = NW == 4 ? __dp4a((int)dw[3], k.c3, 0) : 0;
+  int rr = NW == 4 ? __dp4a((int)dw[3], k.c3, (int)k.off) : (int)k.off;
   rr = __dp4a((int)dw[2], k.c2, rr);
   rr = __dp4a((int)dw[1], k.c1, rr);
   rr = __dp4a((int)dw[0], k.c0, rr);
-  const uint32_t u = (uint32_t)rr + k.off;  // in [0, 2^19 + 256)
-  const int r = (int)(u - __umulhi(u, k.mu) * k.m);
-  return (uint32_t)(r < 0 ? r + (int)k.m : r);
+  const uint32_t u = (uint32_t)rr;  // in [0, 2^19 + 256)
+  return u - __umulhi(u, k.mu) * k.m;
 }
 // Signed digit words of the biased words of one entry.
 __device__ __forceinline__ void digit_words(const uint32_t (&y)[4], uint32_t (&dw)[4]) {
