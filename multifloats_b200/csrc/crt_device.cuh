@@ -450,17 +450,18 @@ __device__ __forceinline__ uint32_t crt_pack4(uint32_t v0, uint32_t v1, uint32_t
 // ---- reconstruction on the tensor cores ---------------------------------------
 // The sums over moduli are an integer matrix product: for an output with
 // residues r_t, the column sums
-//   S_b = sum_t r_t E[t][b]   (E[t][b] = byte b of e_t mod 2^(8 nbe) for b < nbe,
-//                              byte b - nbe of round(c_t 2^24) for the next 3)
+//   S_b = sum_t r_t E[t][b]   (E[t][b] = byte b of round(c_t 2^24) for b < 3,
+//                              0 for b = 3, byte b - 4 of e_t mod 2^(8 nbe)
+//                              for 4 <= b < 4 + nbe)
 // are exact in INT32 (< 36 * 255^2), so
-//   V = sum_{b < nbe} S_b 2^(8b) = sum_t r_t e_t  (mod 2^(8 nbe)),
-//   q = round((S_nbe + S_nbe+1 2^8 + S_nbe+2 2^16) / 2^24)  (error < 36 * 255 * 2^-25 < 1/4),
+//   V = sum_{b < nbe} S_{4+b} 2^(8b) = sum_t r_t e_t  (mod 2^(8 nbe)),
+//   q = round((S_0 + S_1 2^8 + S_2 2^16) / 2^24)  (error < 36 * 255 * 2^-25 < 1/4),
 //   C' = V - q M  (mod 2^(8 nbe)),
 // and |C'| < 2^(8 nbe - 2) makes bit 8 nbe - 1 the sign.  One tcgen05 u8 x u8
 // MMA per output column of a 128-row tile gives the S_b of 128 outputs.
 // nbe = crt_tc_bytes(W, k).
-// MMA columns: nbe + 3 rounded up to 16 (32 or 48).
-__host__ __device__ inline int crt_tc_cols(int nbe) { return (nbe + 3 + 15) / 16 * 16; }
+// MMA columns: nbe + 4 rounded up to 16 (32 or 48).
+__host__ __device__ inline int crt_tc_cols(int nbe) { return (nbe + 4 + 15) / 16 * 16; }
 constexpr int CTC_THREADS = 128;                   // one output row per thread and TMEM lane
 constexpr int CTC_QUADS = 8;                       // column quads per CTA
 constexpr int CTC_B_BYTES = 48 * 128;              // E tile: up to 48 rows of 128 bytes (swizzled)
@@ -523,10 +524,10 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
             const int t = 32 * kt + 16 * h + 4 * q + bb;
             uint32_t v = 0;
             if (t < n && T < nb) {
-              if (T < nbe)
-                v = (cc->ew[t][T >> 2] >> (8 * (T & 3))) & 0xFFu;
-              else if (T < nbe + 3)
-                v = (cc->cfix[t] >> (8 * (T - nbe))) & 0xFFu;
+              if (T < 3)
+                v = (cc->cfix[t] >> (8 * T)) & 0xFFu;
+              else if (T >= 4 && T < 4 + nbe)
+                v = (cc->ew[t][(T - 4) >> 2] >> (8 * (T & 3))) & 0xFFu;
             }
             word |= v << (8 * bb);
           }
@@ -632,20 +633,16 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
       mftc::tmem_wait_ld();
       const int64_t j = 4 * qd + c;
       if (!row_ok || j >= N) continue;
-      // q from the three fixed-point columns after the nbe limb bytes
-      uint64_t Q = 0;
-#pragma unroll
-      for (int L = 1; L <= CRT_NL; ++L)
-        if (4 * L == nbe)
-          Q = (uint64_t)S[4 * L] + ((uint64_t)S[4 * L + 1] << 8) + ((uint64_t)S[4 * L + 2] << 16);
+      // q from the three fixed-point columns
+      const uint64_t Q = (uint64_t)(S[0] + (S[1] << 8)) + ((uint64_t)S[2] << 16);
       const uint32_t q = (uint32_t)((Q + (1u << 23)) >> 24);
       uint32_t limb[CRT_NL];
       int64_t carry = 0;
 #pragma unroll
       for (int w = 0; w < CRT_NL; ++w) {
-        const uint64_t lo = S[4 * w] + ((uint64_t)S[4 * w + 1] << 8);
-        const uint64_t hi = S[4 * w + 2] + ((uint64_t)S[4 * w + 3] << 8);
-        const int64_t v = (int64_t)(lo + (hi << 16)) - (int64_t)((uint64_t)q * Mw[w]) + carry;
+        const uint32_t lo = S[4 + 4 * w] + (S[5 + 4 * w] << 8);  // < 2^30
+        const uint32_t hi = S[6 + 4 * w] + (S[7 + 4 * w] << 8);  // < 2^30
+        const int64_t v = (int64_t)lo + ((int64_t)hi << 16) - (int64_t)((uint64_t)q * Mw[w]) + carry;
         limb[w] = (uint32_t)v;
         carry = v >> 32;  // arithmetic shift
       }
