@@ -56,9 +56,12 @@ int sm_count();
 // Grow-only device staging buffers used by the drop-in (host-pointer) calls.
 // Each drop-in call holds the cache lock for its whole duration, so one
 // process-wide set of buffers per device is enough.
+constexpr int kStagingEvents = 8;
 struct Staging {
   std::unique_lock<std::mutex> lock;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy = nullptr;            // second stream for copies that overlap the compute stream
+  cudaEvent_t ev[kStagingEvents] = {};    // ordering events between the two (no timing)
   void *buf[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 // Acquire staging buffers of the given byte sizes on the current device.

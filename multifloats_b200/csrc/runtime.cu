@@ -60,7 +60,9 @@ bool injected_alloc_failure() {
 namespace {
 struct DeviceStaging {
   std::mutex mu;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr, copy = nullptr;
+  cudaEvent_t ev[kStagingEvents] = {};
+  bool have_ev = false;
   void *buf[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t cap[4] = {0, 0, 0, 0};
 };
@@ -74,7 +76,15 @@ int staging_acquire(Staging &st, const size_t bytes[4]) {
   DeviceStaging &ds = g_staging[dev];
   st.lock = std::unique_lock<std::mutex>(ds.mu);
   if (!ds.stream) MF_TRY_CUDA(cudaStreamCreateWithFlags(&ds.stream, cudaStreamNonBlocking));
+  if (!ds.copy) MF_TRY_CUDA(cudaStreamCreateWithFlags(&ds.copy, cudaStreamNonBlocking));
+  if (!ds.have_ev) {
+    for (int i = 0; i < kStagingEvents; ++i)
+      MF_TRY_CUDA(cudaEventCreateWithFlags(&ds.ev[i], cudaEventDisableTiming));
+    ds.have_ev = true;
+  }
   st.stream = ds.stream;
+  st.copy = ds.copy;
+  for (int i = 0; i < kStagingEvents; ++i) st.ev[i] = ds.ev[i];
   for (int i = 0; i < 4; ++i) {
     if (bytes[i] > ds.cap[i]) {
       if (ds.buf[i]) {

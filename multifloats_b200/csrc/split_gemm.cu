@@ -352,11 +352,13 @@ constexpr int PAIR_SMEM = 6 * (P_STAGE_A + P_HALF_B) + 1024 + 256;  // >= 4 * (1
 __host__ __device__ constexpr int pair_stages(int nsub) { return nsub == 1 ? 6 : 4; }
 
 // Sequence of (diagonal, K chunk, tile) items of one pair (see above).
+// Tiles are those of column tiles tn0 .. of the output (a column panel).
 struct PairSched {
-  int p, np, G, nkc, ntm, ntiles, nsuper;
+  int p, np, G, nkc, ntm, ntiles, tn0, nsuper;
   int r = 0, half = 0;
-  __device__ PairSched(int p_, int np_, int G_, int nkc_, int ntm_, int ntiles_)
-      : p(p_), np(np_), G(G_), nkc(nkc_), ntm(ntm_), ntiles(ntiles_), nsuper(((G_ + 2) / 2) * nkc_ * ntiles_) {}
+  __device__ PairSched(int p_, int np_, int G_, int nkc_, int ntm_, int ntiles_, int tn0_)
+      : p(p_), np(np_), G(G_), nkc(nkc_), ntm(ntm_), ntiles(ntiles_), tn0(tn0_),
+        nsuper(((G_ + 2) / 2) * nkc_ * ntiles_) {}
   __device__ bool next(Item &it) {
     while (true) {
       const int u = r * np + p;
@@ -372,7 +374,7 @@ struct PairSched {
       it.kc = rem / ntiles;
       const int tile = rem % ntiles;
       it.tm = tile % ntm;
-      it.tn = tile / ntm;
+      it.tn = tn0 + tile / ntm;
       if (half == 0) {
         half = 1;
       } else {
@@ -387,7 +389,7 @@ struct PairSched {
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     split_mma_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                           const Plan *plan, int32_t *__restrict__ D, int M_pad, int N_pad, int nkc,
-                          int kblocks, int nsub, int *status) {
+                          int kblocks, int nsub, int tn0, int ntn, int *status) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int nst = pair_stages(nsub);
@@ -410,7 +412,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
   const int S = plan->S, G = S - 1;
   const bool crt = plan->crt != 0;  // CRT form: item g is the single product A_g B_g
   const int tn_cols = BN * nsub;
-  const int ntm = M_pad / BM_PAIR, ntn = N_pad / tn_cols, ntiles = ntm * ntn;
+  const int ntm = M_pad / BM_PAIR, ntiles = ntm * ntn;  // column tiles tn0 .. tn0 + ntn - 1
   const int nacc = 2 / nsub;             // accumulators
   const int acc_cols = BN * nsub;        // columns per accumulator
 
@@ -455,7 +457,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
       bool armed[6];
       for (int s = 0; s < 6; ++s) armed[s] = false;
       bool ok = true;
-      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles);
+      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
       Item it;
       while (ok && sched.next(it)) {
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
@@ -505,7 +507,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
       int acc = 0;
       uint32_t acc_phase = 0;
       bool ok = true;
-      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles);
+      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
       Item it;
       while (ok && sched.next(it)) {
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
@@ -563,7 +565,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     const int nch = acc_cols / 32 / 2, ch0 = ((warp - 2) / 4) * nch;  // this warp's 32-column chunks
     int acc = 0;
     uint32_t acc_phase = 0;
-    PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles);
+    PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
     Item it;
     while (sched.next(it)) {
       bool got = wait_bar(&tfull[acc], acc_phase, abort_flag);
@@ -654,16 +656,16 @@ __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restri
   crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, blockIdx.y, p8);
 }
 // Tensor-core reconstruction (crt_combine_tc_body): block (x, y) takes rows
-// 128 x .. of column quads CTC_QUADS y ..; dynamic shared memory
+// 128 x .. of column quads qbase + CTC_QUADS y .. (columns below N); dynamic shared memory
 // crt_tc_smem(ceil(moduli / 32)).
 __global__ void __launch_bounds__(CTC_THREADS) crt_combine_tc_kernel(
     const uint8_t *__restrict__ D8, const Plan *plan, const CrtConst *cc, const int *sigA, const int *flagA,
     const int *sigB, const int *flagB, int64_t M, int64_t N, int64_t M_pad, int64_t N_pad, int nkc, int64_t k,
-    double *__restrict__ C, int64_t cstride, int mode, int *status) {
+    double *__restrict__ C, int64_t cstride, int mode, int64_t qbase, int *status) {
   extern __shared__ uint8_t ctc_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(ctc_raw) + 1023) & ~uintptr_t(1023));
   crt_combine_tc_body(D8, plan, cc, sigA, flagA, sigB, flagB, M, N, M_pad, N_pad, nkc, k, C, cstride, mode,
-                      (int64_t)blockIdx.x * CTC_THREADS, (int64_t)blockIdx.y * CTC_QUADS, smem, status);
+                      (int64_t)blockIdx.x * CTC_THREADS, qbase + (int64_t)blockIdx.y * CTC_QUADS, smem, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -847,10 +849,23 @@ struct Product {
 // NULL) receives {S, rho_A, rho_B}; a non-NULL info waits for completion.
 // crt = 1 runs the CRT form with `slices` read as the operand bits W (0 = from
 // the target); info then receives {moduli, rho_A, rho_B, W}.
+// A caller that takes the output in column panels (the host-pointer calls
+// copy each panel to the host while later panels are computed): after every
+// product of output columns [j0, j1) has been enqueued on stream s,
+// done(ctx, j0, j1, s) is called.  Used by the CRT form on CTA pairs; other
+// calls report the whole output as one panel.  Results are the same bit for
+// bit for any panel count.
+struct PanelSink {
+  int panels;
+  void (*done)(void *ctx, int64_t j0, int64_t j1, cudaStream_t s);
+  void *ctx;
+};
+
 static int run_products(const double *const *aview, const int64_t *astride, int nA,
                         const double *const *bview, const int64_t *bstride, int nB,
                         const Product *prods, int nprod, int64_t m, int64_t k, int64_t n, int slices,
-                        double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info, int crt = 0) {
+                        double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info, int crt = 0,
+                        const PanelSink *sink = nullptr) {
   Layout L = layout(m, k, n, nA, nB, crt ? crt_slices_max(k, slices) : SMAX);
   if (L.M_pad > INT32_MAX / 2 || L.N_pad > INT32_MAX / 2 || L.kblocks > INT32_MAX / 2 ||
       L.N_pad > 65535 || L.K_pad / 64 > 65535)
@@ -942,33 +957,48 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     }
     const unsigned cgx = (unsigned)(((m + 3) / 4 + COMBINE_THREADS - 1) / COMBINE_THREADS);
     mark(2, s);
-    for (int q = 0; q < nprod && rc == MFCUDA_OK; ++q) {
-      const int ia = prods[q].a, ib = nA + prods[q].b;
-      CUtensorMap tmA, tmB;
-      if (!make_map(&tmA, sl[ia], L.M_pad, L.K_pad, BM, L.nsl) ||
-          !make_map(&tmB, sl[ib], L.N_pad, L.K_pad, L.pair ? 128 : BN, L.nsl)) {
+    CUtensorMap tmA[4], tmB[4];
+    for (int q = 0; q < nprod; ++q)
+      if (!make_map(&tmA[q], sl[prods[q].a], L.M_pad, L.K_pad, BM, L.nsl) ||
+          !make_map(&tmB[q], sl[nA + prods[q].b], L.N_pad, L.K_pad, L.pair ? 128 : BN, L.nsl))
         rc = MFCUDA_ERR_CUDA;
-        break;
+    // column panels (CRT form on CTA pairs, when a sink wants the output panel
+    // by panel): every product of panel p, then the sink, then panel p + 1
+    const int tn_cols = BN * L.nsub;
+    const int ntn_all = (int)(L.N_pad / tn_cols);
+    const int npan = (sink && crt && L.pair) ? std::max(1, std::min(sink->panels, ntn_all)) : 1;
+    for (int pp = 0; pp < npan && rc == MFCUDA_OK; ++pp) {
+      const int tn0 = (int)((int64_t)ntn_all * pp / npan), tn1 = (int)((int64_t)ntn_all * (pp + 1) / npan);
+      const int64_t j0 = npan == 1 ? 0 : (int64_t)tn0 * tn_cols;
+      const int64_t j1 = npan == 1 ? n : std::min<int64_t>(n, (int64_t)tn1 * tn_cols);
+      int pgrid = grid;
+      if (L.pair && npan > 1) {
+        const int supers = ((L.nsl + 1) / 2) * (int)L.nkc * (int)(L.M_pad / tile_m) * (tn1 - tn0);
+        pgrid = std::min(pair_grid(), 2 * supers);
       }
-      if (L.pair)
-        split_mma_pair_kernel<<<grid, PAIR_THREADS, PAIR_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad,
-                                                                   (int)L.N_pad, (int)L.nkc,
-                                                                   (int)L.kblocks, L.nsub, status);
-      else
-        split_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM, s>>>(tmA, tmB, plan, D, (int)L.M_pad,
-                                                             (int)L.N_pad, (int)L.nkc, (int)L.kblocks,
-                                                             status);
-      if (q == nprod - 1) mark(3, s);
-      if (crt)
-        crt_combine_tc_kernel<<<dim3((unsigned)((m + CTC_THREADS - 1) / CTC_THREADS),
-                                     (unsigned)(((n + 3) / 4 + CTC_QUADS - 1) / CTC_QUADS)),
-                                CTC_THREADS, crt_tc_smem((L.nsl + 31) / 32), s>>>(
-            reinterpret_cast<const uint8_t *>(D), plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, n, L.M_pad,
-            L.N_pad, (int)L.nkc, k, prods[q].out, prods[q].ostride, prods[q].mode, status);
-      else
-        combine_kernel<<<dim3(cgx, (unsigned)n), COMBINE_THREADS, 0, s>>>(D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n,
-                                                    L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,
-                                                    prods[q].ostride, prods[q].mode);
+      for (int q = 0; q < nprod && rc == MFCUDA_OK; ++q) {
+        const int ia = prods[q].a, ib = nA + prods[q].b;
+        if (L.pair)
+          split_mma_pair_kernel<<<pgrid, PAIR_THREADS, PAIR_SMEM, s>>>(
+              tmA[q], tmB[q], plan, D, (int)L.M_pad, (int)L.N_pad, (int)L.nkc, (int)L.kblocks, L.nsub, tn0,
+              npan == 1 ? ntn_all : tn1 - tn0, status);
+        else
+          split_mma_kernel<<<pgrid, MMA_THREADS, MMA_SMEM, s>>>(tmA[q], tmB[q], plan, D, (int)L.M_pad,
+                                                                (int)L.N_pad, (int)L.nkc, (int)L.kblocks,
+                                                                status);
+        if (q == nprod - 1 && pp == npan - 1) mark(3, s);
+        if (crt)
+          crt_combine_tc_kernel<<<dim3((unsigned)((m + CTC_THREADS - 1) / CTC_THREADS),
+                                       (unsigned)(((j1 - j0 + 3) / 4 + CTC_QUADS - 1) / CTC_QUADS)),
+                                  CTC_THREADS, crt_tc_smem((L.nsl + 31) / 32), s>>>(
+              reinterpret_cast<const uint8_t *>(D), plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, j1,
+              L.M_pad, L.N_pad, (int)L.nkc, k, prods[q].out, prods[q].ostride, prods[q].mode, j0 / 4, status);
+        else
+          combine_kernel<<<dim3(cgx, (unsigned)n), COMBINE_THREADS, 0, s>>>(
+              D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n, L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,
+              prods[q].ostride, prods[q].mode);
+      }
+      if (sink && rc == MFCUDA_OK) sink->done(sink->ctx, j0, j1, s);
     }
     mark(4, s);
     if (rc == MFCUDA_OK && cudaGetLastError() != cudaSuccess) rc = MFCUDA_ERR_CUDA;
@@ -1025,7 +1055,8 @@ int run(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t
 
 // CRT form of run(): bits = W (0: from the target); info = {moduli, rho_A, rho_B, W}.
 int run_crt(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k, int64_t n,
-            int bits, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info) {
+            int bits, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info,
+            const PanelSink *sink = nullptr) {
   int rc = check_args(a, b, c, m, k, n, 0, target);
   if (bits < 0 || (bits > 0 && bits < 8) || bits > CRT_WMAX) return MFCUDA_ERR_INVALID_ARG;
   if (rc == -1) return MFCUDA_OK;
@@ -1040,7 +1071,7 @@ int run_crt(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int
   const double *bv[1] = {reinterpret_cast<const double *>(b)};
   int64_t one[1] = {1};
   Product p = {0, 0, reinterpret_cast<double *>(c), 1, 0};
-  return run_products(av, one, 1, bv, one, 1, &p, 1, m, k, n, bits, target, ws, ws_bytes, s, info, 1);
+  return run_products(av, one, 1, bv, one, 1, &p, 1, m, k, n, bits, target, ws, ws_bytes, s, info, 1, sink);
 }
 
 // Complex: re = Ar Br - Ai Bi, im = Ar Bi + Ai Br (the Fortran cdd_matmul_mm
@@ -1075,7 +1106,8 @@ int run_complex(const complex64x2 *a, const complex64x2 *b, complex64x2 *c, int6
 // moduli set for all four (planned from all four operands), the four parts
 // reduced to residues once.
 int run_complex_crt(const complex64x2 *a, const complex64x2 *b, complex64x2 *c, int64_t m, int64_t k,
-                    int64_t n, int bits, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info) {
+                    int64_t n, int bits, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info,
+                    const PanelSink *sink = nullptr) {
   int rc = check_args(a, b, c, m, k, n, 0, target);
   if (bits < 0 || (bits > 0 && bits < 8) || bits > CRT_WMAX) return MFCUDA_ERR_INVALID_ARG;
   if (rc == -1) return MFCUDA_OK;
@@ -1096,7 +1128,7 @@ int run_complex_crt(const complex64x2 *a, const complex64x2 *b, complex64x2 *c, 
                   {1, 1, Cd, 2, 1},       // re -= Ai Bi
                   {0, 1, Cd + 2, 2, 0},   // im  = Ar Bi
                   {1, 0, Cd + 2, 2, 2}};  // im += Ai Br
-  return run_products(av, two, 2, bv, two, 2, p, 4, m, k, n, bits, target, ws, ws_bytes, s, info, 1);
+  return run_products(av, two, 2, bv, two, 2, p, 4, m, k, n, bits, target, ws, ws_bytes, s, info, 1, sink);
 }
 
 }  // namespace split
@@ -1135,6 +1167,39 @@ static int split_host(const void *a, const void *b, void *c, int64_t m, int64_t 
   return MFCUDA_OK;
 }
 
+// Device-to-host copies of the output, one per finished column panel, on the
+// staging copy stream (each waits for its panel through an event).
+struct PanelCopies {
+  char *host;
+  const char *dev;
+  size_t col_bytes;  // bytes per output column
+  cudaStream_t copy;
+  cudaEvent_t *ev;
+  int nev, used = 0;
+  int64_t next = 0;  // columns [0, next) are on their way
+  int rc = MFCUDA_OK;
+};
+static void copy_panel(void *ctx, int64_t j0, int64_t j1, cudaStream_t s) {
+  auto *pc = static_cast<PanelCopies *>(ctx);
+  if (pc->rc != MFCUDA_OK || j1 <= j0) return;
+  cudaStream_t cs = s;
+  if (pc->used < pc->nev) {  // otherwise copied on the compute stream itself
+    cudaEvent_t e = pc->ev[pc->used++];
+    if (cudaEventRecord(e, s) != cudaSuccess || cudaStreamWaitEvent(pc->copy, e, 0) != cudaSuccess) {
+      pc->rc = MFCUDA_ERR_CUDA;
+      return;
+    }
+    cs = pc->copy;
+  }
+  if (cudaMemcpyAsync(pc->host + j0 * pc->col_bytes, pc->dev + j0 * pc->col_bytes, (j1 - j0) * pc->col_bytes,
+                      cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+    pc->rc = MFCUDA_ERR_CUDA;
+  pc->next = j1;
+}
+
+// The host-pointer CRT call: operands copied in, the product computed in
+// kPanels column panels, each panel copied back as soon as it is complete
+// (overlapping the copy with the remaining panels' tensor-core work).
 template <bool CPLX>
 static int crt_host(const void *a, const void *b, void *c, int64_t m, int64_t k, int64_t n, int bits,
                     double *bound_out) {
@@ -1153,16 +1218,32 @@ static int crt_host(const void *a, const void *b, void *c, int64_t m, int64_t k,
   if (ba) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[0], a, ba, cudaMemcpyHostToDevice, st.stream));
   if (bb) MF_TRY_CUDA(cudaMemcpyAsync(st.buf[1], b, bb, cudaMemcpyHostToDevice, st.stream));
   int info[4] = {0, 0, 0, 0};
+  PanelCopies pc;
+  pc.host = static_cast<char *>(c);
+  pc.dev = static_cast<const char *>(st.buf[2]);
+  pc.col_bytes = (size_t)m * elem;
+  pc.copy = st.copy;
+  pc.ev = st.ev;
+  pc.nev = kStagingEvents;
+  constexpr int kPanels = 4;
+  const split::PanelSink sink = {kPanels, copy_panel, &pc};
+  int rc;
   if (CPLX)
-    MF_TRY(split::run_complex_crt(static_cast<complex64x2 *>(st.buf[0]), static_cast<complex64x2 *>(st.buf[1]),
-                                  static_cast<complex64x2 *>(st.buf[2]), m, k, n, bits, 8.0, st.buf[3], wsb,
-                                  st.stream, info));
+    rc = split::run_complex_crt(static_cast<complex64x2 *>(st.buf[0]), static_cast<complex64x2 *>(st.buf[1]),
+                                static_cast<complex64x2 *>(st.buf[2]), m, k, n, bits, 8.0, st.buf[3], wsb,
+                                st.stream, info, &sink);
   else
-    MF_TRY(split::run_crt(static_cast<float64x2 *>(st.buf[0]), static_cast<float64x2 *>(st.buf[1]),
-                          static_cast<float64x2 *>(st.buf[2]), m, k, n, bits, 8.0, st.buf[3], wsb, st.stream,
-                          info));
-  MF_TRY_CUDA(cudaMemcpyAsync(c, st.buf[2], bc, cudaMemcpyDeviceToHost, st.stream));
-  MF_TRY_CUDA(cudaStreamSynchronize(st.stream));
+    rc = split::run_crt(static_cast<float64x2 *>(st.buf[0]), static_cast<float64x2 *>(st.buf[1]),
+                        static_cast<float64x2 *>(st.buf[2]), m, k, n, bits, 8.0, st.buf[3], wsb, st.stream, info,
+                        &sink);
+  if (rc == MFCUDA_OK && pc.rc == MFCUDA_OK && pc.next < n)  // columns no panel reported (k = 0)
+    copy_panel(&pc, pc.next, n, st.stream);
+  // no copy may still be writing the caller's memory when this returns
+  const cudaError_t e1 = cudaStreamSynchronize(st.stream), e2 = cudaStreamSynchronize(st.copy);
+  MF_TRY(rc);
+  MF_TRY(pc.rc);
+  MF_TRY_CUDA(e1);
+  MF_TRY_CUDA(e2);
   if (bound_out) *bound_out = info[0] > 0 ? split::crt_bound(info[3], info[1], info[2], k) : 0.0;
   return MFCUDA_OK;
 }

@@ -131,6 +131,25 @@ def test_host_dropin(cuda_lib):
     assert bound.value == pytest.approx(O.crt_bound(info[3], info[1], info[2], k)) and bound.value <= 8.0
 
 
+def test_host_dropin_column_panels(cuda_lib, dev):
+    """The host-pointer call computes the output in column panels and copies
+    each back while the next is computed: the same bits as the device call,
+    with uneven panels (five 512-column tiles in four panels, the last one
+    ragged)."""
+    m, k, n = 300, 700, 2100
+    A, B = W.dd_rowcol_scaled(m, k, 16, "row", 18), W.dd_rowcol_scaled(k, n, 16, "col", 19)
+    got, info = dev_crt(cuda_lib, dev, A, B, m, k, n)
+    for _ in range(2):  # twice: the second call reuses the staging streams and events
+        c = np.full(2 * m * n, np.nan)
+        bound = C.c_double()
+        cuda_lib.matmuldd_mm_crt(A.ctypes.data, B.ctypes.data, c.ctypes.data, m, k, n, 0, C.byref(bound))
+        assert cuda_lib.mfcuda_last_error() == 0
+        assert O.same_bits(c, got).all()
+    want, _ = O.crt_gemm(A, B, m, k, n, rows=(150, 152))
+    sub = np.ascontiguousarray(c.reshape(n, m, 2)[:, 150:152, :]).reshape(-1)
+    assert O.same_bits(sub, want).all()
+
+
 @pytest.mark.parametrize("R", [0, 16, 64])
 def test_4096_error_bound_and_sampled_rows(cuda_lib, dev, R):
     """The benchmark shape: every sampled output within the a-priori bound of
