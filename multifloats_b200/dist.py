@@ -11,8 +11,9 @@ path has a real exchange step:
   to ranks (:func:`assign_by_cost`), each rank then runs its own batch plan;
 * one large GEMM: column panels (:func:`matmul_columns`): every rank holds A
   and its panel of B and computes its panel of C.  K is never split, so every
-  output equals the single-device call bit for bit (for the split form the
-  ranks first agree on the slice count, the one the single call would pick);
+  output equals the single-device call bit for bit (for the split forms the
+  ranks first agree on the slice count or the operand width, the one the
+  single call would pick);
   :func:`gather_columns` assembles C when a caller wants it on every rank;
 * reductions: the one real exchange.  Each rank reduces its shard to a few DD
   values (:func:`reduce` -> ``mfcuda_reduce_partial``), the values are
@@ -124,6 +125,17 @@ class CudaBackend:
         _lib.check(rc, "mfcuda_matmuldd_mm_split")
         return c, int(info[0])
 
+    def gemm_crt(self, a, b, m: int, k: int, n: int, bits: int, target: float):
+        """CRT form; returns (C, operand width W used)."""
+        import torch
+
+        c = torch.empty(2 * m * n, dtype=torch.float64, device=b.device)
+        info = (C.c_int * 4)()
+        rc = _lib.lib().mfcuda_matmuldd_mm_crt(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, k, n, bits, target,
+                                               None, 0, info, self._stream())
+        _lib.check(rc, "mfcuda_matmuldd_mm_crt")
+        return c, int(info[3])
+
 
 _default_backend = None
 
@@ -211,7 +223,11 @@ def matmul_columns(a, b_local, m: int, k: int, n_local: int, form: str = "plain"
     rank first runs with its own automatic slice count and the ranks agree on
     the largest one (the count the single call derives from the exponent
     spreads of all of B); a rank that used fewer recomputes with that count
-    (`target` as in mfcuda_matmuldd_mm_split).  Returns (C panel, slices used or 0 for the plain form)."""
+    (`target` as in mfcuda_matmuldd_mm_split).  form "crt" (the CRT split
+    form): the same agreement on the operand width W (`slices` is then the
+    width, 0 = from the target; the single call's W grows with the spreads, so
+    it is the ranks' largest).  Returns (C panel, slices or W used, 0 for the
+    plain form)."""
     import torch
     import torch.distributed as dist
 
@@ -220,10 +236,11 @@ def matmul_columns(a, b_local, m: int, k: int, n_local: int, form: str = "plain"
         if n_local == 0:
             return b_local.new_empty(0), 0
         return be.gemm_plain(a, b_local, m, k, n_local, renorm_interval), 0
-    if form != "split":
+    if form not in ("split", "crt"):
         raise ValueError(f"unknown form {form!r}")
+    run = be.gemm_split if form == "split" else be.gemm_crt
     if n_local > 0:
-        c, s_used = be.gemm_split(a, b_local, m, k, n_local, slices, target)
+        c, s_used = run(a, b_local, m, k, n_local, slices, target)
     else:
         c, s_used = b_local.new_empty(0), 0
     if slices == 0:
@@ -231,7 +248,7 @@ def matmul_columns(a, b_local, m: int, k: int, n_local: int, form: str = "plain"
         dist.all_reduce(s, op=dist.ReduceOp.MAX, group=group)
         s_all = int(s.item())
         if n_local > 0 and s_used != s_all:
-            c, s_used = be.gemm_split(a, b_local, m, k, n_local, s_all, target)
+            c, s_used = run(a, b_local, m, k, n_local, s_all, target)
     return c, s_used
 
 

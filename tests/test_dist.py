@@ -1,6 +1,7 @@
 """Multi-process logic of multifloats_b200.dist on CPU (gloo, world sizes 2 and
 3): shard bounds, cost-balanced assignment, the rank-order combine of
-reduction partials, and column-panel GEMMs that agree on the slice count.
+reduction partials, and column-panel GEMMs that agree on the slice count (or,
+in the CRT form, on the operand width).
 
 Each rank's local compute is the oracle (the CPU restatement of the device
 kernels), so a rank here computes what a GPU rank computes, bit for bit."""
@@ -64,6 +65,12 @@ class OracleBackend:
 
         c, info = O.split_gemm(a.numpy(), b.numpy(), m, k, n, slices=slices, target=target)
         return torch.from_numpy(c.copy()), info[0]
+
+    def gemm_crt(self, a, b, m, k, n, bits, target):
+        import torch
+
+        c, info = O.crt_gemm(a.numpy(), b.numpy(), m, k, n, bits=bits, target=target)
+        return torch.from_numpy(c.copy()), info[3]
 
 
 def _free_port():
@@ -149,6 +156,15 @@ def _worker(rank, world, port, errq):
         assert O.same_bits(full, want).all()
         # the test is only meaningful if some rank's own count differed
         flags = torch.tensor([int(own != info[0])])
+        dist.all_reduce(flags)
+        assert int(flags.item()) >= 1
+        # ---- CRT form: ranks agree on the operand width of the whole problem ----
+        own_w = O.crt_gemm(A, Bs[2 * K * j0: 2 * K * j1], M, K, j1 - j0)[1][3]
+        c, w_used = D.matmul_columns(torch.from_numpy(A), bl, M, K, j1 - j0, "crt", backend=be)
+        want, info = O.crt_gemm(A, Bs, M, K, NCOL)
+        assert w_used == info[3]
+        assert O.same_bits(D.gather_columns(c, M, NCOL).numpy(), want).all()
+        flags = torch.tensor([int(own_w != info[3])])
         dist.all_reduce(flags)
         assert int(flags.item()) >= 1
         dist.barrier()

@@ -194,3 +194,30 @@ def test_complex_bit_exact_and_host(cuda_lib, dev, shape):
     bound = C.c_double()
     cuda_lib.cmatmuldd_mm_crt(A.ctypes.data, B.ctypes.data, h.ctypes.data, m, k, n, 0, C.byref(bound))
     assert cuda_lib.mfcuda_last_error() == 0 and O.same_bits(h, want).all()
+
+
+def test_column_panels_agree_on_width(cuda_lib, dev):
+    """dist.CudaBackend.gemm_crt on three column panels of B (one process
+    standing in for three ranks): each panel with its own width W, then all
+    with the largest one, as dist.matmul_columns does; the panels together
+    equal the single call bit for bit."""
+    import torch
+
+    from multifloats_b200 import dist as D
+
+    m, k, n = 140, 300, 390
+    A = W.dd_rowcol_scaled(m, k, 0, "row", seed=61)
+    parts = [W.dd_rowcol_scaled(k, 130, 0, "col", seed=62), W.dd_rowcol_scaled(k, 130, 0, "col", seed=63),
+             W.dd_rowcol_scaled(k, 130, 6, "row", seed=64)]  # the last panel spans several binades per column
+    B = np.concatenate(parts)
+    be = D.CudaBackend()
+    a = to_dev(A, dev)
+    own = [be.gemm_crt(a, to_dev(p, dev), m, k, 130, 0, 8.0)[1] for p in parts]
+    w_all = max(own)
+    assert len(set(own)) > 1
+    panels = [be.gemm_crt(a, to_dev(p, dev), m, k, 130, w_all, 8.0) for p in parts]
+    assert all(w == w_all for _, w in panels)
+    got = to_host(torch.cat([c for c, _ in panels]))
+    want, info = dev_crt(cuda_lib, dev, A, B, m, k, n)
+    assert info[3] == w_all
+    assert O.same_bits(got, want).all()
