@@ -324,10 +324,14 @@ __device__ __forceinline__ GItem decode_item(const SProb &P, int64_t local) {
 }
 
 // Persistent tensor-core kernel over every problem's items (static
-// round-robin).  Same warp roles and barriers as split_mma_kernel; per item it
-// looks up the problem, skips diagonals beyond the problem's plan, and uses the
-// problem's tensor maps (global memory) and tile width.
-__global__ void __launch_bounds__(MMA_THREADS, 1)
+// round-robin).  The warp roles and barriers of split_mma_kernel, with eight
+// epilogue warps (two per TMEM lane quadrant, each draining half of the
+// accumulator's columns); per item it looks up the problem, skips diagonals
+// beyond the problem's plan, and uses the problem's tensor maps (global
+// memory) and tile width.
+constexpr int G_EPI_WARPS = 8;
+constexpr int G_THREADS = 64 + 32 * G_EPI_WARPS;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+__global__ void __launch_bounds__(G_THREADS, 1)
     g_mma(const SProb *__restrict__ probs, const CUtensorMap *__restrict__ maps,
           const int64_t *__restrict__ prefix, int nprob, int64_t items, int *status) {
   extern __shared__ uint8_t smem_raw[];
@@ -350,7 +354,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mftc::mbar_init(&tfull[a], 1);
-      mftc::mbar_init(&tempty[a], 4);
+      mftc::mbar_init(&tempty[a], G_EPI_WARPS);
     }
     mftc::mbar_init(drain, 1);
     *abort_flag = 0;
@@ -477,7 +481,8 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
       }
     }
   } else {
-    const int quad = warp & 3;
+    const int quad = warp & 3;           // TMEM lanes this warp may read
+    const int half = (warp - 2) / 4;     // which half of the accumulator's columns
     const int row = quad * 32 + lane;
     int acc = 0;
     uint32_t acc_phase = 0;
@@ -494,9 +499,10 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
       mftc::tc_fence_after();
       const int64_t off = ((int64_t)(it.g * P.nkc + it.kc) * P.N_pad + (int64_t)it.tn * P.bn) * P.M_pad +
                           (int64_t)it.tm * BM + row;
+      const int nch = P.bn / 64, ch0 = half * nch;  // this warp's 32-column chunks
       if (P.crt) {  // residues modulo m_g, four columns per 32-bit word (crt_device.cuh)
-        uint32_t *dst = reinterpret_cast<uint32_t *>(P.D) + crt_word_index(off, P.M_pad);
-        for (int chunk = 0; chunk < P.bn / 32; ++chunk) {
+        uint32_t *dst = reinterpret_cast<uint32_t *>(P.D) + crt_word_index(off, P.M_pad) + (int64_t)ch0 * 8 * P.M_pad;
+        for (int chunk = ch0; chunk < ch0 + nch; ++chunk) {
           uint32_t r[32];
           mftc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * BN + chunk * 32), r);
           mftc::tmem_wait_ld();
@@ -508,7 +514,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         }
       } else {
         int32_t *dst_base = P.D + off;
-        for (int chunk = 0; chunk < P.bn / 32; ++chunk) {
+        for (int chunk = ch0; chunk < ch0 + nch; ++chunk) {
           uint32_t r[32];
           mftc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * BN + chunk * 32), r);
           mftc::tmem_wait_ld();
@@ -969,7 +975,7 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
       g_crt_slice_b<<<(unsigned)total[PH_SLICE_B], 256, 0, cs>>>(dp, dprefix + PH_SLICE_B * np, np);
     else if (total[PH_SLICE_B])
       g_slice_b<<<(unsigned)total[PH_SLICE_B], 256, 0, cs>>>(dp, dprefix + PH_SLICE_B * np, np);
-    g_mma<<<mma_grid, MMA_THREADS, MMA_SMEM, cs>>>(dp, dmaps, dprefix + PH_ITEMS * np, np, total[PH_ITEMS],
+    g_mma<<<mma_grid, G_THREADS, MMA_SMEM, cs>>>(dp, dmaps, dprefix + PH_ITEMS * np, np, total[PH_ITEMS],
                                                    b->status);
     for (int ph : {PH_COMBINE, PH_COMBINE2}) {
       if (!total[ph]) continue;

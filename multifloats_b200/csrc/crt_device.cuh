@@ -43,12 +43,16 @@ constexpr int CRT_WMAX = 110;
 
 // Reconstruction constants of the plan's N moduli, computed on the device:
 // e_t = (M / m_t) ((M / m_t)^-1 mod m_t) and M = prod m_t modulo 2^256 in
-// 32-bit limbs, and c_t = e_t / M = ((M / m_t)^-1 mod m_t) / m_t as 24-bit
-// fixed point, round(c_t 2^24).
+// 32-bit limbs, c_t = e_t / M = ((M / m_t)^-1 mod m_t) / m_t as 24-bit fixed
+// point, round(c_t 2^24), and the E matrix of the tensor-core reconstruction
+// (crt_combine_tc_body) ready to copy: row b (an MMA column), byte t (a
+// modulus), zero for t >= N.
+constexpr int CRT_EB_ROWS = 48, CRT_EB_BYTES = 64;
 struct CrtConst {
   uint32_t ew[CRT_NMAX][CRT_NL];
   uint32_t Mw[CRT_NL];
   uint32_t cfix[CRT_NMAX];
+  alignas(16) uint8_t eb[CRT_EB_ROWS][CRT_EB_BYTES];
 };
 
 // ceil(log2 k) for k >= 1.
@@ -86,6 +90,9 @@ inline int crt_slices_max(int64_t k, int bits) {
 __host__ __device__ inline int crt_tc_bytes(int W, int64_t k) {
   return 4 * ((2 * W + ceil_log2(k) + 2 + 31) / 32);
 }
+// MMA columns of the reconstruction: the three bytes of round(c_t 2^24), a
+// zero column, then nbe bytes of e_t, rounded up to 16 (32 or 48).
+__host__ __device__ inline int crt_tc_cols(int nbe) { return (nbe + 4 + 15) / 16 * 16; }
 
 // Inverse of a modulo m (gcd(a, m) = 1, m <= 256), extended Euclid.
 __device__ __forceinline__ uint32_t inv_mod_small(uint32_t a, uint32_t m) {
@@ -107,7 +114,7 @@ __device__ __forceinline__ uint32_t inv_mod_small(uint32_t a, uint32_t m) {
 __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, double target, int64_t k,
                                               Plan *plan, CrtConst *cc) {
   __shared__ int red[2][32];
-  __shared__ int sh_n;
+  __shared__ int sh_n, sh_nbe;
   int r[2] = {0, 0};
   for (int o = 0; o < st.n; ++o)
     for (int64_t i = threadIdx.x; i < st.count[o]; i += blockDim.x)
@@ -145,6 +152,7 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
     plan->crt = 1;
     plan->nl = crt_tc_bytes(W, k) / 4;
     sh_n = n;
+    sh_nbe = crt_tc_bytes(W, k);
   }
   __syncthreads();
   const int n = sh_n;
@@ -176,7 +184,19 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
       carry = v >> 32;
     }
     for (int l = 0; l < CRT_NL; ++l) cc->ew[t][l] = ev[l];
-    cc->cfix[t] = (uint32_t)((((uint64_t)inv << 24) + mt / 2) / mt);
+    const uint32_t cf = (uint32_t)((((uint64_t)inv << 24) + mt / 2) / mt);
+    cc->cfix[t] = cf;
+    // column t of E: rows 0-2 the bytes of cf, row 3 zero, rows 4 .. 4 + nbe - 1
+    // the bytes of e_t, zero above
+    const int nbe = sh_nbe;
+    for (int b = 0; b < CRT_EB_ROWS; ++b) {
+      uint32_t v = 0;
+      if (b < 3)
+        v = (cf >> (8 * b)) & 0xFFu;
+      else if (b >= 4 && b < 4 + nbe)
+        v = (ev[(b - 4) >> 2] >> (8 * ((b - 4) & 3))) & 0xFFu;
+      cc->eb[b][t] = (uint8_t)v;
+    }
     if (t == 0) {  // M = (M / m_0) m_0
       uint64_t cy = 0;
       for (int l = 0; l < CRT_NL; ++l) {
@@ -185,6 +205,8 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
         cy = v >> 32;
       }
     }
+  } else if (threadIdx.x < (unsigned)CRT_EB_BYTES) {  // moduli slots beyond N
+    for (int b = 0; b < CRT_EB_ROWS; ++b) cc->eb[b][threadIdx.x] = 0;
   }
   __syncthreads();
   for (int o = 0; o < st.n; ++o)
@@ -292,9 +314,13 @@ __device__ __forceinline__ void crt_slice_a_body(const double *__restrict__ A, i
       for (int w = 0; w < 4; ++w) y[e][w] = bias_word(w);  // X = 0: every residue zero
     }
   }
-  for_each_residue_word(y, n, W, [&](int sl, uint64_t word) {
+  auto put = [&](int sl, uint64_t word) {
     *reinterpret_cast<uint64_t *>(&tile[(sl * SA_ROWS + ii) * SA_STRIDE + grp * 8]) = word;
-  });
+  };
+  if (row_ok && p0 + grp * 8 < K)
+    for_each_residue_word(y, n, W, put);
+  else  // padding only (rows beyond M, entries beyond K): every residue zero
+    for (int sl = 0; sl < n; ++sl) put(sl, 0);
   __syncthreads();
   const int row = t / 8, seg = (t % 8) * 8;
   for (int s = 0; s < n; ++s) {
@@ -323,9 +349,13 @@ __device__ __forceinline__ void crt_slice_b_one(const double *__restrict__ B, in
       for (int w = 0; w < 4; ++w) y[e][w] = bias_word(w);
     }
   }
-  for_each_residue_word(y, n, W, [&](int sl, uint64_t word) {
+  auto put = [&](int sl, uint64_t word) {
     *reinterpret_cast<uint64_t *>(Bs + (((int64_t)sl * N_pad + j) * K_pad + p8)) = word;
-  });
+  };
+  if (col_ok && p8 < K)
+    for_each_residue_word(y, n, W, put);
+  else  // padding only: every residue zero
+    for (int sl = 0; sl < n; ++sl) put(sl, 0);
 }
 
 // ---- reconstruction ---------------------------------------------------------------
@@ -460,8 +490,6 @@ __device__ __forceinline__ uint32_t crt_pack4(uint32_t v0, uint32_t v1, uint32_t
 // and |C'| < 2^(8 nbe - 2) makes bit 8 nbe - 1 the sign.  One tcgen05 u8 x u8
 // MMA per output column of a 128-row tile gives the S_b of 128 outputs.
 // nbe = crt_tc_bytes(W, k).
-// MMA columns: nbe + 4 rounded up to 16 (32 or 48).
-__host__ __device__ inline int crt_tc_cols(int nbe) { return (nbe + 4 + 15) / 16 * 16; }
 constexpr int CTC_THREADS = 128;                   // one output row per thread and TMEM lane
 constexpr int CTC_QUADS = 8;                       // column quads per CTA
 constexpr int CTC_B_BYTES = 48 * 128;              // E tile: up to 48 rows of 128 bytes (swizzled)
@@ -512,30 +540,10 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
     mftc::tmem_relinquish();
   }
   // the E tile: row b = T holds E[t][b] at byte t (moduli 32 kt .. in bytes 32 kt ..)
-  if (T < 48) {
+  if (T < CRT_EB_ROWS)
     for (int kt = 0; kt < ktn; ++kt)
-      for (int h = 0; h < 2; ++h) {
-        uint32_t w4[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          uint32_t word = 0;
-#pragma unroll
-          for (int bb = 0; bb < 4; ++bb) {
-            const int t = 32 * kt + 16 * h + 4 * q + bb;
-            uint32_t v = 0;
-            if (t < n && T < nb) {
-              if (T < 3)
-                v = (cc->cfix[t] >> (8 * T)) & 0xFFu;
-              else if (T >= 4 && T < 4 + nbe)
-                v = (cc->ew[t][(T - 4) >> 2] >> (8 * (T & 3))) & 0xFFu;
-            }
-            word |= v << (8 * bb);
-          }
-          w4[q] = word;
-        }
-        sw128_store16(sB, T, 2 * kt + h, make_uint4(w4[0], w4[1], w4[2], w4[3]));
-      }
-  }
+      for (int h = 0; h < 2; ++h)
+        sw128_store16(sB, T, 2 * kt + h, *reinterpret_cast<const uint4 *>(&cc->eb[T][32 * kt + 16 * h]));
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   mftc::tc_fence_before();
   __syncthreads();
