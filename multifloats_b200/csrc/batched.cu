@@ -954,7 +954,7 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
   // the residue tile of g_crt_slice_a holds the most moduli of any product
   int nsl_max = 1;
   for (int q = 0; q < np; ++q) nsl_max = std::max(nsl_max, probs[q].nsl);
-  const size_t crt_tile = (size_t)nsl_max * SA_ROWS * SA_STRIDE;
+  const size_t crt_tile = (size_t)std::min(nsl_max, CRT_SA_MODULI) * SA_ROWS * SA_STRIDE;
   int mma_grid = sm_count();
   if (mma_grid > total[PH_ITEMS]) mma_grid = (int)std::max<int64_t>(total[PH_ITEMS], 1);
   int rc = capture(b, [&](cudaStream_t cs) {

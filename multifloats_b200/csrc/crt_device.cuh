@@ -263,10 +263,10 @@ __device__ __forceinline__ void digit_words(const uint32_t (&y)[4], uint32_t (&d
   for (int w = 0; w < 4; ++w) dw[w] = y[w] ^ bias_word(w);
 }
 // Calls f(t, word) with the residues modulo m_t of 8 entries packed in entry
-// order (byte e = entry e), for t < n.
+// order (byte e = entry e), for t0 <= t < t1.
 template <int NW, class F>
-__device__ __forceinline__ void residue_words_nw(const uint32_t (&dw)[8][4], int n, F f) {
-  for (int t = 0; t < n; ++t) {
+__device__ __forceinline__ void residue_words_nw(const uint32_t (&dw)[8][4], int t0, int t1, F f) {
+  for (int t = t0; t < t1; ++t) {
     const ModConst k = mod_const(t);
     uint32_t r[8];
 #pragma unroll
@@ -278,19 +278,20 @@ __device__ __forceinline__ void residue_words_nw(const uint32_t (&dw)[8][4], int
   }
 }
 template <class F>
-__device__ __forceinline__ void for_each_residue_word(const uint32_t (&y)[8][4], int n, int W, F f) {
-  uint32_t dw[8][4];
-#pragma unroll
-  for (int e = 0; e < 8; ++e) digit_words(y[e], dw[e]);
+__device__ __forceinline__ void for_each_residue_word(const uint32_t (&dw)[8][4], int t0, int t1, int W, F f) {
   if (W <= 94)
-    residue_words_nw<3>(dw, n, f);
+    residue_words_nw<3>(dw, t0, t1, f);
   else
-    residue_words_nw<4>(dw, n, f);
+    residue_words_nw<4>(dw, t0, t1, f);
 }
+// Moduli whose residues the A slicer's transposing tile holds at once (the
+// tile is reused for the rest): a smaller tile lets more CTAs share an SM.
+constexpr int CRT_SA_MODULI = 18;
 
 // A (m x k column-major view) -> As[t][i][p], as slice_a_body with residues
 // for digits; the transposing tile lives in dynamic shared memory
-// (n * SA_ROWS * SA_STRIDE bytes).
+// (min(n, CRT_SA_MODULI) * SA_ROWS * SA_STRIDE bytes) and takes the moduli in
+// groups of CRT_SA_MODULI.
 __device__ __forceinline__ void crt_slice_a_body(const double *__restrict__ A, int64_t M, int64_t K,
                                                  int64_t stride, int64_t M_pad, int64_t K_pad, const int *sig,
                                                  const int *flag, const Plan *plan, int8_t *__restrict__ As,
@@ -314,18 +315,26 @@ __device__ __forceinline__ void crt_slice_a_body(const double *__restrict__ A, i
       for (int w = 0; w < 4; ++w) y[e][w] = bias_word(w);  // X = 0: every residue zero
     }
   }
-  auto put = [&](int sl, uint64_t word) {
-    *reinterpret_cast<uint64_t *>(&tile[(sl * SA_ROWS + ii) * SA_STRIDE + grp * 8]) = word;
-  };
-  if (row_ok && p0 + grp * 8 < K)
-    for_each_residue_word(y, n, W, put);
-  else  // padding only (rows beyond M, entries beyond K): every residue zero
-    for (int sl = 0; sl < n; ++sl) put(sl, 0);
-  __syncthreads();
+  uint32_t dw[8][4];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) digit_words(y[e], dw[e]);
+  const bool any = row_ok && p0 + grp * 8 < K;  // else padding only: every residue zero
   const int row = t / 8, seg = (t % 8) * 8;
-  for (int s = 0; s < n; ++s) {
-    uint64_t v = *reinterpret_cast<const uint64_t *>(&tile[(s * SA_ROWS + row) * SA_STRIDE + seg]);
-    *reinterpret_cast<uint64_t *>(As + ((s * M_pad + i0 + row) * K_pad + p0 + seg)) = v;
+  for (int t0 = 0; t0 < n; t0 += CRT_SA_MODULI) {  // moduli t0 .. t1 - 1 in tile slots 0 ..
+    const int t1 = min(n, t0 + CRT_SA_MODULI);
+    auto put = [&](int sl, uint64_t word) {
+      *reinterpret_cast<uint64_t *>(&tile[((sl - t0) * SA_ROWS + ii) * SA_STRIDE + grp * 8]) = word;
+    };
+    if (t0 > 0) __syncthreads();  // the previous moduli's rows have been copied out
+    if (any)
+      for_each_residue_word(dw, t0, t1, W, put);
+    else
+      for (int sl = t0; sl < t1; ++sl) put(sl, 0);
+    __syncthreads();
+    for (int s = t0; s < t1; ++s) {
+      uint64_t v = *reinterpret_cast<const uint64_t *>(&tile[((s - t0) * SA_ROWS + row) * SA_STRIDE + seg]);
+      *reinterpret_cast<uint64_t *>(As + ((s * M_pad + i0 + row) * K_pad + p0 + seg)) = v;
+    }
   }
 }
 
@@ -352,10 +361,14 @@ __device__ __forceinline__ void crt_slice_b_one(const double *__restrict__ B, in
   auto put = [&](int sl, uint64_t word) {
     *reinterpret_cast<uint64_t *>(Bs + (((int64_t)sl * N_pad + j) * K_pad + p8)) = word;
   };
-  if (col_ok && p8 < K)
-    for_each_residue_word(y, n, W, put);
-  else  // padding only: every residue zero
+  if (col_ok && p8 < K) {
+    uint32_t dw[8][4];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) digit_words(y[e], dw[e]);
+    for_each_residue_word(dw, 0, n, W, put);
+  } else {  // padding only: every residue zero
     for (int sl = 0; sl < n; ++sl) put(sl, 0);
+  }
 }
 
 // ---- reconstruction ---------------------------------------------------------------

@@ -932,7 +932,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     const dim3 gb((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad);
     for (int o = 0; o < nops; ++o) {
       if (o < nA && crt)
-        crt_slice_a_kernel<<<ga, 256, L.nsl * SA_ROWS * SA_STRIDE, s>>>(aview[o], m, k, astride[o], L.M_pad,
+        crt_slice_a_kernel<<<ga, 256, std::min(L.nsl, CRT_SA_MODULI) * SA_ROWS * SA_STRIDE, s>>>(aview[o], m, k, astride[o], L.M_pad,
                                                                        L.K_pad, sig[o], flag[o], plan, sl[o]);
       else if (o < nA)
         slice_a_kernel<<<ga, 256, 0, s>>>(aview[o], m, k, astride[o], L.M_pad, L.K_pad, sig[o], flag[o], plan,
