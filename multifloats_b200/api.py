@@ -123,6 +123,117 @@ def cmatmuldd_mm(a, b, m: int, k: int, n: int, renorm_interval: int = 8, out=Non
     return c
 
 
+# ---- split-INT8 forms (no reference counterpart) --------------------------------------
+_SPLIT_SYMS = {("split", False): ("mfcuda_matmuldd_mm_split", "matmuldd_mm_split"),
+               ("split", True): ("mfcuda_cmatmuldd_mm_split", "cmatmuldd_mm_split"),
+               ("crt", False): ("mfcuda_matmuldd_mm_crt", "matmuldd_mm_crt"),
+               ("crt", True): ("mfcuda_cmatmuldd_mm_crt", "cmatmuldd_mm_crt")}
+
+
+def _split_call(form: str, cplx: bool, a, b, m: int, k: int, n: int, arg: int, target: float, out):
+    L = lib()
+    w = 4 if cplx else 2
+    dev_sym, host_sym = _SPLIT_SYMS[(form, cplx)]
+    if _is_dev(a):
+        a, b = _dev_check(a, w * m * k, "a"), _dev_check(b, w * k * n, "b")
+        c = out if out is not None else _empty_like_kind(a, w * m * n)
+        nfo = (C.c_int * 4)()
+        check(getattr(L, dev_sym)(_ptr(a), _ptr(b), _ptr(c), m, k, n, arg, target, None, 0, nfo, _stream()),
+              dev_sym)
+        if form == "split":
+            return c, {"slices": nfo[0], "rho_a": nfo[1], "rho_b": nfo[2]}
+        return c, {"moduli": nfo[0], "rho_a": nfo[1], "rho_b": nfo[2], "bits": nfo[3]}
+    if target != 8.0:
+        raise ValueError("the host-pointer split calls use the target 8 (k 2^-104 (|A||B|)_ij units); "
+                         "pass CUDA tensors for another target")
+    a, b = _host(a, w * m * k, "a"), _host(b, w * k * n, "b")
+    c = out if out is not None else np.empty(w * m * n)
+    bound = C.c_double(0.0)
+    getattr(L, host_sym)(_ptr(a), _ptr(b), _ptr(c), m, k, n, arg, C.byref(bound))
+    check_last(host_sym)
+    return c, {"bound": bound.value}
+
+
+def matmuldd_mm_split(a, b, m: int, k: int, n: int, slices: int = 0, target: float = 8.0, out=None):
+    """C = A B by the digit-sliced split-INT8 form, within target k 2^-104
+    (|A||B|)_ij.  Returns (C, info): the plan (slices, rho_a, rho_b) for CUDA
+    tensors, the a-priori bound for host arrays."""
+    return _split_call("split", False, a, b, m, k, n, slices, target, out)
+
+
+def matmuldd_mm_crt(a, b, m: int, k: int, n: int, bits: int = 0, target: float = 8.0, out=None):
+    """C = A B by the CRT (modular) split form; `bits` fixes the operand width W
+    (0: the smallest meeting `target`).  Returns (C, info): the plan (moduli,
+    rho_a, rho_b, bits) for CUDA tensors, the a-priori bound for host arrays."""
+    return _split_call("crt", False, a, b, m, k, n, bits, target, out)
+
+
+def cmatmuldd_mm_split(a, b, m: int, k: int, n: int, slices: int = 0, target: float = 8.0, out=None):
+    """Complex (complex64x2) digit-sliced form; see matmuldd_mm_split."""
+    return _split_call("split", True, a, b, m, k, n, slices, target, out)
+
+
+def cmatmuldd_mm_crt(a, b, m: int, k: int, n: int, bits: int = 0, target: float = 8.0, out=None):
+    """Complex (complex64x2) CRT form; see matmuldd_mm_crt."""
+    return _split_call("crt", True, a, b, m, k, n, bits, target, out)
+
+
+# ---- batch plans (no reference counterpart) ------------------------------------------
+FORM = {"plain": 0, "split": 1, "crt": 2}
+
+
+class GemmBatch:
+    """A plan over many independent products of CUDA tensors, replayed as one
+    CUDA-graph launch (mfcuda_batch_create_gemm / _cgemm).  problems: a list of
+    (a, b, c, m, k, n); the tensors must outlive the plan, and refilling them
+    between runs is how new data enters.  form: "plain", "split" or "crt";
+    `slices` is the slice count (split) or the operand width (crt)."""
+
+    def __init__(self, problems, form: str = "split", renorm_interval: int = 8, slices: int = 0,
+                 target: float = 8.0, tune: bool = False, complex_: bool = False):
+        from ._lib import gemm_desc
+
+        w = 4 if complex_ else 2
+        descs = (gemm_desc * max(len(problems), 1))()
+        for i, (a, b, c, m, k, n) in enumerate(problems):
+            if m * n:
+                _dev_check(c, w * m * n, "c")
+            if m * k * n:
+                _dev_check(a, w * m * k, "a")
+                _dev_check(b, w * k * n, "b")
+            descs[i].a, descs[i].b, descs[i].c = _ptr(a) or None, _ptr(b) or None, _ptr(c) or None
+            descs[i].m, descs[i].k, descs[i].n = m, k, n
+        self._keep = problems
+        self._plan = C.c_void_p()
+        fn = "mfcuda_batch_create_cgemm" if complex_ else "mfcuda_batch_create_gemm"
+        check(getattr(lib(), fn)(descs, len(problems), FORM[form], renorm_interval, slices, target, int(tune),
+                                 C.byref(self._plan)), fn)
+
+    def run(self):
+        check(lib().mfcuda_batch_run(self._plan, _stream()), "mfcuda_batch_run")
+
+    def status(self) -> int:
+        """Waits for the device; MFCUDA_ERR_TIMEOUT if a bounded device wait of the last run expired."""
+        return lib().mfcuda_batch_status(self._plan)
+
+    def close(self):
+        if self._plan:
+            lib().mfcuda_batch_destroy(self._plan)
+            self._plan = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---- elementwise ---------------------------------------------------------------
 def unary(op: str, x, out=None):
     """y[i] = op(x[i]) for op in exp, log, sin, cos, sqrt, exp2, log2, log10."""

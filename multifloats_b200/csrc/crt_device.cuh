@@ -136,12 +136,19 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
     }
     int W = bits;
     if (W <= 0) {
-      W = CRT_WMAX;
-      for (int w = 8; w <= CRT_WMAX; ++w)
-        if (crt_bound(w, ra, rb, k) <= target) {
-          W = w;
-          break;
+      // the smallest w in [8, CRT_WMAX] with crt_bound <= target (CRT_WMAX if
+      // none); the bound falls strictly with w, so bisection finds it
+      int lo = 8, hi = CRT_WMAX;
+      if (crt_bound(hi, ra, rb, k) <= target) {
+        while (lo < hi) {
+          const int mid = (lo + hi) / 2;
+          if (crt_bound(mid, ra, rb, k) <= target)
+            hi = mid;
+          else
+            lo = mid + 1;
         }
+      }
+      W = hi;
     }
     const int n = crt_moduli(W, k, crt_lg);
     plan->S = n;

@@ -221,3 +221,40 @@ def test_column_panels_agree_on_width(cuda_lib, dev):
     want, info = dev_crt(cuda_lib, dev, A, B, m, k, n)
     assert info[3] == w_all
     assert O.same_bits(got, want).all()
+
+
+def test_python_api_split_forms_and_batch(cuda_lib, dev):
+    """multifloats_b200.api: the split and CRT wrappers on host arrays and CUDA
+    tensors, and GemmBatch, give the C ABI's bits."""
+    import torch
+
+    from multifloats_b200 import api
+
+    m, k, n = 130, 170, 90
+    A, B = W.dd_rowcol_scaled(m, k, 16, "row", 81), W.dd_rowcol_scaled(k, n, 16, "col", 82)
+    want, winfo = O.crt_gemm(A, B, m, k, n)
+    c, info = api.matmuldd_mm_crt(to_dev(A, dev), to_dev(B, dev), m, k, n)
+    assert O.same_bits(to_host(c), want).all()
+    assert [info["moduli"], info["rho_a"], info["rho_b"], info["bits"]] == winfo
+    h, hinfo = api.matmuldd_mm_crt(A, B, m, k, n)
+    assert O.same_bits(h, want).all() and hinfo["bound"] == pytest.approx(O.crt_bound(winfo[3], winfo[1], winfo[2], k))
+    swant, sinfo = O.split_gemm(A, B, m, k, n)
+    s, si = api.matmuldd_mm_split(to_dev(A, dev), to_dev(B, dev), m, k, n)
+    assert O.same_bits(to_host(s), swant).all() and si["slices"] == sinfo[0]
+    with pytest.raises(ValueError):
+        api.matmuldd_mm_crt(A, B, m, k, n, target=4.0)  # host calls have the fixed target 8
+    Z = (W.complex_from_parts(A, W.dd_rowcol_scaled(m, k, 16, "row", 83)),
+         W.complex_from_parts(B, W.dd_rowcol_scaled(k, n, 16, "col", 84)))
+    zc, _ = api.cmatmuldd_mm_crt(to_dev(Z[0], dev), to_dev(Z[1], dev), m, k, n)
+    assert O.same_bits(to_host(zc), O.crt_cgemm(Z[0], Z[1], m, k, n)[0]).all()
+    shapes = [(m, k, n), (40, 300, 70), (1, 5, 3)]
+    probs = []
+    for i, (mm, kk, nn) in enumerate(shapes):
+        a = to_dev(W.dd_uniform(mm * kk, seed=90 + i), dev)
+        b = to_dev(W.dd_uniform(kk * nn, seed=95 + i), dev)
+        probs.append((a, b, torch.empty(2 * mm * nn, dtype=torch.float64, device=dev), mm, kk, nn))
+    with api.GemmBatch(probs, form="crt") as bt:
+        bt.run()
+        assert bt.status() == 0
+        for a, b, cc, mm, kk, nn in probs:
+            assert O.same_bits(to_host(cc), O.crt_gemm(to_host(a), to_host(b), mm, kk, nn)[0]).all()
