@@ -705,7 +705,7 @@ static int pair_nsub() {
   return v;
 }
 
-static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB, int nsl = SMAX) {
+static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB, int nsl = SMAX, bool crt = false) {
   Layout L;
   L.nsl = nsl;
   L.pair = use_pair(m);
@@ -730,7 +730,8 @@ static Layout layout(int64_t m, int64_t k, int64_t n, int nA, int nB, int nsl = 
     L.off_stats[o] = take(3 * sizeof(int) * rows);
     L.off_slices[o] = take((size_t)nsl * rows * L.K_pad);
   }
-  L.off_D = take((size_t)nsl * L.nkc * L.N_pad * L.M_pad * sizeof(int32_t));
+  // INT32 diagonal sums, or (CRT) one residue byte per output, modulus and K chunk
+  L.off_D = take((size_t)nsl * L.nkc * L.N_pad * L.M_pad * (crt ? 1 : sizeof(int32_t)));
   L.total = off + 256 /* status word */;
   return L;
 }
@@ -813,7 +814,7 @@ size_t workspace_size(int64_t m, int64_t k, int64_t n, bool complex_operands) {
 }
 size_t crt_workspace_size(int64_t m, int64_t k, int64_t n, int bits, bool complex_operands) {
   int no = complex_operands ? 2 : 1;
-  return layout(m, k, n, no, no, crt_slices_max(k, bits)).total;
+  return layout(m, k, n, no, no, crt_slices_max(k, bits), true).total;
 }
 
 static std::once_flag g_attr_once;
@@ -866,7 +867,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                         const Product *prods, int nprod, int64_t m, int64_t k, int64_t n, int slices,
                         double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info, int crt = 0,
                         const PanelSink *sink = nullptr) {
-  Layout L = layout(m, k, n, nA, nB, crt ? crt_slices_max(k, slices) : SMAX);
+  Layout L = layout(m, k, n, nA, nB, crt ? crt_slices_max(k, slices) : SMAX, crt != 0);
   if (L.M_pad > INT32_MAX / 2 || L.N_pad > INT32_MAX / 2 || L.kblocks > INT32_MAX / 2 ||
       L.N_pad > 65535 || L.K_pad / 64 > 65535)
     return MFCUDA_ERR_UNSUPPORTED;
