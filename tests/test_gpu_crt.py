@@ -258,3 +258,15 @@ def test_python_api_split_forms_and_batch(cuda_lib, dev):
         assert bt.status() == 0
         for a, b, cc, mm, kk, nn in probs:
             assert O.same_bits(to_host(cc), O.crt_gemm(to_host(a), to_host(b), mm, kk, nn)[0]).all()
+
+
+def test_widest_plan_two_k_steps_in_reconstruction(cuda_lib, dev):
+    """W = 110 with k = 300000 needs 33 moduli: the reconstruction's MMA takes
+    two K steps of 32 moduli, its E matrix 48 columns, and the residues of 33
+    K chunks are summed per modulus first."""
+    m, k, n = 5, 300000, 7
+    A, B = W.dd_uniform(m * k, seed=201), W.dd_uniform(k * n, seed=202)
+    got, info = dev_crt(cuda_lib, dev, A, B, m, k, n, bits=110)
+    want, winfo = O.crt_gemm(A, B, m, k, n, bits=110)
+    assert info == winfo and info[0] == 33 and info[3] == 110
+    assert O.same_bits(got, want).all()
