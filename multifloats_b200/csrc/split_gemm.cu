@@ -33,6 +33,14 @@
 // With |a_ip| >= 2^(sigma_i - rho_A) and |b_pj| >= 2^(tau_j - rho_B) this is at
 // most (S+1) 2^(106 - 8S + rho_A + rho_B) times k 2^-104 (|A||B|)_ij, which is
 // how the plan picks S for a target (S = 14 gives 15/16 for rho_A = rho_B = 1).
+//
+// The CRT form (crt_device.cuh) shares steps 1 and 3's rounding and the
+// tensor-core kernels: residues modulo N moduli instead of digits, one product
+// per modulus (u8 x u8), the epilogue reducing each INT32 sum to a residue
+// byte, and a tensor-core reconstruction (crt_combine_tc_kernel).  Large
+// outputs run on CTA pairs (split_mma_pair_kernel, 256 x 512 tiles, eight
+// epilogue warps); host-pointer CRT calls compute the output in column panels
+// and copy each back while the next is computed (PanelSink).
 #include <cudaTypedefs.h>
 
 #include <mutex>
