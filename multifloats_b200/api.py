@@ -47,10 +47,21 @@ def _host(x, n_doubles: int, name: str) -> np.ndarray:
 
 
 def _dev_check(x, n_doubles: int, name: str):
+    """A device call's operand must be a contiguous float64 CUDA tensor: a host
+    pointer handed to a kernel would fault, so mixed host / device operands
+    are refused here."""
     import torch
 
-    if x.dtype != torch.float64 or not x.is_contiguous() or x.numel() != n_doubles:
+    if (not _is_dev(x) or x.dtype != torch.float64 or not x.is_contiguous() or x.numel() != n_doubles):
         raise ValueError(f"{name}: expected a contiguous float64 CUDA tensor of {n_doubles} doubles")
+    return x
+
+
+def _host_out(x, n_doubles: int, name: str) -> np.ndarray:
+    """A caller-supplied host output must be written in place: a C-contiguous
+    float64 numpy array of exactly n_doubles entries."""
+    if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous and x.size == n_doubles):
+        raise ValueError(f"{name}: expected a C-contiguous float64 numpy array of {n_doubles} doubles")
     return x
 
 
@@ -68,12 +79,12 @@ def matmuldd_mm(a, b, m: int, k: int, n: int, renorm_interval: int = 8, out=None
     L = lib()
     if _is_dev(a):
         a, b = _dev_check(a, 2 * m * k, "a"), _dev_check(b, 2 * k * n, "b")
-        c = out if out is not None else _empty_like_kind(a, 2 * m * n)
+        c = _dev_check(out, 2 * m * n, "out") if out is not None else _empty_like_kind(a, 2 * m * n)
         check(L.mfcuda_matmuldd_mm(_ptr(a), _ptr(b), _ptr(c), m, k, n, renorm_interval, _stream()),
               "mfcuda_matmuldd_mm")
         return c
     a, b = _host(a, 2 * m * k, "a"), _host(b, 2 * k * n, "b")
-    c = out if out is not None else np.empty(2 * m * n)
+    c = _host_out(out, 2 * m * n, "out") if out is not None else np.empty(2 * m * n)
     L.matmuldd_mm(_ptr(a), _ptr(b), _ptr(c), m, k, n, renorm_interval)
     check_last("matmuldd_mm")
     return c
@@ -112,12 +123,12 @@ def cmatmuldd_mm(a, b, m: int, k: int, n: int, renorm_interval: int = 8, out=Non
     L = lib()
     if _is_dev(a):
         a, b = _dev_check(a, 4 * m * k, "a"), _dev_check(b, 4 * k * n, "b")
-        c = out if out is not None else _empty_like_kind(a, 4 * m * n)
+        c = _dev_check(out, 4 * m * n, "out") if out is not None else _empty_like_kind(a, 4 * m * n)
         check(L.mfcuda_cmatmuldd_mm(_ptr(a), _ptr(b), _ptr(c), m, k, n, renorm_interval, _stream()),
               "mfcuda_cmatmuldd_mm")
         return c
     a, b = _host(a, 4 * m * k, "a"), _host(b, 4 * k * n, "b")
-    c = out if out is not None else np.empty(4 * m * n)
+    c = _host_out(out, 4 * m * n, "out") if out is not None else np.empty(4 * m * n)
     L.cmatmuldd_mm(_ptr(a), _ptr(b), _ptr(c), m, k, n, renorm_interval)
     check_last("cmatmuldd_mm")
     return c
@@ -136,7 +147,7 @@ def _split_call(form: str, cplx: bool, a, b, m: int, k: int, n: int, arg: int, t
     dev_sym, host_sym = _SPLIT_SYMS[(form, cplx)]
     if _is_dev(a):
         a, b = _dev_check(a, w * m * k, "a"), _dev_check(b, w * k * n, "b")
-        c = out if out is not None else _empty_like_kind(a, w * m * n)
+        c = _dev_check(out, w * m * n, "out") if out is not None else _empty_like_kind(a, w * m * n)
         nfo = (C.c_int * 4)()
         check(getattr(L, dev_sym)(_ptr(a), _ptr(b), _ptr(c), m, k, n, arg, target, None, 0, nfo, _stream()),
               dev_sym)
@@ -147,7 +158,7 @@ def _split_call(form: str, cplx: bool, a, b, m: int, k: int, n: int, arg: int, t
         raise ValueError("the host-pointer split calls use the target 8 (k 2^-104 (|A||B|)_ij units); "
                          "pass CUDA tensors for another target")
     a, b = _host(a, w * m * k, "a"), _host(b, w * k * n, "b")
-    c = out if out is not None else np.empty(w * m * n)
+    c = _host_out(out, w * m * n, "out") if out is not None else np.empty(w * m * n)
     bound = C.c_double(0.0)
     getattr(L, host_sym)(_ptr(a), _ptr(b), _ptr(c), m, k, n, arg, C.byref(bound))
     check_last(host_sym)
@@ -242,11 +253,11 @@ def unary(op: str, x, out=None):
     n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 2
     if _is_dev(x):
         x = _dev_check(x, 2 * n, "x")
-        y = out if out is not None else _empty_like_kind(x, 2 * n)
+        y = _dev_check(out, 2 * n, "out") if out is not None else _empty_like_kind(x, 2 * n)
         check(L.mfcuda_unary_dd(code, _ptr(x), _ptr(y), n, _stream()), "mfcuda_unary_dd")
         return y
     x = _host(x, 2 * n, "x")
-    y = out if out is not None else np.empty(2 * n)
+    y = _host_out(out, 2 * n, "out") if out is not None else np.empty(2 * n)
     getattr(L, f"{op}dd_array")(_ptr(x), _ptr(y), n)
     check_last(f"{op}dd_array")
     return y
@@ -258,13 +269,13 @@ def sincos(x, s=None, c=None):
     n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 2
     if _is_dev(x):
         x = _dev_check(x, 2 * n, "x")
-        s = s if s is not None else _empty_like_kind(x, 2 * n)
-        c = c if c is not None else _empty_like_kind(x, 2 * n)
+        s = _dev_check(s, 2 * n, "s") if s is not None else _empty_like_kind(x, 2 * n)
+        c = _dev_check(c, 2 * n, "c") if c is not None else _empty_like_kind(x, 2 * n)
         check(L.mfcuda_sincos_dd(_ptr(x), _ptr(s), _ptr(c), n, _stream()), "mfcuda_sincos_dd")
         return s, c
     x = _host(x, 2 * n, "x")
-    s = s if s is not None else np.empty(2 * n)
-    c = c if c is not None else np.empty(2 * n)
+    s = _host_out(s, 2 * n, "s") if s is not None else np.empty(2 * n)
+    c = _host_out(c, 2 * n, "c") if c is not None else np.empty(2 * n)
     L.sincosdd_array(_ptr(x), _ptr(s), _ptr(c), n)
     check_last("sincosdd_array")
     return s, c
@@ -276,11 +287,11 @@ def cexpi(x, out=None):
     n = (x.numel() if _is_dev(x) else np.asarray(x).size) // 2
     if _is_dev(x):
         x = _dev_check(x, 2 * n, "x")
-        z = out if out is not None else _empty_like_kind(x, 4 * n)
+        z = _dev_check(out, 4 * n, "out") if out is not None else _empty_like_kind(x, 4 * n)
         check(L.mfcuda_cexpi_dd(_ptr(x), _ptr(z), n, _stream()), "mfcuda_cexpi_dd")
         return z
     x = _host(x, 2 * n, "x")
-    z = out if out is not None else np.empty(4 * n)
+    z = _host_out(out, 4 * n, "out") if out is not None else np.empty(4 * n)
     L.cexpidd_array(_ptr(x), _ptr(z), n)
     check_last("cexpidd_array")
     return z
@@ -292,11 +303,11 @@ def cexp(z, out=None):
     n = (z.numel() if _is_dev(z) else np.asarray(z).size) // 4
     if _is_dev(z):
         z = _dev_check(z, 4 * n, "z")
-        w = out if out is not None else _empty_like_kind(z, 4 * n)
+        w = _dev_check(out, 4 * n, "out") if out is not None else _empty_like_kind(z, 4 * n)
         check(L.mfcuda_cexp_dd(_ptr(z), _ptr(w), n, _stream()), "mfcuda_cexp_dd")
         return w
     z = _host(z, 4 * n, "z")
-    w = out if out is not None else np.empty(4 * n)
+    w = _host_out(out, 4 * n, "out") if out is not None else np.empty(4 * n)
     L.cexpdd_array(_ptr(z), _ptr(w), n)
     check_last("cexpdd_array")
     return w

@@ -243,6 +243,8 @@ def test_python_api_split_forms_and_batch(cuda_lib, dev):
     assert O.same_bits(to_host(s), swant).all() and si["slices"] == sinfo[0]
     with pytest.raises(ValueError):
         api.matmuldd_mm_crt(A, B, m, k, n, target=4.0)  # host calls have the fixed target 8
+    with pytest.raises(ValueError):  # a host operand beside a device one is refused, not dereferenced
+        api.matmuldd_mm_crt(to_dev(A, dev), torch.from_numpy(B), m, k, n)
     Z = (W.complex_from_parts(A, W.dd_rowcol_scaled(m, k, 16, "row", 83)),
          W.complex_from_parts(B, W.dd_rowcol_scaled(k, n, 16, "col", 84)))
     zc, _ = api.cmatmuldd_mm_crt(to_dev(Z[0], dev), to_dev(Z[1], dev), m, k, n)
