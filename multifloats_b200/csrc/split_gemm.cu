@@ -1234,7 +1234,7 @@ static int crt_host(const void *a, const void *b, void *c, int64_t m, int64_t k,
   pc.copy = st.copy;
   pc.ev = st.ev;
   pc.nev = kStagingEvents;
-  constexpr int kPanels = 4;
+  constexpr int kPanels = 8;  // small panels: the first copy starts early (copy-bound call)
   const split::PanelSink sink = {kPanels, copy_panel, &pc};
   int rc;
   if (CPLX)

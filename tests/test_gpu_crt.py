@@ -134,8 +134,8 @@ def test_host_dropin(cuda_lib):
 def test_host_dropin_column_panels(cuda_lib, dev):
     """The host-pointer call computes the output in column panels and copies
     each back while the next is computed: the same bits as the device call,
-    with uneven panels (five 512-column tiles in four panels, the last one
-    ragged)."""
+    with a ragged last panel (2100 columns: five 512-column tiles, one panel
+    each, the last one 52 columns wide)."""
     m, k, n = 300, 700, 2100
     A, B = W.dd_rowcol_scaled(m, k, 16, "row", 18), W.dd_rowcol_scaled(k, n, 16, "col", 19)
     got, info = dev_crt(cuda_lib, dev, A, B, m, k, n)
