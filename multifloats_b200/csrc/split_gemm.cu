@@ -658,10 +658,10 @@ __global__ void __launch_bounds__(256) crt_slice_a_kernel(const double *__restri
 __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restrict__ B, int64_t K, int64_t N,
                                                           int64_t stride, int64_t N_pad, int64_t K_pad,
                                                           const int *sig, const int *flag, const Plan *plan,
-                                                          int8_t *__restrict__ Bs) {
+                                                          int8_t *__restrict__ Bs, int64_t j0) {
   const int64_t p8 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 8;
   if (p8 >= K_pad) return;
-  crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, blockIdx.y, p8);
+  crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, j0 + blockIdx.y, p8);  // column j0 + y
 }
 // Tensor-core reconstruction (crt_combine_tc_body): block (x, y) takes rows
 // 128 x .. of column quads qbase + CTC_QUADS y .. (columns below N); dynamic shared memory
@@ -939,7 +939,14 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     mark(1, s);
     const dim3 ga((unsigned)(L.M_pad / 32), (unsigned)(L.K_pad / 64));
     const dim3 gb((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad);
+    // column panels (CRT form on CTA pairs, when a sink wants the output panel
+    // by panel): B's residues, every product and the reconstruction of panel p,
+    // then the sink, then panel p + 1
+    const int tn_cols = BN * L.nsub;
+    const int ntn_all = (int)(L.N_pad / tn_cols);
+    const int npan = (sink && crt && L.pair) ? std::max(1, std::min(sink->panels, ntn_all)) : 1;
     for (int o = 0; o < nops; ++o) {
+      if (o >= nA && npan > 1) continue;  // sliced panel by panel below
       if (o < nA && crt)
         crt_slice_a_kernel<<<ga, 256, std::min(L.nsl, CRT_SA_MODULI) * SA_ROWS * SA_STRIDE, s>>>(aview[o], m, k, astride[o], L.M_pad,
                                                                        L.K_pad, sig[o], flag[o], plan, sl[o]);
@@ -948,7 +955,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                                           sl[o]);
       else if (crt)
         crt_slice_b_kernel<<<gb, 256, 0, s>>>(bview[o - nA], k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o],
-                                              flag[o], plan, sl[o]);
+                                              flag[o], plan, sl[o], 0);
       else
         slice_b_kernel<<<gb, 256, 0, s>>>(bview[o - nA], k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o],
                                           flag[o], plan, sl[o]);
@@ -971,15 +978,15 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
       if (!make_map(&tmA[q], sl[prods[q].a], L.M_pad, L.K_pad, BM, L.nsl) ||
           !make_map(&tmB[q], sl[nA + prods[q].b], L.N_pad, L.K_pad, L.pair ? 128 : BN, L.nsl))
         rc = MFCUDA_ERR_CUDA;
-    // column panels (CRT form on CTA pairs, when a sink wants the output panel
-    // by panel): every product of panel p, then the sink, then panel p + 1
-    const int tn_cols = BN * L.nsub;
-    const int ntn_all = (int)(L.N_pad / tn_cols);
-    const int npan = (sink && crt && L.pair) ? std::max(1, std::min(sink->panels, ntn_all)) : 1;
     for (int pp = 0; pp < npan && rc == MFCUDA_OK; ++pp) {
       const int tn0 = (int)((int64_t)ntn_all * pp / npan), tn1 = (int)((int64_t)ntn_all * (pp + 1) / npan);
       const int64_t j0 = npan == 1 ? 0 : (int64_t)tn0 * tn_cols;
       const int64_t j1 = npan == 1 ? n : std::min<int64_t>(n, (int64_t)tn1 * tn_cols);
+      if (npan > 1)  // this panel's columns of B (padding columns included)
+        for (int o = nA; o < nops; ++o)
+          crt_slice_b_kernel<<<dim3(gb.x, (unsigned)((tn1 - tn0) * tn_cols)), 256, 0, s>>>(
+              bview[o - nA], k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o], flag[o], plan, sl[o],
+              (int64_t)tn0 * tn_cols);
       int pgrid = grid;
       if (L.pair && npan > 1) {
         const int supers = ((L.nsl + 1) / 2) * (int)L.nkc * (int)(L.M_pad / tile_m) * (tn1 - tn0);
