@@ -532,6 +532,22 @@ __device__ __forceinline__ void crt_transpose4(uint32_t a, uint32_t b, uint32_t 
   o[3] = __byte_perm(ab1, cd1, 0x7632);
 }
 
+// The residue word of one modulus when the K dimension came in nkc chunks:
+// per column the chunks' residues summed and reduced again.  Kept out of line
+// so that the reconstruction's main path stays small in the instruction cache.
+static __device__ __noinline__ uint32_t crt_chunk_residue_word(const uint32_t *src, int nkc, int64_t kstride, int t) {
+  uint32_t sum[4] = {0, 0, 0, 0};
+  for (int kc = 0; kc < nkc; ++kc) {
+    const uint32_t v = __ldcs(src + kc * kstride);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) sum[r] += (v >> (8 * r)) & 0xFFu;
+  }
+  uint32_t w = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) w |= crt_mod_small(sum[r], t) << (8 * r);
+  return w;
+}
+
 // CTA of CTC_THREADS threads: rows i0 .. i0+127 of column quads qd0 ..
 // qd0+CTC_QUADS-1 (thread T: row i0+T, columns 4 qd .. 4 qd + 3).  `smem`
 // is 1024-aligned, crt_tc_smem(ceil(n / 32)) bytes.  `status` receives
@@ -582,24 +598,13 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
   // the residue words of column quad qd (modulus t: four columns in a word)
   auto load_words = [&](int64_t qd, uint32_t (&wv)[CRT_NMAX]) {
     const uint32_t *src = reinterpret_cast<const uint32_t *>(D8) + qd * M_pad + (row_ok ? i : 0);
+    if (nkc == 1) {  // the common case, kept compact: one load per modulus
 #pragma unroll
-    for (int t = 0; t < CRT_NMAX; ++t) {
-      uint32_t w = 0;
-      if (row_ok && t < n) {
-        if (nkc == 1) {
-          w = __ldcs(src + t * gstride);
-        } else {  // per-column sums of the chunks' residues, reduced again
-          uint32_t sum[4] = {0, 0, 0, 0};
-          for (int kc = 0; kc < nkc; ++kc) {
-            const uint32_t v = __ldcs(src + t * gstride + kc * kstride);
+      for (int t = 0; t < CRT_NMAX; ++t) wv[t] = (row_ok && t < n) ? __ldcs(src + t * gstride) : 0u;
+    } else {
 #pragma unroll
-            for (int r = 0; r < 4; ++r) sum[r] += (v >> (8 * r)) & 0xFFu;
-          }
-#pragma unroll
-          for (int r = 0; r < 4; ++r) w |= crt_mod_small(sum[r], t) << (8 * r);
-        }
-      }
-      wv[t] = w;
+      for (int t = 0; t < CRT_NMAX; ++t)
+        wv[t] = (row_ok && t < n) ? crt_chunk_residue_word(src + t * gstride, nkc, kstride, t) : 0u;
     }
   };
   uint32_t wv[CRT_NMAX];
