@@ -534,14 +534,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
               break;
             }
             mftc::tc_fence_after();
-            const uint32_t a0 = mftc::smem_u32(sA + stage * P_STAGE_A);
-            const uint32_t b0 = mftc::smem_u32(sB + stage * stage_b);
+            // stage descriptors built once; a K step or the second B half only moves
+            // the start-address field (address / 16, far below its 14-bit limit)
+            const uint64_t ad0 = mftc::smem_desc_k_sw128(mftc::smem_u32(sA + stage * P_STAGE_A));
+            const uint64_t bd0 = mftc::smem_desc_k_sw128(mftc::smem_u32(sB + stage * stage_b));
 #pragma unroll
             for (int kk = 0; kk < BK / UMMA_K; ++kk) {
-              const uint64_t adesc = mftc::smem_desc_k_sw128(a0 + kk * UMMA_K);
-              for (int h = 0; h < nsub; ++h)
-                mftc::umma_i8_pair(d_tmem + (uint32_t)(h * BN), adesc,
-                                   mftc::smem_desc_k_sw128(b0 + h * P_HALF_B + kk * UMMA_K), idesc, accumulate);
+              const uint64_t adesc = ad0 + (uint64_t)(kk * UMMA_K / 16);
+              mftc::umma_i8_pair(d_tmem, adesc, bd0 + (uint64_t)(kk * UMMA_K / 16), idesc, accumulate);
+              if (nsub == 2)
+                mftc::umma_i8_pair(d_tmem + (uint32_t)BN, adesc, bd0 + (uint64_t)((P_HALF_B + kk * UMMA_K) / 16),
+                                   idesc, accumulate);
               accumulate = 1;
             }
             mftc::umma_commit_pair(&empty[stage], 0x3);
