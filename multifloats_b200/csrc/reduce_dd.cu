@@ -408,13 +408,22 @@ static void *g_noalloc_addr[kNoAllocMaxDevices];
 
 // Device address of g_noalloc_partials on the current device.  In host code
 // the array's name only stands in for the symbol, so the address is looked up
-// once per device (with that device current) and cached.
-static int noalloc_scratch(void **p) {
+// with the device current.  Outside stream capture it is looked up on every
+// call (a cheap query), so an address cached before a cudaDeviceReset or the
+// re-creation of the primary context is never reused; inside a capture the
+// address cached by an earlier call on this device is used (the first call
+// on a device must therefore come before any capture).
+static int noalloc_scratch(void **p, cudaStream_t s) {
   int dev = 0;
   MF_TRY_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNoAllocMaxDevices) return MFCUDA_ERR_NO_DEVICE;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {  // e.g. the legacy stream while another captures
+    (void)cudaGetLastError();
+    cap = cudaStreamCaptureStatusActive;  // treat as capturing: no query, the cached address
+  }
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone || !g_noalloc_addr[dev]) {
     void *addr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_partials);
     if (e != cudaSuccess || !addr) {
@@ -436,7 +445,7 @@ static int dot_noalloc(const double *x, const double *y, int64_t n, int64_t ri, 
   if (blocks > kNoAllocMaxPartials) return MFCUDA_ERR_UNSUPPORTED;
   MF_TRY(require_device());
   void *scratch = nullptr;
-  MF_TRY(noalloc_scratch(&scratch));
+  MF_TRY(noalloc_scratch(&scratch, s));
   // Every partial slot [0, blocks) is written by stage 1 before stage 2 reads
   // it, so the contents left by an earlier call never leak into this one.
   dd *part = static_cast<dd *>(scratch);

@@ -49,11 +49,13 @@ def test_matches_existing_entry_point_on_consecutive_calls(cuda_lib, dev):
     # two calls in a row, the second smaller than the first so that stale
     # partials from the first call are still sitting in the shared array
     for n, ri, seed in [(MAX_N - 5, 8, 1), (123457, 3, 2)]:
-        a = to_dev(W.dd_uniform(n, seed=seed), dev)
-        b = to_dev(W.dd_uniform(n, seed=seed + 100), dev)
+        ha, hb = W.dd_uniform(n, seed=seed), W.dd_uniform(n, seed=seed + 100)
+        a, b = to_dev(ha, dev), to_dev(hb, dev)
         got = _dot_noalloc(cuda_lib, a, b, n, ri, stream)
         want = _dot_existing(cuda_lib, a, b, n, ri, stream)
         assert O.same_bits(got, want).all(), (n, got, want)
+        # and directly against the CPU restatement of the device's blocked order
+        assert O.same_bits(got, O.reduce_blocked("dot", ha, hb, ri)).all(), n
 
 
 def test_small_and_empty(cuda_lib, dev):
@@ -67,15 +69,22 @@ def test_small_and_empty(cuda_lib, dev):
                            _dot_existing(cuda_lib, a, b, n, 8, stream)).all()
 
 
-def test_rejects_sizes_beyond_capacity(cuda_lib, dev):
+def test_capacity_edge(cuda_lib, dev):
+    """n = 4,194,304 (one partial per slot of the array) is accepted and
+    exact; one element more is rejected before anything is read or launched."""
     import torch
 
-    a = torch.zeros(2, dtype=torch.float64, device=dev)
-    out = torch.zeros(2, dtype=torch.float64, device=dev)
-    # the size check comes before any pointer use: nothing is read or launched
-    rc = cuda_lib.mfcuda_dotdd_noalloc(a.data_ptr(), a.data_ptr(), MAX_N + 4096, 8, out.data_ptr(), None)
-    assert rc == 7  # MFCUDA_ERR_UNSUPPORTED
-    assert cuda_lib.mfcuda_error_string(rc) == b"unsupported shape or parameter"
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ha, hb = W.dd_uniform(MAX_N, seed=21), W.dd_uniform(MAX_N, seed=22)
+    a, b = to_dev(ha, dev), to_dev(hb, dev)
+    got = _dot_noalloc(cuda_lib, a, b, MAX_N, 8, stream)
+    assert O.same_bits(got, O.reduce_blocked("dot", ha, hb, 8)).all()
+    out = torch.full((2,), 7.0, dtype=torch.float64, device=dev)
+    for n in (MAX_N + 1, MAX_N + 4096):
+        rc = cuda_lib.mfcuda_dotdd_noalloc(a.data_ptr(), b.data_ptr(), n, 8, out.data_ptr(), None)
+        assert rc == 7  # MFCUDA_ERR_UNSUPPORTED
+    assert cuda_lib.mfcuda_error_string(7) == b"unsupported shape or parameter"
+    assert (to_host(out) == 7.0).all()  # the rejected calls wrote nothing
 
 
 _CHILD = r"""
