@@ -75,6 +75,7 @@ def orc():
         L.orc_crt_bound.argtypes = [C.c_int, C.c_int, C.c_int, I64]
         L.orc_crt_bound.restype = C.c_double
         L.orc_crt_plan.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, I64, C.POINTER(C.c_int)]
+        L.orc_grid_round.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(I64)]
         L.orc_wgemm.argtypes = [C.c_char, C.c_char, I64, I64, I64, P, P, I64, P, I64, P, P, I64]
         L.orc_wgemm_info.argtypes = [C.c_char, C.c_char, I64, I64, I64, I64, I64, I64]
         L.orc_wtrsm.argtypes = [C.c_char, C.c_char, C.c_char, C.c_char, I64, I64, P, P, I64, P, I64]
@@ -130,10 +131,35 @@ def pair(kind: str, x):
     return (y0, y1) if kind == "sincos" else y0
 
 
-def unary(op: str, x) -> np.ndarray:
+def parallel_map(fn, items, threads: int = 0) -> list:
+    """[fn(item) for item in items] on a thread pool.  The C restatement keeps
+    no global state and ctypes releases the GIL during a call, so oracle calls
+    on independent data run in parallel."""
+    import concurrent.futures as cf
+
+    threads = threads or os.cpu_count() or 1
+    if threads <= 1 or len(items) <= 1:
+        return [fn(it) for it in items]
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        return list(ex.map(fn, items))
+
+
+def unary(op: str, x, threads: int = 1) -> np.ndarray:
+    """The C restatement of op over an array (element ranges split over
+    `threads` threads; 0 = every host core)."""
     x = _c(x)
     y = np.empty_like(x)
-    orc().orc_unary(OPS[op], _p(x), _p(y), x.size // 2)
+    n = x.size // 2
+    L = orc()
+    threads = threads or os.cpu_count() or 1
+    bounds = np.linspace(0, n, max(1, min(threads, n // 4096 + 1)) + 1).astype(np.int64)
+    spans = [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
+
+    def run(span):
+        a, b = span
+        L.orc_unary(OPS[op], _p(x) + 16 * a, _p(y) + 16 * a, b - a)
+
+    parallel_map(run, spans, threads)
     return y
 
 
@@ -149,6 +175,24 @@ def matmul_mm(a, b, m, k, n, ri=8) -> np.ndarray:
     c = np.empty(2 * m * n)
     orc().orc_matmul_mm(_p(a), _p(b), _p(c), m, k, n, ri)
     return c
+
+
+def matmul_mm_rows(a, b, m, k, n, ri, rows, threads: int = 0) -> np.ndarray:
+    """Rows `rows` of C = A B (row indices): every output runs the same
+    sequential MAC over p whatever the shape, so row i of C is the 1 x n
+    product of row i of A with B.  Returns len(rows) x n x 2 (one thread per row)."""
+    a3, b = _c(a).reshape(k, m, 2), _c(b)
+    return np.stack(parallel_map(
+        lambda i: matmul_mm(np.ascontiguousarray(a3[:, i, :]), b, 1, k, n, ri).reshape(n, 2), list(rows),
+        threads))
+
+
+def matmul_mm_columns(a, b, m, k, n, ri, cols, threads: int = 0) -> np.ndarray:
+    """Columns `cols` of C = A B (column indices): column j of C is the m x 1
+    product of A with column j of B.  Returns len(cols) x m x 2 (one thread per column)."""
+    a, b3 = _c(a), _c(b).reshape(n, k, 2)
+    return np.stack(parallel_map(
+        lambda j: matmul_mm(a, np.ascontiguousarray(b3[j]), m, k, 1, ri).reshape(m, 2), list(cols), threads))
 
 
 def matmul_mm_cols(a, b, m, k, n, ri, j0, j1) -> np.ndarray:
