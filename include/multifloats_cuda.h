@@ -255,6 +255,28 @@ MULTIFLOATS_CUDA_API int mfcuda_cmatmuldd_mm_split(const complex64x2 *a, const c
 MULTIFLOATS_CUDA_API void mfcuda_phase_profile_begin(void);
 MULTIFLOATS_CUDA_API int mfcuda_phase_profile_end(double *phase_ms_sum, int64_t *calls);
 
+/* Bounded waits of the tensor-core kernels (split and CRT forms, single calls
+ * and batches).  No reference counterpart (the reference runs on the CPU).
+ * Every wait of these kernels for a pipeline stage, an accumulator hand-off or
+ * the reconstruction's own MMAs gives up after a limit (2 s by default),
+ * records the failure and lets the kernel leave once its own copies and MMAs
+ * in flight have finished, so the context stays usable; the call's outputs
+ * are then unspecified.  A call given info_out reports MFCUDA_ERR_TIMEOUT.
+ *
+ * mfcuda_set_wait_limit_ns sets the limit, process-wide, for kernels launched
+ * (and batch plans created) from then on; 0 restores the default.  It
+ * returns the previous setting (0 = default).  It exists to test the failure
+ * path: a limit far below a kernel's running time makes its waits give up.
+ *
+ * mfcuda_timeout_status returns MFCUDA_ERR_TIMEOUT if any of these kernels
+ * gave up a wait on the current device since the last clearing query, else
+ * MFCUDA_OK (MFCUDA_ERR_CUDA if the query itself fails); clear != 0 resets
+ * the record.  For callers of the device-pointer forms that passed
+ * info_out = NULL, and for batch runs: synchronise the streams of the calls
+ * in question first. */
+MULTIFLOATS_CUDA_API uint64_t mfcuda_set_wait_limit_ns(uint64_t ns);
+MULTIFLOATS_CUDA_API int mfcuda_timeout_status(int clear);
+
 /* op: 0 exp, 1 log, 2 sin, 3 cos, 4 sqrt */
 enum {
   MFCUDA_EXP = 0,
@@ -303,8 +325,10 @@ MULTIFLOATS_CUDA_API int mfcuda_cnorm2dd(const complex64x2 *x, int64_t n, float6
  * 16 KiB device array inside the library, so:
  *   - n is limited to 4,194,304 elements; larger n returns
  *     MFCUDA_ERR_UNSUPPORTED without launching anything;
- *   - the first call on each device looks up that array's device address
- *     (once per device, with that device current); make that first call
+ *   - every call outside stream capture looks up that array's device
+ *     address on the current device (so a cudaDeviceReset between calls is
+ *     harmless); a call inside a capture reuses the address found by an
+ *     earlier call on that device, so make the first call on each device
  *     before any stream capture;
  *   - all calls share the one array, so calls that overlap on the GPU (for
  *     example on two streams at once) race and corrupt each other's result;

@@ -33,7 +33,7 @@ SOURCES = [
     "blas_dd.cu",
 ]
 HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh", "split_device.cuh", "gemm_tile.cuh",
-           "crt_device.cuh", "crt_tables.h"]
+           "crt_device.cuh", "crt_tables.h", "grid_round.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [

@@ -296,7 +296,7 @@ static int64_t crt_combine_blocks(int64_t m, int64_t n) {
   return ((m + CTC_THREADS - 1) / CTC_THREADS) * (((n + 3) / 4 + CTC_QUADS - 1) / CTC_QUADS);
 }
 __global__ void __launch_bounds__(CTC_THREADS) g_crt_combine(const SProb *probs, const int64_t *prefix, int nprob,
-                                                             int *status) {
+                                                             int *status, uint64_t wait_ns) {
   extern __shared__ uint8_t ctc_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(ctc_raw) + 1023) & ~uintptr_t(1023));
   const int p = find_prob(prefix, nprob, blockIdx.x);
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(CTC_THREADS) g_crt_combine(const SProb *probs,
   const int64_t l = blockIdx.x - prefix[p], nbx = (P.m + CTC_THREADS - 1) / CTC_THREADS;
   crt_combine_tc_body(reinterpret_cast<const uint8_t *>(P.D), P.plan, P.cc, P.sigA, P.flagA, P.sigB, P.flagB, P.m,
                       P.n, P.M_pad, P.N_pad, P.nkc, P.k, P.C, P.cstride, P.mode, (l % nbx) * CTC_THREADS,
-                      (l / nbx) * CTC_QUADS, smem, status);
+                      (l / nbx) * CTC_QUADS, smem, status, wait_ns);
 }
 
 struct GItem {
@@ -333,7 +333,7 @@ constexpr int G_EPI_WARPS = 8;
 constexpr int G_THREADS = 64 + 32 * G_EPI_WARPS;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 __global__ void __launch_bounds__(G_THREADS, 1)
     g_mma(const SProb *__restrict__ probs, const CUtensorMap *__restrict__ maps,
-          const int64_t *__restrict__ prefix, int nprob, int64_t items, int *status) {
+          const int64_t *__restrict__ prefix, int nprob, int64_t items, int *status, uint64_t wait_ns) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t *sA = smem;
@@ -370,8 +370,10 @@ __global__ void __launch_bounds__(G_THREADS, 1)
   const uint32_t tmem_base = *tmem_slot;
   auto fail = [&](int code) {
     *abort_flag = 1;
-    atomicOr(status, code);
+    record_abort(status, code);
   };
+  ArmedStages<NSTAGE> arm;  // the producer's armed stages
+  arm.clear();
   // item -> (problem, decoded item, active?)
   auto lookup = [&](int64_t w, int &p, GItem &it) -> bool {
     p = find_prob(prefix, nprob, w);
@@ -384,9 +386,6 @@ __global__ void __launch_bounds__(G_THREADS, 1)
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      bool armed[NSTAGE];
-      uint32_t armed_parity[NSTAGE];
-      for (int s = 0; s < NSTAGE; ++s) armed[s] = false;
       bool ok = true;
       for (int64_t w = blockIdx.x; w < items && ok; w += gridDim.x) {
         int p;
@@ -397,7 +396,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         const uint32_t bytes = (uint32_t)(A_STAGE + P.bn * BK);
         for (int s = P.crt ? it.g : 0; s <= it.g && ok; ++s) {  // CRT: the single product A_g B_g
           for (int kb = kb0; kb < kb1; ++kb) {
-            if (!wait_bar(&empty[stage], phase ^ 1, abort_flag)) {
+            if (!wait_bar(&empty[stage], phase ^ 1, abort_flag, wait_ns)) {
               fail(1);
               ok = false;
               break;
@@ -406,22 +405,13 @@ __global__ void __launch_bounds__(G_THREADS, 1)
             mftc::tma_load_3d(sA + stage * A_STAGE, &maps[2 * p], &full[stage], kb * BK, it.tm * BM, s);
             mftc::tma_load_3d(sB + stage * B_STAGE, &maps[2 * p + 1], &full[stage], kb * BK, it.tn * P.bn,
                               P.crt ? s : it.g - s);
-            armed[stage] = true;
-            armed_parity[stage] = phase;
+            arm.arm(stage, phase);
             if (++stage == NSTAGE) {
               stage = 0;
               phase ^= 1;
             }
           }
         }
-      }
-      if (!ok) {
-        for (int s = 0; s < NSTAGE; ++s)
-          if (armed[s]) {
-            uint64_t t0 = globaltimer();
-            while (!mftc::mbar_try_wait(&full[s], armed_parity[s]) && globaltimer() - t0 < WAIT_NS) {
-            }
-          }
       }
     }
   } else if (warp == 1) {
@@ -438,7 +428,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         const SProb &P = probs[p];
         const int kb0 = it.kc * P.kcb, kb1 = min(P.kblocks, kb0 + P.kcb);
         const uint32_t idesc = P.crt ? mftc::idesc_u8(BM, P.bn) : mftc::idesc_i8(BM, P.bn);  // CRT residues unsigned
-        if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag)) {
+        if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag, wait_ns)) {
           fail(2);
           break;
         }
@@ -447,7 +437,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         uint32_t accumulate = 0;
         for (int s = P.crt ? it.g : 0; s <= it.g && ok; ++s) {
           for (int kb = kb0; kb < kb1; ++kb) {
-            if (!wait_bar(&full[stage], phase, abort_flag)) {
+            if (!wait_bar(&full[stage], phase, abort_flag, wait_ns)) {
               fail(4);
               ok = false;
               break;
@@ -491,7 +481,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
       GItem it;
       if (!lookup(w, p, it)) continue;
       const SProb &P = probs[p];
-      bool got = wait_bar(&tfull[acc], acc_phase, abort_flag);
+      bool got = wait_bar(&tfull[acc], acc_phase, abort_flag, wait_ns);
       if (!__all_sync(0xffffffffu, got)) {
         if (lane == 0) fail(8);
         break;
@@ -535,6 +525,11 @@ __global__ void __launch_bounds__(G_THREADS, 1)
   mftc::tc_fence_before();
   __syncthreads();
   mftc::tc_fence_after();
+  if (*abort_flag) {  // read after the barrier: the same value in every thread
+    // copies in flight that no MMA consumed land before shared memory is released
+    if (warp == 0 && lane == 0) arm.drain(full, NSTAGE);
+    __syncthreads();
+  }
   if (warp == 1) {
     __syncwarp();
     mftc::tmem_dealloc(tmem_base, TMEM_COLS);
@@ -957,6 +952,7 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
   const size_t crt_tile = (size_t)std::min(nsl_max, CRT_SA_MODULI) * SA_ROWS * SA_STRIDE;
   int mma_grid = sm_count();
   if (mma_grid > total[PH_ITEMS]) mma_grid = (int)std::max<int64_t>(total[PH_ITEMS], 1);
+  const uint64_t wait_ns = wait_limit_ns();  // captured into the graph with the plan
   int rc = capture(b, [&](cudaStream_t cs) {
     cudaMemsetAsync(b->status, 0, sizeof(int), cs);
     if (np == 0) return;
@@ -976,12 +972,12 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
     else if (total[PH_SLICE_B])
       g_slice_b<<<(unsigned)total[PH_SLICE_B], 256, 0, cs>>>(dp, dprefix + PH_SLICE_B * np, np);
     g_mma<<<mma_grid, G_THREADS, MMA_SMEM, cs>>>(dp, dmaps, dprefix + PH_ITEMS * np, np, total[PH_ITEMS],
-                                                   b->status);
+                                                   b->status, wait_ns);
     for (int ph : {PH_COMBINE, PH_COMBINE2}) {
       if (!total[ph]) continue;
       if (crt)
         g_crt_combine<<<(unsigned)total[ph], CTC_THREADS, crt_tc_smem((nsl_max + 31) / 32), cs>>>(
-            dp, dprefix + ph * np, np, b->status);
+            dp, dprefix + ph * np, np, b->status, wait_ns);
       else
         g_combine<<<(unsigned)total[ph], kCombineThreads, 0, cs>>>(dp, dprefix + ph * np, np);
     }
@@ -993,6 +989,9 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
   *out = b;
   return MFCUDA_OK;
 }
+
+// Given-up waits of the grouped tensor-core kernels (this file's record).
+int wait_sticky_batched(bool clear) { return take_wait_sticky(clear); }
 
 static bool split_args_ok(const mfcuda_gemm_desc &g) {
   return aligned16(g.a) && aligned16(g.b) && aligned16(g.c) && g.n <= 65535;

@@ -72,6 +72,10 @@ int staging_acquire(Staging &st, const size_t bytes[4]);
 // reports MFCUDA_ERR_ALLOC without calling the CUDA allocator.
 bool injected_alloc_failure();
 
+// Limit (ns) of the bounded waits in the tensor-core kernels launched from
+// now on (mfcuda_set_wait_limit_ns; 2 s unless set).
+uint64_t wait_limit_ns();
+
 // Stream-ordered workspace allocation for device-pointer calls given no workspace.
 int ws_alloc(void **p, size_t bytes, cudaStream_t s);
 void ws_free(void *p, cudaStream_t s);

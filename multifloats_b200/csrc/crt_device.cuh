@@ -551,13 +551,14 @@ static __device__ __noinline__ uint32_t crt_chunk_residue_word(const uint32_t *s
 // CTA of CTC_THREADS threads: rows i0 .. i0+127 of column quads qd0 ..
 // qd0+CTC_QUADS-1 (thread T: row i0+T, columns 4 qd .. 4 qd + 3).  `smem`
 // is 1024-aligned, crt_tc_smem(ceil(n / 32)) bytes.  `status` receives
-// MFCUDA_ERR_TIMEOUT-style bit 2 if a bounded wait for the MMAs expires.
+// bit 2 if the wait for the MMAs (limit wait_ns) expires.
 __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ D8, const Plan *plan,
                                                     const CrtConst *cc, const int *sigA, const int *flagA,
                                                     const int *sigB, const int *flagB, int64_t M, int64_t N,
                                                     int64_t M_pad, int64_t N_pad, int nkc, int64_t k,
                                                     double *__restrict__ C, int64_t cstride, int mode,
-                                                    int64_t i0, int64_t qd0, uint8_t *smem, int *status) {
+                                                    int64_t i0, int64_t qd0, uint8_t *smem, int *status,
+                                                    uint64_t wait_ns) {
   const int T = threadIdx.x, warp = T >> 5;
   const int n = plan->S, W = plan->W;
   const int ktn = (n + 31) / 32;
@@ -645,12 +646,15 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
       mftc::umma_commit(bar);
     }
     if (qd + 1 < qend) load_words(qd + 1, wv);  // in flight during the MMAs and this quad's outputs
-    const bool ok = mftc::mbar_wait(bar, phase, 1u << 22);
-    phase ^= 1;
+    const bool ok = wait_bar_ns(bar, phase, wait_ns);
     if (__syncthreads_or(!ok)) {  // uniform: every thread leaves together
-      if (T == 0) atomicOr(status, 2);  // a bounded wait expired
+      if (T == 0) record_abort(status, 2);  // a bounded wait expired
+      // this round's MMAs may still be writing tensor memory: give them the
+      // default limit to finish before the CTA frees it
+      (void)wait_bar_ns(bar, phase, WAIT_NS);
       break;
     }
+    phase ^= 1;
     mftc::tc_fence_after();
     const int4 sb4 = *reinterpret_cast<const int4 *>(sigB + 4 * qd);
     const int4 fb4 = *reinterpret_cast<const int4 *>(flagB + 4 * qd);

@@ -57,6 +57,13 @@ bool injected_alloc_failure() {
   return counter.fetch_add(1) + 1 == target;
 }
 
+static std::atomic<uint64_t> g_wait_limit_ns{0};  // 0: the default
+static constexpr uint64_t kDefaultWaitNs = 2000000000ull;
+uint64_t wait_limit_ns() {
+  const uint64_t v = g_wait_limit_ns.load(std::memory_order_relaxed);
+  return v ? v : kDefaultWaitNs;
+}
+
 namespace {
 struct DeviceStaging {
   std::mutex mu;
@@ -135,5 +142,9 @@ MULTIFLOATS_CUDA_API const char *mfcuda_error_string(int code) {
 }
 
 MULTIFLOATS_CUDA_API const char *mfcuda_version(void) { return "0.1.0"; }
+
+MULTIFLOATS_CUDA_API uint64_t mfcuda_set_wait_limit_ns(uint64_t ns) {
+  return mfcuda::g_wait_limit_ns.exchange(ns);
+}
 
 }  // extern "C"

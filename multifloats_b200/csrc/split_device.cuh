@@ -5,6 +5,7 @@
 #include <cstdint>
 
 #include "dd_device.cuh"
+#include "grid_round.cuh"
 #include "tcgen05.cuh"
 
 namespace mfcuda {
@@ -23,7 +24,13 @@ constexpr int MMA_THREADS = 192;   // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr int MMA_SMEM = NSTAGE * STAGE + 1024 /*align*/ + 256 /*barriers*/;
 // K chunk: (SMAX pairs) * K_chunk * 2^14 < 2^31  ->  73 blocks of 128
 constexpr int KC_BLOCKS = (int)(2147483647LL / ((long long)SMAX * 16384LL * BK));
-constexpr uint64_t WAIT_NS = 2000000000ull;  // bounded waits: 2 s
+// Bounded waits.  WAIT_NS (2 s) is the default limit of every wait in the
+// tensor-core kernels; a smaller limit can be set from the host
+// (mfcuda_set_wait_limit_ns) and reaches the kernels as an argument.  The
+// waits of an abort path (copies in flight landing, issued MMAs draining) keep
+// WAIT_NS whatever that setting, so a kernel that gave up still lets its own
+// asynchronous work finish before it frees tensor memory and exits.
+constexpr uint64_t WAIT_NS = 2000000000ull;
 
 // S: slices per operand (CRT form: moduli), G = S - 1, W: bits of the fixed-point
 // operands; crt = 1 selects the CRT form (one product per item, slice t of A
@@ -40,15 +47,80 @@ __device__ __forceinline__ uint64_t globaltimer() {
   return t;
 }
 
-// Bounded wait that also gives up as soon as another role of the CTA aborted.
-__device__ __forceinline__ bool wait_bar(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
+// Bounded wait (limit_ns) that also gives up as soon as another role of the
+// CTA aborted.
+__device__ __forceinline__ bool wait_bar(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                         uint64_t limit_ns) {
   if (mftc::mbar_try_wait(bar, parity)) return true;
   uint64_t t0 = globaltimer();
   while (true) {
     if (mftc::mbar_try_wait(bar, parity)) return true;
     if (*abort_flag) return false;
-    if (globaltimer() - t0 > WAIT_NS) return false;
+    if (globaltimer() - t0 > limit_ns) return false;
   }
+}
+// Bounded wait without an abort flag, backing off after the first polls.
+__device__ __forceinline__ bool wait_bar_ns(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
+  if (mftc::mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  for (int i = 0;; ++i) {
+    if (mftc::mbar_try_wait(bar, parity)) return true;
+    if (globaltimer() - t0 > limit_ns) return false;
+    if (i > 64) __nanosleep(64);
+  }
+}
+// The TMA producer's record of the stages it armed (the parity of each
+// stage's last arming).  After an abort, copies may be in flight that no MMA
+// consumed; drain() waits (default limit) for each armed stage's last phase,
+// so they land before the CTA frees its shared memory.
+template <int NS>
+struct ArmedStages {
+  bool armed[NS];
+  uint32_t parity[NS];
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) armed[s] = false;
+  }
+  __device__ __forceinline__ void arm(int s, uint32_t p) {
+    armed[s] = true;
+    parity[s] = p;
+  }
+  __device__ __forceinline__ void drain(uint64_t *full, int nst) {
+    for (int s = 0; s < nst && s < NS; ++s)
+      if (armed[s]) (void)wait_bar_ns(&full[s], parity[s], WAIT_NS);
+  }
+};
+// Spins for ns nanoseconds (abort paths only).
+__device__ __forceinline__ void settle_ns(uint64_t ns) {
+  const uint64_t t0 = globaltimer();
+  while (globaltimer() - t0 < ns) __nanosleep(256);
+}
+
+// Per-device record of given-up waits, for callers that did not ask a call
+// for its status: every kernel that gives up a wait ORs its code here as well
+// as into the call's status word; mfcuda_timeout_status reads and clears it.
+// (One copy per translation unit; the host reads every copy.)
+static __device__ int g_wait_sticky;
+__device__ __forceinline__ void record_abort(int *status, int code) {
+  atomicOr(status, code);
+  atomicOr(&g_wait_sticky, code);
+}
+// This translation unit's record on the current device (-1 if the query
+// fails), zeroed afterwards when `clear` (synchronous copies).
+static inline int take_wait_sticky(bool clear) {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_wait_sticky, sizeof(int)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return -1;
+  }
+  if (clear && v) {
+    const int z = 0;
+    if (cudaMemcpyToSymbol(g_wait_sticky, &z, sizeof(int)) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return -1;
+    }
+  }
+  return v;
 }
 
 constexpr int SENT_LO = -100000, SENT_HI = 100000;
@@ -82,55 +154,20 @@ __device__ __forceinline__ double scale2(double x, int e) {
   return (e >= -1022 && e <= 1023) ? x * pow2(e) : ldexp(x, e);
 }
 
-// x * 2^t for the finite double x = m 2^e (integer m, |m| < 2^53, read from
-// the IEEE-754 fields) as a fixed-point integer with FRAC fractional bits,
-// floor for the bits below.
-constexpr int FRAC = 16;
-__device__ __forceinline__ __int128 scaled_fixed(double x, int t) {
-  if (x == 0.0) return 0;
-  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
-  const int E = (int)((b >> 52) & 0x7FF);
-  long long m = (long long)(b & ((1ull << 52) - 1));
-  int e;
-  if (E) {
-    m |= 1ll << 52;
-    e = E - 1075;
-  } else {
-    e = -1074;
-  }
-  if (b >> 63) m = -m;
-  int sh = e + t + FRAC;
-  if (sh >= 0) return (__int128)m << sh;
-  if (sh <= -64) return m < 0 ? (__int128)-1 : (__int128)0;
-  return (__int128)(m >> (-sh));
-}
-
-// The entry rounded to the fixed-point grid of its row / column:
-// X = round((hi + lo) 2^(W - sigma)) (each limb floored at FRAC fractional
-// bits, summed, rounded half up), clamped to |X| <= 2^W - 1 (W = 8S-2 <= 110).
-// Returned as the four 32-bit words of Y = X + sum_{q<14} 128 * 256^q.  The
-// balanced base-256 representation X = sum_q d_q 256^q with d_q in
-// [-128, 127] is unique, and 0 <= Y < 256^14, so byte q of Y is exactly
-// d_q + 128: digit q as a signed byte is byte q of Y xor 0x80, with no carry
-// chain.  Slice s of the S-slice representation (most significant first) is
-// digit q = S-1-s; digits q >= S are zero.
+// The entry rounded to the fixed-point grid of its row / column
+// (grid_round.cuh: X = rint(H) + rint((H - rint(H)) + L), H = hi 2^(W - sigma),
+// L = lo 2^(W - sigma), clamped to |X| <= 2^W - 1; W <= 110), returned as the
+// four 32-bit words of Y = X + sum_{q<14} 128 * 256^q: byte q of Y is
+// balanced digit q of X plus 128.  Slice s of the S-slice representation
+// (most significant first) is digit q = S-1-s; digits q >= S are zero.
 // Word w of the bias (X = 0 gives all digits zero).
 __host__ __device__ constexpr uint32_t bias_word(int w) { return w < 3 ? 0x80808080u : 0x00008080u; }
 __device__ __forceinline__ void biased_bytes(double hi, double lo, int sigma, int W, uint32_t (&y)[4]) {
-  const int t = W - sigma;
-  const __int128 xf = scaled_fixed(hi, t) + scaled_fixed(lo, t);
-  __int128 X = (xf + ((__int128)1 << (FRAC - 1))) >> FRAC;
-  const __int128 lim = ((__int128)1 << W) - 1;
-  if (X > lim) X = lim;
-  if (X < -lim) X = -lim;
-  const unsigned __int128 bias =
-      (unsigned __int128)0x8080808080808080ull | ((unsigned __int128)0x808080808080ull << 64);
-  const unsigned __int128 Y = (unsigned __int128)X + bias;
-  const uint64_t ylo = (uint64_t)Y, yhi = (uint64_t)(Y >> 64);
-  y[0] = (uint32_t)ylo;
-  y[1] = (uint32_t)(ylo >> 32);
-  y[2] = (uint32_t)yhi;
-  y[3] = (uint32_t)(yhi >> 32);
+  const GridLimits g = grid_limits(W);
+  int64_t T;
+  uint64_t R;
+  grid_round(hi, lo, sigma, g, W, T, R);
+  grid_biased_words(T, R, y);
 }
 // Byte k of each of a, b, c, d packed as bytes 0..3.
 __device__ __forceinline__ uint32_t gather_byte(uint32_t a, uint32_t b, uint32_t c, uint32_t d, int k) {

@@ -111,7 +111,7 @@ __device__ __forceinline__ Item decode(int w, int G, int nkc, int ntm, int ntile
 __global__ void __launch_bounds__(MMA_THREADS, 1)
     split_mma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const Plan *plan, int32_t *__restrict__ D, int M_pad, int N_pad, int nkc,
-                     int kblocks, int *status) {
+                     int kblocks, int *status, uint64_t wait_ns) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t *sA = smem;
@@ -158,17 +158,16 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
 
   auto fail = [&](int code) {
     *abort_flag = 1;
-    atomicOr(status, code);
+    record_abort(status, code);
   };
+  ArmedStages<NSTAGE> arm;  // the producer's armed stages
+  arm.clear();
 
   if (warp == 0) {
     if (lane == 0) {
       // ---- TMA producer ----
       int stage = 0;
       uint32_t phase = 0;
-      uint32_t armed_parity[NSTAGE];
-      bool armed[NSTAGE];
-      for (int s = 0; s < NSTAGE; ++s) armed[s] = false;
       bool ok = true;
       for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
         Item it = decode(w, G, nkc, ntm, ntiles);
@@ -176,7 +175,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         for (int s = crt ? it.g : 0; s <= it.g && ok; ++s) {
           int t = crt ? s : it.g - s;
           for (int kb = kb0; kb < kb1; ++kb) {
-            if (!wait_bar(&empty[stage], phase ^ 1, abort_flag)) {
+            if (!wait_bar(&empty[stage], phase ^ 1, abort_flag, wait_ns)) {
               fail(1);
               ok = false;
               break;
@@ -184,23 +183,13 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
             mftc::mbar_arrive_expect_tx(&full[stage], STAGE);
             mftc::tma_load_3d(sA + stage * A_STAGE, &tmA, &full[stage], kb * BK, it.tm * BM, s);
             mftc::tma_load_3d(sB + stage * B_STAGE, &tmB, &full[stage], kb * BK, it.tn * BN, t);
-            armed[stage] = true;
-            armed_parity[stage] = phase;
+            arm.arm(stage, phase);
             if (++stage == NSTAGE) {
               stage = 0;
               phase ^= 1;
             }
           }
         }
-      }
-      if (!ok) {
-        // let copies already in flight land before the CTA leaves
-        for (int s = 0; s < NSTAGE; ++s)
-          if (armed[s]) {
-            uint64_t t0 = globaltimer();
-            while (!mftc::mbar_try_wait(&full[s], armed_parity[s]) && globaltimer() - t0 < WAIT_NS) {
-            }
-          }
       }
     }
   } else if (warp == 1) {
@@ -215,7 +204,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
       for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
         Item it = decode(w, G, nkc, ntm, ntiles);
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
-        if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag)) {
+        if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag, wait_ns)) {
           fail(2);
           break;
         }
@@ -224,7 +213,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
         uint32_t accumulate = 0;
         for (int s = crt ? it.g : 0; s <= it.g && ok; ++s) {
           for (int kb = kb0; kb < kb1; ++kb) {
-            if (!wait_bar(&full[stage], phase, abort_flag)) {
+            if (!wait_bar(&full[stage], phase, abort_flag, wait_ns)) {
               fail(4);
               ok = false;
               break;
@@ -266,7 +255,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
     uint32_t acc_phase = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x) {
       Item it = decode(w, G, nkc, ntm, ntiles);
-      bool got = wait_bar(&tfull[acc], acc_phase, abort_flag);
+      bool got = wait_bar(&tfull[acc], acc_phase, abort_flag, wait_ns);
       if (!__all_sync(0xffffffffu, got)) {
         if (lane == 0) fail(8);
         break;
@@ -315,6 +304,12 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
   mftc::tc_fence_before();
   __syncthreads();
   mftc::tc_fence_after();
+  if (*abort_flag) {  // read after the barrier: the same value in every thread
+    // an abort can leave copies in flight that no MMA consumed; they land
+    // before the CTA's shared memory is released
+    if (warp == 0 && lane == 0) arm.drain(full, NSTAGE);
+    __syncthreads();
+  }
   if (warp == 1) mftc::tmem_dealloc(tmem_base, TMEM_COLS);
 }
 
@@ -397,7 +392,7 @@ struct PairSched {
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     split_mma_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                           const Plan *plan, int32_t *__restrict__ D, int M_pad, int N_pad, int nkc,
-                          int kblocks, int nsub, int tn0, int ntn, int *status) {
+                          int kblocks, int nsub, int tn0, int ntn, int *status, uint64_t wait_ns) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int nst = pair_stages(nsub);
@@ -453,17 +448,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
 
   auto fail = [&](int code) {
     *abort_flag = 1;
-    atomicOr(status, code);
+    record_abort(status, code);
   };
+  ArmedStages<6> arm;  // stages the even CTA's producer armed
+  arm.clear();
 
   if (warp == 0) {
     if (lane == 0) {
       // ---- TMA producer (both CTAs) ----
       int stage = 0;
       uint32_t phase = 0;
-      uint32_t armed_parity[6];
-      bool armed[6];
-      for (int s = 0; s < 6; ++s) armed[s] = false;
       bool ok = true;
       PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
       Item it;
@@ -474,15 +468,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
         for (int s = crt ? it.g : 0; s <= it.g && ok; ++s) {
           int t = crt ? s : it.g - s;
           for (int kb = kb0; kb < kb1; ++kb) {
-            if (!wait_bar(&empty[stage], phase ^ 1, abort_flag)) {
+            if (!wait_bar(&empty[stage], phase ^ 1, abort_flag, wait_ns)) {
               fail(1);
               ok = false;
               break;
             }
             if (leader) {
               mftc::mbar_arrive_expect_tx(&full[stage], 2 * stage_bytes);
-              armed[stage] = true;
-              armed_parity[stage] = phase;
+              arm.arm(stage, phase);
             }
             const uint32_t fb = mftc::cluster_addr(&full[stage], 0);
             mftc::tma_load_3d_pair(sA + stage * P_STAGE_A, &tmA, fb, kb * BK, arow, s);
@@ -494,16 +487,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
             }
           }
         }
-      }
-      if (!ok) {
-        // The even CTA waits for the copies of both CTAs that complete on its
-        // barriers; neither CTA leaves before the closing cluster barrier.
-        for (int s = 0; s < nst; ++s)
-          if (armed[s]) {
-            uint64_t t0 = globaltimer();
-            while (!mftc::mbar_try_wait(&full[s], armed_parity[s]) && globaltimer() - t0 < WAIT_NS) {
-            }
-          }
       }
     }
   } else if (warp == 1) {
@@ -519,7 +502,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
       Item it;
       while (ok && sched.next(it)) {
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
-        if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag)) {
+        if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag, wait_ns)) {
           fail(2);
           break;
         }
@@ -528,7 +511,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
         uint32_t accumulate = 0;
         for (int s = crt ? it.g : 0; s <= it.g && ok; ++s) {
           for (int kb = kb0; kb < kb1; ++kb) {
-            if (!wait_bar(&full[stage], phase, abort_flag)) {
+            if (!wait_bar(&full[stage], phase, abort_flag, wait_ns)) {
               fail(4);
               ok = false;
               break;
@@ -579,7 +562,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
     Item it;
     while (sched.next(it)) {
-      bool got = wait_bar(&tfull[acc], acc_phase, abort_flag);
+      bool got = wait_bar(&tfull[acc], acc_phase, abort_flag, wait_ns);
       if (!__all_sync(0xffffffffu, got)) {
         if (lane == 0) fail(8);
         break;
@@ -629,6 +612,23 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
   mftc::tc_fence_before();
   mftc::cluster_sync();  // no CTA leaves while its peer may still signal it or read its shared memory
   mftc::tc_fence_after();
+  // Either CTA's abort flag, read after the cluster barrier: the same value in
+  // every thread of the pair.
+  const uint32_t peer_abort = mftc::ld_cluster_u32(mftc::cluster_addr((const void *)abort_flag, rank ^ 1u));
+  if ((*abort_flag | (int)peer_abort) != 0) {
+    if (warp == 0 && lane == 0) {
+      // copies in flight that no MMA consumed land before shared memory is
+      // released: the even CTA waits for every stage it armed (both CTAs'
+      // copies complete there); a copy the odd CTA issued for a stage the even
+      // CTA gave up before arming completes on no barrier anyone waits for,
+      // so both also give in-flight copies time to land (a 16 KiB tile takes
+      // a few microseconds)
+      if (leader) arm.drain(full, nst);
+      settle_ns(50000);
+    }
+    __syncwarp();
+    mftc::cluster_sync();
+  }
   if (warp == 1) mftc::tmem_dealloc_pair(tmem_base, TMEM_COLS);
 }
 
@@ -672,11 +672,12 @@ __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restri
 __global__ void __launch_bounds__(CTC_THREADS) crt_combine_tc_kernel(
     const uint8_t *__restrict__ D8, const Plan *plan, const CrtConst *cc, const int *sigA, const int *flagA,
     const int *sigB, const int *flagB, int64_t M, int64_t N, int64_t M_pad, int64_t N_pad, int nkc, int64_t k,
-    double *__restrict__ C, int64_t cstride, int mode, int64_t qbase, int *status) {
+    double *__restrict__ C, int64_t cstride, int mode, int64_t qbase, int *status, uint64_t wait_ns) {
   extern __shared__ uint8_t ctc_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(ctc_raw) + 1023) & ~uintptr_t(1023));
   crt_combine_tc_body(D8, plan, cc, sigA, flagA, sigB, flagB, M, N, M_pad, N_pad, nkc, k, C, cstride, mode,
-                      (int64_t)blockIdx.x * CTC_THREADS, qbase + (int64_t)blockIdx.y * CTC_QUADS, smem, status);
+                      (int64_t)blockIdx.x * CTC_THREADS, qbase + (int64_t)blockIdx.y * CTC_QUADS, smem, status,
+                      wait_ns);
 }
 
 // ---------------------------------------------------------------------------
@@ -904,6 +905,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     flag[o] = mu[o] + rows;
     sl[o] = reinterpret_cast<int8_t *>(base + L.off_slices[o]);
   }
+  const uint64_t wait_ns = wait_limit_ns();
   int rc = MFCUDA_OK;
   do {
     std::call_once(g_attr_once, [] {
@@ -1000,18 +1002,19 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
         if (L.pair)
           split_mma_pair_kernel<<<pgrid, PAIR_THREADS, PAIR_SMEM, s>>>(
               tmA[q], tmB[q], plan, D, (int)L.M_pad, (int)L.N_pad, (int)L.nkc, (int)L.kblocks, L.nsub, tn0,
-              npan == 1 ? ntn_all : tn1 - tn0, status);
+              npan == 1 ? ntn_all : tn1 - tn0, status, wait_ns);
         else
           split_mma_kernel<<<pgrid, MMA_THREADS, MMA_SMEM, s>>>(tmA[q], tmB[q], plan, D, (int)L.M_pad,
                                                                 (int)L.N_pad, (int)L.nkc, (int)L.kblocks,
-                                                                status);
+                                                                status, wait_ns);
         if (q == nprod - 1 && pp == npan - 1) mark(3, s);
         if (crt)
           crt_combine_tc_kernel<<<dim3((unsigned)((m + CTC_THREADS - 1) / CTC_THREADS),
                                        (unsigned)(((j1 - j0 + 3) / 4 + CTC_QUADS - 1) / CTC_QUADS)),
                                   CTC_THREADS, crt_tc_smem((L.nsl + 31) / 32), s>>>(
               reinterpret_cast<const uint8_t *>(D), plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, j1,
-              L.M_pad, L.N_pad, (int)L.nkc, k, prods[q].out, prods[q].ostride, prods[q].mode, j0 / 4, status);
+              L.M_pad, L.N_pad, (int)L.nkc, k, prods[q].out, prods[q].ostride, prods[q].mode, j0 / 4, status,
+              wait_ns);
         else
           combine_kernel<<<dim3(cgx, (unsigned)n), COMBINE_THREADS, 0, s>>>(
               D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n, L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,
@@ -1151,6 +1154,19 @@ int run_complex_crt(const complex64x2 *a, const complex64x2 *b, complex64x2 *c, 
 }
 
 }  // namespace split
+
+namespace batch {
+int wait_sticky_batched(bool clear);  // batched.cu
+}
+
+// MFCUDA_ERR_TIMEOUT when a tensor-core kernel of this file or of the
+// grouped pipeline gave up a bounded wait on the current device.
+static int timeout_status(bool clear) {
+  MF_TRY(require_device());
+  const int a = split::take_wait_sticky(clear), b = batch::wait_sticky_batched(clear);
+  if (a < 0 || b < 0) return MFCUDA_ERR_CUDA;
+  return (a | b) ? MFCUDA_ERR_TIMEOUT : MFCUDA_OK;
+}
 
 template <bool CPLX>
 static int split_host(const void *a, const void *b, void *c, int64_t m, int64_t k, int64_t n, int slices,
@@ -1306,6 +1322,8 @@ MULTIFLOATS_CUDA_API double mfcuda_crt_bound(int bits, int rho_a, int rho_b, int
   if (bits < 8 || bits > mfcuda::split::CRT_WMAX || k < 1) return -1.0;
   return mfcuda::split::crt_bound(bits, rho_a, rho_b, k);
 }
+
+MULTIFLOATS_CUDA_API int mfcuda_timeout_status(int clear) { return mfcuda::timeout_status(clear != 0); }
 
 MULTIFLOATS_CUDA_API void mfcuda_phase_profile_begin(void) { mfcuda::split::profile_begin(); }
 MULTIFLOATS_CUDA_API int mfcuda_phase_profile_end(double *phase_ms_sum, int64_t *calls) {

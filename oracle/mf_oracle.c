@@ -975,24 +975,29 @@ void orc_reduce_error(int kind, const double *x, const double *y, int64_t n, con
  * order is fixed, so the device result must match this bit for bit. */
 #define SPLIT_SMAX 14
 #define SPLIT_KC (73 * 128) /* K elements per chunk, as KC_BLOCKS * BK on the device */
-#define SPLIT_FRAC 16
-
-static __int128 split_scaled_fixed(double x, int t) {
-  if (x == 0.0) return 0;
-  int e = ilogb(x);
-  long long m = (long long)ldexp(x, 52 - e);
-  int sh = e - 52 + t + SPLIT_FRAC;
-  if (sh >= 0) return (__int128)m << sh;
-  if (sh <= -64) return m < 0 ? (__int128)-1 : (__int128)0;
-  return (__int128)(m >> (-sh));
-}
-static void split_digits(double hi, double lo, int sigma, int S, int W, int8_t *d) {
+/* The rounding of an entry to the W-bit grid of its row / column
+ * (t = W - sigma), IEEE double operations rounding to nearest even:
+ *   H = ldexp(hi, t), L = ldexp(lo, t), P = rint(H), X = P + rint((H - P) + L),
+ * clamped to |X| <= 2^W - 1.  |X - (hi + lo) 2^t| <= 1. */
+static __int128 split_round(double hi, double lo, int sigma, int W) {
   int t = W - sigma;
-  __int128 xf = split_scaled_fixed(hi, t) + split_scaled_fixed(lo, t);
-  __int128 X = (xf + ((__int128)1 << (SPLIT_FRAC - 1))) >> SPLIT_FRAC;
+  double H = ldexp(hi, t), L = ldexp(lo, t);
+  double P = rint(H);
+  double Q = rint((H - P) + L);
+  __int128 X = (__int128)P + (__int128)Q;
   __int128 lim = ((__int128)1 << W) - 1;
   if (X > lim) X = lim;
   if (X < -lim) X = -lim;
+  return X;
+}
+/* X of split_round as two 64-bit words (low, high; two's complement). */
+void orc_grid_round(double hi, double lo, int sigma, int W, int64_t *out) {
+  __int128 X = split_round(hi, lo, sigma, W);
+  out[0] = (int64_t)(uint64_t)X;
+  out[1] = (int64_t)(X >> 64);
+}
+static void split_digits(double hi, double lo, int sigma, int S, int W, int8_t *d) {
+  __int128 X = split_round(hi, lo, sigma, W);
   for (int s = S - 1; s >= 1; --s) {
     int v = (int)(X & 0xFF);
     v = (v ^ 0x80) - 0x80;
@@ -1376,15 +1381,7 @@ int orc_crt_plan(int bits, double target, int ra, int rb, int64_t k, int *nmod) 
   return W;
 }
 /* the split form's rounding to the W-bit grid */
-static __int128 crt_round(double hi, double lo, int sigma, int W) {
-  int t = W - sigma;
-  __int128 xf = split_scaled_fixed(hi, t) + split_scaled_fixed(lo, t);
-  __int128 X = (xf + ((__int128)1 << (SPLIT_FRAC - 1))) >> SPLIT_FRAC;
-  __int128 lim = ((__int128)1 << W) - 1;
-  if (X > lim) X = lim;
-  if (X < -lim) X = -lim;
-  return X;
-}
+static __int128 crt_round(double hi, double lo, int sigma, int W) { return split_round(hi, lo, sigma, W); }
 /* acc (256-bit two's complement, 4 little-endian words) += x * y */
 static void acc_add_prod(uint64_t acc[4], __int128 x, __int128 y) {
   int neg = (x < 0) != (y < 0);

@@ -26,3 +26,16 @@ def test_operand_sizes_are_checked():
         api.matmuldd_mm_crt(np.zeros(2 * 6), np.zeros(2 * 7), 2, 3, 2)
     with pytest.raises(ValueError):  # host calls have the fixed target 8
         api.matmuldd_mm_crt(np.zeros(2 * 6), np.zeros(2 * 6), 2, 3, 2, target=2.0)
+
+
+def test_wait_limit_setter_round_trip():
+    """mfcuda_set_wait_limit_ns returns the previous setting (0 = the 2 s
+    default) and touches no device."""
+    from multifloats_b200 import _lib
+
+    L = _lib.lib()
+    prev = L.mfcuda_set_wait_limit_ns(12345)
+    try:
+        assert L.mfcuda_set_wait_limit_ns(777) == 12345
+    finally:
+        assert L.mfcuda_set_wait_limit_ns(prev) == 777
