@@ -9,7 +9,10 @@ from conftest import ROOT
 
 GEN = os.path.join(ROOT, "multifloats_b200", "csrc", "gen_dd_tables.py")
 HEADER = os.path.join(ROOT, "multifloats_b200", "csrc", "dd_tables.h")
-REF_HEADER = "/root/reference/src/dd_constants.hh"
+# the reference source tree: $MULTIFLOATS_REFERENCE, else a checkout named
+# "reference" beside this repository (absent on machines without it: skipped)
+REF_DIR = os.environ.get("MULTIFLOATS_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
+REF_HEADER = os.path.join(REF_DIR, "src", "dd_constants.hh")
 
 
 def _gen():
