@@ -434,6 +434,60 @@ MULTIFLOATS_CUDA_API int mfcuda_unary_dd_ragged(int op, const float64x2 *const *
                                                 float64x2 *const *ys, const int64_t *ns,
                                                 int64_t count, void *stream);
 
+/* ---- one process per GPU over an NCCL communicator ---------------------------
+ * No reference counterpart (the reference is single-process).  nccl_comm is
+ * the caller's ncclComm_t (one rank per GPU, this rank's device current);
+ * NCCL is found at run time in the process (the library that created the
+ * communicator), else as libnccl.so.2 -- mfcuda_nccl_available() says whether
+ * it was.  Every rank makes the same calls with the same sizes, form, flags
+ * and target, on streams of its own device; each call enqueues the same
+ * collectives in the same order on every rank (an empty shard included) and
+ * is asynchronous on the stream unless info_out is given.
+ *
+ * mfcuda_shard_bounds: the contiguous shard [start, stop) of n items that
+ * rank `rank` of `world` owns (the first n % world ranks own one more).
+ *
+ * mfcuda_matmuldd_mm_nccl: C = A B (column-major DD, device pointers) in
+ * column panels: this rank computes columns [j0, j1) = shard_bounds(n) of C
+ * from all of A and the same columns of B.  K is never split, so every
+ * output equals the single-device call of `form` bit for bit:
+ *   MFCUDA_FORM_PLAIN  mfcuda_matmuldd_mm,        param = renorm_interval;
+ *   MFCUDA_FORM_SPLIT  mfcuda_matmuldd_mm_split,  param = slices (0 = from target);
+ *   MFCUDA_FORM_CRT    mfcuda_matmuldd_mm_crt,    param = bits (0 = from target).
+ * For the split forms the ranks agree on the slice count / operand width the
+ * single call derives from all of B (one MAX all-reduce of an int on the
+ * stream; no host synchronisation).  flags:
+ *   0                    b and c are the full k x n and m x n matrices; only
+ *                        this rank's columns of B are read and of C written;
+ *   MFCUDA_SHARD_PANELS  b and c hold only this rank's columns (k x (j1-j0),
+ *                        m x (j1-j0));
+ *   MFCUDA_SHARD_GATHER  full matrices, and afterwards every rank's c holds
+ *                        all of C (each panel broadcast by its owner).
+ * workspace: NULL (allocated on the stream) or at least the single call's
+ * workspace size for (m, k, max panel width).  info_out: NULL or 4 ints, the
+ * single call's info for this rank's panel (plan values after agreement).
+ *
+ * mfcuda_reduce_nccl: a reduction (kind MFCUDA_RED_*) of the array whose
+ * contiguous shard of n elements this rank holds (x, y device pointers): the
+ * per-shard partials (mfcuda_reduce_partial) are all-gathered in rank order
+ * and folded left to right (mfcuda_reduce_combine); every rank's out (device,
+ * the single call's format) receives the result, deterministic for a given
+ * shard split and within the single call's error bound.
+ *
+ * Errors: MFCUDA_ERR_UNSUPPORTED when NCCL cannot be found, MFCUDA_ERR_CUDA
+ * when an NCCL or CUDA call fails.  Argument errors are the same on every
+ * rank (they depend on the common arguments only), so no rank is left
+ * waiting in a collective the others skipped. */
+enum { MFCUDA_SHARD_PANELS = 1, MFCUDA_SHARD_GATHER = 2 };
+MULTIFLOATS_CUDA_API void mfcuda_shard_bounds(int64_t n, int rank, int world, int64_t *start, int64_t *stop);
+MULTIFLOATS_CUDA_API int mfcuda_nccl_available(void);
+MULTIFLOATS_CUDA_API int mfcuda_matmuldd_mm_nccl(int form, const float64x2 *a, const float64x2 *b, float64x2 *c,
+                                                 int64_t m, int64_t k, int64_t n, int64_t param, double target,
+                                                 int flags, void *workspace, size_t workspace_bytes,
+                                                 int *info_out, void *nccl_comm, void *stream);
+MULTIFLOATS_CUDA_API int mfcuda_reduce_nccl(int kind, const void *x, const void *y, int64_t n,
+                                            int64_t renorm_interval, void *out, void *nccl_comm, void *stream);
+
 /* ---- BLAS-style shims over DD matrices ------------------------------------
  * DGEMM / DTRSM argument semantics as in the reference's BLAS shims
  * test/integration/blas/wgemm.f90 and wtrsm.f90 (the `blas-multifloat`

@@ -90,6 +90,11 @@ SIGNATURES = {
     "mfcuda_phase_profile_begin": (None, []),
     "mfcuda_phase_profile_end": (C.c_int, [C.POINTER(C.c_double), C.POINTER(I64)]),
     "mfcuda_set_wait_limit_ns": (C.c_uint64, [C.c_uint64]),
+    "mfcuda_shard_bounds": (None, [I64, C.c_int, C.c_int, C.POINTER(I64), C.POINTER(I64)]),
+    "mfcuda_nccl_available": (C.c_int, []),
+    "mfcuda_matmuldd_mm_nccl": (C.c_int, [C.c_int, P, P, P, I64, I64, I64, I64, C.c_double, C.c_int, P,
+                                          C.c_size_t, P, P, P]),
+    "mfcuda_reduce_nccl": (C.c_int, [C.c_int, P, P, I64, I64, P, P, P]),
     "mfcuda_timeout_status": (C.c_int, [C.c_int]),
     "mfcuda_matmuldd_mm_split": (C.c_int, [P, P, P, I64, I64, I64, C.c_int, C.c_double, P, C.c_size_t,
                                            P, P]),

@@ -31,6 +31,7 @@ SOURCES = [
     "split_gemm.cu",
     "batched.cu",
     "blas_dd.cu",
+    "shard.cu",
 ]
 HEADERS = ["common.cuh", "dd_device.cuh", "dd_tables.h", "tcgen05.cuh", "split_device.cuh", "gemm_tile.cuh",
            "crt_device.cuh", "crt_tables.h", "grid_round.cuh"]
@@ -86,7 +87,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         tmp = LIB + ".tmp"
         cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs,
-               "-Xcompiler", "-fPIC", "-Xlinker", "--exclude-libs,ALL"]
+               "-Xcompiler", "-fPIC", "-Xlinker", "--exclude-libs,ALL", "-ldl"]
         proc = subprocess.run(cmd, capture_output=True, text=True)
         if proc.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{proc.stdout}\n{proc.stderr}")

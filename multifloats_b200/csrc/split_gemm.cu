@@ -68,8 +68,10 @@ __global__ void __launch_bounds__(256) scan_b_kernel(const double *__restrict__ 
                                                      int64_t stride, int *sig, int *mu, int *flag) {
   scan_b_body(B, K, N, stride, sig, mu, flag, blockIdx.x, blockIdx.y);
 }
-__global__ void plan_kernel(StatSet st, int slices, double target, Plan *plan) {
-  plan_body(st, slices, target, plan);
+// slices_dev (may be NULL): read the slice count there instead (ranks that
+// agreed on one through a collective).
+__global__ void plan_kernel(StatSet st, int slices, double target, Plan *plan, const int *slices_dev) {
+  plan_body(st, slices_dev ? *slices_dev : slices, target, plan);
 }
 __global__ void __launch_bounds__(256) slice_a_kernel(const double *__restrict__ A, int64_t M, int64_t K,
                                                       int64_t stride, int64_t M_pad, int64_t K_pad,
@@ -446,8 +448,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
   mftc::tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
+  // the peer CTA's abort flag (written before the closing cluster barrier,
+  // while both CTAs are running): an abort in either CTA stops both
+  const uint32_t peer_abort = mftc::cluster_addr((const void *)abort_flag, rank ^ 1u);
   auto fail = [&](int code) {
     *abort_flag = 1;
+    mftc::st_cluster_u32(peer_abort, 1u);
     record_abort(status, code);
   };
   ArmedStages<6> arm;  // stages the even CTA's producer armed
@@ -612,10 +618,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
   mftc::tc_fence_before();
   mftc::cluster_sync();  // no CTA leaves while its peer may still signal it or read its shared memory
   mftc::tc_fence_after();
-  // Either CTA's abort flag, read after the cluster barrier: the same value in
-  // every thread of the pair.
-  const uint32_t peer_abort = mftc::ld_cluster_u32(mftc::cluster_addr((const void *)abort_flag, rank ^ 1u));
-  if ((*abort_flag | (int)peer_abort) != 0) {
+  // An abort in either CTA set both flags before the barrier: the flag read
+  // after it has the same value in every thread of the pair.
+  if (*abort_flag) {
     if (warp == 0 && lane == 0) {
       // copies in flight that no MMA consumed land before shared memory is
       // released: the even CTA waits for every stage it armed (both CTAs'
@@ -648,8 +653,11 @@ constexpr int COMBINE_THREADS = 128;
 // ---------------------------------------------------------------------------
 // CRT form (crt_device.cuh): plan, residue slicing, reconstruction
 // ---------------------------------------------------------------------------
-__global__ void crt_plan_kernel(StatSet st, int bits, double target, int64_t k, Plan *plan, CrtConst *cc) {
-  crt_plan_body(st, bits, target, k, plan, cc);
+// bits_dev (may be NULL): read the operand width there instead (ranks that
+// agreed on one through a collective).
+__global__ void crt_plan_kernel(StatSet st, int bits, double target, int64_t k, Plan *plan, CrtConst *cc,
+                                const int *bits_dev) {
+  crt_plan_body(st, bits_dev ? *bits_dev : bits, target, k, plan, cc);
 }
 __global__ void __launch_bounds__(256) crt_slice_a_kernel(const double *__restrict__ A, int64_t M, int64_t K,
                                                           int64_t stride, int64_t M_pad, int64_t K_pad,
@@ -873,12 +881,20 @@ struct PanelSink {
   void (*done)(void *ctx, int64_t j0, int64_t j1, cudaStream_t s);
   void *ctx;
 };
+// Agreement between ranks that compute column panels of one product:
+// fn(ctx, v, s) replaces the int at device address v (the plan's slice count
+// or operand width) by its maximum over the ranks, enqueued on stream s;
+// returns an MFCUDA status.
+struct Agree {
+  int (*fn)(void *ctx, int *v, cudaStream_t s);
+  void *ctx;
+};
 
 static int run_products(const double *const *aview, const int64_t *astride, int nA,
                         const double *const *bview, const int64_t *bstride, int nB,
                         const Product *prods, int nprod, int64_t m, int64_t k, int64_t n, int slices,
                         double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info, int crt = 0,
-                        const PanelSink *sink = nullptr) {
+                        const PanelSink *sink = nullptr, const Agree *agree = nullptr) {
   Layout L = layout(m, k, n, nA, nB, crt ? crt_slices_max(k, slices) : SMAX, crt != 0);
   if (L.M_pad > INT32_MAX / 2 || L.N_pad > INT32_MAX / 2 || L.kblocks > INT32_MAX / 2 ||
       L.N_pad > 65535 || L.K_pad / 64 > 65535)
@@ -938,9 +954,21 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
       st.side[o] = aside ? 0 : 1;
     }
     if (crt)
-      crt_plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, k, plan, cc);
+      crt_plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, k, plan, cc, nullptr);
     else
-      plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, plan);
+      plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, plan, nullptr);
+    if (agree) {
+      // ranks holding other column panels of the same product agree on the
+      // largest slice count / operand width (the one the single call would
+      // pick from all of B) before anything depends on it
+      int *val = crt ? &plan->W : &plan->S;
+      rc = agree->fn(agree->ctx, val, s);
+      if (rc != MFCUDA_OK) break;
+      if (crt)
+        crt_plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, k, plan, cc, val);
+      else
+        plan_kernel<<<1, 1024, 0, s>>>(st, slices, target, plan, val);
+    }
     mark(1, s);
     const dim3 ga((unsigned)(L.M_pad / 32), (unsigned)(L.K_pad / 64));
     const dim3 gb((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad);
@@ -1094,6 +1122,35 @@ int run_crt(const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int
   int64_t one[1] = {1};
   Product p = {0, 0, reinterpret_cast<double *>(c), 1, 0};
   return run_products(av, one, 1, bv, one, 1, &p, 1, m, k, n, bits, target, ws, ws_bytes, s, info, 1, sink);
+}
+
+// One rank's column panel (n columns of B and C) of a real product computed
+// by several ranks, which agree on the plan through `agree` before it is used
+// (crt: the CRT form, arg = bits; else the digit-sliced form, arg = slices).
+// k == 0 and m == 0 return before the agreement: every rank sees the same m
+// and k, so every rank skips it alike.  n must be positive (a rank with an
+// empty panel takes part in the agreement on its own).
+int run_panel(bool crt, const float64x2 *a, const float64x2 *b, float64x2 *c, int64_t m, int64_t k, int64_t n,
+              int arg, double target, void *ws, size_t ws_bytes, cudaStream_t s, int *info, const Agree *agree) {
+  int rc = check_args(a, b, c, m, k, n, crt ? 0 : arg, target);
+  if (crt && (arg < 0 || (arg > 0 && arg < 8) || arg > CRT_WMAX)) return MFCUDA_ERR_INVALID_ARG;
+  if (rc == -1) return MFCUDA_OK;
+  MF_TRY(rc);
+  MF_TRY(require_device());
+  if (k == 0) {
+    MF_TRY_CUDA(cudaMemsetAsync(c, 0, (size_t)(m * n) * sizeof(float64x2), s));
+    if (info) {
+      info[0] = info[1] = info[2] = 0;
+      if (crt) info[3] = 0;
+    }
+    return MFCUDA_OK;
+  }
+  const double *av[1] = {reinterpret_cast<const double *>(a)};
+  const double *bv[1] = {reinterpret_cast<const double *>(b)};
+  int64_t one[1] = {1};
+  Product p = {0, 0, reinterpret_cast<double *>(c), 1, 0};
+  return run_products(av, one, 1, bv, one, 1, &p, 1, m, k, n, arg, target, ws, ws_bytes, s, info, crt ? 1 : 0,
+                      nullptr, agree);
 }
 
 // Complex: re = Ar Br - Ai Bi, im = Ar Bi + Ai Br (the Fortran cdd_matmul_mm

@@ -173,10 +173,8 @@ __device__ __forceinline__ uint32_t cluster_addr(const void *p, uint32_t rank) {
   return r;
 }
 // Arrive on an mbarrier given by its shared::cluster address (own or peer CTA).
-__device__ __forceinline__ uint32_t ld_cluster_u32(uint32_t addr_cluster) {
-  uint32_t v;
-  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr_cluster) : "memory");
-  return v;
+__device__ __forceinline__ void st_cluster_u32(uint32_t addr_cluster, uint32_t v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr_cluster), "r"(v) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
   asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
