@@ -37,7 +37,10 @@
 
 /* Interchange types.  When the reference header multifloats/float64x2.h has
  * already been included (it defines MULTIFLOATS_ABI_VERSION) its identical
- * structs are used instead. */
+ * structs are used instead: in C they are the global struct float64x2 /
+ * complex64x2; in C++ the reference declares them in namespace multifloats
+ * (include/multifloats/float64x2.h:72, :125, :348), so they are brought into
+ * the global namespace here for the declarations below. */
 #ifndef MULTIFLOATS_ABI_VERSION
 struct float64x2 {
   double limbs[2];
@@ -50,6 +53,9 @@ struct complex64x2 {
 typedef struct float64x2 float64x2;
 typedef struct complex64x2 complex64x2;
 #endif
+#elif defined(__cplusplus)
+using multifloats::complex64x2;
+using multifloats::float64x2;
 #endif
 
 #ifdef __cplusplus

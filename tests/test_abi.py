@@ -75,3 +75,18 @@ def test_drop_in_without_gpu_latches_error(cuda_lib):
     r = cuda_lib.sumdd_array(x.ctypes.data, 4)
     assert cuda_lib.mfcuda_last_error() == 4
     assert np.isnan(r.hi)
+
+
+def test_compiled_c_consumer_links_and_reports_no_device():
+    """The compiled C caller (tests/consumer/consumer.c, built by
+    oracle/Makefile) links against the library alone; without a GPU every
+    drop-in latches an error and it exits 2, with one it exits 0."""
+    import subprocess
+
+    import torch
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "consumer_c_own")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "own-consumer"], check=True)
+    proc = subprocess.run([exe, os.devnull], capture_output=True, text=True, timeout=120)
+    assert proc.returncode == (0 if torch.cuda.is_available() else 2), (proc.returncode, proc.stderr)
