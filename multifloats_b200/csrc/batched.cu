@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kCombineThreads) g_combine(const SProb *probs,
 static int64_t crt_combine_blocks(int64_t m, int64_t n) {
   return ((m + CTC_THREADS - 1) / CTC_THREADS) * (((n + 3) / 4 + CTC_QUADS - 1) / CTC_QUADS);
 }
-__global__ void __launch_bounds__(CTC_THREADS) g_crt_combine(const SProb *probs, const int64_t *prefix, int nprob,
+__global__ void __launch_bounds__(CTC_THREADS, 4) g_crt_combine(const SProb *probs, const int64_t *prefix, int nprob,
                                                              int *status, uint64_t wait_ns) {
   extern __shared__ uint8_t ctc_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(ctc_raw) + 1023) & ~uintptr_t(1023));

@@ -677,7 +677,7 @@ __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restri
 // Tensor-core reconstruction (crt_combine_tc_body): block (x, y) takes rows
 // 128 x .. of column quads qbase + CTC_QUADS y .. (columns below N); dynamic shared memory
 // crt_tc_smem(ceil(moduli / 32)).
-__global__ void __launch_bounds__(CTC_THREADS) crt_combine_tc_kernel(
+__global__ void __launch_bounds__(CTC_THREADS, 4) crt_combine_tc_kernel(
     const uint8_t *__restrict__ D8, const Plan *plan, const CrtConst *cc, const int *sigA, const int *flagA,
     const int *sigB, const int *flagB, int64_t M, int64_t N, int64_t M_pad, int64_t N_pad, int nkc, int64_t k,
     double *__restrict__ C, int64_t cstride, int mode, int64_t qbase, int *status, uint64_t wait_ns) {
