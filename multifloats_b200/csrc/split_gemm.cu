@@ -7,8 +7,8 @@
 //               nonzero entry; non-finite entries are flagged.
 //   2. plan   : slice count S (given, or the smallest S meeting the requested
 //               bound for the measured exponent spreads), W = 8S-2 bits.
-//   3. slice  : every DD entry is rounded exactly (128-bit integer arithmetic)
-//               to X = round(a 2^(W - sigma_i)), |X| < 2^W, and cut into S
+//   3. slice  : every DD entry is rounded to the grid of its row / column
+//               (grid_round.cuh: |X - a 2^(W - sigma_i)| <= 1, |X| < 2^W) and cut into S
 //               balanced signed 8-bit digits, most significant first:
 //               X = sum_s d_s 256^(S-1-s), d_s in [-128, 127].  Slices are
 //               stored K-major ([S][rows][K_pad] int8), zero-padded.
@@ -27,12 +27,15 @@
 //               up, then scaled exactly.
 //
 // Error (a priori, per output):
-//   |C - AB|_ij <= 2^-(W+1) (2^sigma_i sum_p |b_pj| + 2^tau_j sum_p |a_ip|)   (rounding of the operands)
+//   |C - AB|_ij <= 2^-W (2^sigma_i sum_p |b_pj| + 2^tau_j sum_p |a_ip|)      (rounding of the operands,
+//                                                                         at most one grid unit each)
 //                + k S 2^(sigma_i + tau_j + 2 - 8S)                          (diagonals g >= S dropped)
 //                + 2^-105 |C_ij|                                           (final DD rounding)
-// With |a_ip| >= 2^(sigma_i - rho_A) and |b_pj| >= 2^(tau_j - rho_B) this is at
-// most (S+1) 2^(106 - 8S + rho_A + rho_B) times k 2^-104 (|A||B|)_ij, which is
-// how the plan picks S for a target (S = 14 gives 15/16 for rho_A = rho_B = 1).
+// (sums over the p whose other factor is nonzero; the products of two rounding
+// errors add at most 2^(104 - 2W + rho_A + rho_B) / k in the units below).  With |a_ip| >= 2^(sigma_i - rho_A) and
+// |b_pj| >= 2^(tau_j - rho_B) for nonzero entries and rho >= 1 this is at most
+// (S+1) 2^(106 - 8S + rho_A + rho_B) times k 2^-104 (|A||B|)_ij, which is how
+// the plan picks S for a target (S = 14 gives 15/16 for rho_A = rho_B = 1).
 //
 // The CRT form (crt_device.cuh) shares steps 1 and 3's rounding and the
 // tensor-core kernels: residues modulo N moduli instead of digits, one product
