@@ -41,17 +41,17 @@ namespace split {
 constexpr int CRT_NL = 8;  // most 32-bit limbs of a reconstruction (256 bits)
 constexpr int CRT_WMAX = 110;
 
-// Reconstruction constants of the plan's N moduli, computed on the device:
-// e_t = (M / m_t) ((M / m_t)^-1 mod m_t) and M = prod m_t modulo 2^256 in
-// 32-bit limbs, c_t = e_t / M = ((M / m_t)^-1 mod m_t) / m_t as 24-bit fixed
-// point, round(c_t 2^24), and the E matrix of the tensor-core reconstruction
+// Reconstruction constants of the plan's N moduli (from the per-count tables
+// of crt_tables.h, generated offline): M = prod m_t modulo 2^256 in 32-bit
+// limbs, and the E matrix of the tensor-core reconstruction
 // (crt_combine_tc_body) ready to copy: row b (an MMA column), byte t (a
-// modulus), zero for t >= N.
+// modulus) holds the bytes of round(c_t 2^24) in rows 0-2 (c_t = e_t / M), a
+// zero row 3, and the bytes of e_t = (M / m_t)((M / m_t)^-1 mod m_t) mod
+// 2^256 in rows 4-35; zero for t >= N and in rows 36-47.  Rows beyond
+// 4 + nbe feed only limbs the reconstruction discards.
 constexpr int CRT_EB_ROWS = 48, CRT_EB_BYTES = 64;
 struct CrtConst {
-  uint32_t ew[CRT_NMAX][CRT_NL];
   uint32_t Mw[CRT_NL];
-  uint32_t cfix[CRT_NMAX];
   alignas(16) uint8_t eb[CRT_EB_ROWS][CRT_EB_BYTES];
 };
 
@@ -94,27 +94,12 @@ __host__ __device__ inline int crt_tc_bytes(int W, int64_t k) {
 // zero column, then nbe bytes of e_t, rounded up to 16 (32 or 48).
 __host__ __device__ inline int crt_tc_cols(int nbe) { return (nbe + 4 + 15) / 16 * 16; }
 
-// Inverse of a modulo m (gcd(a, m) = 1, m <= 256), extended Euclid.
-__device__ __forceinline__ uint32_t inv_mod_small(uint32_t a, uint32_t m) {
-  int t = 0, nt = 1, r = (int)m, nr = (int)(a % m);
-  while (nr != 0) {
-    const int q = r / nr;
-    int tmp = t - q * nt;
-    t = nt;
-    nt = tmp;
-    tmp = r - q * nr;
-    r = nr;
-    nr = tmp;
-  }
-  return (uint32_t)(t < 0 ? t + (int)m : t);
-}
-
 // One block: exponent spreads (as the digit-sliced plan), then W, the moduli
 // count N and the reconstruction constants.  bits > 0 forces W.
 __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, double target, int64_t k,
                                               Plan *plan, CrtConst *cc) {
   __shared__ int red[2][32];
-  __shared__ int sh_n, sh_nbe;
+  __shared__ int sh_n;
   int r[2] = {0, 0};
   for (int o = 0; o < st.n; ++o)
     for (int64_t i = threadIdx.x; i < st.count[o]; i += blockDim.x)
@@ -159,61 +144,25 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
     plan->crt = 1;
     plan->nl = crt_tc_bytes(W, k) / 4;
     sh_n = n;
-    sh_nbe = crt_tc_bytes(W, k);
   }
   __syncthreads();
   const int n = sh_n;
-  // M = prod m_t (9 limbs: M < 2^267), e_t = (M / m_t) inv_t mod 2^256
-  if (threadIdx.x < (unsigned)n) {
+  // the constants of the n-moduli set, from the tables: column t of E
+  if (threadIdx.x < (unsigned)CRT_EB_BYTES) {
     const int t = threadIdx.x;
-    const uint32_t mt = crt_mod[t];
-    uint32_t q[CRT_NL + 1];  // M / m_t = prod_{s != t} m_s
-    for (int l = 0; l <= CRT_NL; ++l) q[l] = 0;
-    q[0] = 1;
-    uint32_t rem = 1;  // (M / m_t) mod m_t
-    for (int s = 0; s < n; ++s) {
-      if (s == t) continue;
-      const uint32_t ms = crt_mod[s];
-      uint64_t carry = 0;
-      for (int l = 0; l <= CRT_NL; ++l) {
-        const uint64_t v = (uint64_t)q[l] * ms + carry;
-        q[l] = (uint32_t)v;
-        carry = v >> 32;
-      }
-      rem = (rem * (ms % mt)) % mt;
-    }
-    const uint32_t inv = inv_mod_small(rem, mt);
-    uint32_t ev[CRT_NL + 1];  // e_t mod 2^288
-    uint64_t carry = 0;
-    for (int l = 0; l <= CRT_NL; ++l) {
-      const uint64_t v = (uint64_t)q[l] * inv + carry;
-      ev[l] = (uint32_t)v;
-      carry = v >> 32;
-    }
-    for (int l = 0; l < CRT_NL; ++l) cc->ew[t][l] = ev[l];
-    const uint32_t cf = (uint32_t)((((uint64_t)inv << 24) + mt / 2) / mt);
-    cc->cfix[t] = cf;
-    // column t of E: rows 0-2 the bytes of cf, row 3 zero, rows 4 .. 4 + nbe - 1
-    // the bytes of e_t, zero above
-    const int nbe = sh_nbe;
+    const uint32_t cf = t < n ? crt_c_n[n - 1][t] : 0u;
     for (int b = 0; b < CRT_EB_ROWS; ++b) {
       uint32_t v = 0;
-      if (b < 3)
-        v = (cf >> (8 * b)) & 0xFFu;
-      else if (b >= 4 && b < 4 + nbe)
-        v = (ev[(b - 4) >> 2] >> (8 * ((b - 4) & 3))) & 0xFFu;
+      if (t < n) {
+        if (b < 3)
+          v = (cf >> (8 * b)) & 0xFFu;
+        else if (b >= 4 && b < 4 + 4 * CRT_NL)
+          v = (crt_e_n[n - 1][t][(b - 4) >> 2] >> (8 * ((b - 4) & 3))) & 0xFFu;
+      }
       cc->eb[b][t] = (uint8_t)v;
     }
-    if (t == 0) {  // M = (M / m_0) m_0
-      uint64_t cy = 0;
-      for (int l = 0; l < CRT_NL; ++l) {
-        const uint64_t v = (uint64_t)q[l] * mt + cy;
-        cc->Mw[l] = (uint32_t)v;
-        cy = v >> 32;
-      }
-    }
-  } else if (threadIdx.x < (unsigned)CRT_EB_BYTES) {  // moduli slots beyond N
-    for (int b = 0; b < CRT_EB_ROWS; ++b) cc->eb[b][threadIdx.x] = 0;
+  } else if (threadIdx.x < (unsigned)(CRT_EB_BYTES + CRT_NL)) {
+    cc->Mw[threadIdx.x - CRT_EB_BYTES] = crt_M_n[n - 1][threadIdx.x - CRT_EB_BYTES];
   }
   __syncthreads();
   for (int o = 0; o < st.n; ++o)

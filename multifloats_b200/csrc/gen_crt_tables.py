@@ -24,6 +24,15 @@ holds:
 * ``crt_off18[t]``     a multiple of m_t of at least 2^18, added to a signed
                        value below that bound first
 
+and, per moduli count N (index N - 1), the reconstruction constants of the
+set m_0 .. m_{N-1} with M = m_0 ... m_{N-1} (global-memory tables,
+``MF_GTABLE``):
+
+* ``crt_M_n[N-1][l]``      M mod 2^256 in 32-bit limbs, least significant first
+* ``crt_e_n[N-1][t][l]``   e_t = (M / m_t) ((M / m_t)^-1 mod m_t) mod 2^256
+* ``crt_c_n[N-1][t]``      round(((M / m_t)^-1 mod m_t) 2^24 / m_t), the 24-bit
+                           fixed point of c_t = e_t / M
+
 Usage::
 
     python gen_crt_tables.py     # (re)write crt_tables.h next to this file
@@ -93,6 +102,31 @@ def main() -> int:
     # offsets making a signed value non-negative before the reduction
     lines.append(f"MF_TABLE uint32_t crt_off18[{NMAX}] = {{" + ", ".join(f"{m * -(-(1 << 18) // m)}u" for m in ms) +
                  "};  // m ceil(2^18 / m): |v| < 2^18")
+    # reconstruction constants per moduli count
+    lines += ["#ifndef MF_GTABLE", "#define MF_GTABLE static const", "#endif"]
+    mw, ew, cw = [], [], []
+    for n in range(1, NMAX + 1):
+        sub = ms[:n]
+        M = 1
+        for m in sub:
+            M *= m
+        mw.append("{" + ", ".join(f"0x{(M >> (32 * l)) & 0xFFFFFFFF:08x}u" for l in range(8)) + "}")
+        rows, cs = [], []
+        for t in range(NMAX):
+            if t < n:
+                q = M // sub[t]
+                inv = pow(q % sub[t], -1, sub[t]) if sub[t] > 1 else 0
+                e = (q * inv) % (1 << 256)
+                c = ((inv << 24) + sub[t] // 2) // sub[t]
+            else:
+                e, c = 0, 0
+            rows.append("{" + ", ".join(f"0x{(e >> (32 * l)) & 0xFFFFFFFF:08x}u" for l in range(8)) + "}")
+            cs.append(f"{c}u")
+        ew.append("{" + ",\n     ".join(rows) + "}")
+        cw.append("{" + ", ".join(cs) + "}")
+    lines.append(f"MF_GTABLE uint32_t crt_M_n[{NMAX}][8] = {{" + ",\n    ".join(mw) + "};")
+    lines.append(f"MF_GTABLE uint32_t crt_e_n[{NMAX}][{NMAX}][8] = {{" + ",\n    ".join(ew) + "};")
+    lines.append(f"MF_GTABLE uint32_t crt_c_n[{NMAX}][{NMAX}] = {{" + ",\n    ".join(cw) + "};")
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "crt_tables.h")
     with open(out, "w") as f:
         f.write("\n".join(lines) + "\n")
