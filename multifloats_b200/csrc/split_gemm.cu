@@ -509,7 +509,95 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
       bool ok = true;
       PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
       Item it;
-      while (ok && sched.next(it)) {
+      // nsub = 2: one 512-column accumulator whose two 256-column halves are
+      // handed back separately (tempty[0], tempty[1]).  The epilogue drains
+      // half 0 first, so an item's half-0 MMAs start while half 1 of the
+      // previous item still drains; the stages consumed meanwhile are held
+      // (pend) and their half-1 MMAs issued, and the stages released in ring
+      // order, as soon as half 1 is free -- at the latest when every stage of
+      // the ring is held.
+      int pend[6];
+      int npend = 0;
+      uint32_t acc1 = 0;
+      auto half1 = [&](int st) {
+        const uint64_t ad = mftc::smem_desc_k_sw128(mftc::smem_u32(sA + st * P_STAGE_A));
+        const uint64_t bd = mftc::smem_desc_k_sw128(mftc::smem_u32(sB + st * stage_b));
+#pragma unroll
+        for (int kk = 0; kk < BK / UMMA_K; ++kk) {
+          mftc::umma_i8_pair(tmem_base + (uint32_t)BN, ad + (uint64_t)(kk * UMMA_K / 16),
+                             bd + (uint64_t)((P_HALF_B + kk * UMMA_K) / 16), idesc, acc1);
+          acc1 = 1;
+        }
+        mftc::umma_commit_pair(&empty[st], 0x3);
+      };
+      while (ok && nsub == 2 && sched.next(it)) {
+        const int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
+        if (!wait_bar(&tempty[0], acc_phase ^ 1, abort_flag, wait_ns)) {
+          fail(2);
+          break;
+        }
+        mftc::tc_fence_after();
+        bool h1 = false;  // half 1 handed back for this item
+        uint32_t acc0 = 0;
+        acc1 = 0;
+        auto catch_up = [&]() {
+          for (int q = 0; q < npend; ++q) half1(pend[q]);
+          npend = 0;
+        };
+        for (int s = crt ? it.g : 0; s <= it.g && ok; ++s) {
+          for (int kb = kb0; kb < kb1; ++kb) {
+            if (!h1 && npend == nst) {  // every stage held: half 1 first
+              if (!wait_bar(&tempty[1], acc_phase ^ 1, abort_flag, wait_ns)) {
+                fail(2);
+                ok = false;
+                break;
+              }
+              mftc::tc_fence_after();
+              h1 = true;
+              catch_up();
+            }
+            if (!wait_bar(&full[stage], phase, abort_flag, wait_ns)) {
+              fail(4);
+              ok = false;
+              break;
+            }
+            mftc::tc_fence_after();
+            const uint64_t ad0 = mftc::smem_desc_k_sw128(mftc::smem_u32(sA + stage * P_STAGE_A));
+            const uint64_t bd0 = mftc::smem_desc_k_sw128(mftc::smem_u32(sB + stage * stage_b));
+#pragma unroll
+            for (int kk = 0; kk < BK / UMMA_K; ++kk) {
+              mftc::umma_i8_pair(tmem_base, ad0 + (uint64_t)(kk * UMMA_K / 16), bd0 + (uint64_t)(kk * UMMA_K / 16),
+                                 idesc, acc0);
+              acc0 = 1;
+            }
+            if (!h1 && mftc::mbar_test_wait(&tempty[1], acc_phase ^ 1)) {
+              mftc::tc_fence_after();
+              h1 = true;
+              catch_up();
+            }
+            if (h1)
+              half1(stage);
+            else
+              pend[npend++] = stage;
+            if (++stage == nst) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+        }
+        if (!ok) break;
+        if (!h1) {
+          if (!wait_bar(&tempty[1], acc_phase ^ 1, abort_flag, wait_ns)) {
+            fail(2);
+            break;
+          }
+          mftc::tc_fence_after();
+          catch_up();
+        }
+        mftc::umma_commit_pair(&tfull[0], 0x3);
+        acc_phase ^= 1;
+      }
+      while (ok && nsub == 1 && sched.next(it)) {
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
         if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag, wait_ns)) {
           fail(2);
@@ -534,9 +622,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
             for (int kk = 0; kk < BK / UMMA_K; ++kk) {
               const uint64_t adesc = ad0 + (uint64_t)(kk * UMMA_K / 16);
               mftc::umma_i8_pair(d_tmem, adesc, bd0 + (uint64_t)(kk * UMMA_K / 16), idesc, accumulate);
-              if (nsub == 2)
-                mftc::umma_i8_pair(d_tmem + (uint32_t)BN, adesc, bd0 + (uint64_t)((P_HALF_B + kk * UMMA_K) / 16),
-                                   idesc, accumulate);
               accumulate = 1;
             }
             mftc::umma_commit_pair(&empty[stage], 0x3);
@@ -561,11 +646,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
       }
     }
   } else {
-    // ---- epilogue: warps 2..9 of both CTAs, TMEM lane quadrant = warp % 4,
-    // warps 2-5 drain the first half of the accumulator's columns, 6-9 the second ----
+    // ---- epilogue: warps 2..9 of both CTAs, TMEM lane quadrant = warp % 4;
+    // the two warps of a quadrant split each 256-column half of the
+    // accumulator.  nsub = 2: half 0 is drained and handed back (tempty[0])
+    // before half 1 (tempty[1]); nsub = 1: each accumulator is one half. ----
     const int quad = warp & 3;
     const int row = quad * 32 + lane;
-    const int nch = acc_cols / 32 / 2, ch0 = ((warp - 2) / 4) * nch;  // this warp's 32-column chunks
+    const int sel = (warp - 2) / 4;  // which 4 of a half's 8 32-column chunks
     int acc = 0;
     uint32_t acc_phase = 0;
     PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
@@ -580,39 +667,51 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
       const int64_t off = ((int64_t)(it.g * nkc + it.kc) * N_pad + (int64_t)it.tn * tn_cols) * M_pad +
                           (int64_t)it.tm * BM_PAIR + (int64_t)rank * 128 + row;
       const uint32_t tm_addr = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * acc_cols);
-      if (crt) {  // residues modulo m_g, four columns per 32-bit word (crt_device.cuh)
-        uint32_t *dst = reinterpret_cast<uint32_t *>(D) + crt_word_index(off, M_pad) + (int64_t)ch0 * 8 * M_pad;
+      // chunks [c0, c0 + 4) of the accumulator (32 columns each) to the scratch
+      auto drain = [&](int c0) {
+        if (crt) {  // residues modulo m_g, four columns per 32-bit word (crt_device.cuh)
+          uint32_t *dst = reinterpret_cast<uint32_t *>(D) + crt_word_index(off, M_pad) + (int64_t)c0 * 8 * M_pad;
 #pragma unroll 1
-        for (int chunk = ch0; chunk < ch0 + nch; ++chunk) {
-          uint32_t v[32];
-          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
-          mftc::tmem_wait_ld();
+          for (int chunk = c0; chunk < c0 + 4; ++chunk) {
+            uint32_t v[32];
+            mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
+            mftc::tmem_wait_ld();
 #pragma unroll
-          for (int g = 0; g < 8; ++g) {
-            __stcs(dst, crt_pack4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3], it.g));
-            dst += M_pad;
+            for (int g = 0; g < 8; ++g) {
+              __stcs(dst, crt_pack4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3], it.g));
+              dst += M_pad;
+            }
+          }
+        } else {
+          int32_t *dst = D + off + (int64_t)c0 * 32 * M_pad;
+#pragma unroll 1
+          for (int chunk = c0; chunk < c0 + 4; ++chunk) {
+            uint32_t v[32];
+            mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
+            mftc::tmem_wait_ld();
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+              __stcs(dst, (int32_t)v[q]);  // evict-first: keep L2 for the slices
+              dst += M_pad;
+            }
           }
         }
-      } else {
-        int32_t *dst = D + off + (int64_t)ch0 * 32 * M_pad;
-#pragma unroll 1
-        for (int chunk = ch0; chunk < ch0 + nch; ++chunk) {
-          uint32_t v[32];
-          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
-          mftc::tmem_wait_ld();
-#pragma unroll
-          for (int q = 0; q < 32; ++q) {
-            __stcs(dst, (int32_t)v[q]);  // evict-first: keep L2 for the slices
-            dst += M_pad;
-          }
-        }
-      }
-      mftc::tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mftc::mbar_arrive_cluster(mftc::cluster_addr(&tempty[acc], 0));
-      if (++acc == nacc) {
-        acc = 0;
+        mftc::tc_fence_before();
+        __syncwarp();
+      };
+      if (nsub == 2) {
+        drain(4 * sel);
+        if (lane == 0) mftc::mbar_arrive_cluster(mftc::cluster_addr(&tempty[0], 0));
+        drain(8 + 4 * sel);
+        if (lane == 0) mftc::mbar_arrive_cluster(mftc::cluster_addr(&tempty[1], 0));
         acc_phase ^= 1;
+      } else {
+        drain(4 * sel);
+        if (lane == 0) mftc::mbar_arrive_cluster(mftc::cluster_addr(&tempty[acc], 0));
+        if (++acc == nacc) {
+          acc = 0;
+          acc_phase ^= 1;
+        }
       }
     }
   }
