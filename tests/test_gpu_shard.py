@@ -87,8 +87,9 @@ def test_reduction_equals_rank_order_fold(cuda_lib, dev, comm, kind, code):
     x = W.dd_uniform(per * n, seed=31)
     y = W.dd_uniform(per * n, seed=32)
     out = torch.empty(4, dtype=torch.float64, device=dev)
-    rc = cuda_lib.mfcuda_reduce_nccl(code, to_dev(x, dev).data_ptr(), to_dev(y, dev).data_ptr(), n, 8,
-                                     out.data_ptr(), comm.handle, _stream())
+    dx, dy = to_dev(x, dev), to_dev(y, dev)  # held: the call runs asynchronously on the stream
+    rc = cuda_lib.mfcuda_reduce_nccl(code, dx.data_ptr(), dy.data_ptr(), n, 8, out.data_ptr(), comm.handle,
+                                     _stream())
     assert rc == 0
     nd = 4 if kind in ("csum", "cdot") else 2
     want = O.reduce_combine(kind, O.reduce_partial(kind, x, y if "dot" in kind else None, 8))
