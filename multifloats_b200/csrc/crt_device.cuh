@@ -663,7 +663,8 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
 // entries at once, so per entry and modulus only the Barrett step and the
 // packing remain on the CUDA cores.
 //
-// CTA of CRT_RT_THREADS threads = 4 warps, tile of 4 "lines" x 128 K entries:
+// CTA of CRT_RT_THREADS threads = 4 warps, rounds of 4 "lines" x 128 K entries
+// (CRT_RT_TILES consecutive rounds per CTA, reusing its TMEM and weights):
 // warp w takes line r0 + w (a row of A, a column of B), lane l the entries
 // p0 + 4 l .. p0 + 4 l + 3 (group g = entry p0 + 4 l + g), so the residue
 // bytes of one modulus for a lane's four entries form one 32-bit word and a
@@ -672,7 +673,8 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
 // Works for at most 32 moduli (the host uses the dp4a slicers otherwise).
 constexpr int CRT_RT_THREADS = 128;
 constexpr int CRT_RT_LINES = 4;       // rows of A / columns of B per CTA
-constexpr int CRT_RT_P = 128;         // K entries per CTA
+constexpr int CRT_RT_P = 128;         // K entries per MMA round
+constexpr int CRT_RT_TILES = 4;       // MMA rounds (consecutive K blocks) per CTA
 constexpr int CRT_RT_NMOD = 32;       // MMA N: moduli per pass
 constexpr int CRT_RT_A_BYTES = 128 * 128;  // entries tile: 128 rows of 128 bytes (4 groups of 32)
 constexpr int CRT_RT_W_BYTES = 32 * 128;   // weights tile: 32 rows (moduli) of 128 bytes
@@ -692,7 +694,7 @@ template <int MODE>
 __device__ __forceinline__ void crt_slice_tc_body(const double *__restrict__ X, int64_t M, int64_t K, int64_t lines,
                                                   int64_t stride, int64_t lines_pad, int64_t K_pad, const int *sig,
                                                   const int *flag, const Plan *plan, uint8_t *__restrict__ S,
-                                                  int64_t line0, int64_t p0, uint8_t *smem, int *status,
+                                                  int64_t line0, int64_t p_first, uint8_t *smem, int *status,
                                                   uint64_t wait_ns) {
   const int T = threadIdx.x, warp = T >> 5, lane = T & 31;
   const int n = plan->S, W = plan->W;
@@ -715,49 +717,61 @@ __device__ __forceinline__ void crt_slice_tc_body(const double *__restrict__ X, 
     sw128_store16(sW, T, 0, wv);
     sw128_store16(sW, T, 1, make_uint4(0u, 0u, 0u, 0u));
   }
-  // entries: row T, group g in bytes [32 g, 32 g + 32): the 16 bytes of Y
-  // (byte 14 set to the constant 1) and 16 zero bytes
+#pragma unroll
+  for (int g = 0; g < 4; ++g) sw128_store16(sA, T, 2 * g + 1, make_uint4(0u, 0u, 0u, 0u));  // K padding
   const int64_t line = line0 + warp;
   const bool line_ok = line < lines && !flag[line < lines ? line : 0];
   const int sg = line < lines ? sig[line] : 0;
   const GridLimits gl = grid_limits(W);
-#pragma unroll
-  for (int g = 0; g < 4; ++g) {
-    const int64_t p = p0 + 4 * lane + g;
-    uint32_t y[4];
-    if (line_ok && p < K) {
-      const int64_t e = MODE == 0 ? p * M + line : line * K + p;
-      const double2 v = __ldg(reinterpret_cast<const double2 *>(X) + e * stride);
-      int64_t Tq;
-      uint64_t Rq;
-      grid_round(v.x, v.y, sg, gl, W, Tq, Rq);
-      grid_biased_words(Tq, Rq, y);
-    } else {
-#pragma unroll
-      for (int w = 0; w < 4; ++w) y[w] = bias_word(w);  // X = 0: every residue zero
-    }
-    sw128_store16(sA, T, 2 * g, make_uint4(y[0], y[1], y[2], y[3] | (1u << 16)));
-    sw128_store16(sA, T, 2 * g + 1, make_uint4(0u, 0u, 0u, 0u));
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  const int64_t plane = lines_pad * K_pad / 4;  // 32-bit words per residue plane
+  uint32_t phase = 0;
   mftc::tc_fence_before();
   __syncthreads();
   mftc::tc_fence_after();
   const uint32_t tmem = *tslot;
-  if (T == 0) {
-    const uint32_t idesc = mftc::idesc_u8(128, CRT_RT_NMOD);
-    const uint64_t wdesc = mftc::smem_desc_k_sw128(mftc::smem_u32(sW));
+  // CRT_RT_TILES consecutive blocks of 128 K entries, one MMA round each
+  for (int it = 0; it < CRT_RT_TILES; ++it) {
+    const int64_t p0 = p_first + (int64_t)it * CRT_RT_P;
+    if (p0 >= K_pad) break;  // uniform
+    // entries: row T, group g in bytes [32 g, 32 g + 16): the 16 bytes of Y
+    // (byte 14 set to the constant 1); bytes [32 g + 16, 32 g + 32) stay zero
 #pragma unroll
-    for (int g = 0; g < 4; ++g)
-      mftc::umma_i8(tmem + (uint32_t)(g * CRT_RT_NMOD), mftc::smem_desc_k_sw128(mftc::smem_u32(sA + 32 * g)), wdesc,
-                    idesc, 0u);
-    mftc::umma_commit(bar);
-  }
-  const bool ok = wait_bar_ns(bar, 0, wait_ns);
-  if (__syncthreads_or(!ok)) {  // uniform: every thread leaves together
-    if (T == 0) record_abort(status, 2);
-    (void)wait_bar_ns(bar, 0, WAIT_NS);  // the MMAs finish before tensor memory is freed
-  } else {
+    for (int g = 0; g < 4; ++g) {
+      const int64_t p = p0 + 4 * lane + g;
+      uint32_t y[4];
+      if (line_ok && p < K) {
+        const int64_t e = MODE == 0 ? p * M + line : line * K + p;
+        const double2 v = __ldg(reinterpret_cast<const double2 *>(X) + e * stride);
+        int64_t Tq;
+        uint64_t Rq;
+        grid_round(v.x, v.y, sg, gl, W, Tq, Rq);
+        grid_biased_words(Tq, Rq, y);
+      } else {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) y[w] = bias_word(w);  // X = 0: every residue zero
+      }
+      sw128_store16(sA, T, 2 * g, make_uint4(y[0], y[1], y[2], y[3] | (1u << 16)));
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mftc::tc_fence_before();  // also orders the previous round's TMEM loads before this round's MMAs
+    __syncthreads();
+    if (T == 0) {
+      mftc::tc_fence_after();
+      const uint32_t idesc = mftc::idesc_u8(128, CRT_RT_NMOD);
+      const uint64_t wdesc = mftc::smem_desc_k_sw128(mftc::smem_u32(sW));
+#pragma unroll
+      for (int g = 0; g < 4; ++g)
+        mftc::umma_i8(tmem + (uint32_t)(g * CRT_RT_NMOD), mftc::smem_desc_k_sw128(mftc::smem_u32(sA + 32 * g)),
+                      wdesc, idesc, 0u);
+      mftc::umma_commit(bar);
+    }
+    const bool ok = wait_bar_ns(bar, phase, wait_ns);
+    if (__syncthreads_or(!ok)) {  // uniform: every thread leaves together
+      if (T == 0) record_abort(status, 2);
+      (void)wait_bar_ns(bar, phase, WAIT_NS);  // the MMAs finish before tensor memory is freed
+      break;
+    }
+    phase ^= 1;
     mftc::tc_fence_after();
     uint32_t word[CRT_RT_NMOD];
 #pragma unroll
@@ -769,16 +783,18 @@ __device__ __forceinline__ void crt_slice_tc_body(const double *__restrict__ X, 
       mftc::tmem_wait_ld();
 #pragma unroll
       for (int t = 0; t < CRT_RT_NMOD; ++t) {
-        const uint32_t r = u[t] - __umulhi(u[t], crt_mu[t < CRT_NMAX ? t : 0]) * crt_mod[t < CRT_NMAX ? t : 0];
-        word[t] += r << (8 * g);
+        if (t >= n) break;  // uniform
+        const uint32_t r = u[t] - __umulhi(u[t], crt_mu[t]) * crt_mod[t];
+        word[t] |= r << (8 * g);
       }
     }
-    if (line < lines_pad && p0 + 4 * lane < K_pad) {
+    if (line < lines_pad) {
       uint32_t *dst = reinterpret_cast<uint32_t *>(S + (line * K_pad + p0 + 4 * lane));
-      const int64_t plane = lines_pad * K_pad / 4;  // words per residue plane
 #pragma unroll
-      for (int t = 0; t < CRT_RT_NMOD; ++t)
-        if (t < n) dst[t * plane] = word[t];
+      for (int t = 0; t < CRT_RT_NMOD; ++t) {
+        if (t >= n) break;
+        dst[t * plane] = word[t];
+      }
     }
   }
   mftc::tc_fence_before();

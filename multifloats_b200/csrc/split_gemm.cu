@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restri
   crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, j0 + blockIdx.y, p8);  // column j0 + y
 }
 // Residues on the tensor cores (crt_slice_tc_body): MODE 0 slices A (block x:
-// rows 4 x .., block y: K entries 128 y ..), MODE 1 slices B (block x: columns
+// rows 4 x .., block y: K entries 512 y ..), MODE 1 slices B (block x: columns
 // line_base + 4 x .., block y as for A).  `rows` is m for A (the view's row
 // count, its column stride); `lines` the rows of A or the columns of B.
 template <int MODE>
@@ -788,7 +788,8 @@ __global__ void __launch_bounds__(CRT_RT_THREADS) crt_slice_tc_kernel(
   extern __shared__ uint8_t crt_rt_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(crt_rt_raw) + 1023) & ~uintptr_t(1023));
   crt_slice_tc_body<MODE>(X, rows, K, lines, stride, lines_pad, K_pad, sig, flag, plan, S,
-                          line_base + (int64_t)blockIdx.x * CRT_RT_LINES, (int64_t)blockIdx.y * CRT_RT_P, smem,
+                          line_base + (int64_t)blockIdx.x * CRT_RT_LINES,
+                          (int64_t)blockIdx.y * CRT_RT_P * CRT_RT_TILES, smem,
                           status, wait_ns);
 }
 // Tensor-core reconstruction (crt_combine_tc_body): block (x, y) takes rows
@@ -832,12 +833,12 @@ static bool use_pair(int64_t m) {
   return enabled && m > BM;
 }
 
-// CRT residues on the tensor cores (crt_slice_tc_kernel); MFCUDA_CRT_TC_RESIDUES=0
-// selects the dp4a slicers (same bytes).
+// CRT residues on the tensor cores (crt_slice_tc_kernel) when
+// MFCUDA_CRT_TC_RESIDUES=1; the dp4a slicers otherwise (same bytes).
 static bool use_tc_residues() {
   static const bool enabled = [] {
     const char *e = getenv("MFCUDA_CRT_TC_RESIDUES");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
   }();
   return enabled;
 }
@@ -1110,9 +1111,10 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     // CRT residues on the tensor cores when every plan this call can make has
     // at most 32 moduli (the dp4a slicers otherwise; both give the same bytes)
     const bool tc_res = crt && L.nsl <= CRT_RT_NMOD && use_tc_residues();
-    const dim3 gra((unsigned)(L.M_pad / CRT_RT_LINES), (unsigned)(L.K_pad / CRT_RT_P));
+    const unsigned rt_y = (unsigned)((L.K_pad / CRT_RT_P + CRT_RT_TILES - 1) / CRT_RT_TILES);
+    const dim3 gra((unsigned)(L.M_pad / CRT_RT_LINES), rt_y);
     auto slice_b_tc = [&](int o, int64_t jb, int64_t ncols) {
-      crt_slice_tc_kernel<1><<<dim3((unsigned)(ncols / CRT_RT_LINES), (unsigned)(L.K_pad / CRT_RT_P)),
+      crt_slice_tc_kernel<1><<<dim3((unsigned)(ncols / CRT_RT_LINES), rt_y),
                                CRT_RT_THREADS, CRT_RT_SMEM, s>>>(
           bview[o - nA], k, k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o], flag[o], plan,
           reinterpret_cast<uint8_t *>(sl[o]), jb, status, wait_ns);

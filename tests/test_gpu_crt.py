@@ -298,17 +298,18 @@ print(int(ok))
 """
 
 
-def test_dp4a_residue_slicers_give_the_same_bytes():
-    """MFCUDA_CRT_TC_RESIDUES=0 selects the CUDA-core (dp4a) residue slicers
-    instead of the tensor-core ones: the results are the restatement's bits
-    either way (the default path is what every other CRT test runs)."""
+@pytest.mark.parametrize("tc", ["0", "1"])
+def test_residue_slicers_give_the_same_bytes(tc):
+    """MFCUDA_CRT_TC_RESIDUES=1 selects the tensor-core residue slicers, 0 (the
+    default) the CUDA-core (dp4a) ones: the results are the restatement's bits
+    either way."""
     import os
     import subprocess
     import sys
 
     from conftest import ROOT
 
-    env = dict(os.environ, MFCUDA_CRT_TC_RESIDUES="0")
+    env = dict(os.environ, MFCUDA_CRT_TC_RESIDUES=tc)
     proc = subprocess.run([sys.executable, "-c", _DP4A_CHILD.format(root=ROOT)], env=env, capture_output=True,
                           text=True, timeout=600)
     assert proc.returncode == 0, proc.stderr
