@@ -150,15 +150,22 @@ __device__ __forceinline__ void crt_plan_body(const StatSet &st, int bits, doubl
   // the constants of the n-moduli set, from the tables: column t of E
   if (threadIdx.x < (unsigned)CRT_EB_BYTES) {
     const int t = threadIdx.x;
-    const uint32_t cf = t < n ? crt_c_n[n - 1][t] : 0u;
+    // the table words first (independent loads), then the 48 bytes of column t
+    uint32_t cf = 0u, ev[CRT_NL];
+#pragma unroll
+    for (int l = 0; l < CRT_NL; ++l) ev[l] = 0u;
+    if (t < n) {
+      cf = crt_c_n[n - 1][t];
+#pragma unroll
+      for (int l = 0; l < CRT_NL; ++l) ev[l] = crt_e_n[n - 1][t][l];
+    }
+#pragma unroll
     for (int b = 0; b < CRT_EB_ROWS; ++b) {
       uint32_t v = 0;
-      if (t < n) {
-        if (b < 3)
-          v = (cf >> (8 * b)) & 0xFFu;
-        else if (b >= 4 && b < 4 + 4 * CRT_NL)
-          v = (crt_e_n[n - 1][t][(b - 4) >> 2] >> (8 * ((b - 4) & 3))) & 0xFFu;
-      }
+      if (b < 3)
+        v = (cf >> (8 * b)) & 0xFFu;
+      else if (b >= 4 && b < 4 + 4 * CRT_NL)
+        v = (ev[(b - 4) >> 2] >> (8 * ((b - 4) & 3))) & 0xFFu;
       cc->eb[b][t] = (uint8_t)v;
     }
   } else if (threadIdx.x < (unsigned)(CRT_EB_BYTES + CRT_NL)) {
@@ -648,159 +655,6 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
   __syncthreads();
   mftc::tc_fence_after();
   if (warp == 0) mftc::tmem_dealloc(tmem, ncols);
-}
-
-// ---- residues on the tensor cores ----------------------------------------------
-// The residues of an entry X modulo the n moduli are a small integer matrix
-// product: with Y = X + sum_{q<14} 128 * 256^q (grid_biased_words; bytes y_q
-// in [0, 255], y_14 = 0) and the constant 1 put in byte 14,
-//   u_t = sum_{q<=14} y_q w_{q,t},  w_{q,t} = 256^q mod m_t (q < 14),
-//                                   w_{14,t} = (-bias) mod m_t       (crt_resw)
-// is congruent to X modulo m_t and below 15 * 255^2 < 2^20, so one Barrett
-// step u - umulhi(u, ceil(2^32 / m)) m gives the residue in [0, m_t) -- the
-// same residue the dp4a slicers compute, bit for bit.  One u8 x u8 -> s32
-// tcgen05.mma (M = 128 entries, N = 32 moduli, K = 32 bytes) forms u for 128
-// entries at once, so per entry and modulus only the Barrett step and the
-// packing remain on the CUDA cores.
-//
-// CTA of CRT_RT_THREADS threads = 4 warps, rounds of 4 "lines" x 128 K entries
-// (CRT_RT_TILES consecutive rounds per CTA, reusing its TMEM and weights):
-// warp w takes line r0 + w (a row of A, a column of B), lane l the entries
-// p0 + 4 l .. p0 + 4 l + 3 (group g = entry p0 + 4 l + g), so the residue
-// bytes of one modulus for a lane's four entries form one 32-bit word and a
-// warp writes 128 contiguous bytes of a line's residue row.  TMEM lane T of
-// the accumulator is thread T; group g's sums sit in columns [32 g, 32 g + 32).
-// Works for at most 32 moduli (the host uses the dp4a slicers otherwise).
-constexpr int CRT_RT_THREADS = 128;
-constexpr int CRT_RT_LINES = 4;       // rows of A / columns of B per CTA
-constexpr int CRT_RT_P = 128;         // K entries per MMA round
-constexpr int CRT_RT_TILES = 4;       // MMA rounds (consecutive K blocks) per CTA
-constexpr int CRT_RT_NMOD = 32;       // MMA N: moduli per pass
-constexpr int CRT_RT_A_BYTES = 128 * 128;  // entries tile: 128 rows of 128 bytes (4 groups of 32)
-constexpr int CRT_RT_W_BYTES = 32 * 128;   // weights tile: 32 rows (moduli) of 128 bytes
-// Dynamic shared memory of a CTA: the tiles, barrier and slot, alignment --
-// padded to 56 KiB so that at most four CTAs share an SM, the number whose
-// 128-column TMEM allocations fit its 512 columns (a fifth would wait inside
-// tcgen05.alloc holding its SM slot).
-constexpr int CRT_RT_SMEM_USED = CRT_RT_A_BYTES + CRT_RT_W_BYTES + 64 + 1024;
-constexpr int CRT_RT_SMEM = 56 * 1024;
-static_assert(CRT_RT_SMEM >= CRT_RT_SMEM_USED, "tiles must fit");
-
-// mode 0: A (m x k column-major view: entry (i, p) at (p M + i) stride);
-// mode 1: B (k x n column-major view: entry (j, p) at (j K + p) stride).
-// line0 = first line of this CTA, p0 = first K entry; lines = M (A) or N (B),
-// lines_pad = the padded line count of the residue planes S[t][line][K_pad].
-template <int MODE>
-__device__ __forceinline__ void crt_slice_tc_body(const double *__restrict__ X, int64_t M, int64_t K, int64_t lines,
-                                                  int64_t stride, int64_t lines_pad, int64_t K_pad, const int *sig,
-                                                  const int *flag, const Plan *plan, uint8_t *__restrict__ S,
-                                                  int64_t line0, int64_t p_first, uint8_t *smem, int *status,
-                                                  uint64_t wait_ns) {
-  const int T = threadIdx.x, warp = T >> 5, lane = T & 31;
-  const int n = plan->S, W = plan->W;
-  uint8_t *sA = smem;
-  uint8_t *sW = smem + CRT_RT_A_BYTES;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + CRT_RT_A_BYTES + CRT_RT_W_BYTES);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
-  if (T == 0) {
-    mftc::mbar_init(bar, 1);
-    mftc::fence_mbar_init();
-  }
-  if (warp == 0) {
-    mftc::tmem_alloc(tslot, 128);
-    mftc::tmem_relinquish();
-  }
-  // weights: row t holds w_{q,t} in bytes 0..15 (zero for t >= n), zeros in 16..31
-  if (T < CRT_RT_NMOD) {
-    const uint4 wv = T < n ? make_uint4(crt_resw[T][0], crt_resw[T][1], crt_resw[T][2], crt_resw[T][3])
-                           : make_uint4(0u, 0u, 0u, 0u);
-    sw128_store16(sW, T, 0, wv);
-    sw128_store16(sW, T, 1, make_uint4(0u, 0u, 0u, 0u));
-  }
-#pragma unroll
-  for (int g = 0; g < 4; ++g) sw128_store16(sA, T, 2 * g + 1, make_uint4(0u, 0u, 0u, 0u));  // K padding
-  const int64_t line = line0 + warp;
-  const bool line_ok = line < lines && !flag[line < lines ? line : 0];
-  const int sg = line < lines ? sig[line] : 0;
-  const GridLimits gl = grid_limits(W);
-  const int64_t plane = lines_pad * K_pad / 4;  // 32-bit words per residue plane
-  uint32_t phase = 0;
-  mftc::tc_fence_before();
-  __syncthreads();
-  mftc::tc_fence_after();
-  const uint32_t tmem = *tslot;
-  // CRT_RT_TILES consecutive blocks of 128 K entries, one MMA round each
-  for (int it = 0; it < CRT_RT_TILES; ++it) {
-    const int64_t p0 = p_first + (int64_t)it * CRT_RT_P;
-    if (p0 >= K_pad) break;  // uniform
-    // entries: row T, group g in bytes [32 g, 32 g + 16): the 16 bytes of Y
-    // (byte 14 set to the constant 1); bytes [32 g + 16, 32 g + 32) stay zero
-#pragma unroll
-    for (int g = 0; g < 4; ++g) {
-      const int64_t p = p0 + 4 * lane + g;
-      uint32_t y[4];
-      if (line_ok && p < K) {
-        const int64_t e = MODE == 0 ? p * M + line : line * K + p;
-        const double2 v = __ldg(reinterpret_cast<const double2 *>(X) + e * stride);
-        int64_t Tq;
-        uint64_t Rq;
-        grid_round(v.x, v.y, sg, gl, W, Tq, Rq);
-        grid_biased_words(Tq, Rq, y);
-      } else {
-#pragma unroll
-        for (int w = 0; w < 4; ++w) y[w] = bias_word(w);  // X = 0: every residue zero
-      }
-      sw128_store16(sA, T, 2 * g, make_uint4(y[0], y[1], y[2], y[3] | (1u << 16)));
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mftc::tc_fence_before();  // also orders the previous round's TMEM loads before this round's MMAs
-    __syncthreads();
-    if (T == 0) {
-      mftc::tc_fence_after();
-      const uint32_t idesc = mftc::idesc_u8(128, CRT_RT_NMOD);
-      const uint64_t wdesc = mftc::smem_desc_k_sw128(mftc::smem_u32(sW));
-#pragma unroll
-      for (int g = 0; g < 4; ++g)
-        mftc::umma_i8(tmem + (uint32_t)(g * CRT_RT_NMOD), mftc::smem_desc_k_sw128(mftc::smem_u32(sA + 32 * g)),
-                      wdesc, idesc, 0u);
-      mftc::umma_commit(bar);
-    }
-    const bool ok = wait_bar_ns(bar, phase, wait_ns);
-    if (__syncthreads_or(!ok)) {  // uniform: every thread leaves together
-      if (T == 0) record_abort(status, 2);
-      (void)wait_bar_ns(bar, phase, WAIT_NS);  // the MMAs finish before tensor memory is freed
-      break;
-    }
-    phase ^= 1;
-    mftc::tc_fence_after();
-    uint32_t word[CRT_RT_NMOD];
-#pragma unroll
-    for (int t = 0; t < CRT_RT_NMOD; ++t) word[t] = 0u;
-#pragma unroll
-    for (int g = 0; g < 4; ++g) {
-      uint32_t u[32];
-      mftc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(g * CRT_RT_NMOD), u);
-      mftc::tmem_wait_ld();
-#pragma unroll
-      for (int t = 0; t < CRT_RT_NMOD; ++t) {
-        if (t >= n) break;  // uniform
-        const uint32_t r = u[t] - __umulhi(u[t], crt_mu[t]) * crt_mod[t];
-        word[t] |= r << (8 * g);
-      }
-    }
-    if (line < lines_pad) {
-      uint32_t *dst = reinterpret_cast<uint32_t *>(S + (line * K_pad + p0 + 4 * lane));
-#pragma unroll
-      for (int t = 0; t < CRT_RT_NMOD; ++t) {
-        if (t >= n) break;
-        dst[t * plane] = word[t];
-      }
-    }
-  }
-  mftc::tc_fence_before();
-  __syncthreads();
-  mftc::tc_fence_after();
-  if (warp == 0) mftc::tmem_dealloc(tmem, 128);
 }
 
 }  // namespace split

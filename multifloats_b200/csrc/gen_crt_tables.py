@@ -23,12 +23,6 @@ holds:
                        too large; one correction)
 * ``crt_off18[t]``     a multiple of m_t of at least 2^18, added to a signed
                        value below that bound first
-* ``crt_resw[t][w]``   unsigned byte weights for residues on the tensor cores:
-                       byte q < 14 is 256^q mod m_t, byte 14 is (-bias) mod m_t
-                       with bias = sum_{q<14} 128 * 256^q, byte 15 is zero.  For
-                       Y = X + bias < 256^14 (bytes y_q) and a constant 1 in
-                       byte 14, sum_q y_q w_q + w_14 is congruent to X modulo m_t
-                       and below 15 * 255^2 < 2^20
 
 and, per moduli count N (index N - 1), the reconstruction constants of the
 set m_0 .. m_{N-1} with M = m_0 ... m_{N-1} (global-memory tables,
@@ -108,14 +102,6 @@ def main() -> int:
     # offsets making a signed value non-negative before the reduction
     lines.append(f"MF_TABLE uint32_t crt_off18[{NMAX}] = {{" + ", ".join(f"{m * -(-(1 << 18) // m)}u" for m in ms) +
                  "};  // m ceil(2^18 / m): |v| < 2^18")
-    # unsigned weights of the tensor-core residue computation
-    bias = sum(128 * 256 ** q for q in range(DIGITS))
-    rw = []
-    for m in ms:
-        bts = [pow(256, q, m) for q in range(DIGITS)] + [(-bias) % m, 0]
-        rw.append("{" + ", ".join(f"0x{sum(bts[4 * k + b] << (8 * b) for b in range(4)):08x}u" for k in range(4)) +
-                  "}")
-    lines.append(f"MF_TABLE uint32_t crt_resw[{NMAX}][4] = {{" + ",\n    ".join(rw) + "};")
     # reconstruction constants per moduli count
     lines += ["#ifndef MF_GTABLE", "#define MF_GTABLE static const", "#endif"]
     mw, ew, cw = [], [], []

@@ -776,22 +776,6 @@ __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restri
   if (p8 >= K_pad) return;
   crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, j0 + blockIdx.y, p8);  // column j0 + y
 }
-// Residues on the tensor cores (crt_slice_tc_body): MODE 0 slices A (block x:
-// rows 4 x .., block y: K entries 512 y ..), MODE 1 slices B (block x: columns
-// line_base + 4 x .., block y as for A).  `rows` is m for A (the view's row
-// count, its column stride); `lines` the rows of A or the columns of B.
-template <int MODE>
-__global__ void __launch_bounds__(CRT_RT_THREADS) crt_slice_tc_kernel(
-    const double *__restrict__ X, int64_t rows, int64_t K, int64_t lines, int64_t stride, int64_t lines_pad,
-    int64_t K_pad, const int *sig, const int *flag, const Plan *plan, uint8_t *__restrict__ S, int64_t line_base,
-    int *status, uint64_t wait_ns) {
-  extern __shared__ uint8_t crt_rt_raw[];
-  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(crt_rt_raw) + 1023) & ~uintptr_t(1023));
-  crt_slice_tc_body<MODE>(X, rows, K, lines, stride, lines_pad, K_pad, sig, flag, plan, S,
-                          line_base + (int64_t)blockIdx.x * CRT_RT_LINES,
-                          (int64_t)blockIdx.y * CRT_RT_P * CRT_RT_TILES, smem,
-                          status, wait_ns);
-}
 // Tensor-core reconstruction (crt_combine_tc_body): block (x, y) takes rows
 // 128 x .. of column quads qbase + CTC_QUADS y .. (columns below N); dynamic shared memory
 // crt_tc_smem(ceil(moduli / 32)).
@@ -831,16 +815,6 @@ static bool use_pair(int64_t m) {
     return !(e && e[0] == '0');
   }();
   return enabled && m > BM;
-}
-
-// CRT residues on the tensor cores (crt_slice_tc_kernel) when
-// MFCUDA_CRT_TC_RESIDUES=1; the dp4a slicers otherwise (same bytes).
-static bool use_tc_residues() {
-  static const bool enabled = [] {
-    const char *e = getenv("MFCUDA_CRT_TC_RESIDUES");
-    return e && e[0] == '1';
-  }();
-  return enabled;
 }
 
 // Output columns per pair tile in 256-column halves (1 or 2; 2 halves the
@@ -1057,8 +1031,6 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
       cudaFuncSetAttribute(split_mma_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM);
       cudaFuncSetAttribute(crt_slice_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            CRT_NMAX * SA_ROWS * SA_STRIDE);
-      cudaFuncSetAttribute(crt_slice_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, CRT_RT_SMEM);
-      cudaFuncSetAttribute(crt_slice_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, CRT_RT_SMEM);
       cudaFuncSetAttribute(crt_combine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            crt_tc_smem((CRT_NMAX + 31) / 32));
     });
@@ -1108,26 +1080,9 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     const int tn_cols = BN * L.nsub;
     const int ntn_all = (int)(L.N_pad / tn_cols);
     const int npan = (sink && crt && L.pair) ? std::max(1, std::min(sink->panels, ntn_all)) : 1;
-    // CRT residues on the tensor cores when every plan this call can make has
-    // at most 32 moduli (the dp4a slicers otherwise; both give the same bytes)
-    const bool tc_res = crt && L.nsl <= CRT_RT_NMOD && use_tc_residues();
-    const unsigned rt_y = (unsigned)((L.K_pad / CRT_RT_P + CRT_RT_TILES - 1) / CRT_RT_TILES);
-    const dim3 gra((unsigned)(L.M_pad / CRT_RT_LINES), rt_y);
-    auto slice_b_tc = [&](int o, int64_t jb, int64_t ncols) {
-      crt_slice_tc_kernel<1><<<dim3((unsigned)(ncols / CRT_RT_LINES), rt_y),
-                               CRT_RT_THREADS, CRT_RT_SMEM, s>>>(
-          bview[o - nA], k, k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o], flag[o], plan,
-          reinterpret_cast<uint8_t *>(sl[o]), jb, status, wait_ns);
-    };
     for (int o = 0; o < nops; ++o) {
       if (o >= nA && npan > 1) continue;  // sliced panel by panel below
-      if (o < nA && tc_res)
-        crt_slice_tc_kernel<0><<<gra, CRT_RT_THREADS, CRT_RT_SMEM, s>>>(
-            aview[o], m, k, m, astride[o], L.M_pad, L.K_pad, sig[o], flag[o], plan,
-            reinterpret_cast<uint8_t *>(sl[o]), 0, status, wait_ns);
-      else if (o >= nA && tc_res)
-        slice_b_tc(o, 0, L.N_pad);
-      else if (o < nA && crt)
+      if (o < nA && crt)
         crt_slice_a_kernel<<<ga, 256, std::min(L.nsl, CRT_SA_MODULI) * SA_ROWS * SA_STRIDE, s>>>(aview[o], m, k, astride[o], L.M_pad,
                                                                        L.K_pad, sig[o], flag[o], plan, sl[o]);
       else if (o < nA)
@@ -1162,9 +1117,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
       const int tn0 = (int)((int64_t)ntn_all * pp / npan), tn1 = (int)((int64_t)ntn_all * (pp + 1) / npan);
       const int64_t j0 = npan == 1 ? 0 : (int64_t)tn0 * tn_cols;
       const int64_t j1 = npan == 1 ? n : std::min<int64_t>(n, (int64_t)tn1 * tn_cols);
-      if (npan > 1 && tc_res)  // this panel's columns of B (padding columns included)
-        for (int o = nA; o < nops; ++o) slice_b_tc(o, (int64_t)tn0 * tn_cols, (int64_t)(tn1 - tn0) * tn_cols);
-      else if (npan > 1)
+      if (npan > 1)  // this panel's columns of B (padding columns included)
         for (int o = nA; o < nops; ++o)
           crt_slice_b_kernel<<<dim3(gb.x, (unsigned)((tn1 - tn0) * tn_cols)), 256, 0, s>>>(
               bview[o - nA], k, n, bstride[o - nA], L.N_pad, L.K_pad, sig[o], flag[o], plan, sl[o],

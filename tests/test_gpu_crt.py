@@ -273,44 +273,3 @@ def test_widest_plan_two_k_steps_in_reconstruction(cuda_lib, dev):
     assert info == winfo and info[0] == 33 and info[3] == 110
     assert O.same_bits(got, want).all()
 
-
-_DP4A_CHILD = r"""
-import ctypes as C, sys
-sys.path.insert(0, {root!r})
-import numpy as np, torch
-from multifloats_b200 import _lib
-from multifloats_b200 import workloads as W
-from oracle import oracle as O
-L = _lib.lib()
-d = torch.device('cuda:0')
-ok = True
-for (m, k, n) in ((300, 700, 520), (96, 130, 64)):
-    a = W.dd_rowcol_scaled(m, k, 16, "row", 11)
-    b = W.dd_rowcol_scaled(k, n, 16, "col", 12)
-    da, db = torch.from_numpy(a).to(d), torch.from_numpy(b).to(d)
-    dc = torch.empty(2 * m * n, dtype=torch.float64, device=d)
-    info = (C.c_int * 4)()
-    rc = L.mfcuda_matmuldd_mm_crt(da.data_ptr(), db.data_ptr(), dc.data_ptr(), m, k, n, 0, 8.0, None, 0, info,
-                                  C.c_void_p(torch.cuda.current_stream().cuda_stream))
-    want, winfo = O.crt_gemm(a, b, m, k, n)
-    ok = ok and rc == 0 and list(info) == winfo and bool(O.same_bits(dc.cpu().numpy(), want).all())
-print(int(ok))
-"""
-
-
-@pytest.mark.parametrize("tc", ["0", "1"])
-def test_residue_slicers_give_the_same_bytes(tc):
-    """MFCUDA_CRT_TC_RESIDUES=1 selects the tensor-core residue slicers, 0 (the
-    default) the CUDA-core (dp4a) ones: the results are the restatement's bits
-    either way."""
-    import os
-    import subprocess
-    import sys
-
-    from conftest import ROOT
-
-    env = dict(os.environ, MFCUDA_CRT_TC_RESIDUES=tc)
-    proc = subprocess.run([sys.executable, "-c", _DP4A_CHILD.format(root=ROOT)], env=env, capture_output=True,
-                          text=True, timeout=600)
-    assert proc.returncode == 0, proc.stderr
-    assert proc.stdout.split()[-1] == "1"
