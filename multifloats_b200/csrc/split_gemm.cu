@@ -668,50 +668,33 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
                           (int64_t)it.tm * BM_PAIR + (int64_t)rank * 128 + row;
       const uint32_t tm_addr = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * acc_cols);
       // chunks [c0, c0 + 4) of the accumulator (32 columns each) to the scratch
-      // the next chunk's TMEM load is issued before this chunk is processed, so
-      // its latency overlaps the processing (tcgen05.wait::ld after it covers it)
       auto drain = [&](int c0) {
-        uint32_t va[32], vb[32];
-        mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(c0 * 32), va);
-        mftc::tmem_wait_ld();
         if (crt) {  // residues modulo m_g, four columns per 32-bit word (crt_device.cuh)
           uint32_t *dst = reinterpret_cast<uint32_t *>(D) + crt_word_index(off, M_pad) + (int64_t)c0 * 8 * M_pad;
-          auto put = [&](const uint32_t (&v)[32]) {
+#pragma unroll 1
+          for (int chunk = c0; chunk < c0 + 4; ++chunk) {
+            uint32_t v[32];
+            mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
+            mftc::tmem_wait_ld();
 #pragma unroll
             for (int g = 0; g < 8; ++g) {
               __stcs(dst, crt_pack4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3], it.g));
               dst += M_pad;
             }
-          };
-          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)((c0 + 1) * 32), vb);
-          put(va);
-          mftc::tmem_wait_ld();
-          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)((c0 + 2) * 32), va);
-          put(vb);
-          mftc::tmem_wait_ld();
-          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)((c0 + 3) * 32), vb);
-          put(va);
-          mftc::tmem_wait_ld();
-          put(vb);
+          }
         } else {
           int32_t *dst = D + off + (int64_t)c0 * 32 * M_pad;
-          auto put = [&](const uint32_t (&v)[32]) {
+#pragma unroll 1
+          for (int chunk = c0; chunk < c0 + 4; ++chunk) {
+            uint32_t v[32];
+            mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)(chunk * 32), v);
+            mftc::tmem_wait_ld();
 #pragma unroll
             for (int q = 0; q < 32; ++q) {
               __stcs(dst, (int32_t)v[q]);  // evict-first: keep L2 for the slices
               dst += M_pad;
             }
-          };
-          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)((c0 + 1) * 32), vb);
-          put(va);
-          mftc::tmem_wait_ld();
-          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)((c0 + 2) * 32), va);
-          put(vb);
-          mftc::tmem_wait_ld();
-          mftc::tmem_ld_32x32b_x32(tm_addr + (uint32_t)((c0 + 3) * 32), vb);
-          put(va);
-          mftc::tmem_wait_ld();
-          put(vb);
+          }
         }
         mftc::tc_fence_before();
         __syncwarp();
