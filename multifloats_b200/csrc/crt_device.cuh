@@ -454,6 +454,32 @@ __device__ __forceinline__ uint32_t crt_pack4(uint32_t v0, uint32_t v1, uint32_t
 }
 
 // ---- reconstruction on the tensor cores ---------------------------------------
+// C' of one output from the column sums S_b of the reconstruction product
+// (below): q from the three fixed-point columns, then V - q M in CRT_NL
+// two's complement limbs, the limbs above nbe bytes filled with the sign
+// (bit 8 nbe - 1).
+__device__ __forceinline__ void crt_limbs_of_sums(const uint32_t (&S)[48], const uint32_t (&Mw)[CRT_NL], int nbe,
+                                                  uint32_t (&limb)[CRT_NL]) {
+  const uint64_t Q = (uint64_t)(S[0] + (S[1] << 8)) + ((uint64_t)S[2] << 16);
+  const uint32_t q = (uint32_t)((Q + (1u << 23)) >> 24);
+  int64_t carry = 0;
+#pragma unroll
+  for (int w = 0; w < CRT_NL; ++w) {
+    const uint32_t lo = S[4 + 4 * w] + (S[5 + 4 * w] << 8);  // < 2^30
+    const uint32_t hi = S[6 + 4 * w] + (S[7 + 4 * w] << 8);  // < 2^30
+    const int64_t v = (int64_t)lo + ((int64_t)hi << 16) - (int64_t)((uint64_t)q * Mw[w]) + carry;
+    limb[w] = (uint32_t)v;
+    carry = v >> 32;  // arithmetic shift
+  }
+  // C' mod 2^(8 nbe): the top bit of limb nbe / 4 - 1 is the sign, copied above
+  uint32_t top = 0;
+#pragma unroll
+  for (int w = 0; w < CRT_NL; ++w) top = 4 * (w + 1) == nbe ? limb[w] : top;
+  const uint32_t fill = (top >> 31) ? 0xFFFFFFFFu : 0u;
+#pragma unroll
+  for (int w = 0; w < CRT_NL; ++w) limb[w] = 4 * w < nbe ? limb[w] : fill;
+}
+
 // The sums over moduli are an integer matrix product: for an output with
 // residues r_t, the column sums
 //   S_b = sum_t r_t E[t][b]   (E[t][b] = byte b of round(c_t 2^24) for b < 3,
@@ -626,26 +652,8 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
       mftc::tmem_wait_ld();
       const int64_t j = 4 * qd + c;
       if (!row_ok || j >= N) continue;
-      // q from the three fixed-point columns
-      const uint64_t Q = (uint64_t)(S[0] + (S[1] << 8)) + ((uint64_t)S[2] << 16);
-      const uint32_t q = (uint32_t)((Q + (1u << 23)) >> 24);
       uint32_t limb[CRT_NL];
-      int64_t carry = 0;
-#pragma unroll
-      for (int w = 0; w < CRT_NL; ++w) {
-        const uint32_t lo = S[4 + 4 * w] + (S[5 + 4 * w] << 8);  // < 2^30
-        const uint32_t hi = S[6 + 4 * w] + (S[7 + 4 * w] << 8);  // < 2^30
-        const int64_t v = (int64_t)lo + ((int64_t)hi << 16) - (int64_t)((uint64_t)q * Mw[w]) + carry;
-        limb[w] = (uint32_t)v;
-        carry = v >> 32;  // arithmetic shift
-      }
-      // C' mod 2^(8 nbe): the top bit of limb nbe / 4 - 1 is the sign, copied above
-      uint32_t top = 0;
-#pragma unroll
-      for (int w = 0; w < CRT_NL; ++w) top = 4 * (w + 1) == nbe ? limb[w] : top;
-      const uint32_t fill = (top >> 31) ? 0xFFFFFFFFu : 0u;
-#pragma unroll
-      for (int w = 0; w < CRT_NL; ++w) limb[w] = 4 * w < nbe ? limb[w] : fill;
+      crt_limbs_of_sums(S, Mw, nbe, limb);
       const int sbc = c == 0 ? sb4.x : c == 1 ? sb4.y : c == 2 ? sb4.z : sb4.w;
       const int fbc = c == 0 ? fb4.x : c == 1 ? fb4.y : c == 2 ? fb4.z : fb4.w;
       crt_emit(limb, (fa | fbc) != 0, sa + sbc - 2 * W, C + 2 * (j * M + i) * cstride, mode);
@@ -655,6 +663,552 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
   __syncthreads();
   mftc::tc_fence_after();
   if (warp == 0) mftc::tmem_dealloc(tmem, ncols);
+}
+
+// ---- per-output arithmetic specialised on the limb count ------------------------
+// NL = max(5, nbe / 4) 32-bit limbs; the results are those of
+// crt_limbs_of_sums and crt_to_dd (same integer, same rounding), with the
+// multi-word additions as PTX carry chains:
+//   crt_limb_chain: r = lo + H + q Mn  (mod 2^(32 NL)),
+//   crt_inc_chain:  m = x + c          (mod 2^(32 NL)).
+template <int NL>
+__device__ __forceinline__ void crt_limb_chain(const uint32_t (&lo)[NL], const uint32_t (&H)[NL], uint32_t q,
+                                               const uint32_t (&Mn)[NL], uint32_t (&r)[NL]);
+template <int NL>
+__device__ __forceinline__ void crt_inc_chain(const uint32_t (&x)[NL], uint32_t c, uint32_t (&m)[NL]);
+template <>
+__device__ __forceinline__ void crt_limb_chain<5>(const uint32_t (&lo)[5], const uint32_t (&H)[5], uint32_t q,
+                                                   const uint32_t (&Mn)[5], uint32_t (&r)[5]) {
+  asm("{\n\t"
+      "add.cc.u32 %0, %5, %10;\n\t"
+      "addc.cc.u32 %1, %6, %11;\n\t"
+      "addc.cc.u32 %2, %7, %12;\n\t"
+      "addc.cc.u32 %3, %8, %13;\n\t"
+      "addc.u32 %4, %9, %14;\n\t"
+      "mad.lo.cc.u32 %0, %15, %16, %0;\n\t"
+      "madc.lo.cc.u32 %1, %15, %17, %1;\n\t"
+      "madc.lo.cc.u32 %2, %15, %18, %2;\n\t"
+      "madc.lo.cc.u32 %3, %15, %19, %3;\n\t"
+      "madc.lo.u32 %4, %15, %20, %4;\n\t"
+      "mad.hi.cc.u32 %1, %15, %16, %1;\n\t"
+      "madc.hi.cc.u32 %2, %15, %17, %2;\n\t"
+      "madc.hi.cc.u32 %3, %15, %18, %3;\n\t"
+      "madc.hi.u32 %4, %15, %19, %4;\n\t"
+      "}"
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4])
+      : "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(H[0]), "r"(H[1]), "r"(H[2]), "r"(H[3]), "r"(H[4]), "r"(q), "r"(Mn[0]), "r"(Mn[1]), "r"(Mn[2]), "r"(Mn[3]), "r"(Mn[4]));
+}
+template <>
+__device__ __forceinline__ void crt_limb_chain<6>(const uint32_t (&lo)[6], const uint32_t (&H)[6], uint32_t q,
+                                                   const uint32_t (&Mn)[6], uint32_t (&r)[6]) {
+  asm("{\n\t"
+      "add.cc.u32 %0, %6, %12;\n\t"
+      "addc.cc.u32 %1, %7, %13;\n\t"
+      "addc.cc.u32 %2, %8, %14;\n\t"
+      "addc.cc.u32 %3, %9, %15;\n\t"
+      "addc.cc.u32 %4, %10, %16;\n\t"
+      "addc.u32 %5, %11, %17;\n\t"
+      "mad.lo.cc.u32 %0, %18, %19, %0;\n\t"
+      "madc.lo.cc.u32 %1, %18, %20, %1;\n\t"
+      "madc.lo.cc.u32 %2, %18, %21, %2;\n\t"
+      "madc.lo.cc.u32 %3, %18, %22, %3;\n\t"
+      "madc.lo.cc.u32 %4, %18, %23, %4;\n\t"
+      "madc.lo.u32 %5, %18, %24, %5;\n\t"
+      "mad.hi.cc.u32 %1, %18, %19, %1;\n\t"
+      "madc.hi.cc.u32 %2, %18, %20, %2;\n\t"
+      "madc.hi.cc.u32 %3, %18, %21, %3;\n\t"
+      "madc.hi.cc.u32 %4, %18, %22, %4;\n\t"
+      "madc.hi.u32 %5, %18, %23, %5;\n\t"
+      "}"
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5])
+      : "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(H[0]), "r"(H[1]), "r"(H[2]), "r"(H[3]), "r"(H[4]), "r"(H[5]), "r"(q), "r"(Mn[0]), "r"(Mn[1]), "r"(Mn[2]), "r"(Mn[3]), "r"(Mn[4]), "r"(Mn[5]));
+}
+template <>
+__device__ __forceinline__ void crt_limb_chain<7>(const uint32_t (&lo)[7], const uint32_t (&H)[7], uint32_t q,
+                                                   const uint32_t (&Mn)[7], uint32_t (&r)[7]) {
+  asm("{\n\t"
+      "add.cc.u32 %0, %7, %14;\n\t"
+      "addc.cc.u32 %1, %8, %15;\n\t"
+      "addc.cc.u32 %2, %9, %16;\n\t"
+      "addc.cc.u32 %3, %10, %17;\n\t"
+      "addc.cc.u32 %4, %11, %18;\n\t"
+      "addc.cc.u32 %5, %12, %19;\n\t"
+      "addc.u32 %6, %13, %20;\n\t"
+      "mad.lo.cc.u32 %0, %21, %22, %0;\n\t"
+      "madc.lo.cc.u32 %1, %21, %23, %1;\n\t"
+      "madc.lo.cc.u32 %2, %21, %24, %2;\n\t"
+      "madc.lo.cc.u32 %3, %21, %25, %3;\n\t"
+      "madc.lo.cc.u32 %4, %21, %26, %4;\n\t"
+      "madc.lo.cc.u32 %5, %21, %27, %5;\n\t"
+      "madc.lo.u32 %6, %21, %28, %6;\n\t"
+      "mad.hi.cc.u32 %1, %21, %22, %1;\n\t"
+      "madc.hi.cc.u32 %2, %21, %23, %2;\n\t"
+      "madc.hi.cc.u32 %3, %21, %24, %3;\n\t"
+      "madc.hi.cc.u32 %4, %21, %25, %4;\n\t"
+      "madc.hi.cc.u32 %5, %21, %26, %5;\n\t"
+      "madc.hi.u32 %6, %21, %27, %6;\n\t"
+      "}"
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6])
+      : "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(lo[6]), "r"(H[0]), "r"(H[1]), "r"(H[2]), "r"(H[3]), "r"(H[4]), "r"(H[5]), "r"(H[6]), "r"(q), "r"(Mn[0]), "r"(Mn[1]), "r"(Mn[2]), "r"(Mn[3]), "r"(Mn[4]), "r"(Mn[5]), "r"(Mn[6]));
+}
+template <>
+__device__ __forceinline__ void crt_limb_chain<8>(const uint32_t (&lo)[8], const uint32_t (&H)[8], uint32_t q,
+                                                   const uint32_t (&Mn)[8], uint32_t (&r)[8]) {
+  asm("{\n\t"
+      "add.cc.u32 %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32 %7, %15, %23;\n\t"
+      "mad.lo.cc.u32 %0, %24, %25, %0;\n\t"
+      "madc.lo.cc.u32 %1, %24, %26, %1;\n\t"
+      "madc.lo.cc.u32 %2, %24, %27, %2;\n\t"
+      "madc.lo.cc.u32 %3, %24, %28, %3;\n\t"
+      "madc.lo.cc.u32 %4, %24, %29, %4;\n\t"
+      "madc.lo.cc.u32 %5, %24, %30, %5;\n\t"
+      "madc.lo.cc.u32 %6, %24, %31, %6;\n\t"
+      "madc.lo.u32 %7, %24, %32, %7;\n\t"
+      "mad.hi.cc.u32 %1, %24, %25, %1;\n\t"
+      "madc.hi.cc.u32 %2, %24, %26, %2;\n\t"
+      "madc.hi.cc.u32 %3, %24, %27, %3;\n\t"
+      "madc.hi.cc.u32 %4, %24, %28, %4;\n\t"
+      "madc.hi.cc.u32 %5, %24, %29, %5;\n\t"
+      "madc.hi.cc.u32 %6, %24, %30, %6;\n\t"
+      "madc.hi.u32 %7, %24, %31, %7;\n\t"
+      "}"
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]), "=&r"(r[7])
+      : "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(lo[6]), "r"(lo[7]), "r"(H[0]), "r"(H[1]), "r"(H[2]), "r"(H[3]), "r"(H[4]), "r"(H[5]), "r"(H[6]), "r"(H[7]), "r"(q), "r"(Mn[0]), "r"(Mn[1]), "r"(Mn[2]), "r"(Mn[3]), "r"(Mn[4]), "r"(Mn[5]), "r"(Mn[6]), "r"(Mn[7]));
+}
+template <>
+__device__ __forceinline__ void crt_inc_chain<5>(const uint32_t (&x)[5], uint32_t c, uint32_t (&m)[5]) {
+  asm("{\n\t"
+      "add.cc.u32 %0, %5, %10;\n\t"
+      "addc.cc.u32 %1, %6, 0;\n\t"
+      "addc.cc.u32 %2, %7, 0;\n\t"
+      "addc.cc.u32 %3, %8, 0;\n\t"
+      "addc.u32 %4, %9, 0;\n\t"
+      "}"
+      : "=&r"(m[0]), "=&r"(m[1]), "=&r"(m[2]), "=&r"(m[3]), "=&r"(m[4])
+      : "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3]), "r"(x[4]), "r"(c));
+}
+template <>
+__device__ __forceinline__ void crt_inc_chain<6>(const uint32_t (&x)[6], uint32_t c, uint32_t (&m)[6]) {
+  asm("{\n\t"
+      "add.cc.u32 %0, %6, %12;\n\t"
+      "addc.cc.u32 %1, %7, 0;\n\t"
+      "addc.cc.u32 %2, %8, 0;\n\t"
+      "addc.cc.u32 %3, %9, 0;\n\t"
+      "addc.cc.u32 %4, %10, 0;\n\t"
+      "addc.u32 %5, %11, 0;\n\t"
+      "}"
+      : "=&r"(m[0]), "=&r"(m[1]), "=&r"(m[2]), "=&r"(m[3]), "=&r"(m[4]), "=&r"(m[5])
+      : "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3]), "r"(x[4]), "r"(x[5]), "r"(c));
+}
+template <>
+__device__ __forceinline__ void crt_inc_chain<7>(const uint32_t (&x)[7], uint32_t c, uint32_t (&m)[7]) {
+  asm("{\n\t"
+      "add.cc.u32 %0, %7, %14;\n\t"
+      "addc.cc.u32 %1, %8, 0;\n\t"
+      "addc.cc.u32 %2, %9, 0;\n\t"
+      "addc.cc.u32 %3, %10, 0;\n\t"
+      "addc.cc.u32 %4, %11, 0;\n\t"
+      "addc.cc.u32 %5, %12, 0;\n\t"
+      "addc.u32 %6, %13, 0;\n\t"
+      "}"
+      : "=&r"(m[0]), "=&r"(m[1]), "=&r"(m[2]), "=&r"(m[3]), "=&r"(m[4]), "=&r"(m[5]), "=&r"(m[6])
+      : "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3]), "r"(x[4]), "r"(x[5]), "r"(x[6]), "r"(c));
+}
+template <>
+__device__ __forceinline__ void crt_inc_chain<8>(const uint32_t (&x)[8], uint32_t c, uint32_t (&m)[8]) {
+  asm("{\n\t"
+      "add.cc.u32 %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, 0;\n\t"
+      "addc.cc.u32 %2, %10, 0;\n\t"
+      "addc.cc.u32 %3, %11, 0;\n\t"
+      "addc.cc.u32 %4, %12, 0;\n\t"
+      "addc.cc.u32 %5, %13, 0;\n\t"
+      "addc.cc.u32 %6, %14, 0;\n\t"
+      "addc.u32 %7, %15, 0;\n\t"
+      "}"
+      : "=&r"(m[0]), "=&r"(m[1]), "=&r"(m[2]), "=&r"(m[3]), "=&r"(m[4]), "=&r"(m[5]), "=&r"(m[6]), "=&r"(m[7])
+      : "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3]), "r"(x[4]), "r"(x[5]), "r"(x[6]), "r"(x[7]), "r"(c));
+}
+
+// C' = V - q M modulo 2^(32 NL) from the column sums S, as crt_limbs_of_sums:
+// q = round((S_0 + S_1 2^8 + S_2 2^16) / 2^24) in 32-bit steps (dividing by
+// 2^8 first changes no floor; S_b < 2^22), V = sum_w lo_w 2^(32 w) + sum_w
+// hi_w 2^(32 w + 16) with the second sum re-cut at limb boundaries (H_w =
+// hi_w 2^16 mod 2^32 + floor(hi_(w-1) / 2^16): disjoint bits), and -q M added
+// as q Mn, Mn = -M mod 2^(32 NL).  nbe < 4 NL only when NL = 5: the limbs
+// above nbe bytes are then filled with the sign (bit 8 nbe - 1).
+template <int NL>
+__device__ __forceinline__ void crt_limbs_nl(const uint32_t (&S)[48], const uint32_t (&Mn)[NL], int nbe,
+                                             uint32_t (&r)[NL]) {
+  const uint32_t q = ((((S[0] + (1u << 23)) >> 8) + S[1] + (S[2] << 8)) >> 16);
+  uint32_t lo[NL], hi[NL], H[NL];
+#pragma unroll
+  for (int w = 0; w < NL; ++w) {
+    lo[w] = S[4 + 4 * w] + (S[5 + 4 * w] << 8);  // < 2^30
+    hi[w] = S[6 + 4 * w] + (S[7 + 4 * w] << 8);  // < 2^30
+  }
+  H[0] = hi[0] << 16;
+#pragma unroll
+  for (int w = 1; w < NL; ++w) H[w] = __funnelshift_l(hi[w - 1], hi[w], 16);
+  crt_limb_chain<NL>(lo, H, q, Mn, r);
+  if (NL == 5 && nbe < 20) {
+    uint32_t top = 0;
+#pragma unroll
+    for (int w = 0; w < NL; ++w) top = 4 * (w + 1) == nbe ? r[w] : top;
+    const uint32_t fill = (uint32_t)((int32_t)top >> 31);
+#pragma unroll
+    for (int w = 0; w < NL; ++w) r[w] = 4 * w < nbe ? r[w] : fill;
+  }
+}
+// The signed NL-limb integer as a double-double scaled by 2^e, exactly as
+// crt_to_dd (magnitude, whole-limb and bit normalisation to a 160-bit window,
+// hi rounded to nearest even, lo summed in doubles, fast_two_sum).
+template <int NL>
+__device__ __forceinline__ void crt_to_dd_nl(const uint32_t (&limb)[NL], double &h, double &l, int &e) {
+  const uint32_t mask = (uint32_t)((int32_t)limb[NL - 1] >> 31);
+  uint32_t x[NL], m[NL];
+#pragma unroll
+  for (int q = 0; q < NL; ++q) x[q] = limb[q] ^ mask;
+  crt_inc_chain<NL>(x, mask & 1u, m);  // the magnitude: two's complement negation when negative
+  int E = 32 * (NL - 5);                // weight of window bit 0 before any shift
+#pragma unroll
+  for (int step = 4; step >= 1; step >>= 1) {
+    bool zero = true;
+#pragma unroll
+    for (int q = NL - step; q < NL; ++q) zero = zero && m[q] == 0;
+    if (zero) {
+#pragma unroll
+      for (int q = NL - 1; q >= 0; --q) m[q] = q >= step ? m[q - step] : 0u;
+      E -= 32 * step;
+    }
+  }
+  if (m[NL - 1] == 0) {
+    h = l = 0.0;
+    e = 0;
+    return;
+  }
+  const int s = __clz((int)m[NL - 1]);
+  uint32_t n[5];
+#pragma unroll
+  for (int w = 0; w < 5; ++w) n[w] = __funnelshift_l(NL - 6 + w >= 0 ? m[NL - 6 + w] : 0u, m[NL - 5 + w], s);
+  E -= s;
+  const uint64_t T64 = ((uint64_t)n[4] << 32) | n[3];
+  uint64_t keep = T64 >> 11;
+  const uint32_t r11 = (uint32_t)(T64 & 0x7FF);
+  const bool lowz = (n[2] | n[1] | n[0]) == 0;
+  const bool up = r11 > 0x400 || (r11 == 0x400 && (!lowz || (keep & 1)));
+  keep += up;
+  const int D = (int)r11 - (up ? 2048 : 0);
+  double lo = mfdev::mul((double)D, pow2(96));
+  lo = mfdev::add(lo, mfdev::mul((double)n[2], pow2(64)));
+  lo = mfdev::add(lo, mfdev::mul((double)n[1], pow2(32)));
+  lo = mfdev::add(lo, (double)n[0]);
+  double hi = (double)keep;
+  lo = mfdev::mul(lo, pow2(-107));  // into units of 2^(E + 107): exact
+  mfdev::fast_two_sum(hi, lo, h, l);
+  if (mask) {
+    h = -h;
+    l = -l;
+  }
+  e = E + 107;
+}
+// crt_emit for NL limbs.
+template <int NL>
+__device__ __forceinline__ void crt_emit_nl(const uint32_t (&limb)[NL], bool nan, int shift,
+                                            double *__restrict__ dst, int mode) {
+  double2 out;
+  if (nan) {
+    out = make_double2(CUDART_NAN, 0.0);
+  } else {
+    double hi, lo;
+    int e;
+    crt_to_dd_nl<NL>(limb, hi, lo, e);
+    out = make_double2(scale2(hi, e + shift), scale2(lo, e + shift));
+  }
+  double2 *d2 = reinterpret_cast<double2 *>(dst);
+  if (mode != 0) {
+    const double2 prev = *d2;
+    const mfdev::dd p = mfdev::make(out.x, out.y), pv = mfdev::make(prev.x, prev.y);
+    const mfdev::dd res = mode == 1 ? mfdev::dd_sub(pv, p) : mfdev::dd_add(pv, p);
+    out = make_double2(res.hi, res.lo);
+  }
+  __stcs(d2, out);
+}
+
+// ---- reconstruction fed by TMA ---------------------------------------------------
+// Work unit: 32 rows x one column quad = 128 outputs, the M dimension of one
+// reconstruction MMA, M index 4 r + c <-> row i0 + r, column 4 qd + c.  In
+// the residue scratch the 128 bytes of (modulus t, unit) are contiguous (rows
+// i0 .. i0 + 31, four columns per row), so one TMA box of 128 bytes x 32 ktn
+// moduli lands in shared memory as an MN-major operand with the 128-byte
+// swizzle -- 8 moduli x 128 bytes per 1024-byte atom, atoms consecutive along
+// K -- and no thread touches the residues.  The TMEM lane of an output is its
+// M index, so a thread's output is row i0 + 8 (lane quadrant) + lane / 4,
+// column 4 qd + lane % 4.
+//
+// Persistent CTA per SM: warp 0 loads (a ring of CR_RING_BYTES of boxes), warp 1
+// issues one MMA per 32 moduli per unit into one of the TMEM slots (nb
+// columns each), and CR_EPI_WARPS / 4 sets of four epilogue warps (one per
+// lane quadrant) take the units in turn: each copies its slot to registers,
+// hands it back, and forms and stores the 128 outputs.  Planes of moduli
+// t >= N (up to the allocated count, and zero-filled beyond it) meet zero
+// rows of E.  K chunks (nkc > 1) are folded into chunk 0 beforehand
+// (crt_fold_kernel).  All waits are bounded.
+// Walks units u0, u0 + step, ... as (row block rb, quad offset qd), u = qd
+// nrb + rb, without a division in the loop.
+struct UnitCursor {
+  int64_t u, rb, qd, step, drb, dqd, nrb;
+  __device__ __forceinline__ UnitCursor(int64_t u0, int64_t step_, int64_t nrb_)
+      : u(u0), rb(u0 % nrb_), qd(u0 / nrb_), step(step_), drb(step_ % nrb_), dqd(step_ / nrb_), nrb(nrb_) {}
+  __device__ __forceinline__ void advance() {
+    u += step;
+    rb += drb;
+    qd += dqd;
+    if (rb >= nrb) {
+      rb -= nrb;
+      ++qd;
+    }
+  }
+};
+constexpr int CR_EPI_WARPS = 16;
+constexpr int CR_SETS = CR_EPI_WARPS / 4;
+constexpr int CR_THREADS = 64 + 32 * CR_EPI_WARPS;
+constexpr int CR_RING_BYTES = 128 * 1024;
+constexpr int CR_STAGES_MAX = 32;  // CR_RING_BYTES / CR_BOX_BYTES
+constexpr int CR_TMEM_COLS = 512;
+constexpr int CR_BOX_BYTES = 4096;  // 128 bytes x 32 moduli
+__host__ __device__ constexpr int cr_slot_cols(int nb) { return nb <= 32 ? 32 : 64; }
+__host__ __device__ constexpr int cr_smem(int ktn) {
+  return CR_RING_BYTES + CTC_B_BYTES + 1024 + 1024;  // ring, E, barriers, alignment
+}
+
+// The epilogue warps of crt_recon_body: set e (four warps, one per TMEM
+// lane quadrant) takes units e, e + CR_SETS, ... of the CTA; per unit it
+// copies its slot to registers, hands the slot back, and forms and stores its
+// 128 outputs with NL-limb arithmetic.
+struct RecEpi {
+  const CrtConst *cc;
+  const int *sigA, *flagA, *sigB, *flagB;
+  int64_t M, N, qbase, nrb, units;
+  double *C;
+  int64_t cstride;
+  int mode, W, nbe, nb, slot_cols, nslots;
+  uint32_t tmem;
+  uint64_t *tfull, *tempty;
+  volatile int *abort_flag;
+  int *status;
+  uint64_t wait_ns;
+};
+template <int NL>
+__device__ __forceinline__ void crt_recon_epilogue(const RecEpi &p) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quad = warp & 3, set = (warp - 2) >> 2;
+  const int mrow = quad * 32 + lane;  // M index = TMEM lane
+  uint32_t Mn[NL];                    // -M mod 2^(32 NL)
+  {
+    uint64_t carry = 1;
+#pragma unroll
+    for (int w = 0; w < NL; ++w) {
+      const uint64_t v = (uint64_t)(~p.cc->Mw[w]) + carry;
+      Mn[w] = (uint32_t)v;
+      carry = v >> 32;
+    }
+  }
+  int slot = set;  // nslots is a multiple of CR_SETS
+  uint32_t tph = 0;
+  for (UnitCursor c(blockIdx.x + (int64_t)set * gridDim.x, (int64_t)CR_SETS * gridDim.x, p.nrb); c.u < p.units;
+       c.advance()) {
+    const int64_t i = c.rb * 32 + (mrow >> 2), j = 4 * (p.qbase + c.qd) + (mrow & 3);
+    const bool live = i < p.M && j < p.N;
+    int shift = 0, bad = 0;
+    if (live) {  // loaded before the wait, in flight meanwhile
+      shift = p.sigA[i] + p.sigB[j] - 2 * p.W;
+      bad = p.flagA[i] | p.flagB[j];
+    }
+    const bool got = wait_bar(&p.tfull[slot], tph, p.abort_flag, p.wait_ns);
+    if (!__all_sync(0xffffffffu, got)) {
+      if (lane == 0) {
+        *p.abort_flag = 1;
+        record_abort(p.status, 2);
+      }
+      break;
+    }
+    mftc::tc_fence_after();
+    uint32_t S[48];
+#pragma unroll
+    for (int b = 32; b < 48; ++b) S[b] = 0;
+    const uint32_t taddr = p.tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(slot * p.slot_cols);
+    mftc::tmem_ld_32x32b_x32(taddr, *reinterpret_cast<uint32_t(*)[32]>(S));
+    if (NL == 8) mftc::tmem_ld_32x32b_x16(taddr + 32u, *reinterpret_cast<uint32_t(*)[16]>(S + 32));
+    mftc::tmem_wait_ld();
+    mftc::tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mftc::mbar_arrive(&p.tempty[slot]);  // the slot is in registers: hand it back
+    slot += CR_SETS;
+    if (slot >= p.nslots) {
+      slot -= p.nslots;
+      tph ^= 1;
+    }
+    if (live) {
+      uint32_t limb[NL];
+      crt_limbs_nl<NL>(S, Mn, p.nbe, limb);
+      crt_emit_nl<NL>(limb, bad != 0, shift, p.C + 2 * (j * p.M + i) * p.cstride, p.mode);
+    }
+  }
+}
+
+__device__ __forceinline__ void crt_recon_body(const CUtensorMap *tmD, const Plan *plan, const CrtConst *cc,
+                                               const int *sigA, const int *flagA, const int *sigB,
+                                               const int *flagB, int64_t M, int64_t N, int64_t qbase,
+                                               int64_t nrb, int64_t units, int64_t k, double *__restrict__ C,
+                                               int64_t cstride, int mode, uint8_t *smem, int *status,
+                                               uint64_t wait_ns) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = plan->S, W = plan->W;
+  const int ktn = (n + 31) / 32;
+  const int nbe = crt_tc_bytes(W, k), nb = crt_tc_cols(nbe);
+  const int slot_cols = cr_slot_cols(nb), nslots = CR_TMEM_COLS / slot_cols;
+  const int box_bytes = CR_BOX_BYTES * ktn;
+  uint8_t *ring = smem;
+  const int nst = CR_RING_BYTES / box_bytes;  // stages of the ring
+  uint8_t *sB = smem + CR_RING_BYTES;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sB + CTC_B_BYTES);
+  uint64_t *empty = full + CR_STAGES_MAX;
+  uint64_t *tfull = empty + CR_STAGES_MAX;  // 16 slots at most
+  uint64_t *tempty = tfull + 16;
+  uint64_t *drain = tempty + 16;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tslot + 1);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < nst; ++s) {
+      mftc::mbar_init(&full[s], 1);
+      mftc::mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 16; ++a) {
+      mftc::mbar_init(&tfull[a], 1);
+      mftc::mbar_init(&tempty[a], 4);  // the four warps of a set
+    }
+    mftc::mbar_init(drain, 1);
+    *abort_flag = 0;
+    mftc::fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) mftc::prefetch_tmap(tmD);
+  if (warp == 1) {
+    mftc::tmem_alloc(tslot, CR_TMEM_COLS);
+    mftc::tmem_relinquish();
+  }
+  // the E tile (the B operand, K-major): row b holds E[t][b] at byte t
+  {
+    const int T = (int)threadIdx.x - 64;
+    if (T >= 0 && T < CRT_EB_ROWS)
+      for (int kt = 0; kt < ktn; ++kt)
+        for (int h = 0; h < 2; ++h)
+          sw128_store16(sB, T, 2 * kt + h, *reinterpret_cast<const uint4 *>(&cc->eb[T][32 * kt + 16 * h]));
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mftc::tc_fence_before();
+  __syncthreads();
+  mftc::tc_fence_after();
+  const uint32_t tmem = *tslot;
+  auto fail = [&](int code) {
+    *abort_flag = 1;
+    record_abort(status, code);
+  };
+  ArmedStages<CR_STAGES_MAX> arm;
+  arm.clear();
+
+  if (warp == 0) {
+    if (lane == 0) {  // ---- TMA producer ----
+      int stage = 0;
+      uint32_t ph = 0;
+      for (UnitCursor c(blockIdx.x, gridDim.x, nrb); c.u < units; c.advance()) {
+        if (!wait_bar(&empty[stage], ph ^ 1, abort_flag, wait_ns)) {
+          fail(2);
+          break;
+        }
+        mftc::mbar_arrive_expect_tx(&full[stage], (uint32_t)box_bytes);
+        for (int kt = 0; kt < ktn; ++kt)  // boxes of 32 moduli
+          mftc::tma_load_3d(ring + stage * box_bytes + kt * CR_BOX_BYTES, tmD, &full[stage], (int32_t)(c.rb * 128),
+                            (int32_t)(qbase + c.qd), 32 * kt);
+        arm.arm(stage, ph);
+        if (++stage == nst) {
+          stage = 0;
+          ph ^= 1;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // ---- MMA issuer ----
+      const uint32_t idesc = mftc::idesc_u8(128, nb) | (1u << 15);  // A (residues) MN-major
+      const uint64_t bdesc = mftc::smem_desc_k_sw128(mftc::smem_u32(sB));
+      int stage = 0, slot = 0;
+      uint32_t ph = 0, tph = 0;
+      for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+        if (!wait_bar(&full[stage], ph, abort_flag, wait_ns) ||
+            !wait_bar(&tempty[slot], tph ^ 1, abort_flag, wait_ns)) {
+          fail(2);
+          break;
+        }
+        mftc::tc_fence_after();
+        const uint64_t adesc = mftc::smem_desc_k_sw128(mftc::smem_u32(ring + stage * box_bytes));
+        for (int kt = 0; kt < ktn; ++kt)  // start-address steps: 4096 and 32 bytes per 32 moduli
+          mftc::umma_i8(tmem + (uint32_t)(slot * slot_cols), adesc + (uint64_t)(kt * (CR_BOX_BYTES / 16)),
+                        bdesc + (uint64_t)(kt * 2), idesc, kt > 0 ? 1u : 0u);
+        mftc::umma_commit(&empty[stage]);
+        mftc::umma_commit(&tfull[slot]);
+        if (++stage == nst) {
+          stage = 0;
+          ph ^= 1;
+        }
+        if (++slot == nslots) {
+          slot = 0;
+          tph ^= 1;
+        }
+      }
+      // every MMA issued by this thread has finished once `drain` flips
+      mftc::umma_commit(drain);
+      (void)wait_bar_ns(drain, 0, WAIT_NS);
+    }
+  } else {  // ---- epilogue ----
+    const int nl = nbe / 4;
+    const RecEpi ep{cc, sigA, flagA, sigB, flagB, M, N, qbase, nrb, units, C, cstride, mode, W, nbe, nb, slot_cols,
+                    nslots, tmem, tfull, tempty, abort_flag, status, wait_ns};
+    if (nl <= 5)
+      crt_recon_epilogue<5>(ep);
+    else if (nl == 6)
+      crt_recon_epilogue<6>(ep);
+    else if (nl == 7)
+      crt_recon_epilogue<7>(ep);
+    else
+      crt_recon_epilogue<8>(ep);
+  }
+
+  mftc::tc_fence_before();
+  __syncthreads();
+  mftc::tc_fence_after();
+  if (*abort_flag) {  // read after the barrier: the same value in every thread
+    // copies in flight that no MMA consumed land before shared memory is released
+    if (warp == 0 && lane == 0) arm.drain(full, nst);
+    __syncthreads();
+  }
+  if (warp == 1) mftc::tmem_dealloc(tmem, CR_TMEM_COLS);
+}
+
+// Folds the K chunks of the residue products into chunk 0: per modulus t <
+// N and word, the chunks' residues summed and reduced modulo m_t.
+__device__ __forceinline__ void crt_fold_body(uint32_t *D, const Plan *plan, int nkc, int64_t plane_words,
+                                              int t, int64_t w) {
+  if (t >= plan->S || w >= plane_words) return;
+  uint32_t *src = D + (int64_t)t * nkc * plane_words + w;
+  *src = crt_chunk_residue_word(src, nkc, plane_words, t);
 }
 
 }  // namespace split

@@ -361,13 +361,30 @@ __host__ __device__ constexpr int pair_stages(int nsub) { return nsub == 1 ? 6 :
 
 // Sequence of (diagonal, K chunk, tile) items of one pair (see above).
 // Tiles are those of column tiles tn0 .. of the output (a column panel).
+// In the CRT form every item is one product of equal length, so no pairing
+// is needed: round r gives pair p item r P + p of a modulus-major list, and
+// at any moment the pairs read the residue planes of at most two moduli
+// (2 x 2 x 16.8 MB at 4096^3), which stay in L2 for all their tiles.
 struct PairSched {
   int p, np, G, nkc, ntm, ntiles, tn0, nsuper;
+  bool crt;
   int r = 0, half = 0;
-  __device__ PairSched(int p_, int np_, int G_, int nkc_, int ntm_, int ntiles_, int tn0_)
+  __device__ PairSched(int p_, int np_, int G_, int nkc_, int ntm_, int ntiles_, int tn0_, bool crt_)
       : p(p_), np(np_), G(G_), nkc(nkc_), ntm(ntm_), ntiles(ntiles_), tn0(tn0_),
-        nsuper(((G_ + 2) / 2) * nkc_ * ntiles_) {}
+        nsuper(crt_ ? (G_ + 1) * nkc_ * ntiles_ : ((G_ + 2) / 2) * nkc_ * ntiles_), crt(crt_) {}
   __device__ bool next(Item &it) {
+    if (crt) {
+      const int u = r * np + p;
+      if (u >= nsuper) return false;
+      ++r;
+      const int per_g = nkc * ntiles;
+      const int rem = u % per_g, tile = rem % ntiles;
+      it.g = u / per_g;
+      it.kc = rem / ntiles;
+      it.tm = tile % ntm;
+      it.tn = tn0 + tile / ntm;
+      return true;
+    }
     while (true) {
       const int u = r * np + p;
       if (u >= nsuper) return false;
@@ -468,7 +485,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
-      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
+      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0, crt);
       Item it;
       while (ok && sched.next(it)) {
         int kb0 = it.kc * KC_BLOCKS, kb1 = min(kblocks, kb0 + KC_BLOCKS);
@@ -507,7 +524,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
       int acc = 0;
       uint32_t acc_phase = 0;
       bool ok = true;
-      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
+      PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0, crt);
       Item it;
       // nsub = 2: one 512-column accumulator whose two 256-column halves are
       // handed back separately (tempty[0], tempty[1]).  The epilogue drains
@@ -655,7 +672,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     const int sel = (warp - 2) / 4;  // which 4 of a half's 8 32-column chunks
     int acc = 0;
     uint32_t acc_phase = 0;
-    PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0);
+    PairSched sched(pair_id, npairs, G, nkc, ntm, ntiles, tn0, crt);
     Item it;
     while (sched.next(it)) {
       bool got = wait_bar(&tfull[acc], acc_phase, abort_flag, wait_ns);
@@ -790,6 +807,27 @@ __global__ void __launch_bounds__(CTC_THREADS, 4) crt_combine_tc_kernel(
                       wait_ns);
 }
 
+// Reconstruction fed by TMA (crt_recon_body): persistent, one CTA per SM;
+// units of 32 rows x one column quad, rows below M, quads qbase .. (columns
+// below N).  Dynamic shared memory cr_smem(ceil(moduli / 32)).
+__global__ void __launch_bounds__(CR_THREADS, 1) crt_recon_kernel(
+    const __grid_constant__ CUtensorMap tmD, const Plan *plan, const CrtConst *cc, const int *sigA,
+    const int *flagA, const int *sigB, const int *flagB, int64_t M, int64_t N, int64_t qbase, int64_t nrb,
+    int64_t units, int64_t k, double *__restrict__ C, int64_t cstride, int mode, int *status, uint64_t wait_ns) {
+  extern __shared__ uint8_t cr_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(cr_raw) + 1023) & ~uintptr_t(1023));
+  crt_recon_body(&tmD, plan, cc, sigA, flagA, sigB, flagB, M, N, qbase, nrb, units, k, C, cstride, mode, smem,
+                 status, wait_ns);
+}
+// K chunks of the residue products folded into chunk 0 (block row y =
+// modulus), words w0 .. w1 - 1 of each plane (the column quads of a panel:
+// folding is not idempotent, so each word is folded once).
+__global__ void __launch_bounds__(256) crt_fold_kernel(uint32_t *D, const Plan *plan, int nkc,
+                                                       int64_t plane_words, int64_t w0, int64_t w1) {
+  const int64_t w = w0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < w1) crt_fold_body(D, plan, nkc, plane_words, (int)blockIdx.y, w);
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -878,6 +916,23 @@ static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, 
   cuuint32_t box[3] = {(cuuint32_t)BK, box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// The residue scratch of the CRT form as the reconstruction's TMA source:
+// bytes of (quad, rows) lines (4 M_pad per quad), quads, moduli (chunk 0 of
+// each, nkc chunks apart); boxes of 128 bytes x 1 quad x 32 moduli with the
+// 128-byte swizzle (planes beyond nsl read as zero).
+static bool make_residue_map(CUtensorMap *map, void *D8, int64_t M_pad, int64_t N_pad, int64_t nkc, int nsl) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)(4 * M_pad), (cuuint64_t)(N_pad / 4), (cuuint64_t)nsl};
+  cuuint64_t strides[2] = {(cuuint64_t)(4 * M_pad), (cuuint64_t)(nkc * N_pad * M_pad)};
+  cuuint32_t box[3] = {128, 1, 32};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, D8, dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
@@ -1033,6 +1088,8 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                            CRT_NMAX * SA_ROWS * SA_STRIDE);
       cudaFuncSetAttribute(crt_combine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            crt_tc_smem((CRT_NMAX + 31) / 32));
+      cudaFuncSetAttribute(crt_recon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           cr_smem((CRT_NMAX + 31) / 32));
     });
     prof_call_begin();
     mark(0, s);
@@ -1099,8 +1156,9 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     int items_max = L.nsl * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
     int grid = sm_count();
     if (L.pair) {
-      // super-items (pairs of diagonals, or pairs of moduli) of the largest plan
-      const int supers_max = ((L.nsl + 1) / 2) * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
+      // super-items (pairs of diagonals) or, in the CRT form, single products of the largest plan
+      const int supers_max = crt ? items_max
+                                 : ((L.nsl + 1) / 2) * (int)L.nkc * (int)((L.M_pad / tile_m) * (L.N_pad / (BN * L.nsub)));
       grid = pair_grid();
       if (grid > 2 * supers_max) grid = 2 * supers_max;
     } else if (grid > items_max) {
@@ -1108,7 +1166,8 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     }
     const unsigned cgx = (unsigned)(((m + 3) / 4 + COMBINE_THREADS - 1) / COMBINE_THREADS);
     mark(2, s);
-    CUtensorMap tmA[4], tmB[4];
+    CUtensorMap tmA[4], tmB[4], tmD;
+    if (crt && !make_residue_map(&tmD, D, L.M_pad, L.N_pad, L.nkc, L.nsl)) rc = MFCUDA_ERR_CUDA;
     for (int q = 0; q < nprod; ++q)
       if (!make_map(&tmA[q], sl[prods[q].a], L.M_pad, L.K_pad, BM, L.nsl) ||
           !make_map(&tmB[q], sl[nA + prods[q].b], L.N_pad, L.K_pad, L.pair ? 128 : BN, L.nsl))
@@ -1124,7 +1183,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
               (int64_t)tn0 * tn_cols);
       int pgrid = grid;
       if (L.pair && npan > 1) {
-        const int supers = ((L.nsl + 1) / 2) * (int)L.nkc * (int)(L.M_pad / tile_m) * (tn1 - tn0);
+        const int supers = (crt ? L.nsl : (L.nsl + 1) / 2) * (int)L.nkc * (int)(L.M_pad / tile_m) * (tn1 - tn0);
         pgrid = std::min(pair_grid(), 2 * supers);
       }
       for (int q = 0; q < nprod && rc == MFCUDA_OK; ++q) {
@@ -1138,14 +1197,17 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
                                                                 (int)L.N_pad, (int)L.nkc, (int)L.kblocks,
                                                                 status, wait_ns);
         if (q == nprod - 1 && pp == npan - 1) mark(3, s);
-        if (crt)
-          crt_combine_tc_kernel<<<dim3((unsigned)((m + CTC_THREADS - 1) / CTC_THREADS),
-                                       (unsigned)(((j1 - j0 + 3) / 4 + CTC_QUADS - 1) / CTC_QUADS)),
-                                  CTC_THREADS, crt_tc_smem((L.nsl + 31) / 32), s>>>(
-              reinterpret_cast<const uint8_t *>(D), plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, j1,
-              L.M_pad, L.N_pad, (int)L.nkc, k, prods[q].out, prods[q].ostride, prods[q].mode, j0 / 4, status,
-              wait_ns);
-        else
+        if (crt) {
+          const int64_t q0 = j0 / 4, q1 = (j1 + 3) / 4, nrb = (m + 31) / 32, units = nrb * (q1 - q0);
+          if (L.nkc > 1) {
+            const int64_t plane_words = L.N_pad * L.M_pad / 4, nw = (q1 - q0) * L.M_pad;
+            crt_fold_kernel<<<dim3((unsigned)((nw + 255) / 256), (unsigned)L.nsl), 256, 0, s>>>(
+                reinterpret_cast<uint32_t *>(D), plan, (int)L.nkc, plane_words, q0 * L.M_pad, q1 * L.M_pad);
+          }
+          crt_recon_kernel<<<(unsigned)std::min<int64_t>(units, sm_count()), CR_THREADS, cr_smem((L.nsl + 31) / 32),
+                             s>>>(tmD, plan, cc, sig[ia], flag[ia], sig[ib], flag[ib], m, j1, q0, nrb, units, k,
+                                  prods[q].out, prods[q].ostride, prods[q].mode, status, wait_ns);
+        } else
           combine_kernel<<<dim3(cgx, (unsigned)n), COMBINE_THREADS, 0, s>>>(
               D, plan, sig[ia], flag[ia], sig[ib], flag[ib], m, n, L.M_pad, L.N_pad, (int)L.nkc, prods[q].out,
               prods[q].ostride, prods[q].mode);
