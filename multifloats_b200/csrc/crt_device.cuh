@@ -301,6 +301,43 @@ __device__ __forceinline__ void crt_slice_a_body(const double *__restrict__ A, i
   }
 }
 
+// A (m x k column-major view) -> As[t][p][i]: the MN-major residue planes
+// of the main path's tensor-core kernels (the rows of one K index
+// contiguous, so a thread's eight residues of consecutive rows are one
+// 64-bit store and a warp's stores are contiguous; no transposition).
+// Entries i8 .. i8+7 of column p.
+__device__ __forceinline__ void crt_slice_a_mn_one(const double *__restrict__ A, int64_t M, int64_t K,
+                                                   int64_t stride, int64_t M_pad, int64_t K_pad, const int *sig,
+                                                   const int *flag, const Plan *plan, int8_t *__restrict__ As,
+                                                   int64_t i8, int64_t p) {
+  const int n = plan->S, W = plan->W;
+  uint32_t y[8][4];
+  bool any = false;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int64_t i = i8 + e;
+    if (p < K && i < M && !flag[i]) {
+      const double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i) * stride);
+      biased_bytes(v.x, v.y, sig[i], W, y[e]);
+      any = true;
+    } else {
+#pragma unroll
+      for (int w = 0; w < 4; ++w) y[e][w] = bias_word(w);  // X = 0: every residue zero
+    }
+  }
+  auto put = [&](int sl, uint64_t word) {
+    *reinterpret_cast<uint64_t *>(As + (((int64_t)sl * K_pad + p) * M_pad + i8)) = word;
+  };
+  if (any) {
+    uint32_t dw[8][4];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) digit_words(y[e], dw[e]);
+    for_each_residue_word(dw, 0, n, W, put);
+  } else {  // padding or flagged rows only: every residue zero
+    for (int sl = 0; sl < n; ++sl) put(sl, 0);
+  }
+}
+
 // B (k x n column-major view) -> Bs[t][j][p]: entries p8 .. p8+7 of column j.
 __device__ __forceinline__ void crt_slice_b_one(const double *__restrict__ B, int64_t K, int64_t N,
                                                 int64_t stride, int64_t N_pad, int64_t K_pad, const int *sig,
@@ -1147,7 +1184,7 @@ __device__ __forceinline__ void crt_recon_body(const CUtensorMap *tmD, const Pla
     }
   } else if (warp == 1) {
     if (lane == 0) {  // ---- MMA issuer ----
-      const uint32_t idesc = mftc::idesc_u8(128, nb) | (1u << 15);  // A (residues) MN-major
+      const uint32_t idesc = mftc::idesc_u8(128, nb) | mftc::IDESC_A_MN;  // A (residues) MN-major
       const uint64_t bdesc = mftc::smem_desc_k_sw128(mftc::smem_u32(sB));
       int stage = 0, slot = 0;
       uint32_t ph = 0, tph = 0;

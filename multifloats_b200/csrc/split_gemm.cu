@@ -186,7 +186,10 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
               break;
             }
             mftc::mbar_arrive_expect_tx(&full[stage], STAGE);
-            mftc::tma_load_3d(sA + stage * A_STAGE, &tmA, &full[stage], kb * BK, it.tm * BM, s);
+            if (crt)  // MN-major residue planes: (row, K index, modulus)
+              mftc::tma_load_3d(sA + stage * A_STAGE, &tmA, &full[stage], it.tm * BM, kb * BK, s);
+            else
+              mftc::tma_load_3d(sA + stage * A_STAGE, &tmA, &full[stage], kb * BK, it.tm * BM, s);
             mftc::tma_load_3d(sB + stage * B_STAGE, &tmB, &full[stage], kb * BK, it.tn * BN, t);
             arm.arm(stage, phase);
             if (++stage == NSTAGE) {
@@ -200,7 +203,9 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       // ---- MMA issuer ----
-      const uint32_t idesc = crt ? mftc::idesc_u8(BM, BN) : mftc::idesc_i8(BM, BN);  // CRT residues are unsigned
+      // CRT residues are unsigned, and A's planes MN-major (a K step of 32 rows is 4096 bytes)
+      const uint32_t idesc = crt ? mftc::idesc_u8(BM, BN) | mftc::IDESC_A_MN : mftc::idesc_i8(BM, BN);
+      const uint32_t a_kstep = crt ? 32 * 128 : UMMA_K;
       int stage = 0;
       uint32_t phase = 0;
       int acc = 0;
@@ -228,7 +233,7 @@ __global__ void __launch_bounds__(MMA_THREADS, 1)
             const uint32_t b0 = mftc::smem_u32(sB + stage * B_STAGE);
 #pragma unroll
             for (int kk = 0; kk < BK / UMMA_K; ++kk) {
-              mftc::umma_i8(d_tmem, mftc::smem_desc_k_sw128(a0 + kk * UMMA_K),
+              mftc::umma_i8(d_tmem, mftc::smem_desc_k_sw128(a0 + kk * a_kstep),
                             mftc::smem_desc_k_sw128(b0 + kk * UMMA_K), idesc, accumulate);
               accumulate = 1;
             }
@@ -504,7 +509,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
               arm.arm(stage, phase);
             }
             const uint32_t fb = mftc::cluster_addr(&full[stage], 0);
-            mftc::tma_load_3d_pair(sA + stage * P_STAGE_A, &tmA, fb, kb * BK, arow, s);
+            if (crt)  // MN-major residue planes: (row, K index, modulus)
+              mftc::tma_load_3d_pair(sA + stage * P_STAGE_A, &tmA, fb, arow, kb * BK, s);
+            else
+              mftc::tma_load_3d_pair(sA + stage * P_STAGE_A, &tmA, fb, kb * BK, arow, s);
             for (int h = 0; h < nsub; ++h)
               mftc::tma_load_3d_pair(sB + stage * stage_b + h * P_HALF_B, &tmB, fb, kb * BK, brow + h * BN, t);
             if (++stage == nst) {
@@ -518,7 +526,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
   } else if (warp == 1) {
     if (lane == 0 && leader) {
       // ---- MMA issuer (even CTA) ----
-      const uint32_t idesc = crt ? mftc::idesc_u8(BM_PAIR, BN) : mftc::idesc_i8(BM_PAIR, BN);  // CRT residues are unsigned
+      // CRT residues are unsigned, and A's planes MN-major (a K step of 32 rows is 4096 bytes)
+      const uint32_t idesc = crt ? mftc::idesc_u8(BM_PAIR, BN) | mftc::IDESC_A_MN : mftc::idesc_i8(BM_PAIR, BN);
+      const uint64_t a_kstep = crt ? 32 * 128 / 16 : UMMA_K / 16;  // descriptor units of 16 bytes
       int stage = 0;
       uint32_t phase = 0;
       int acc = 0;
@@ -541,7 +551,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
         const uint64_t bd = mftc::smem_desc_k_sw128(mftc::smem_u32(sB + st * stage_b));
 #pragma unroll
         for (int kk = 0; kk < BK / UMMA_K; ++kk) {
-          mftc::umma_i8_pair(tmem_base + (uint32_t)BN, ad + (uint64_t)(kk * UMMA_K / 16),
+          mftc::umma_i8_pair(tmem_base + (uint32_t)BN, ad + (uint64_t)kk * a_kstep,
                              bd + (uint64_t)((P_HALF_B + kk * UMMA_K) / 16), idesc, acc1);
           acc1 = 1;
         }
@@ -583,7 +593,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
             const uint64_t bd0 = mftc::smem_desc_k_sw128(mftc::smem_u32(sB + stage * stage_b));
 #pragma unroll
             for (int kk = 0; kk < BK / UMMA_K; ++kk) {
-              mftc::umma_i8_pair(tmem_base, ad0 + (uint64_t)(kk * UMMA_K / 16), bd0 + (uint64_t)(kk * UMMA_K / 16),
+              mftc::umma_i8_pair(tmem_base, ad0 + (uint64_t)kk * a_kstep, bd0 + (uint64_t)(kk * UMMA_K / 16),
                                  idesc, acc0);
               acc0 = 1;
             }
@@ -637,7 +647,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
             const uint64_t bd0 = mftc::smem_desc_k_sw128(mftc::smem_u32(sB + stage * stage_b));
 #pragma unroll
             for (int kk = 0; kk < BK / UMMA_K; ++kk) {
-              const uint64_t adesc = ad0 + (uint64_t)(kk * UMMA_K / 16);
+              const uint64_t adesc = ad0 + (uint64_t)kk * a_kstep;
               mftc::umma_i8_pair(d_tmem, adesc, bd0 + (uint64_t)(kk * UMMA_K / 16), idesc, accumulate);
               accumulate = 1;
             }
@@ -778,12 +788,14 @@ __global__ void crt_plan_kernel(StatSet st, int bits, double target, int64_t k, 
                                 const int *bits_dev) {
   crt_plan_body(st, bits_dev ? *bits_dev : bits, target, k, plan, cc);
 }
+// Block (x, y): column x (a K index) of A, rows 2048 y ..; MN-major planes.
 __global__ void __launch_bounds__(256) crt_slice_a_kernel(const double *__restrict__ A, int64_t M, int64_t K,
                                                           int64_t stride, int64_t M_pad, int64_t K_pad,
                                                           const int *sig, const int *flag, const Plan *plan,
                                                           int8_t *__restrict__ As) {
-  extern __shared__ __align__(16) uint8_t crt_tile[];
-  crt_slice_a_body(A, M, K, stride, M_pad, K_pad, sig, flag, plan, As, crt_tile, blockIdx.x, blockIdx.y);
+  const int64_t i8 = ((int64_t)blockIdx.y * blockDim.x + threadIdx.x) * 8;
+  if (i8 >= M_pad) return;
+  crt_slice_a_mn_one(A, M, K, stride, M_pad, K_pad, sig, flag, plan, As, i8, blockIdx.x);
 }
 __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restrict__ B, int64_t K, int64_t N,
                                                           int64_t stride, int64_t N_pad, int64_t K_pad,
@@ -914,6 +926,21 @@ static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, 
   cuuint64_t dims[3] = {(cuuint64_t)K_pad, (cuuint64_t)rows, (cuuint64_t)nsl};
   cuuint64_t strides[2] = {(cuuint64_t)K_pad, (cuuint64_t)(rows * K_pad)};
   cuuint32_t box[3] = {(cuuint32_t)BK, box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// MN-major residue planes (row, K index, modulus) of the CRT form's A side:
+// boxes of 128 rows x BK K indices, 128-byte swizzle.
+static bool make_map_mn(CUtensorMap *map, void *base, int64_t M_pad, int64_t K_pad, int nsl) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)M_pad, (cuuint64_t)K_pad, (cuuint64_t)nsl};
+  cuuint64_t strides[2] = {(cuuint64_t)M_pad, (cuuint64_t)(M_pad * K_pad)};
+  cuuint32_t box[3] = {128, (cuuint32_t)BK, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -1084,8 +1111,6 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     std::call_once(g_attr_once, [] {
       cudaFuncSetAttribute(split_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
       cudaFuncSetAttribute(split_mma_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM);
-      cudaFuncSetAttribute(crt_slice_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           CRT_NMAX * SA_ROWS * SA_STRIDE);
       cudaFuncSetAttribute(crt_combine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            crt_tc_smem((CRT_NMAX + 31) / 32));
       cudaFuncSetAttribute(crt_recon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1131,6 +1156,7 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     mark(1, s);
     const dim3 ga((unsigned)(L.M_pad / 32), (unsigned)(L.K_pad / 64));
     const dim3 gb((unsigned)((L.K_pad / 8 + 255) / 256), (unsigned)L.N_pad);
+    const dim3 gca((unsigned)L.K_pad, (unsigned)((L.M_pad / 8 + 255) / 256));
     // column panels (CRT form on CTA pairs, when a sink wants the output panel
     // by panel): B's residues, every product and the reconstruction of panel p,
     // then the sink, then panel p + 1
@@ -1140,8 +1166,8 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     for (int o = 0; o < nops; ++o) {
       if (o >= nA && npan > 1) continue;  // sliced panel by panel below
       if (o < nA && crt)
-        crt_slice_a_kernel<<<ga, 256, std::min(L.nsl, CRT_SA_MODULI) * SA_ROWS * SA_STRIDE, s>>>(aview[o], m, k, astride[o], L.M_pad,
-                                                                       L.K_pad, sig[o], flag[o], plan, sl[o]);
+        crt_slice_a_kernel<<<gca, 256, 0, s>>>(aview[o], m, k, astride[o], L.M_pad, L.K_pad, sig[o], flag[o], plan,
+                                               sl[o]);
       else if (o < nA)
         slice_a_kernel<<<ga, 256, 0, s>>>(aview[o], m, k, astride[o], L.M_pad, L.K_pad, sig[o], flag[o], plan,
                                           sl[o]);
@@ -1169,7 +1195,8 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     CUtensorMap tmA[4], tmB[4], tmD;
     if (crt && !make_residue_map(&tmD, D, L.M_pad, L.N_pad, L.nkc, L.nsl)) rc = MFCUDA_ERR_CUDA;
     for (int q = 0; q < nprod; ++q)
-      if (!make_map(&tmA[q], sl[prods[q].a], L.M_pad, L.K_pad, BM, L.nsl) ||
+      if (!(crt ? make_map_mn(&tmA[q], sl[prods[q].a], L.M_pad, L.K_pad, L.nsl)
+                : make_map(&tmA[q], sl[prods[q].a], L.M_pad, L.K_pad, BM, L.nsl)) ||
           !make_map(&tmB[q], sl[nA + prods[q].b], L.N_pad, L.K_pad, L.pair ? 128 : BN, L.nsl))
         rc = MFCUDA_ERR_CUDA;
     for (int pp = 0; pp < npan && rc == MFCUDA_OK; ++pp) {

@@ -118,6 +118,12 @@ __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
 __host__ __device__ constexpr uint32_t idesc_u8(int M, int N) {
   return (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
+// Bit 15 of the instruction descriptor: A MN-major (its shared-memory tile
+// holds rows of M contiguous per K index; with the 128-byte swizzle, 8 K rows
+// of 128 bytes per 1024-byte atom, atoms consecutive along K: the descriptor
+// fields are those of smem_desc_k_sw128, the stride byte offset now stepping
+// between 8-row K groups).  Valid for the 8-bit integer kinds.
+constexpr uint32_t IDESC_A_MN = 1u << 15;
 
 // D[tmem] (+)= A[smem] * B[smem]^T, issued by a single thread.
 __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
