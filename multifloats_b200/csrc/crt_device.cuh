@@ -990,11 +990,13 @@ __device__ __forceinline__ void crt_emit_nl(const uint32_t (&limb)[NL], bool nan
 // M index, so a thread's output is row i0 + 8 (lane quadrant) + lane / 4,
 // column 4 qd + lane % 4.
 //
-// Persistent CTA per SM: warp 0 loads (a ring of CR_RING_BYTES of boxes), warp 1
-// issues one MMA per 32 moduli per unit into one of the TMEM slots (nb
-// columns each), and CR_EPI_WARPS / 4 sets of four epilogue warps (one per
-// lane quadrant) take the units in turn: each copies its slot to registers,
-// hands it back, and forms and stores the 128 outputs.  Planes of moduli
+// Persistent CTA per SM: warp 0 loads (a ring of CR_RING_BYTES of boxes, one
+// stage per group of CR_SETS consecutive units of the CTA), warp 1 issues one
+// MMA per 32 moduli per unit into the TMEM slots (nb columns each) of one
+// slot group, with one commit per group, and CR_EPI_WARPS / 4 sets of four
+// epilogue warps (one per lane quadrant) take the units in turn -- set e
+// unit e of every group: each copies its slot to registers, hands the group
+// back (every epilogue warp arrives), and forms and stores the 128 outputs.  Planes of moduli
 // t >= N (up to the allocated count, and zero-filled beyond it) meet zero
 // rows of E.  K chunks (nkc > 1) are folded into chunk 0 beforehand
 // (crt_fold_kernel).  All waits are bounded.
@@ -1069,7 +1071,7 @@ __device__ __forceinline__ void crt_recon_epilogue(const RecEpi &p) {
       shift = p.sigA[i] + p.sigB[j] - 2 * p.W;
       bad = p.flagA[i] | p.flagB[j];
     }
-    const bool got = wait_bar(&p.tfull[slot], tph, p.abort_flag, p.wait_ns);
+    const bool got = wait_bar(&p.tfull[slot / CR_SETS], tph, p.abort_flag, p.wait_ns);
     if (!__all_sync(0xffffffffu, got)) {
       if (lane == 0) {
         *p.abort_flag = 1;
@@ -1087,7 +1089,7 @@ __device__ __forceinline__ void crt_recon_epilogue(const RecEpi &p) {
     mftc::tmem_wait_ld();
     mftc::tc_fence_before();
     __syncwarp();
-    if (lane == 0) mftc::mbar_arrive(&p.tempty[slot]);  // the slot is in registers: hand it back
+    if (lane == 0) mftc::mbar_arrive(&p.tempty[slot / CR_SETS]);  // the slot is in registers: hand it back
     slot += CR_SETS;
     if (slot >= p.nslots) {
       slot -= p.nslots;
@@ -1113,12 +1115,17 @@ __device__ __forceinline__ void crt_recon_body(const CUtensorMap *tmD, const Pla
   const int nbe = crt_tc_bytes(W, k), nb = crt_tc_cols(nbe);
   const int slot_cols = cr_slot_cols(nb), nslots = CR_TMEM_COLS / slot_cols;
   const int box_bytes = CR_BOX_BYTES * ktn;
+  // one stage and one TMEM slot group per CR_SETS consecutive units of the
+  // CTA (one unit per epilogue set): a barrier round trip and a commit serve
+  // CR_SETS units
+  const int stage_bytes = CR_SETS * box_bytes;
+  const int nsg = nslots / CR_SETS;  // slot groups
   uint8_t *ring = smem;
-  const int nst = CR_RING_BYTES / box_bytes;  // stages of the ring
+  const int nst = CR_RING_BYTES / stage_bytes;  // stages of the ring
   uint8_t *sB = smem + CR_RING_BYTES;
   uint64_t *full = reinterpret_cast<uint64_t *>(sB + CTC_B_BYTES);
   uint64_t *empty = full + CR_STAGES_MAX;
-  uint64_t *tfull = empty + CR_STAGES_MAX;  // 16 slots at most
+  uint64_t *tfull = empty + CR_STAGES_MAX;  // per slot group (4 at most)
   uint64_t *tempty = tfull + 16;
   uint64_t *drain = tempty + 16;
   uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
@@ -1131,7 +1138,7 @@ __device__ __forceinline__ void crt_recon_body(const CUtensorMap *tmD, const Pla
     }
     for (int a = 0; a < 16; ++a) {
       mftc::mbar_init(&tfull[a], 1);
-      mftc::mbar_init(&tempty[a], 4);  // the four warps of a set
+      mftc::mbar_init(&tempty[a], 4 * CR_SETS);  // every epilogue warp
     }
     mftc::mbar_init(drain, 1);
     *abort_flag = 0;
@@ -1163,18 +1170,21 @@ __device__ __forceinline__ void crt_recon_body(const CUtensorMap *tmD, const Pla
   arm.clear();
 
   if (warp == 0) {
-    if (lane == 0) {  // ---- TMA producer ----
+    if (lane == 0) {  // ---- TMA producer: a stage per group of CR_SETS units ----
       int stage = 0;
       uint32_t ph = 0;
-      for (UnitCursor c(blockIdx.x, gridDim.x, nrb); c.u < units; c.advance()) {
+      for (UnitCursor c(blockIdx.x, gridDim.x, nrb); c.u < units;) {
         if (!wait_bar(&empty[stage], ph ^ 1, abort_flag, wait_ns)) {
           fail(2);
           break;
         }
-        mftc::mbar_arrive_expect_tx(&full[stage], (uint32_t)box_bytes);
-        for (int kt = 0; kt < ktn; ++kt)  // boxes of 32 moduli
-          mftc::tma_load_3d(ring + stage * box_bytes + kt * CR_BOX_BYTES, tmD, &full[stage], (int32_t)(c.rb * 128),
-                            (int32_t)(qbase + c.qd), 32 * kt);
+        const int64_t rem = (units - c.u + gridDim.x - 1) / gridDim.x;  // units of this CTA left
+        const int ne = rem < CR_SETS ? (int)rem : CR_SETS;
+        mftc::mbar_arrive_expect_tx(&full[stage], (uint32_t)(ne * box_bytes));
+        for (int e = 0; e < ne; ++e, c.advance())
+          for (int kt = 0; kt < ktn; ++kt)  // boxes of 32 moduli
+            mftc::tma_load_3d(ring + stage * stage_bytes + e * box_bytes + kt * CR_BOX_BYTES, tmD, &full[stage],
+                              (int32_t)(c.rb * 128), (int32_t)(qbase + c.qd), 32 * kt);
         arm.arm(stage, ph);
         if (++stage == nst) {
           stage = 0;
@@ -1183,30 +1193,35 @@ __device__ __forceinline__ void crt_recon_body(const CUtensorMap *tmD, const Pla
       }
     }
   } else if (warp == 1) {
-    if (lane == 0) {  // ---- MMA issuer ----
+    if (lane == 0) {  // ---- MMA issuer: CR_SETS units per stage, one commit each ----
       const uint32_t idesc = mftc::idesc_u8(128, nb) | mftc::IDESC_A_MN;  // A (residues) MN-major
       const uint64_t bdesc = mftc::smem_desc_k_sw128(mftc::smem_u32(sB));
-      int stage = 0, slot = 0;
+      int stage = 0, sg = 0;
       uint32_t ph = 0, tph = 0;
-      for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+      for (int64_t o = blockIdx.x; o < units; o += (int64_t)CR_SETS * gridDim.x) {
+        const int64_t rem = (units - o + gridDim.x - 1) / gridDim.x;
+        const int ne = rem < CR_SETS ? (int)rem : CR_SETS;
         if (!wait_bar(&full[stage], ph, abort_flag, wait_ns) ||
-            !wait_bar(&tempty[slot], tph ^ 1, abort_flag, wait_ns)) {
+            !wait_bar(&tempty[sg], tph ^ 1, abort_flag, wait_ns)) {
           fail(2);
           break;
         }
         mftc::tc_fence_after();
-        const uint64_t adesc = mftc::smem_desc_k_sw128(mftc::smem_u32(ring + stage * box_bytes));
-        for (int kt = 0; kt < ktn; ++kt)  // start-address steps: 4096 and 32 bytes per 32 moduli
-          mftc::umma_i8(tmem + (uint32_t)(slot * slot_cols), adesc + (uint64_t)(kt * (CR_BOX_BYTES / 16)),
-                        bdesc + (uint64_t)(kt * 2), idesc, kt > 0 ? 1u : 0u);
+        for (int e = 0; e < ne; ++e) {
+          const uint64_t adesc = mftc::smem_desc_k_sw128(mftc::smem_u32(ring + stage * stage_bytes + e * box_bytes));
+          const uint32_t dst = tmem + (uint32_t)((sg * CR_SETS + e) * slot_cols);
+          for (int kt = 0; kt < ktn; ++kt)  // start-address steps: 4096 and 32 bytes per 32 moduli
+            mftc::umma_i8(dst, adesc + (uint64_t)(kt * (CR_BOX_BYTES / 16)), bdesc + (uint64_t)(kt * 2), idesc,
+                          kt > 0 ? 1u : 0u);
+        }
         mftc::umma_commit(&empty[stage]);
-        mftc::umma_commit(&tfull[slot]);
+        mftc::umma_commit(&tfull[sg]);
         if (++stage == nst) {
           stage = 0;
           ph ^= 1;
         }
-        if (++slot == nslots) {
-          slot = 0;
+        if (++sg == nsg) {
+          sg = 0;
           tph ^= 1;
         }
       }
