@@ -40,7 +40,7 @@
 // The CRT form (crt_device.cuh) shares steps 1 and 3's rounding and the
 // tensor-core kernels: residues modulo N moduli instead of digits, one product
 // per modulus (u8 x u8), the epilogue reducing each INT32 sum to a residue
-// byte, and a tensor-core reconstruction (crt_combine_tc_kernel).  Large
+// byte, and a tensor-core reconstruction fed by TMA (crt_recon_kernel).  Large
 // outputs run on CTA pairs (split_mma_pair_kernel, 256 x 512 tiles, eight
 // epilogue warps); host-pointer CRT calls compute the output in column panels
 // and copy each back while the next is computed (PanelSink).
@@ -805,20 +805,6 @@ __global__ void __launch_bounds__(256) crt_slice_b_kernel(const double *__restri
   if (p8 >= K_pad) return;
   crt_slice_b_one(B, K, N, stride, N_pad, K_pad, sig, flag, plan, Bs, j0 + blockIdx.y, p8);  // column j0 + y
 }
-// Tensor-core reconstruction (crt_combine_tc_body): block (x, y) takes rows
-// 128 x .. of column quads qbase + CTC_QUADS y .. (columns below N); dynamic shared memory
-// crt_tc_smem(ceil(moduli / 32)).
-__global__ void __launch_bounds__(CTC_THREADS, 4) crt_combine_tc_kernel(
-    const uint8_t *__restrict__ D8, const Plan *plan, const CrtConst *cc, const int *sigA, const int *flagA,
-    const int *sigB, const int *flagB, int64_t M, int64_t N, int64_t M_pad, int64_t N_pad, int nkc, int64_t k,
-    double *__restrict__ C, int64_t cstride, int mode, int64_t qbase, int *status, uint64_t wait_ns) {
-  extern __shared__ uint8_t ctc_raw[];
-  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(ctc_raw) + 1023) & ~uintptr_t(1023));
-  crt_combine_tc_body(D8, plan, cc, sigA, flagA, sigB, flagB, M, N, M_pad, N_pad, nkc, k, C, cstride, mode,
-                      (int64_t)blockIdx.x * CTC_THREADS, qbase + (int64_t)blockIdx.y * CTC_QUADS, smem, status,
-                      wait_ns);
-}
-
 // Reconstruction fed by TMA (crt_recon_body): persistent, one CTA per SM;
 // units of 32 rows x one column quad, rows below M, quads qbase .. (columns
 // below N).  Dynamic shared memory cr_smem(ceil(moduli / 32)).
@@ -1111,8 +1097,6 @@ static int run_products(const double *const *aview, const int64_t *astride, int 
     std::call_once(g_attr_once, [] {
       cudaFuncSetAttribute(split_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
       cudaFuncSetAttribute(split_mma_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM);
-      cudaFuncSetAttribute(crt_combine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           crt_tc_smem((CRT_NMAX + 31) / 32));
       cudaFuncSetAttribute(crt_recon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            cr_smem((CRT_NMAX + 31) / 32));
     });
