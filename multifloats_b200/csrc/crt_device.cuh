@@ -15,7 +15,7 @@
 // times the bytes of e_t and of c_t = e_t / M in fixed point), so the
 // reconstruction runs on the tensor cores too (crt_combine_tc_body), with the
 // carries, q M and the sign in 32-bit integer limbs.
-// C' is then converted to a double-double (crt_to_dd: hi = C' rounded to 53
+// C' is then converted to a double-double (crt_to_dd_nl: hi = C' rounded to 53
 // bits, lo the rest summed in doubles, renormalised) and scaled by
 // 2^(sigma_i + tau_j - 2W).  Compared with the digit-sliced form (S(S+1)/2 slice products for S
 // slices) the tensor work is N products: 26 instead of 105 at 4096^3.
@@ -371,101 +371,6 @@ __device__ __forceinline__ void crt_slice_b_one(const double *__restrict__ B, in
   }
 }
 
-// ---- reconstruction ---------------------------------------------------------------
-// The signed integer held in nl little-endian 32-bit limbs (two's complement,
-// nl <= 8) as a double-double scaled by 2^e:
-//   the magnitude is normalised (whole-limb shifts, then a funnel shift) so
-//   that its leading one is bit 159 of a 160-bit window n4..n0 (bit 0 of
-//   weight 2^E; bits below the window dropped);
-//   hi = the window rounded to 53 bits (nearest, ties to even, the bits below
-//   bit 107 of the window deciding), exact as a double: keep 2^(E + 107);
-//   lo = the rest D 2^96 + n2 2^64 + n1 2^32 + n0 (D = the low 11 bits of the
-//   top 64 minus 2048 when rounded up) summed in doubles in that order,
-//   times 2^E; then fast_two_sum(hi, lo) in units of 2^(E + 107).
-// Returns (h, l) with value (h + l) 2^e, e = E + 107.
-__device__ __forceinline__ void crt_to_dd(const uint32_t *limb, int nl, double &h, double &l, int &e) {
-  const bool neg = (limb[nl - 1] >> 31) != 0;
-  uint32_t m[CRT_NL];
-  uint32_t carry = 1;
-#pragma unroll
-  for (int q = 0; q < CRT_NL; ++q) {
-    uint32_t x = q < nl ? limb[q] : (neg ? 0xFFFFFFFFu : 0u);
-    if (neg) {  // magnitude: two's complement negation
-      x = ~x;
-      const uint32_t sm = x + carry;
-      carry = sm < x ? 1u : 0u;
-      x = sm;
-    }
-    m[q] = x;
-  }
-  // whole-limb normalisation: the leading nonzero limb into m[7]
-  int E = 32 * (CRT_NL - 5);  // weight of window bit 0 before any shift
-#pragma unroll
-  for (int step = 4; step >= 1; step >>= 1) {
-    bool zero = true;
-#pragma unroll
-    for (int q = CRT_NL - step; q < CRT_NL; ++q) zero = zero && m[q] == 0;
-    if (zero) {
-#pragma unroll
-      for (int q = CRT_NL - 1; q >= 0; --q) m[q] = q >= step ? m[q - step] : 0u;
-      E -= 32 * step;
-    }
-  }
-  if (m[CRT_NL - 1] == 0) {  // the value is zero
-    h = l = 0.0;
-    e = 0;
-    return;
-  }
-  const int s = __clz((int)m[CRT_NL - 1]);
-  uint32_t n[5];
-#pragma unroll
-  for (int w = 0; w < 5; ++w) n[w] = __funnelshift_l(m[CRT_NL - 6 + w], m[CRT_NL - 5 + w], s);
-  E -= s;
-  const uint64_t T64 = ((uint64_t)n[4] << 32) | n[3];
-  uint64_t keep = T64 >> 11;
-  const uint32_t r11 = (uint32_t)(T64 & 0x7FF);
-  const bool lowz = (n[2] | n[1] | n[0]) == 0;
-  const bool up = r11 > 0x400 || (r11 == 0x400 && (!lowz || (keep & 1)));
-  keep += up;
-  const int D = (int)r11 - (up ? 2048 : 0);
-  double lo = mfdev::mul((double)D, pow2(96));
-  lo = mfdev::add(lo, mfdev::mul((double)n[2], pow2(64)));
-  lo = mfdev::add(lo, mfdev::mul((double)n[1], pow2(32)));
-  lo = mfdev::add(lo, (double)n[0]);
-  double hi = (double)keep;
-  lo = mfdev::mul(lo, pow2(-107));  // into units of 2^(E + 107): exact
-  mfdev::fast_two_sum(hi, lo, h, l);
-  if (neg) {
-    h = -h;
-    l = -l;
-  }
-  e = E + 107;
-}
-
-// Writes the two's complement integer C' held in CRT_NL limbs, times
-// 2^shift, as a DD to dst (NaN when `nan`); mode 0 stores it, 1 subtracts it
-// from the DD at dst, 2 adds it.
-__device__ __forceinline__ void crt_emit(const uint32_t (&limb)[CRT_NL], bool nan, int shift,
-                                         double *__restrict__ dst, int mode) {
-  double2 out;
-  if (nan) {
-    out = make_double2(CUDART_NAN, 0.0);
-  } else {
-    double hi, lo;
-    int e;
-    crt_to_dd(limb, CRT_NL, hi, lo, e);
-    out = make_double2(scale2(hi, e + shift), scale2(lo, e + shift));
-  }
-  double2 *d2 = reinterpret_cast<double2 *>(dst);
-  if (mode != 0) {
-    const double2 prev = *d2;
-    const mfdev::dd p = mfdev::make(out.x, out.y), pv = mfdev::make(prev.x, prev.y);
-    const mfdev::dd res = mode == 1 ? mfdev::dd_sub(pv, p) : mfdev::dd_add(pv, p);
-    out = make_double2(res.hi, res.lo);
-  }
-  __stcs(d2, out);
-}
-
 // Residue layout of one product (modulus t, K chunk kc): N_pad x M_pad bytes,
 // four consecutive columns interleaved per row -- byte (j, i) at
 // ((j / 4) M_pad + i) 4 + j % 4 -- so a thread holding one row writes one
@@ -476,47 +381,15 @@ __device__ __forceinline__ int64_t crt_word_index(int64_t off, int64_t M_pad) {
   const int64_t rest = off - plane;                        // j % 4 == 0 within the quad: rest = i
   return plane / 4 + rest;
 }
-// The residues of four INT32 sums packed in column order.
-__device__ __forceinline__ uint32_t crt_pack4(uint32_t v0, uint32_t v1, uint32_t v2, uint32_t v3, int t);
-
-// The residue of one product reduced in the tensor-core kernel's epilogue:
-// v = the INT32 sum of one K chunk of unsigned residue products
-// (0 <= v < 73 * 128 * 255^2 < 2^30), stored as v mod m_t in [0, m_t).
-__device__ __forceinline__ uint8_t crt_residue_of_sum(int32_t v, int t) {
-  return (uint8_t)crt_mod_small((uint32_t)v, t);
-}
+// The residues of four INT32 sums of one K chunk of unsigned residue products
+// (0 <= v < 73 * 128 * 255^2 < 2^30), each v mod m_t in [0, m_t), packed in
+// column order (the tensor-core kernel's epilogue).
 __device__ __forceinline__ uint32_t crt_pack4(uint32_t v0, uint32_t v1, uint32_t v2, uint32_t v3, int t) {
   return __byte_perm(__byte_perm(crt_mod_small(v0, t), crt_mod_small(v1, t), 0x0040),
                      __byte_perm(crt_mod_small(v2, t), crt_mod_small(v3, t), 0x0040), 0x5410);
 }
 
 // ---- reconstruction on the tensor cores ---------------------------------------
-// C' of one output from the column sums S_b of the reconstruction product
-// (below): q from the three fixed-point columns, then V - q M in CRT_NL
-// two's complement limbs, the limbs above nbe bytes filled with the sign
-// (bit 8 nbe - 1).
-__device__ __forceinline__ void crt_limbs_of_sums(const uint32_t (&S)[48], const uint32_t (&Mw)[CRT_NL], int nbe,
-                                                  uint32_t (&limb)[CRT_NL]) {
-  const uint64_t Q = (uint64_t)(S[0] + (S[1] << 8)) + ((uint64_t)S[2] << 16);
-  const uint32_t q = (uint32_t)((Q + (1u << 23)) >> 24);
-  int64_t carry = 0;
-#pragma unroll
-  for (int w = 0; w < CRT_NL; ++w) {
-    const uint32_t lo = S[4 + 4 * w] + (S[5 + 4 * w] << 8);  // < 2^30
-    const uint32_t hi = S[6 + 4 * w] + (S[7 + 4 * w] << 8);  // < 2^30
-    const int64_t v = (int64_t)lo + ((int64_t)hi << 16) - (int64_t)((uint64_t)q * Mw[w]) + carry;
-    limb[w] = (uint32_t)v;
-    carry = v >> 32;  // arithmetic shift
-  }
-  // C' mod 2^(8 nbe): the top bit of limb nbe / 4 - 1 is the sign, copied above
-  uint32_t top = 0;
-#pragma unroll
-  for (int w = 0; w < CRT_NL; ++w) top = 4 * (w + 1) == nbe ? limb[w] : top;
-  const uint32_t fill = (top >> 31) ? 0xFFFFFFFFu : 0u;
-#pragma unroll
-  for (int w = 0; w < CRT_NL; ++w) limb[w] = 4 * w < nbe ? limb[w] : fill;
-}
-
 // The sums over moduli are an integer matrix product: for an output with
 // residues r_t, the column sums
 //   S_b = sum_t r_t E[t][b]   (E[t][b] = byte b of round(c_t 2^24) for b < 3,
@@ -567,6 +440,12 @@ static __device__ __noinline__ uint32_t crt_chunk_residue_word(const uint32_t *s
   return w;
 }
 
+// One output from its column sums S with NL-limb arithmetic (defined below,
+// after the limb-count specialisations); Mn8 = -M mod 2^256.
+template <int NL>
+__device__ __forceinline__ void crt_out_nl(const uint32_t (&S)[48], const uint32_t (&Mn8)[CRT_NL], int nbe,
+                                           bool nan, int shift, double *__restrict__ dst, int mode);
+
 // CTA of CTC_THREADS threads: rows i0 .. i0+127 of column quads qd0 ..
 // qd0+CTC_QUADS-1 (thread T: row i0+T, columns 4 qd .. 4 qd + 3).  `smem`
 // is 1024-aligned, crt_tc_smem(ceil(n / 32)) bytes.  `status` receives
@@ -611,9 +490,17 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
   const int sa = row_ok ? sigA[i] : 0, fa = row_ok ? flagA[i] : 1;
   const int64_t nq = (N + 3) / 4;
   const int64_t kstride = N_pad * M_pad / 4, gstride = (int64_t)nkc * kstride;  // in 32-bit words
-  uint32_t Mw[CRT_NL];
+  uint32_t Mn8[CRT_NL];  // -M mod 2^256: its low NL limbs are -M mod 2^(32 NL)
+  {
+    uint64_t carry = 1;
 #pragma unroll
-  for (int w = 0; w < CRT_NL; ++w) Mw[w] = cc->Mw[w];
+    for (int w = 0; w < CRT_NL; ++w) {
+      const uint64_t v = (uint64_t)(~cc->Mw[w]) + carry;
+      Mn8[w] = (uint32_t)v;
+      carry = v >> 32;
+    }
+  }
+  const int nl = nbe / 4;
   uint32_t phase = 0;
   // the residue words of column quad qd (modulus t: four columns in a word)
   auto load_words = [&](int64_t qd, uint32_t (&wv)[CRT_NMAX]) {
@@ -689,11 +576,20 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
       mftc::tmem_wait_ld();
       const int64_t j = 4 * qd + c;
       if (!row_ok || j >= N) continue;
-      uint32_t limb[CRT_NL];
-      crt_limbs_of_sums(S, Mw, nbe, limb);
+
       const int sbc = c == 0 ? sb4.x : c == 1 ? sb4.y : c == 2 ? sb4.z : sb4.w;
       const int fbc = c == 0 ? fb4.x : c == 1 ? fb4.y : c == 2 ? fb4.z : fb4.w;
-      crt_emit(limb, (fa | fbc) != 0, sa + sbc - 2 * W, C + 2 * (j * M + i) * cstride, mode);
+      const bool nan = (fa | fbc) != 0;
+      const int shift = sa + sbc - 2 * W;
+      double *dst = C + 2 * (j * M + i) * cstride;
+      if (nl <= 5)
+        crt_out_nl<5>(S, Mn8, nbe, nan, shift, dst, mode);
+      else if (nl == 6)
+        crt_out_nl<6>(S, Mn8, nbe, nan, shift, dst, mode);
+      else if (nl == 7)
+        crt_out_nl<7>(S, Mn8, nbe, nan, shift, dst, mode);
+      else
+        crt_out_nl<8>(S, Mn8, nbe, nan, shift, dst, mode);
     }
     mftc::tc_fence_before();  // this round's TMEM reads before the next round's MMAs
   }
@@ -703,9 +599,9 @@ __device__ __forceinline__ void crt_combine_tc_body(const uint8_t *__restrict__ 
 }
 
 // ---- per-output arithmetic specialised on the limb count ------------------------
-// NL = max(5, nbe / 4) 32-bit limbs; the results are those of
-// crt_limbs_of_sums and crt_to_dd (same integer, same rounding), with the
-// multi-word additions as PTX carry chains:
+// NL = max(5, nbe / 4) 32-bit limbs (the reconstruction's width, uniform in a
+// launch, so the callers dispatch on it once), with the multi-word additions
+// as PTX carry chains:
 //   crt_limb_chain: r = lo + H + q Mn  (mod 2^(32 NL)),
 //   crt_inc_chain:  m = x + c          (mod 2^(32 NL)).
 template <int NL>
@@ -874,8 +770,8 @@ __device__ __forceinline__ void crt_inc_chain<8>(const uint32_t (&x)[8], uint32_
       : "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3]), "r"(x[4]), "r"(x[5]), "r"(x[6]), "r"(x[7]), "r"(c));
 }
 
-// C' = V - q M modulo 2^(32 NL) from the column sums S, as crt_limbs_of_sums:
-// q = round((S_0 + S_1 2^8 + S_2 2^16) / 2^24) in 32-bit steps (dividing by
+// C' = V - q M modulo 2^(32 NL) from the column sums S of the reconstruction
+// product: q = round((S_0 + S_1 2^8 + S_2 2^16) / 2^24) in 32-bit steps (dividing by
 // 2^8 first changes no floor; S_b < 2^22), V = sum_w lo_w 2^(32 w) + sum_w
 // hi_w 2^(32 w + 16) with the second sum re-cut at limb boundaries (H_w =
 // hi_w 2^16 mod 2^32 + floor(hi_(w-1) / 2^16): disjoint bits), and -q M added
@@ -904,9 +800,17 @@ __device__ __forceinline__ void crt_limbs_nl(const uint32_t (&S)[48], const uint
     for (int w = 0; w < NL; ++w) r[w] = 4 * w < nbe ? r[w] : fill;
   }
 }
-// The signed NL-limb integer as a double-double scaled by 2^e, exactly as
-// crt_to_dd (magnitude, whole-limb and bit normalisation to a 160-bit window,
-// hi rounded to nearest even, lo summed in doubles, fast_two_sum).
+// The signed NL-limb integer (two's complement) as a double-double scaled by
+// 2^e:
+//   the magnitude is normalised (whole-limb shifts, then a funnel shift) so
+//   that its leading one is bit 159 of a 160-bit window n4..n0 (bit 0 of
+//   weight 2^E; bits below the window dropped);
+//   hi = the window rounded to 53 bits (nearest, ties to even, the bits below
+//   bit 107 of the window deciding), exact as a double: keep 2^(E + 107);
+//   lo = the rest D 2^96 + n2 2^64 + n1 2^32 + n0 (D = the low 11 bits of the
+//   top 64 minus 2048 when rounded up) summed in doubles in that order,
+//   times 2^E; then fast_two_sum(hi, lo) in units of 2^(E + 107).
+// Returns (h, l) with value (h + l) 2^e, e = E + 107.
 template <int NL>
 __device__ __forceinline__ void crt_to_dd_nl(const uint32_t (&limb)[NL], double &h, double &l, int &e) {
   const uint32_t mask = (uint32_t)((int32_t)limb[NL - 1] >> 31);
@@ -956,7 +860,9 @@ __device__ __forceinline__ void crt_to_dd_nl(const uint32_t (&limb)[NL], double 
   }
   e = E + 107;
 }
-// crt_emit for NL limbs.
+// Writes the two's complement integer C' held in NL limbs, times 2^shift, as
+// a DD to dst (NaN when `nan`); mode 0 stores it, 1 subtracts it from the DD
+// at dst, 2 adds it.
 template <int NL>
 __device__ __forceinline__ void crt_emit_nl(const uint32_t (&limb)[NL], bool nan, int shift,
                                             double *__restrict__ dst, int mode) {
@@ -977,6 +883,14 @@ __device__ __forceinline__ void crt_emit_nl(const uint32_t (&limb)[NL], bool nan
     out = make_double2(res.hi, res.lo);
   }
   __stcs(d2, out);
+}
+
+template <int NL>
+__device__ __forceinline__ void crt_out_nl(const uint32_t (&S)[48], const uint32_t (&Mn8)[CRT_NL], int nbe,
+                                           bool nan, int shift, double *__restrict__ dst, int mode) {
+  uint32_t limb[NL];
+  crt_limbs_nl<NL>(S, *reinterpret_cast<const uint32_t(*)[NL]>(&Mn8[0]), nbe, limb);
+  crt_emit_nl<NL>(limb, nan, shift, dst, mode);
 }
 
 // ---- reconstruction fed by TMA ---------------------------------------------------

@@ -1,13 +1,16 @@
 """The integer arithmetic of the tensor-core CRT reconstruction
-(crt_device.cuh, crt_combine_tc_body), restated in Python and checked against
+(crt_device.cuh: crt_limbs_nl, used by crt_recon_body and
+crt_combine_tc_body), restated in Python and checked against
 exact integers on the CPU: for every plan width W and inner size k the kernel
 can meet, and for any C' with |C'| < k 2^(2W),
 
 * the column sums S_b = sum_t r_t E[t][b] of the u8 x u8 MMA fit in INT32;
 * q = round((S_0 + S_1 2^8 + S_2 2^16) / 2^24) (24-bit fixed-point c_t) is
   the exact CRT quotient;
-* the 30-bit partial limbs, int64 carries and q M subtraction give C' modulo
-  2^(8 nbe), and bit 8 nbe - 1 is its sign;
+* the 30-bit partial limbs and the q M subtraction give C' modulo
+  2^(8 nbe), and bit 8 nbe - 1 is its sign -- both as a plain int64-carry
+  restatement and as the device's NL-limb form (re-cut high halves, q (-M)
+  added modulo 2^(32 NL), sign fill);
 
 using the moduli table the device reads (crt_tables.h) and the plan's own
 moduli count and byte count."""
@@ -67,9 +70,14 @@ def constants(n, nbe):
     return ms, E, Mw
 
 
-def reconstruct(r, E, Mw, nbe, nb):
+def column_sums(r, E, nb):
     S = [sum(rt * Et[b] for rt, Et in zip(r, E)) if b < nb else 0 for b in range(48)]
     assert max(S) < 2 ** 31  # INT32 accumulators of the MMA
+    return S
+
+
+def reconstruct(r, E, Mw, nbe, nb):
+    S = column_sums(r, E, nb)
     Q = S[0] + (S[1] << 8) + (S[2] << 16)
     q = (Q + (1 << 23)) >> 24
     limb, carry = [], 0
@@ -87,6 +95,33 @@ def reconstruct(r, E, Mw, nbe, nb):
     return val - (1 << 256) if val >> 255 else val
 
 
+def reconstruct_nl(r, E, Mw, nbe, nb):
+    """The device's limb arithmetic (crt_limbs_nl): NL = max(5, nbe / 4) 32-bit
+    limbs, the quotient in 32-bit steps, the high halves re-cut at limb
+    boundaries, r = lo + H + q Mn modulo 2^(32 NL) with Mn = -M mod 2^(32 NL),
+    and for NL = 5 with nbe < 20 the limbs above nbe bytes filled with the sign."""
+    S = column_sums(r, E, nb)
+    m32 = 0xFFFFFFFF
+    NL = max(5, nbe // 4)
+    assert max(S[:3]) < 2 ** 22
+    q = ((((S[0] + (1 << 23)) & m32) >> 8) + S[1] + ((S[2] << 8) & m32)) & m32
+    q >>= 16
+    lo = [(S[4 + 4 * w] + (S[5 + 4 * w] << 8)) & m32 for w in range(NL)]
+    hi = [(S[6 + 4 * w] + (S[7 + 4 * w] << 8)) & m32 for w in range(NL)]
+    H = [(hi[0] << 16) & m32] + [((hi[w] << 16) | (hi[w - 1] >> 16)) & m32 for w in range(1, NL)]
+    M = sum(x << (32 * w) for w, x in enumerate(Mw))
+    mod = 1 << (32 * NL)
+    Mn = (-M) % mod
+    val = (sum(x << (32 * w) for w, x in enumerate(lo)) + sum(x << (32 * w) for w, x in enumerate(H)) +
+           q * Mn) % mod
+    limb = [(val >> (32 * w)) & m32 for w in range(NL)]
+    if NL == 5 and nbe < 20:
+        fill = m32 if limb[nbe // 4 - 1] >> 31 else 0
+        limb = [limb[w] if 4 * w < nbe else fill for w in range(NL)]
+    val = sum(x << (32 * w) for w, x in enumerate(limb))
+    return val - mod if val >> (32 * NL - 1) else val
+
+
 @pytest.mark.parametrize("W,k", [(8, 1), (40, 3), (77, 200), (92, 4096), (91, 8192), (99, 16), (110, 5),
                                  (110, 300000), (110, 2 ** 31 - 1)])
 def test_reconstruction_is_exact(W, k):
@@ -99,3 +134,4 @@ def test_reconstruction_is_exact(W, k):
     for c in cases:
         r = [c % m for m in ms]
         assert reconstruct(r, E, Mw, nbe, nb) == c, (W, k, c)
+        assert reconstruct_nl(r, E, Mw, nbe, nb) == c, (W, k, c)
