@@ -246,15 +246,18 @@ __global__ void __launch_bounds__(256) g_slice_a(const SProb *probs, const int64
   const int64_t nbx = P.M_pad / 32;
   slice_a_body(P.A, P.m, P.k, P.astride, P.M_pad, P.K_pad, P.sigA, P.flagA, P.plan, P.As, l % nbx, l / nbx);
 }
-// CRT form: residues instead of digits (the transposing tile in dynamic shared memory)
+// CRT form: residues instead of digits, in MN-major planes As[t][p][i] (the
+// rows of one K index contiguous); flat: thread t of the problem takes K
+// index t / (M_pad / 8), rows 8 (t % (M_pad / 8)) .. + 7
 __global__ void __launch_bounds__(256) g_crt_slice_a(const SProb *probs, const int64_t *prefix, int nprob) {
-  extern __shared__ __align__(16) uint8_t crt_tile[];
   const int p = find_prob(prefix, nprob, blockIdx.x);
   const SProb &P = probs[p];
-  const int64_t l = blockIdx.x - prefix[p];
-  const int64_t nbx = P.M_pad / 32;
-  crt_slice_a_body(P.A, P.m, P.k, P.astride, P.M_pad, P.K_pad, P.sigA, P.flagA, P.plan, P.As, crt_tile, l % nbx,
-                   l / nbx);
+  const int64_t t = (int64_t)(blockIdx.x - prefix[p]) * 256 + threadIdx.x;
+  const int64_t per_k = P.M_pad / 8;
+  const int64_t kp = t / per_k;
+  if (kp < P.K_pad)
+    crt_slice_a_mn_one(P.A, P.m, P.k, P.astride, P.M_pad, P.K_pad, P.sigA, P.flagA, P.plan, P.As,
+                       (t % per_k) * 8, kp);
 }
 __global__ void __launch_bounds__(256) g_crt_slice_b(const SProb *probs, const int64_t *prefix, int nprob) {
   const int p = find_prob(prefix, nprob, blockIdx.x);
@@ -402,7 +405,10 @@ __global__ void __launch_bounds__(G_THREADS, 1)
               break;
             }
             mftc::mbar_arrive_expect_tx(&full[stage], bytes);
-            mftc::tma_load_3d(sA + stage * A_STAGE, &maps[2 * p], &full[stage], kb * BK, it.tm * BM, s);
+            if (P.crt)  // MN-major residue planes: (row, K index, modulus)
+              mftc::tma_load_3d(sA + stage * A_STAGE, &maps[2 * p], &full[stage], it.tm * BM, kb * BK, s);
+            else
+              mftc::tma_load_3d(sA + stage * A_STAGE, &maps[2 * p], &full[stage], kb * BK, it.tm * BM, s);
             mftc::tma_load_3d(sB + stage * B_STAGE, &maps[2 * p + 1], &full[stage], kb * BK, it.tn * P.bn,
                               P.crt ? s : it.g - s);
             arm.arm(stage, phase);
@@ -427,7 +433,9 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         if (!lookup(w, p, it)) continue;
         const SProb &P = probs[p];
         const int kb0 = it.kc * P.kcb, kb1 = min(P.kblocks, kb0 + P.kcb);
-        const uint32_t idesc = P.crt ? mftc::idesc_u8(BM, P.bn) : mftc::idesc_i8(BM, P.bn);  // CRT residues unsigned
+        // CRT residues are unsigned, and A's planes MN-major (a K step of 32 rows is 4096 bytes)
+        const uint32_t idesc = P.crt ? mftc::idesc_u8(BM, P.bn) | mftc::IDESC_A_MN : mftc::idesc_i8(BM, P.bn);
+        const uint32_t a_kstep = P.crt ? 32 * 128 : UMMA_K;
         if (!wait_bar(&tempty[acc], acc_phase ^ 1, abort_flag, wait_ns)) {
           fail(2);
           break;
@@ -447,7 +455,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
             const uint32_t b0 = mftc::smem_u32(sB + stage * B_STAGE);
 #pragma unroll
             for (int kk = 0; kk < BK / UMMA_K; ++kk) {
-              mftc::umma_i8(d_tmem, mftc::smem_desc_k_sw128(a0 + kk * UMMA_K),
+              mftc::umma_i8(d_tmem, mftc::smem_desc_k_sw128(a0 + kk * a_kstep),
                             mftc::smem_desc_k_sw128(b0 + kk * UMMA_K), idesc, accumulate);
               accumulate = 1;
             }
@@ -753,6 +761,20 @@ static bool make_map(CUtensorMap *map, void *base, int64_t rows, int64_t K_pad, 
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// MN-major residue planes (row, K index, modulus) of the CRT form's A side:
+// boxes of 128 rows x BK K indices, 128-byte swizzle.
+static bool make_map_mn(CUtensorMap *map, void *base, int64_t M_pad, int64_t K_pad, int nsl) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)M_pad, (cuuint64_t)K_pad, (cuuint64_t)nsl};
+  cuuint64_t strides[2] = {(cuuint64_t)M_pad, (cuuint64_t)(M_pad * K_pad)};
+  cuuint32_t box[3] = {128, (cuuint32_t)BK, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // One real product to plan (host side of SProb): operand / output views, its
 // tile width, and where its A operand, B operand and plan come from (-1: its
 // own; else the index of the product that provides them).  A plan owner lists
@@ -842,7 +864,7 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
     const int64_t blocks[PH_COUNT] = {
         P.own_a ? ((P.m + 255) / 256) * ((P.k + 63) / 64) : 0,
         P.own_b && P.k > 0 ? (P.n + 7) / 8 : 0,
-        P.own_a ? (P.M_pad / 32) * (P.K_pad / 64) : 0,
+        P.own_a ? (crt ? (P.K_pad * (P.M_pad / 8) + 255) / 256 : (P.M_pad / 32) * (P.K_pad / 64)) : 0,
         P.own_b ? (P.N_pad * (P.K_pad / 8) + 255) / 256 : 0,
         P.mode == 0 ? comb : 0,
         P.mode != 0 ? comb : 0,
@@ -921,7 +943,8 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
     P.muA2 = g.plan_a2 >= 0 ? probs[g.plan_a2].muA : nullptr;
     P.sigB2 = g.plan_b2 >= 0 ? probs[g.plan_b2].sigB : nullptr;
     P.muB2 = g.plan_b2 >= 0 ? probs[g.plan_b2].muB : nullptr;
-    if (!make_map(&maps[2 * q], P.As, P.M_pad, P.K_pad, BM, P.nsl) ||
+    if (!(crt ? make_map_mn(&maps[2 * q], P.As, P.M_pad, P.K_pad, P.nsl)
+              : make_map(&maps[2 * q], P.As, P.M_pad, P.K_pad, BM, P.nsl)) ||
         !make_map(&maps[2 * q + 1], P.Bs, P.N_pad, P.K_pad, (uint32_t)P.bn, P.nsl)) {
       destroy(b);
       return MFCUDA_ERR_CUDA;
@@ -941,15 +964,12 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
   }
   std::call_once(g_gmma_attr, [] {
     cudaFuncSetAttribute(g_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, MMA_SMEM);
-    cudaFuncSetAttribute(g_crt_slice_a, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         CRT_NMAX * SA_ROWS * SA_STRIDE);
     cudaFuncSetAttribute(g_crt_combine, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          crt_tc_smem((CRT_NMAX + 31) / 32));
   });
-  // the residue tile of g_crt_slice_a holds the most moduli of any product
+  // the reconstruction's shared tiles hold the most moduli of any product
   int nsl_max = 1;
   for (int q = 0; q < np; ++q) nsl_max = std::max(nsl_max, probs[q].nsl);
-  const size_t crt_tile = (size_t)std::min(nsl_max, CRT_SA_MODULI) * SA_ROWS * SA_STRIDE;
   int mma_grid = sm_count();
   if (mma_grid > total[PH_ITEMS]) mma_grid = (int)std::max<int64_t>(total[PH_ITEMS], 1);
   const uint64_t wait_ns = wait_limit_ns();  // captured into the graph with the plan
@@ -964,7 +984,7 @@ static int create_split_specs(std::vector<Spec> specs, int64_t count, int slices
     if (total[PH_SCAN_B]) g_scan_b<<<(unsigned)total[PH_SCAN_B], 256, 0, cs>>>(dp, dprefix + PH_SCAN_B * np, np);
     g_plan<<<np, 256, 0, cs>>>(dp, slices, target);
     if (total[PH_SLICE_A] && crt)
-      g_crt_slice_a<<<(unsigned)total[PH_SLICE_A], 256, crt_tile, cs>>>(dp, dprefix + PH_SLICE_A * np, np);
+      g_crt_slice_a<<<(unsigned)total[PH_SLICE_A], 256, 0, cs>>>(dp, dprefix + PH_SLICE_A * np, np);
     else if (total[PH_SLICE_A])
       g_slice_a<<<(unsigned)total[PH_SLICE_A], 256, 0, cs>>>(dp, dprefix + PH_SLICE_A * np, np);
     if (total[PH_SLICE_B] && crt)

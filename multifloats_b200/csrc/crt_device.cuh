@@ -247,62 +247,8 @@ __device__ __forceinline__ void for_each_residue_word(const uint32_t (&dw)[8][4]
   else
     residue_words_nw<4>(dw, t0, t1, f);
 }
-// Moduli whose residues the A slicer's transposing tile holds at once (the
-// tile is reused for the rest): a smaller tile lets more CTAs share an SM.
-constexpr int CRT_SA_MODULI = 18;
-
-// A (m x k column-major view) -> As[t][i][p], as slice_a_body with residues
-// for digits; the transposing tile lives in dynamic shared memory
-// (min(n, CRT_SA_MODULI) * SA_ROWS * SA_STRIDE bytes) and takes the moduli in
-// groups of CRT_SA_MODULI.
-__device__ __forceinline__ void crt_slice_a_body(const double *__restrict__ A, int64_t M, int64_t K,
-                                                 int64_t stride, int64_t M_pad, int64_t K_pad, const int *sig,
-                                                 const int *flag, const Plan *plan, int8_t *__restrict__ As,
-                                                 uint8_t *tile, int64_t bx, int64_t by) {
-  const int n = plan->S, W = plan->W;
-  const int64_t i0 = bx * SA_ROWS, p0 = by * SA_COLS;
-  const int t = threadIdx.x;
-  const int ii = t % SA_ROWS, grp = t / SA_ROWS;
-  const int64_t i = i0 + ii;
-  const bool row_ok = i < M && !flag[i < M ? i : 0];
-  const int sigma = i < M ? sig[i] : 0;
-  uint32_t y[8][4];
-#pragma unroll
-  for (int e = 0; e < 8; ++e) {
-    int64_t p = p0 + grp * 8 + e;
-    if (row_ok && p < K) {
-      double2 v = __ldg(reinterpret_cast<const double2 *>(A) + (p * M + i) * stride);
-      biased_bytes(v.x, v.y, sigma, W, y[e]);
-    } else {
-#pragma unroll
-      for (int w = 0; w < 4; ++w) y[e][w] = bias_word(w);  // X = 0: every residue zero
-    }
-  }
-  uint32_t dw[8][4];
-#pragma unroll
-  for (int e = 0; e < 8; ++e) digit_words(y[e], dw[e]);
-  const bool any = row_ok && p0 + grp * 8 < K;  // else padding only: every residue zero
-  const int row = t / 8, seg = (t % 8) * 8;
-  for (int t0 = 0; t0 < n; t0 += CRT_SA_MODULI) {  // moduli t0 .. t1 - 1 in tile slots 0 ..
-    const int t1 = min(n, t0 + CRT_SA_MODULI);
-    auto put = [&](int sl, uint64_t word) {
-      *reinterpret_cast<uint64_t *>(&tile[((sl - t0) * SA_ROWS + ii) * SA_STRIDE + grp * 8]) = word;
-    };
-    if (t0 > 0) __syncthreads();  // the previous moduli's rows have been copied out
-    if (any)
-      for_each_residue_word(dw, t0, t1, W, put);
-    else
-      for (int sl = t0; sl < t1; ++sl) put(sl, 0);
-    __syncthreads();
-    for (int s = t0; s < t1; ++s) {
-      uint64_t v = *reinterpret_cast<const uint64_t *>(&tile[((s - t0) * SA_ROWS + row) * SA_STRIDE + seg]);
-      *reinterpret_cast<uint64_t *>(As + ((s * M_pad + i0 + row) * K_pad + p0 + seg)) = v;
-    }
-  }
-}
-
 // A (m x k column-major view) -> As[t][p][i]: the MN-major residue planes
-// of the main path's tensor-core kernels (the rows of one K index
+// of the tensor-core kernels (the rows of one K index
 // contiguous, so a thread's eight residues of consecutive rows are one
 // 64-bit store and a warp's stores are contiguous; no transposition).
 // Entries i8 .. i8+7 of column p.
