@@ -229,7 +229,12 @@ __device__ __forceinline__ void digit_words(const uint32_t (&y)[4], uint32_t (&d
 // order (byte e = entry e), for t0 <= t < t1.
 template <int NW, class F>
 __device__ __forceinline__ void residue_words_nw(const uint32_t (&dw)[8][4], int t0, int t1, F f) {
-  for (int t = t0; t < t1; ++t) {
+  // unrolled over the whole table (leaving at t1): each modulus' constants
+  // are then constant-bank operands at fixed offsets instead of loads
+#pragma unroll
+  for (int t = 0; t < CRT_NMAX; ++t) {
+    if (t >= t1) break;
+    if (t < t0) continue;
     const ModConst k = mod_const(t);
     uint32_t r[8];
 #pragma unroll
